@@ -1,0 +1,128 @@
+/*
+ * libcc_b200 -- B200-native (sm_100a) CCSD(T) triples correction E(T).
+ *
+ * A drop-in for the GPU hooks and the whole-driver entry of libcc's triples.x
+ * (ryanolson/libcc, src/triples-ijk).  Plain C ABI: pointers and sizes only.
+ *
+ * Array conventions (identical to the reference, Fortran column-major):
+ *   eh(no), ep(nu), t1(no,nu), t2(nu,nu,no,no), vm(no,nu,no,no),
+ *   voe(nu,nu,no,no), v1(nu,no), vvvo packed (nutr, nu*no) with
+ *   nutr = nu*(nu+1)/2 and column x*nu+c holding the a>=b triangle of (ab|c x).
+ *
+ * Two groups of entry points:
+ *   1. Fortran-callable legacy hooks (trailing underscore, every argument by
+ *      reference, 8-byte integers as under -sdefault64, 1-based occupied
+ *      indices).  Like the reference they return nothing and stop the program
+ *      with a message on error.
+ *   2. The status-returning ccT_* API (0 = success, see ccT_status).
+ */
+#ifndef LIBCC_B200_H
+#define LIBCC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    CCT_OK = 0,
+    CCT_ERR_INVALID = 1,     /* bad argument: shape, index, null pointer        */
+    CCT_ERR_CUDA = 2,        /* a CUDA runtime call failed                      */
+    CCT_ERR_NOMEM = 3,       /* device allocation failed                        */
+    CCT_ERR_NONFINITE = 4,   /* input or result holds NaN/Inf                   */
+    CCT_ERR_DENOMINATOR = 5, /* some e_i+e_j+e_k-e_a-e_b-e_c >= 0               */
+    CCT_ERR_STATE = 6,       /* call out of order (e.g. forward before inputs)  */
+    CCT_ERR_TIMEOUT = 7,     /* a bounded device-side wait ran out              */
+    CCT_ERR_UNSUPPORTED = 8  /* option not available on this device / build     */
+} ccT_status;
+
+typedef enum {
+    CCT_PREC_FP64 = 0,       /* native FP64 DMMA contractions                   */
+    CCT_PREC_INT8_EMU = 1    /* split-integer emulated FP64 on INT8 tensor cores */
+} ccT_precision;
+
+typedef enum { CCT_MEM_HOST = 0, CCT_MEM_DEVICE = 1 } ccT_memory;
+
+typedef struct {
+    int32_t precision;       /* ccT_precision                                    */
+    int32_t device;          /* CUDA device ordinal                              */
+    int32_t check_inputs;    /* 1: reject NaN/Inf inputs and D >= 0 (default 1)  */
+    int32_t emu_slices;      /* INT8 emulation: 0 = choose per tile, else fixed  */
+    int32_t reserved[4];
+} ccT_options;
+
+typedef struct ccT_plan ccT_plan;
+
+/* Fill *opt with defaults (FP64, device 0, input checks on). */
+void ccT_options_default(ccT_options *opt);
+
+/* Plan for one system of no occupied and nu virtual orbitals.  Allocates the
+ * device-resident HBM buffers that replace the DDI arrays. */
+int ccT_plan_create(ccT_plan **plan, int64_t no, int64_t nu, const ccT_options *opt);
+
+/* Load the inputs (reference layouts).  mem = CCT_MEM_HOST copies from host
+ * memory, CCT_MEM_DEVICE reads device pointers already in HBM.  Replaces
+ * program.F90:195-223 (restart read) plus the DDI put/bcast of T2/VM/VOE/VVVO. */
+int ccT_set_inputs(ccT_plan *plan, const double *eh, const double *ep, const double *t1,
+                   const double *t2, const double *vm, const double *voe,
+                   const double *vvvo_packed, int32_t mem);
+
+/* Number of tuples with work: C(no,3) i>j>k tuples, then no(no-1)/2 (i,j,j)
+ * and no(no-1)/2 (i,i,j) tuples (triples.F90:51-53). */
+int64_t ccT_num_tuples(int64_t no);
+
+/* Run tuples [begin, end) of the global tuple list (i>j>k in DDCC_T_TASK order,
+ * then for each i and j<i the (i,j,j) and (i,i,j) tuples), accumulate
+ * etd and v1, and return ets = 2 sum_{i,a} t1(i,a) v1(a,i), etd, and (if
+ * v1_out != NULL) v1(nu,no) for this range.  A full range reproduces
+ * cc_triples (triples.F90:1-333).  A partial range gives a shard whose
+ * ets/etd/v1 sum linearly with the other shards. */
+int ccT_forward(ccT_plan *plan, int64_t begin, int64_t end, double *ets, double *etd, double *v1_out);
+
+/* Milliseconds of device time the last ccT_forward spent, measured by CUDA
+ * events around its kernels (excludes input upload). */
+double ccT_last_forward_ms(const ccT_plan *plan);
+
+/* Kernel launches issued by the last ccT_forward. */
+int64_t ccT_last_forward_launches(const ccT_plan *plan);
+
+int ccT_plan_destroy(ccT_plan *plan);
+
+/* Message for a status code, or the last error recorded on this thread. */
+const char *ccT_status_string(int status);
+const char *ccT_last_error(void);
+
+/* Measured FP64 mma.sync throughput of this device in TFLOP/s (a short
+ * microbenchmark; the denominator of the FP64 roofline). */
+double ccT_measure_fp64_peak(int32_t device);
+
+/* ------------------------------------------------------------------ legacy hooks
+ * ijk_gpu_init_    replaces the call at src/triples-ijk/triples_cpu.F90:363
+ * ijk_gpu_driver_  replaces src/triples-ijk/ddcc_t_ijk_big_cuda.f:12-14
+ * ijk_gpu_finalize_ replaces the call at src/triples-ijk/triples_cpu.F90:497
+ * The driver hook receives the packed VVVO columns of i, j and k exactly as
+ * triples_cpu.F90:428-450 fetches them (nutr*nu doubles each); it expands and
+ * b<->c-swaps them on the device.  Tuple contributions accumulate on the device
+ * and are added into the host etd and v1 (the v1 pointer given at init) by
+ * ijk_gpu_finalize_. */
+void ijk_gpu_init_(const int64_t *no, const int64_t *nu, const double *eh, const double *ep,
+                   double *v1, const double *t2, const double *vm, const double *voe);
+void ijk_gpu_driver_(const int64_t *nu, const int64_t *no, const int64_t *i, const int64_t *j,
+                     const int64_t *k, const double *ve_i, const double *ve_j, const double *ve_k,
+                     double *t1, const double *eh, const double *ep, double *etd);
+void ijk_gpu_finalize_(const int64_t *no, const int64_t *nu, double *etd);
+
+/* Whole (T) driver with the packed VVVO passed explicitly instead of a DDI
+ * handle: the single-GPU form of cc_triples_acc (src/triples-ijk/triples.F90:1)
+ * and cc_triples (src/triples-abc/triples.f90:193).  v1 (nu,no) is
+ * overwritten; ets and etd are returned as gms_ets/gms_etd are. */
+void cc_triples_b200_(const int64_t *no, const int64_t *nu, const double *eh, const double *ep,
+                      double *v1, const double *t1, const double *t2, const double *vm,
+                      const double *voe, const double *vvvo, double *ets, double *etd);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIBCC_B200_H */

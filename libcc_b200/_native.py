@@ -1,0 +1,97 @@
+"""ctypes binding of ``libcc_b200/_lib/libcc_b200.so`` (C ABI of include/libcc_b200.h).
+
+There is no CPU fallback: if the shared library is missing or cannot be loaded
+every entry point raises ``NativeLibraryError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "_lib" / "libcc_b200.so"
+
+CCT_OK = 0
+STATUS_NAMES = {
+    0: "CCT_OK", 1: "CCT_ERR_INVALID", 2: "CCT_ERR_CUDA", 3: "CCT_ERR_NOMEM", 4: "CCT_ERR_NONFINITE",
+    5: "CCT_ERR_DENOMINATOR", 6: "CCT_ERR_STATE", 7: "CCT_ERR_TIMEOUT", 8: "CCT_ERR_UNSUPPORTED",
+}
+CCT_PREC_FP64, CCT_PREC_INT8_EMU = 0, 1
+CCT_MEM_HOST, CCT_MEM_DEVICE = 0, 1
+
+# every symbol include/libcc_b200.h declares
+EXPORTS = [
+    "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
+    "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
+    "ccT_last_error", "ccT_measure_fp64_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
+    "cc_triples_b200_",
+]
+
+
+class NativeLibraryError(RuntimeError):
+    pass
+
+
+class CctError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {detail}")
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("check_inputs", ctypes.c_int32),
+                ("emu_slices", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise NativeLibraryError(f"{LIB_PATH} is missing: build it with `python -m libcc_b200.build`")
+    try:
+        lib = ctypes.CDLL(str(LIB_PATH))
+    except OSError as e:
+        raise NativeLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+    vp, dp, i64, i32 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int64, ctypes.c_int32
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    lib.ccT_options_default.argtypes = [ctypes.POINTER(Options)]
+    lib.ccT_options_default.restype = None
+    lib.ccT_plan_create.argtypes = [ctypes.POINTER(vp), i64, i64, ctypes.POINTER(Options)]
+    lib.ccT_plan_create.restype = ctypes.c_int
+    lib.ccT_set_inputs.argtypes = [vp] + [vp] * 7 + [i32]
+    lib.ccT_set_inputs.restype = ctypes.c_int
+    lib.ccT_num_tuples.argtypes = [i64]
+    lib.ccT_num_tuples.restype = i64
+    lib.ccT_forward.argtypes = [vp, i64, i64, dp, dp, vp]
+    lib.ccT_forward.restype = ctypes.c_int
+    lib.ccT_last_forward_ms.argtypes = [vp]
+    lib.ccT_last_forward_ms.restype = ctypes.c_double
+    lib.ccT_last_forward_launches.argtypes = [vp]
+    lib.ccT_last_forward_launches.restype = i64
+    lib.ccT_plan_destroy.argtypes = [vp]
+    lib.ccT_plan_destroy.restype = ctypes.c_int
+    lib.ccT_status_string.argtypes = [ctypes.c_int]
+    lib.ccT_status_string.restype = ctypes.c_char_p
+    lib.ccT_last_error.argtypes = []
+    lib.ccT_last_error.restype = ctypes.c_char_p
+    lib.ccT_measure_fp64_peak.argtypes = [i32]
+    lib.ccT_measure_fp64_peak.restype = ctypes.c_double
+    lib.ijk_gpu_init_.argtypes = [i64p, i64p, dp, dp, dp, dp, dp, dp]
+    lib.ijk_gpu_init_.restype = None
+    lib.ijk_gpu_driver_.argtypes = [i64p] * 5 + [dp] * 7
+    lib.ijk_gpu_driver_.restype = None
+    lib.ijk_gpu_finalize_.argtypes = [i64p, i64p, dp]
+    lib.ijk_gpu_finalize_.restype = None
+    lib.cc_triples_b200_.argtypes = [i64p, i64p] + [dp] * 10
+    lib.cc_triples_b200_.restype = None
+    _lib = lib
+    return lib
+
+
+def check(status: int, where: str):
+    if status != CCT_OK:
+        lib = load()
+        raise CctError(status, where, lib.ccT_last_error().decode(errors="replace"))

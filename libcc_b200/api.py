@@ -1,0 +1,170 @@
+"""Host-side mirror of the reference's (T) driver interface over the C ABI.
+
+* ``cc_triples``     -- whole (T) evaluation, the single-GPU form of
+                        ``cc_triples_acc`` (src/triples-ijk/triples.F90:1) with the
+                        packed VVVO passed in place of the DDI handle.
+* ``IjkGpuHooks``    -- ``ijk_gpu_init`` / ``ijk_gpu_driver`` / ``ijk_gpu_finalize``,
+                        the per-tuple GPU hooks of the hybrid CUDA build
+                        (triples_cpu.F90:363,465,497; ddcc_t_ijk_big_cuda.f:12).
+* ``TriplesPlan``    -- the status-returning plan API (create, set inputs once,
+                        forward over any tuple range).
+
+Arrays are flat float64 in the reference's Fortran layouts (see
+libcc_b200/synthetic.py).  Device arrays may be passed as CUDA tensors (any
+object with ``data_ptr()`` and ``is_cuda``); they are read in place.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _host(a, n: int, name: str) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    if a.size != n:
+        raise ValueError(f"{name}: expected {n} elements, got {a.size}")
+    return a
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)
+
+
+def format_energies(ets: float, etd: float) -> str:
+    """The reference's result line (triples.F90:316,332: format '(1x,a,3F15.10)')."""
+    return " ets/etd/ets+etd=" + "".join(f"{x:15.10f}" for x in (ets, etd, ets + etd))
+
+
+def input_sizes(no: int, nu: int):
+    nutr = nu * (nu + 1) // 2
+    return dict(eh=no, ep=nu, t1=no * nu, t2=nu * nu * no * no, vm=no * nu * no * no,
+                voe=nu * nu * no * no, vvvo=nutr * nu * no)
+
+
+class TriplesPlan:
+    """Device plan for one system: owns the HBM buffers that replace the DDI arrays."""
+
+    def __init__(self, no: int, nu: int, precision: str = "fp64", device: int = 0, check_inputs: bool = True):
+        lib = N.load()
+        opt = N.Options()
+        lib.ccT_options_default(ctypes.byref(opt))
+        opt.precision = {"fp64": N.CCT_PREC_FP64, "int8": N.CCT_PREC_INT8_EMU}[precision]
+        opt.device = device
+        opt.check_inputs = 1 if check_inputs else 0
+        h = ctypes.c_void_p()
+        N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
+        self._h = h
+        self.no, self.nu, self.precision, self.device = no, nu, precision, device
+        self.num_tuples = int(lib.ccT_num_tuples(no))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.load().ccT_plan_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_inputs(self, eh, ep, t1, t2, vm, voe, vvvo):
+        """Load the seven input arrays (all host numpy arrays, or all CUDA tensors)."""
+        arrs = dict(eh=eh, ep=ep, t1=t1, t2=t2, vm=vm, voe=voe, vvvo=vvvo)
+        sizes = input_sizes(self.no, self.nu)
+        dev = [_is_device(a) for a in arrs.values()]
+        if any(dev) and not all(dev):
+            raise ValueError("pass either all host arrays or all device tensors")
+        if all(dev):
+            ptrs = []
+            for name, a in arrs.items():
+                if a.numel() != sizes[name] or not a.is_contiguous() or str(a.dtype) != "torch.float64":
+                    raise ValueError(f"{name}: need a contiguous float64 tensor of {sizes[name]} elements")
+                ptrs.append(ctypes.c_void_p(a.data_ptr()))
+            mem = N.CCT_MEM_DEVICE
+            keep = None
+        else:
+            keep = [_host(a, sizes[name], name) for name, a in arrs.items()]
+            ptrs = [ctypes.c_void_p(a.ctypes.data) for a in keep]
+            mem = N.CCT_MEM_HOST
+        N.check(N.load().ccT_set_inputs(self._h, *ptrs, mem), "ccT_set_inputs")
+        del keep
+
+    def set_system(self, inp):
+        """Load a ``synthetic.TriplesInputs``."""
+        self.set_inputs(*inp.arrays())
+
+    def forward(self, begin: int = 0, end: int | None = None, want_v1: bool = True):
+        """Run tuples [begin, end).  Returns (ets, etd, v1[nu*no] or None)."""
+        end = self.num_tuples if end is None else end
+        ets, etd = ctypes.c_double(), ctypes.c_double()
+        v1 = np.zeros(self.nu * self.no) if want_v1 else None
+        vptr = ctypes.c_void_p(v1.ctypes.data) if want_v1 else None
+        N.check(N.load().ccT_forward(self._h, begin, end, ctypes.byref(ets), ctypes.byref(etd), vptr), "ccT_forward")
+        return ets.value, etd.value, v1
+
+    @property
+    def last_forward_ms(self) -> float:
+        return float(N.load().ccT_last_forward_ms(self._h))
+
+    @property
+    def last_forward_launches(self) -> int:
+        return int(N.load().ccT_last_forward_launches(self._h))
+
+
+def cc_triples(no: int, nu: int, eh, ep, t1, t2, vm, voe, vvvo):
+    """Whole (T) on one GPU through ``cc_triples_b200_``.  Returns (ets, etd, v1)."""
+    sizes = input_sizes(no, nu)
+    arrs = [_host(a, sizes[n], n) for n, a in zip(("eh", "ep", "t1", "t2", "vm", "voe", "vvvo"),
+                                                    (eh, ep, t1, t2, vm, voe, vvvo))]
+    v1 = np.zeros(no * nu)
+    ets, etd = ctypes.c_double(), ctypes.c_double()
+    n_o, n_u = ctypes.c_int64(no), ctypes.c_int64(nu)
+    p = lambda a: a.ctypes.data_as(_dp)
+    eh_, ep_, t1_, t2_, vm_, voe_, vvvo_ = arrs
+    N.load().cc_triples_b200_(ctypes.byref(n_o), ctypes.byref(n_u), p(eh_), p(ep_), p(v1), p(t1_), p(t2_), p(vm_),
+                              p(voe_), p(vvvo_), ctypes.byref(ets), ctypes.byref(etd))
+    return ets.value, etd.value, v1
+
+
+def packed_columns(vvvo: np.ndarray, no: int, nu: int, x: int) -> np.ndarray:
+    """The nu packed VVVO columns of occupied index x (0-based), as ddi_get fetches
+    them for the GPU hook (triples_cpu.F90:428-450)."""
+    nutr = nu * (nu + 1) // 2
+    return np.ascontiguousarray(vvvo.reshape(nu * no, nutr)[x * nu:(x + 1) * nu]).ravel()
+
+
+class IjkGpuHooks:
+    """The hybrid build's GPU hooks.  Occupied indices are 1-based as in Fortran."""
+
+    def __init__(self, no: int, nu: int, eh, ep, t2, vm, voe):
+        self.no, self.nu = no, nu
+        sizes = input_sizes(no, nu)
+        self._keep = dict(eh=_host(eh, no, "eh"), ep=_host(ep, nu, "ep"), t2=_host(t2, sizes["t2"], "t2"),
+                          vm=_host(vm, sizes["vm"], "vm"), voe=_host(voe, sizes["voe"], "voe"))
+        self.v1 = np.zeros(no * nu)
+        self.etd = ctypes.c_double(0.0)
+        p = lambda a: a.ctypes.data_as(_dp)
+        k = self._keep
+        N.load().ijk_gpu_init_(ctypes.byref(ctypes.c_int64(no)), ctypes.byref(ctypes.c_int64(nu)), p(k["eh"]),
+                               p(k["ep"]), p(self.v1), p(k["t2"]), p(k["vm"]), p(k["voe"]))
+
+    def driver(self, i: int, j: int, k: int, ve_i, ve_j, ve_k):
+        p = lambda a: a.ctypes.data_as(_dp)
+        n = self.nu * (self.nu + 1) // 2 * self.nu
+        vs = [_host(v, n, "ve") for v in (ve_i, ve_j, ve_k)]
+        c = lambda v: ctypes.byref(ctypes.c_int64(v))
+        N.load().ijk_gpu_driver_(c(self.nu), c(self.no), c(i), c(j), c(k), p(vs[0]), p(vs[1]), p(vs[2]),
+                                 p(self.v1), p(self._keep["eh"]), p(self._keep["ep"]), ctypes.byref(self.etd))
+
+    def finalize(self) -> float:
+        c = lambda v: ctypes.byref(ctypes.c_int64(v))
+        N.load().ijk_gpu_finalize_(c(self.no), c(self.nu), ctypes.byref(self.etd))
+        return self.etd.value

@@ -1,0 +1,105 @@
+// Internal declarations shared by the libcc_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/libcc_b200.h"
+
+namespace cct {
+
+// ----------------------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+const char *last_error();
+
+#define CCT_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      ::cct::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+      return e_ == cudaErrorMemoryAllocation ? CCT_ERR_NOMEM : CCT_ERR_CUDA;                \
+    }                                                                                       \
+  } while (0)
+
+#define CCT_TRY(call)                  \
+  do {                                 \
+    int s_ = (call);                   \
+    if (s_ != CCT_OK) return s_;       \
+  } while (0)
+
+// ----------------------------------------------------------------------------- tiling
+// W-build GEMM tile (FP64 DMMA kernel).  K is padded to KB, the single-index
+// dimension N to BN.
+constexpr int kKB = 16;
+constexpr int kBN = 64;
+// Reduction block edge (elements of a, b, c per block).
+constexpr int kRB = 8;
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Tuple kinds.  Every tuple is stored as (i,j,k) with i>=j>=k, 0-based.
+enum TupleKind : int { kIJK = 0, kIJJ = 1, kIIJ = 2 };
+
+struct Tuple {
+  int kind, i, j, k;
+};
+
+// Global tuple list in the reference's order (i>j>k in DDCC_T_TASK order, then
+// for each i and j<i the (i,j,j) and (i,i,j) tuples).
+std::vector<Tuple> tuple_list(int no);
+
+// One W-build GEMM: X(p,q,s) = sum_kappa A0[(p,q)] B0[s] (+ A1[(q,p)] B1[s]).
+struct GemmJob {
+  const double *a0;   // E + x1*nu*nu*KP  : row (p,q) at ((p*nu+q)*KP)
+  const double *a1;   // E + x2*nu*nu*KP  : row (p,q) read as ((q*nu+p)*KP)
+  const double *b0;   // F + (x2*no+x3)*NP*KP : row s at s*KP
+  const double *b1;   // F + (x1*no+x3)*NP*KP
+  double *out;        // X: row (p,q) at (p*nu+q)*NP
+  int nhalves;        // 1 or 2
+  int pad;
+};
+
+// Shapes shared by the kernels of one system.
+struct Dims {
+  int no, nu;
+  int64_t KP;   // padded contraction length of one half: round_up(nu+no, kKB)
+  int64_t NP;   // padded single-index length: round_up(nu, kBN)
+  int nb;       // reduction blocks per index: ceil(nu / kRB)
+  int64_t ncta; // canonical block triples: nb(nb+1)(nb+2)/6
+};
+
+// Device-side description of one tuple for the reduction kernels.
+struct TupleDev {
+  const double *x[3];   // X buffers of the tuple's GEMM jobs
+  int kind, i, j, k;
+  double weight;        // 1 for i>j>k, 1/2 for degenerate tuples
+};
+
+// ----------------------------------------------------------------------------- launchers
+// layout.cu
+int launch_build_e(const Dims &d, const double *vvvo_packed, const double *t2, double *E, int x_begin,
+                   int x_end, cudaStream_t s);
+int launch_build_e_slice(const Dims &d, const double *packed_slice, const double *t2, double *E, int x,
+                         cudaStream_t s);
+int launch_build_f(const Dims &d, const double *t2, const double *vm, double *F, cudaStream_t s);
+int launch_check_inputs(const Dims &d, const double *eh, const double *ep, const double *t1, const double *t2,
+                        const double *vm, const double *voe, const double *vvvo, int *flags, cudaStream_t s);
+
+// wbuild_f64.cu
+int launch_wbuild_f64(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStream_t s);
+
+// reduce.cu
+int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
+                  const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s);
+int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const double *vpart,
+                    double *etd_acc, double *v1_acc, cudaStream_t s);
+int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const double *etd_acc, double *out3,
+               cudaStream_t s);
+
+// peak.cu
+double measure_fp64_peak(int device);
+
+}  // namespace cct

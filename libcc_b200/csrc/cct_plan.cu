@@ -1,0 +1,505 @@
+// Plan object, tuple scheduler and the exported C ABI.
+//
+// Replaces the triples driver (src/triples-ijk/triples.F90:1-333,
+// src/triples-abc/triples.f90:193-342) for one GPU: the DDI arrays become
+// device-resident HBM buffers owned by the plan, the static/dynamic tuple
+// partition becomes a host-side tuple list walked in the reference's order,
+// and ddi_gsumf becomes fixed-order on-device accumulation.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cct_internal.cuh"
+
+namespace cct {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error() { return g_last_error.c_str(); }
+
+std::vector<Tuple> tuple_list(int no) {
+  std::vector<Tuple> v;
+  // i>j>k in DDCC_T_TASK order (common_functions.f:62-86): i outermost
+  for (int i = 0; i < no; i++)
+    for (int j = 0; j < i; j++)
+      for (int k = 0; k < j; k++) v.push_back({kIJK, i, j, k});
+  // then per i, j<i: (i,j,j) and (i,i,j) (triples-abc/triples.f90:286-313)
+  for (int i = 0; i < no; i++)
+    for (int j = 0; j < i; j++) {
+      v.push_back({kIJJ, i, j, j});
+      v.push_back({kIIJ, i, i, j});
+    }
+  return v;
+}
+
+}  // namespace cct
+
+using namespace cct;
+
+struct ccT_plan {
+  int device = 0;
+  ccT_options opt{};
+  Dims d{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // inputs (device copies, reference layouts)
+  double *eh = nullptr, *ep = nullptr, *t1 = nullptr, *t2 = nullptr, *vm = nullptr, *voe = nullptr;
+  // derived operands
+  double *E = nullptr, *F = nullptr;
+  double *X[3] = {nullptr, nullptr, nullptr};
+  double *xpart = nullptr, *vpart = nullptr;
+  int16_t *cta_table = nullptr;
+  double *acc = nullptr;  // [etd_sum, etd_comp, out3[3], v1(nu*no)]
+  GemmJob *jobs = nullptr;  // 3 per tuple
+  int *flags = nullptr;
+  double *stage = nullptr;  // packed-slice staging for the legacy hook
+  std::vector<Tuple> tuples;
+  std::vector<char> e_built;  // legacy hook: E[x] built
+  bool inputs_ready = false;
+  float last_ms = 0.f;
+  int64_t last_launches = 0;
+  std::vector<double> host_eh, host_ep;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = 0;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    cudaSetDevice(dev);
+  }
+  ~DeviceGuard() { cudaSetDevice(prev); }
+};
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)));
+  return CCT_OK;
+}
+
+double *v1_acc(ccT_plan *p) { return p->acc + 5; }
+
+int build_jobs(ccT_plan *p) {
+  const Dims &d = p->d;
+  const int64_t nu2 = (int64_t)d.nu * d.nu;
+  auto Ex = [&](int x) { return p->E + (int64_t)x * nu2 * d.KP; };
+  auto Fyz = [&](int y, int z) { return p->F + ((int64_t)y * d.no + z) * d.NP * d.KP; };
+  auto G = [&](int x1, int x2, int x3, int slot) {
+    return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[slot], 2, 0};
+  };
+  auto H = [&](int x1, int x2, int x3, int slot) {
+    return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[slot], 1, 0};
+  };
+  std::vector<GemmJob> jobs;
+  jobs.reserve(p->tuples.size() * 3);
+  for (const Tuple &t : p->tuples) {
+    if (t.kind == kIJK) {
+      jobs.push_back(G(t.i, t.j, t.k, 0));
+      jobs.push_back(G(t.i, t.k, t.j, 1));
+      jobs.push_back(G(t.j, t.k, t.i, 2));
+    } else if (t.kind == kIJJ) {  // (i,j,j): G(i,j,j), H(j,j,i)
+      jobs.push_back(G(t.i, t.j, t.j, 0));
+      jobs.push_back(H(t.j, t.j, t.i, 1));
+      jobs.push_back(H(t.j, t.j, t.i, 2));  // unused slot
+    } else {  // (i,i,k): H(i,i,k), G(i,k,i)
+      jobs.push_back(H(t.i, t.i, t.k, 0));
+      jobs.push_back(G(t.i, t.k, t.i, 1));
+      jobs.push_back(G(t.i, t.k, t.i, 2));  // unused slot
+    }
+  }
+  CCT_CUDA(cudaMemcpy(p->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
+  return CCT_OK;
+}
+
+int check_denominators(ccT_plan *p) {
+  // every tuple with work has i>=j>=k not all equal; D_abc <= eh_i+eh_j+eh_k - 3 min(ep)
+  const int no = p->d.no, nu = p->d.nu;
+  double epmin = p->host_ep[0];
+  for (int a = 1; a < nu; a++) epmin = std::fmin(epmin, p->host_ep[a]);
+  double worst = -INFINITY;
+  for (const Tuple &t : p->tuples) {
+    const double dijk = p->host_eh[t.i] + p->host_eh[t.j] + p->host_eh[t.k];
+    worst = std::fmax(worst, dijk - 3.0 * epmin);
+  }
+  (void)no;
+  if (!(worst < 0.0)) {
+    set_error("denominator e_i+e_j+e_k-e_a-e_b-e_c reaches " + std::to_string(worst) + " >= 0");
+    return CCT_ERR_DENOMINATOR;
+  }
+  return CCT_OK;
+}
+
+int run_tuple(ccT_plan *p, int64_t tix) {
+  const Tuple &t = p->tuples[tix];
+  const int njobs = t.kind == kIJK ? 3 : 2;
+  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tix, njobs, p->stream));
+  TupleDev td;
+  td.x[0] = p->X[0];
+  td.x[1] = p->X[1];
+  td.x[2] = p->X[2];
+  td.kind = t.kind;
+  td.i = t.i;
+  td.j = t.j;
+  td.k = t.k;
+  td.weight = t.kind == kIJK ? 1.0 : 0.5;
+  CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->stream));
+  CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->stream));
+  p->last_launches += 3;
+  return CCT_OK;
+}
+
+[[noreturn]] void legacy_stop(const char *where, int status) {
+  std::fprintf(stderr, "libcc_b200: %s failed: %s (%s)\n", where, ccT_status_string(status), last_error());
+  std::fflush(stderr);
+  std::exit(1);
+}
+
+}  // namespace
+
+extern "C" {
+
+void ccT_options_default(ccT_options *opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->precision = CCT_PREC_FP64;
+  opt->device = 0;
+  opt->check_inputs = 1;
+  opt->emu_slices = 0;
+}
+
+const char *ccT_status_string(int status) {
+  switch (status) {
+    case CCT_OK: return "ok";
+    case CCT_ERR_INVALID: return "invalid argument";
+    case CCT_ERR_CUDA: return "CUDA error";
+    case CCT_ERR_NOMEM: return "device out of memory";
+    case CCT_ERR_NONFINITE: return "non-finite input or result";
+    case CCT_ERR_DENOMINATOR: return "non-negative orbital-energy denominator";
+    case CCT_ERR_STATE: return "call out of order";
+    case CCT_ERR_TIMEOUT: return "device wait timed out";
+    case CCT_ERR_UNSUPPORTED: return "unsupported option";
+    default: return "unknown status";
+  }
+}
+
+const char *ccT_last_error(void) { return last_error(); }
+
+int64_t ccT_num_tuples(int64_t no) {
+  if (no < 0) return 0;
+  return no * (no - 1) * (no - 2) / 6 + no * (no - 1);
+}
+
+int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *opt) {
+  if (!out) {
+    set_error("plan pointer is NULL");
+    return CCT_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (no < 2 || nu < 1 || no > 4096 || nu > 8 * 32767) {
+    set_error("need 2 <= no <= 4096 and 1 <= nu (got no=" + std::to_string(no) + ", nu=" + std::to_string(nu) + ")");
+    return CCT_ERR_INVALID;
+  }
+  if (nu * nu > (int64_t)0x7fffffff) {
+    set_error("nu*nu exceeds int32 row indexing");
+    return CCT_ERR_INVALID;
+  }
+  ccT_options o;
+  ccT_options_default(&o);
+  if (opt) o = *opt;
+  if (o.precision != CCT_PREC_FP64 && o.precision != CCT_PREC_INT8_EMU) {
+    set_error("unknown precision");
+    return CCT_ERR_INVALID;
+  }
+  if (o.precision == CCT_PREC_INT8_EMU) {
+    set_error("INT8-emulated precision is not built in this library version");
+    return CCT_ERR_UNSUPPORTED;
+  }
+  int ndev = 0;
+  CCT_CUDA(cudaGetDeviceCount(&ndev));
+  if (o.device < 0 || o.device >= ndev) {
+    set_error("device ordinal out of range");
+    return CCT_ERR_INVALID;
+  }
+  DeviceGuard guard(o.device);
+  ccT_plan *p = new ccT_plan();
+  p->device = o.device;
+  p->opt = o;
+  Dims &d = p->d;
+  d.no = (int)no;
+  d.nu = (int)nu;
+  d.KP = round_up(nu + no, kKB);
+  d.NP = round_up(nu, kBN);
+  d.nb = (int)((nu + kRB - 1) / kRB);
+  d.ncta = (int64_t)d.nb * (d.nb + 1) * (d.nb + 2) / 6;
+  p->tuples = tuple_list((int)no);
+  auto fail = [&](int s) {
+    ccT_plan_destroy(p);
+    return s;
+  };
+  int s;
+  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  const int64_t nu2 = nu * nu;
+  if ((s = dalloc(&p->eh, no)) || (s = dalloc(&p->ep, nu)) || (s = dalloc(&p->t1, no * nu)) ||
+      (s = dalloc(&p->t2, nu2 * no * no)) || (s = dalloc(&p->vm, no * nu * no * no)) ||
+      (s = dalloc(&p->voe, nu2 * no * no)) || (s = dalloc(&p->E, no * nu2 * d.KP)) ||
+      (s = dalloc(&p->F, no * no * d.NP * d.KP)) || (s = dalloc(&p->X[0], nu2 * d.NP)) ||
+      (s = dalloc(&p->X[1], nu2 * d.NP)) || (s = dalloc(&p->X[2], nu2 * d.NP)) ||
+      (s = dalloc(&p->xpart, d.ncta)) || (s = dalloc(&p->vpart, d.ncta * 72)) ||
+      (s = dalloc(&p->cta_table, d.ncta * 3)) || (s = dalloc(&p->acc, 5 + nu * no)) ||
+      (s = dalloc(&p->jobs, p->tuples.size() * 3)) || (s = dalloc(&p->flags, 4)))
+    return fail(s);
+  std::vector<int16_t> table(d.ncta * 3);
+  int64_t idx = 0;
+  for (int C = 0; C < d.nb; C++)
+    for (int B = 0; B <= C; B++)
+      for (int A = 0; A <= B; A++) {
+        table[3 * idx] = (int16_t)A;
+        table[3 * idx + 1] = (int16_t)B;
+        table[3 * idx + 2] = (int16_t)C;
+        idx++;
+      }
+  if (cudaMemcpy(p->cta_table, table.data(), table.size() * sizeof(int16_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(CCT_ERR_CUDA);
+  if ((s = build_jobs(p))) return fail(s);
+  p->e_built.assign(no, 0);
+  *out = p;
+  return CCT_OK;
+}
+
+int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double *t1, const double *t2,
+                   const double *vm, const double *voe, const double *vvvo, int32_t mem) {
+  if (!p) {
+    set_error("plan is NULL");
+    return CCT_ERR_INVALID;
+  }
+  if (!eh || !ep || !t1 || !t2 || !vm || !voe || !vvvo) {
+    set_error("an input pointer is NULL");
+    return CCT_ERR_INVALID;
+  }
+  if (mem != CCT_MEM_HOST && mem != CCT_MEM_DEVICE) {
+    set_error("mem must be CCT_MEM_HOST or CCT_MEM_DEVICE");
+    return CCT_ERR_INVALID;
+  }
+  DeviceGuard guard(p->device);
+  const Dims &d = p->d;
+  const int64_t no = d.no, nu = d.nu, nu2 = nu * nu;
+  const int64_t nvvvo = nu * (nu + 1) / 2 * nu * no;
+  const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  p->inputs_ready = false;
+  CCT_CUDA(cudaMemcpyAsync(p->eh, eh, no * 8, kind, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(p->ep, ep, nu * 8, kind, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(p->t1, t1, no * nu * 8, kind, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(p->t2, t2, nu2 * no * no * 8, kind, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(p->vm, vm, no * nu * no * no * 8, kind, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(p->voe, voe, nu2 * no * no * 8, kind, p->stream));
+  const double *vvvo_dev = vvvo;
+  double *staged = nullptr;
+  if (mem == CCT_MEM_HOST) {
+    // the packed VVVO is only needed to build E; stage it in a transient buffer
+    CCT_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&staged), nvvvo * 8, p->stream));
+    CCT_CUDA(cudaMemcpyAsync(staged, vvvo, nvvvo * 8, cudaMemcpyHostToDevice, p->stream));
+    vvvo_dev = staged;
+  }
+  int s = CCT_OK;
+  if (p->opt.check_inputs) {
+    CCT_CUDA(cudaMemsetAsync(p->flags, 0, 16, p->stream));
+    s = launch_check_inputs(d, p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, vvvo_dev, p->flags, p->stream);
+  }
+  if (s == CCT_OK) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
+  if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
+  if (staged) cudaFreeAsync(staged, p->stream);
+  if (s != CCT_OK) return s;
+  p->host_eh.resize(no);
+  p->host_ep.resize(nu);
+  int hflags[4] = {0, 0, 0, 0};
+  CCT_CUDA(cudaMemcpyAsync(p->host_eh.data(), p->eh, no * 8, cudaMemcpyDeviceToHost, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(p->host_ep.data(), p->ep, nu * 8, cudaMemcpyDeviceToHost, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(hflags, p->flags, 16, cudaMemcpyDeviceToHost, p->stream));
+  CCT_CUDA(cudaStreamSynchronize(p->stream));
+  if (p->opt.check_inputs) {
+    if (hflags[0]) {
+      set_error("an input array holds NaN or Inf");
+      return CCT_ERR_NONFINITE;
+    }
+    CCT_TRY(check_denominators(p));
+  }
+  std::fill(p->e_built.begin(), p->e_built.end(), 1);
+  p->inputs_ready = true;
+  return CCT_OK;
+}
+
+int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *etd, double *v1_out) {
+  if (!p) {
+    set_error("plan is NULL");
+    return CCT_ERR_INVALID;
+  }
+  if (!p->inputs_ready) {
+    set_error("ccT_forward before ccT_set_inputs");
+    return CCT_ERR_STATE;
+  }
+  const int64_t nt = (int64_t)p->tuples.size();
+  if (begin < 0 || end > nt || begin > end) {
+    set_error("tuple range [" + std::to_string(begin) + ", " + std::to_string(end) + ") outside [0, " +
+              std::to_string(nt) + ")");
+    return CCT_ERR_INVALID;
+  }
+  DeviceGuard guard(p->device);
+  const Dims &d = p->d;
+  p->last_launches = 0;
+  CCT_CUDA(cudaMemsetAsync(p->acc, 0, (5 + (int64_t)d.nu * d.no) * 8, p->stream));
+  CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
+  for (int64_t t = begin; t < end; t++) CCT_TRY(run_tuple(p, t));
+  CCT_TRY(launch_ets(d, p->t1, v1_acc(p), p->acc, p->acc + 2, p->stream));
+  p->last_launches += 1;
+  CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
+  double out3[3];
+  CCT_CUDA(cudaMemcpyAsync(out3, p->acc + 2, 3 * 8, cudaMemcpyDeviceToHost, p->stream));
+  if (v1_out)
+    CCT_CUDA(cudaMemcpyAsync(v1_out, v1_acc(p), (int64_t)d.nu * d.no * 8, cudaMemcpyDeviceToHost, p->stream));
+  CCT_CUDA(cudaStreamSynchronize(p->stream));
+  CCT_CUDA(cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1));
+  if (ets) *ets = out3[0];
+  if (etd) *etd = out3[1];
+  if (!std::isfinite(out3[0]) || !std::isfinite(out3[1])) {
+    set_error("E(T) is not finite");
+    return CCT_ERR_NONFINITE;
+  }
+  return CCT_OK;
+}
+
+double ccT_last_forward_ms(const ccT_plan *p) { return p ? (double)p->last_ms : 0.0; }
+int64_t ccT_last_forward_launches(const ccT_plan *p) { return p ? p->last_launches : 0; }
+
+int ccT_plan_destroy(ccT_plan *p) {
+  if (!p) return CCT_OK;
+  DeviceGuard guard(p->device);
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->X[0], p->X[1], p->X[2],
+                    p->xpart, p->vpart, p->acc, p->stage};
+  for (double *b : bufs)
+    if (b) cudaFree(b);
+  if (p->cta_table) cudaFree(p->cta_table);
+  if (p->jobs) cudaFree(p->jobs);
+  if (p->flags) cudaFree(p->flags);
+  if (p->ev0) cudaEventDestroy(p->ev0);
+  if (p->ev1) cudaEventDestroy(p->ev1);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return CCT_OK;
+}
+
+double ccT_measure_fp64_peak(int32_t device) { return measure_fp64_peak(device); }
+
+// ----------------------------------------------------------------------------- legacy hooks
+
+static ccT_plan *g_hook = nullptr;
+static double *g_hook_v1 = nullptr;
+static std::mutex g_hook_mutex;
+
+void ijk_gpu_init_(const int64_t *no, const int64_t *nu, const double *eh, const double *ep, double *v1,
+                   const double *t2, const double *vm, const double *voe) {
+  std::lock_guard<std::mutex> lock(g_hook_mutex);
+  if (!no || !nu || !eh || !ep || !v1 || !t2 || !vm || !voe) legacy_stop("ijk_gpu_init", CCT_ERR_INVALID);
+  if (g_hook) {
+    ccT_plan_destroy(g_hook);
+    g_hook = nullptr;
+  }
+  ccT_plan *p = nullptr;
+  int s = ccT_plan_create(&p, *no, *nu, nullptr);
+  if (s) legacy_stop("ijk_gpu_init", s);
+  DeviceGuard guard(p->device);
+  const int64_t n_o = *no, n_u = *nu, nu2 = n_u * n_u;
+  auto up = [&](double *dst, const double *src, int64_t n) {
+    if (cudaMemcpy(dst, src, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) legacy_stop("ijk_gpu_init", CCT_ERR_CUDA);
+  };
+  up(p->eh, eh, n_o);
+  up(p->ep, ep, n_u);
+  up(p->t2, t2, nu2 * n_o * n_o);
+  up(p->vm, vm, n_o * n_u * n_o * n_o);
+  up(p->voe, voe, nu2 * n_o * n_o);
+  if ((s = launch_build_f(p->d, p->t2, p->vm, p->F, p->stream))) legacy_stop("ijk_gpu_init", s);
+  if ((s = dalloc(&p->stage, n_u * (n_u + 1) / 2 * n_u))) legacy_stop("ijk_gpu_init", s);
+  if (cudaMemsetAsync(p->acc, 0, (5 + n_u * n_o) * 8, p->stream) != cudaSuccess) legacy_stop("ijk_gpu_init", CCT_ERR_CUDA);
+  p->host_eh.assign(eh, eh + n_o);
+  p->host_ep.assign(ep, ep + n_u);
+  std::fill(p->e_built.begin(), p->e_built.end(), 0);
+  p->inputs_ready = true;
+  g_hook = p;
+  g_hook_v1 = v1;
+}
+
+void ijk_gpu_driver_(const int64_t *nu, const int64_t *no, const int64_t *i, const int64_t *j, const int64_t *k,
+                     const double *ve_i, const double *ve_j, const double *ve_k, double *t1, const double *eh,
+                     const double *ep, double *etd) {
+  (void)t1; (void)eh; (void)ep; (void)etd;
+  std::lock_guard<std::mutex> lock(g_hook_mutex);
+  ccT_plan *p = g_hook;
+  if (!p) legacy_stop("ijk_gpu_driver", CCT_ERR_STATE);
+  if (!nu || !no || !i || !j || !k || *nu != p->d.nu || *no != p->d.no) legacy_stop("ijk_gpu_driver", CCT_ERR_INVALID);
+  const int64_t I = *i - 1, J = *j - 1, K = *k - 1;  // reference indices are 1-based
+  if (!(I > J && J > K && K >= 0 && I < p->d.no)) {
+    set_error("need i > j > k >= 1 and i <= no");
+    legacy_stop("ijk_gpu_driver", CCT_ERR_INVALID);
+  }
+  DeviceGuard guard(p->device);
+  const int64_t slice = (int64_t)p->d.nu * (p->d.nu + 1) / 2 * p->d.nu;
+  const int64_t xs[3] = {I, J, K};
+  const double *vs[3] = {ve_i, ve_j, ve_k};
+  for (int r = 0; r < 3; r++) {
+    const int64_t x = xs[r];
+    if (p->e_built[x]) continue;
+    if (!vs[r]) legacy_stop("ijk_gpu_driver", CCT_ERR_INVALID);
+    if (cudaMemcpyAsync(p->stage, vs[r], slice * 8, cudaMemcpyHostToDevice, p->stream) != cudaSuccess)
+      legacy_stop("ijk_gpu_driver", CCT_ERR_CUDA);
+    int s = launch_build_e_slice(p->d, p->stage, p->t2, p->E, (int)x, p->stream);
+    if (s) legacy_stop("ijk_gpu_driver", s);
+    if (cudaStreamSynchronize(p->stream) != cudaSuccess) legacy_stop("ijk_gpu_driver", CCT_ERR_CUDA);
+    p->e_built[x] = 1;
+  }
+  // index of (I,J,K) in the tuple list: DDCC_T_TASK order
+  const int64_t tix = I * (I - 1) * (I - 2) / 6 + J * (J - 1) / 2 + K;
+  int s = run_tuple(p, tix);
+  if (s) legacy_stop("ijk_gpu_driver", s);
+}
+
+void ijk_gpu_finalize_(const int64_t *no, const int64_t *nu, double *etd) {
+  std::lock_guard<std::mutex> lock(g_hook_mutex);
+  ccT_plan *p = g_hook;
+  if (!p) legacy_stop("ijk_gpu_finalize", CCT_ERR_STATE);
+  if (!no || !nu || !etd || *no != p->d.no || *nu != p->d.nu) legacy_stop("ijk_gpu_finalize", CCT_ERR_INVALID);
+  DeviceGuard guard(p->device);
+  const int64_t n = (int64_t)p->d.nu * p->d.no;
+  std::vector<double> v1(n);
+  double e[2];
+  if (cudaMemcpyAsync(e, p->acc, 16, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess ||
+      cudaMemcpyAsync(v1.data(), v1_acc(p), n * 8, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess ||
+      cudaStreamSynchronize(p->stream) != cudaSuccess)
+    legacy_stop("ijk_gpu_finalize", CCT_ERR_CUDA);
+  *etd += e[0] + e[1];
+  for (int64_t q = 0; q < n; q++) g_hook_v1[q] += v1[q];
+  ccT_plan_destroy(p);
+  g_hook = nullptr;
+  g_hook_v1 = nullptr;
+}
+
+void cc_triples_b200_(const int64_t *no, const int64_t *nu, const double *eh, const double *ep, double *v1,
+                      const double *t1, const double *t2, const double *vm, const double *voe, const double *vvvo,
+                      double *ets, double *etd) {
+  if (!no || !nu || !ets || !etd) legacy_stop("cc_triples_b200", CCT_ERR_INVALID);
+  ccT_plan *p = nullptr;
+  int s = ccT_plan_create(&p, *no, *nu, nullptr);
+  if (s) legacy_stop("cc_triples_b200", s);
+  s = ccT_set_inputs(p, eh, ep, t1, t2, vm, voe, vvvo, CCT_MEM_HOST);
+  if (s == CCT_OK) s = ccT_forward(p, 0, ccT_num_tuples(*no), ets, etd, v1);
+  ccT_plan_destroy(p);
+  if (s) legacy_stop("cc_triples_b200", s);
+}
+
+}  // extern "C"

@@ -1,0 +1,442 @@
+"""ORACLE: CPU restatements of libcc's (T) triples correction.
+
+TEST INFRASTRUCTURE ONLY.  Imported solely by tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline / ``--impl reference`` legs, as the checker or as
+the timed stand-in for the reference's CPU ``triples.x``.  The product package
+``libcc_b200`` never imports it.
+
+Parity status: PARTIALLY PINNED (see the header of triples_oracle.c): the TRANT3
+known-answer table and the restart-file sizes are pinned against the reference;
+the energies are not, because the reference's ``triples.restart`` inputs are
+missing from its tree.
+
+Three restatements live here:
+
+* ``c_*``       ctypes front-end of ``triples_oracle.c`` -- the literal
+                triples-abc pipeline with plain-loop DGEMMs (small sizes).
+* ``literal_*`` the same literal sequence with numpy/OpenBLAS DGEMMs (the
+                reference also calls a vendor DGEMM); fast enough for the full
+                workloads, so it is the timed CPU baseline.
+* ``closed_*``  the closed form of W_abc (one expression per reference term
+                label #0..#11, ``ijk_tuple.f90:56-80``) with the unified
+                degenerate-tuple handling; an independent cross-check.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+_lib = None
+
+
+# --------------------------------------------------------------------------- build / load
+
+def build(force: bool = False) -> pathlib.Path:
+    """Compile triples_oracle.c into oracle/_build/liboracle.so with gcc."""
+    src = HERE / "triples_oracle.c"
+    LIB_PATH.parent.mkdir(exist_ok=True)
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        cmd = ["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c11", "-o", str(LIB_PATH), str(src), "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        dp = ctypes.POINTER(ctypes.c_double)
+        i64 = ctypes.c_int64
+        _lib.orc_trant3.argtypes = [dp, i64, ctypes.c_int]
+        _lib.orc_cc_triples.argtypes = [i64, i64] + [dp] * 7 + [dp, dp, dp]
+        _lib.orc_cc_triples.restype = ctypes.c_int
+        _lib.orc_getve.argtypes = [dp, i64, i64, dp]
+        _lib.orc_ijk_formv3.argtypes = [i64] * 5 + [dp] * 6
+        _lib.orc_ijj_formv3.argtypes = [i64] * 4 + [dp] * 5
+        _lib.orc_iij_formv3.argtypes = [i64] * 4 + [dp] * 5
+        _lib.orc_symt311.argtypes = [dp, i64, ctypes.c_int]
+        _lib.orc_t1wt3_fused.argtypes = [i64] * 5 + [dp, dp, dp, dp, dp]
+        _lib.orc_t1wt3_fused.restype = ctypes.c_double
+        _lib.orc_task.argtypes = [i64, i64, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]
+        _lib.orc_div_even.argtypes = [i64, i64, i64, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+        _lib.orc_tuple.argtypes = [ctypes.c_int] + [i64] * 5 + [dp] * 11 + [dp]
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+# --------------------------------------------------------------------------- C oracle front-end
+
+def c_trant3(v: np.ndarray, nu: int, tid: int) -> np.ndarray:
+    """TRANT3_SMP(v, nu, id) in place on a copy of the flat Fortran array."""
+    out = np.ascontiguousarray(v, dtype=np.float64).copy()
+    lib().orc_trant3(_p(out), nu, tid)
+    return out
+
+
+def c_cc_triples(inp):
+    """Whole (T) driver (triples-abc semantics).  Returns (ets, etd, v1[nu*no])."""
+    v1 = np.zeros(inp.nu * inp.no)
+    ets = ctypes.c_double()
+    etd = ctypes.c_double()
+    rc = lib().orc_cc_triples(inp.no, inp.nu, _p(inp.eh), _p(inp.ep), _p(inp.t1), _p(inp.t2),
+                              _p(inp.vm), _p(inp.voe), _p(inp.vvvo), _p(v1),
+                              ctypes.byref(ets), ctypes.byref(etd))
+    if rc != 0:
+        raise MemoryError("oracle out of memory")
+    return ets.value, etd.value, v1
+
+
+def c_task(task: int, no: int):
+    i, j, k = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    lib().orc_task(task, no, ctypes.byref(i), ctypes.byref(j), ctypes.byref(k))
+    return i.value, j.value, k.value
+
+
+def c_div_even(n: int, np_: int, me: int):
+    nr, sr = ctypes.c_int64(), ctypes.c_int64()
+    lib().orc_div_even(n, np_, me, ctypes.byref(nr), ctypes.byref(sr))
+    return nr.value, sr.value
+
+
+def c_getve(inp, x: int) -> np.ndarray:
+    ve = np.zeros(inp.nu ** 3)
+    lib().orc_getve(_p(inp.vvvo), inp.nu, x, _p(ve))
+    return ve
+
+
+def c_tuple_w(inp, kind: int, i: int, j: int, k: int) -> np.ndarray:
+    """W (flat Fortran nu^3) of one tuple from the literal formv3 sequence, after
+    SYMT311/ZEROT3 as the reference's pipeline applies them.  0-based i,j,k."""
+    nu = inp.nu
+    ve = {}
+    for x in {i, j, k}:
+        v = c_getve(inp, x)
+        lib().orc_trant3(_p(v), nu, 1)
+        ve[x] = v
+    v3 = np.zeros(nu ** 3)
+    if kind == 0:
+        lib().orc_ijk_formv3(inp.no, nu, i, j, k, _p(inp.t2), _p(inp.vm), _p(ve[i]), _p(ve[j]), _p(ve[k]), _p(v3))
+    elif kind == 1:  # (i, j, j)
+        lib().orc_ijj_formv3(inp.no, nu, i, j, _p(inp.t2), _p(inp.vm), _p(ve[i]), _p(ve[j]), _p(v3))
+        lib().orc_symt311(_p(v3), nu, 23)
+        v3.reshape(nu, nu, nu)[np.arange(nu), np.arange(nu), np.arange(nu)] = 0.0
+    else:  # (i, i, j)
+        lib().orc_iij_formv3(inp.no, nu, i, k, _p(inp.t2), _p(inp.vm), _p(ve[i]), _p(ve[k]), _p(v3))
+        lib().orc_symt311(_p(v3), nu, 12)
+        v3.reshape(nu, nu, nu)[np.arange(nu), np.arange(nu), np.arange(nu)] = 0.0
+    return v3
+
+
+def c_tuple(inp, kind: int, i: int, j: int, k: int):
+    """One tuple through the reference pipeline: returns (etd contribution, v1 contribution)."""
+    nu, no = inp.nu, inp.no
+    ve = {}
+    for x in {i, j, k}:
+        v = c_getve(inp, x)
+        lib().orc_trant3(_p(v), nu, 1)
+        ve[x] = v
+    v3 = np.zeros(nu ** 3)
+    t3 = np.zeros(nu ** 3)
+    v1 = np.zeros(nu * no)
+    e = ctypes.c_double(0.0)
+    a, b, c = ve[i], ve[j], ve[k]
+    lib().orc_tuple(kind, no, nu, i, j, k, _p(inp.t2), _p(inp.vm), _p(inp.voe), _p(inp.eh), _p(inp.ep),
+                    _p(a), _p(b), _p(c), _p(v3), _p(t3), _p(v1), ctypes.byref(e))
+    return e.value, v1
+
+
+# --------------------------------------------------------------------------- numpy helpers
+
+def _fv(flat: np.ndarray, shape):
+    """Fortran-order view of a flat array."""
+    return flat.reshape(shape, order="F")
+
+
+def _perm(w: np.ndarray, spec: str) -> np.ndarray:
+    """X[a,b,c] = w[spec] e.g. spec='bca' -> X[a,b,c] = w[b,c,a]."""
+    return np.einsum(spec + "->abc", w)
+
+
+def _trant3_np(v: np.ndarray, tid: int) -> np.ndarray:
+    spec = {1: "acb", 2: "bac", 3: "cba", 4: "bca", 5: "cab"}[tid]
+    return np.asfortranarray(_perm(v, spec))
+
+
+def expand_vvvo(inp, x: int) -> np.ndarray:
+    """VEo_x(a,b,c) = (ab|c x) as an (nu,nu,nu) Fortran array (DDCC_T_GETVE)."""
+    nu = inp.nu
+    nutr = nu * (nu + 1) // 2
+    cols = inp.vvvo.reshape(nu * inp.no, nutr)[x * nu:(x + 1) * nu]  # [c][packed]
+    rows, colsidx = np.tril_indices(nu)  # packed order: (I >= J), I outer, J inner
+    ve = np.zeros((nu, nu, nu), order="F")
+    for c in range(nu):
+        sq = np.zeros((nu, nu))
+        sq[rows, colsidx] = cols[c]
+        sq[colsidx, rows] = cols[c]
+        ve[:, :, c] = sq
+    return ve
+
+
+class _Views:
+    def __init__(self, inp):
+        no, nu = inp.no, inp.nu
+        self.no, self.nu = no, nu
+        self.T2 = _fv(inp.t2, (nu * nu, no, no))        # T2(ab, l, x)
+        self.T2f = _fv(inp.t2, (nu, nu, no, no))
+        self.VM = _fv(inp.vm, (no, nu, no, no))
+        self.VOE = _fv(inp.voe, (nu * nu, no, no))
+        self.eh, self.ep = inp.eh, inp.ep
+        self.t1 = _fv(inp.t1, (no, nu))
+
+    def t2x(self, x):            # (nu2, no)
+        return self.T2[:, :, x]
+
+    def t2xy(self, x, y):        # T2(:,:,y,x) as (nu, nu)
+        return self.T2f[:, :, y, x]
+
+    def vmxy(self, x, y):        # (no, nu)
+        return self.VM[:, :, x, y]
+
+
+# --------------------------------------------------------------------------- literal numpy pipeline
+
+def literal_ijk_w(V: _Views, i, j, k, ve_i, ve_j, ve_k) -> np.ndarray:
+    """ijk_tuple_formv3 (triples-abc/ijk_tuple.f90:1-53) with BLAS DGEMMs; ve_x are the
+    swapped slices ve_x(a,b,c) = (ac|b x).  Returns W (nu,nu,nu) Fortran order."""
+    nu = V.nu
+    nu2 = nu * nu
+    v3 = np.zeros((nu, nu, nu), order="F")
+    m2 = lambda v: v.reshape((nu2, nu), order="F")
+    m1 = lambda v: v.reshape((nu, nu2), order="F")
+    vi, vj, vk = m1(ve_i), m1(ve_j), m1(ve_k)
+    m2(v3)[...] = -(V.t2x(i) @ V.vmxy(k, j))                           # #0
+    m2(v3)[...] += vi.T @ V.t2xy(k, j).T                               # #11
+    m1(v3)[...] += V.t2xy(i, k) @ vj                                   # #8
+    m1(v3)[...] -= V.vmxy(i, k).T @ V.t2x(j).T                         # #3
+    v3 = _trant3_np(v3, 1)
+    m2(v3)[...] -= V.t2x(i) @ V.vmxy(j, k)                             # #1
+    m2(v3)[...] += vi.T @ V.t2xy(j, k).T                               # #10
+    m1(v3)[...] += V.t2xy(i, j) @ vk                                   # #6
+    m1(v3)[...] -= V.vmxy(i, j).T @ V.t2x(k).T                         # #5
+    v3 = _trant3_np(v3, 4)
+    m2(v3)[...] -= V.t2x(j) @ V.vmxy(k, i)                             # #2
+    m2(v3)[...] += vj.T @ V.t2xy(k, i).T                               # #9
+    v3 = _trant3_np(v3, 1)
+    m1(v3)[...] -= V.vmxy(j, i).T @ V.t2x(k).T                         # #4
+    m1(v3)[...] += V.t2xy(j, i) @ vk                                   # #7
+    v3 = _trant3_np(v3, 4)
+    r = np.arange(nu)
+    v3[r, r, r] = 0.0                                                  # ZEROT3
+    return v3
+
+
+def literal_ijj_w(V: _Views, i, j, ve_i, ve_j) -> np.ndarray:
+    """ijj_tuple_formv3 (triples-abc/ijj_tuple.f90) + SYMT311(23) + ZEROT3 for (i,j,j)."""
+    nu = V.nu
+    nu2 = nu * nu
+    m2 = lambda v: v.reshape((nu2, nu), order="F")
+    m1 = lambda v: v.reshape((nu, nu2), order="F")
+    v3 = np.zeros((nu, nu, nu), order="F")
+    m2(v3)[...] = -(V.t2x(i) @ V.vmxy(j, j))
+    v3 = _trant3_np(v3, 2)
+    m2(v3)[...] -= V.t2x(j) @ V.vmxy(j, i)
+    v3 = _trant3_np(v3, 1)
+    m2(v3)[...] -= V.t2x(j) @ V.vmxy(i, j)
+    v3 = _trant3_np(v3, 4)
+    m1(v3)[...] += V.t2xy(i, j) @ m1(ve_j)
+    v3 = _trant3_np(v3, 3)
+    m1(v3)[...] += V.t2xy(j, i) @ m1(ve_j)
+    v3 = _trant3_np(v3, 1)
+    m1(v3)[...] += V.t2xy(j, j) @ m1(ve_i)
+    v3 = _trant3_np(v3, 2)
+    v3 = np.asfortranarray(v3 + _perm(v3, "acb"))
+    r = np.arange(nu)
+    v3[r, r, r] = 0.0
+    return v3
+
+
+def literal_iij_w(V: _Views, i, k, ve_i, ve_k) -> np.ndarray:
+    """iij_tuple_formv3 (triples-abc/iij_tuple.f90) + SYMT311(12) + ZEROT3 for (i,i,k)."""
+    nu = V.nu
+    nu2 = nu * nu
+    m2 = lambda v: v.reshape((nu2, nu), order="F")
+    m1 = lambda v: v.reshape((nu, nu2), order="F")
+    v3 = np.zeros((nu, nu, nu), order="F")
+    m2(v3)[...] = -(V.t2x(i) @ V.vmxy(k, i))
+    v3 = _trant3_np(v3, 1)
+    m2(v3)[...] -= V.t2x(i) @ V.vmxy(i, k)
+    v3 = _trant3_np(v3, 2)
+    m2(v3)[...] -= V.t2x(k) @ V.vmxy(i, i)
+    v3 = _trant3_np(v3, 2)
+    m1(v3)[...] += V.t2xy(i, i) @ m1(ve_k)
+    v3 = _trant3_np(v3, 1)
+    m1(v3)[...] += V.t2xy(i, k) @ m1(ve_i)
+    v3 = _trant3_np(v3, 3)
+    m1(v3)[...] += V.t2xy(k, i) @ m1(ve_i)
+    v3 = _trant3_np(v3, 3)
+    v3 = np.asfortranarray(v3 + _perm(v3, "bac"))
+    r = np.arange(nu)
+    v3[r, r, r] = 0.0
+    return v3
+
+
+def _smt3four(v):
+    return 2.0 * (v - _perm(v, "bac")) - _perm(v, "acb") + _perm(v, "bca")
+
+
+def _dinv(V: _Views, i, j, k):
+    ep = V.ep
+    dabc = ep[:, None, None] + ep[None, :, None] + ep[None, None, :]
+    return 1.0 / ((V.eh[i] + V.eh[j] + V.eh[k]) - dabc)
+
+
+def literal_reduce(V: _Views, i, j, k, w: np.ndarray, weight: float, v1: np.ndarray) -> float:
+    """T3SQUA + ADT3DEN + DRT1WT3IJK for a W with W_aaa = 0.  The six T1WT3IJK calls
+    of DRT1WT3IJK (triples-abc/ddcc_aux.f:146-169) are written with the permutation
+    each trant3 step leaves in TI.  ``weight`` is CF (1 or 1/2).  v1 is (nu,no)."""
+    nu = V.nu
+    d = _dinv(V, i, j, k)
+    f = 8.0 * w - 4.0 * (_perm(w, "acb") + _perm(w, "cba") + _perm(w, "bac")) + 2.0 * (_perm(w, "bca") + _perm(w, "cab"))
+    x3 = float(np.sum(f * w * d))
+    ti = np.asfortranarray(w * d)
+    seq = [((i, j, k), None), ((i, k, j), 1), ((j, i, k), 4), ((j, k, i), 1), ((k, i, j), 5), ((k, j, i), 1)]
+    for (I, J, K), t in seq:
+        if t is not None:
+            ti = _trant3_np(ti, t)
+        z = _smt3four(ti)
+        v1[:, I] += weight * (z.reshape((nu, nu * nu), order="F") @ V.VOE[:, J, K])
+    return weight * x3
+
+
+def literal_cc_triples(inp, tuples=None, threads=None):
+    """(T) through the literal numpy pipeline.  ``tuples`` optionally restricts the
+    work to a list of (kind, i, j, k) (kind 0: i>j>k, 1: (i,j,j), 2: (i,i,k));
+    degenerate tuples go through the literal ijj/iij_tuple_formv3 sequences with
+    SYMT311, and the DRT1WT3 reduction with weight 1/2 (tests/test_oracle.py ties
+    that to the reference's DRT1WT3IJ/JK).  Tuple energies are summed with
+    math.fsum.  Returns (ets, etd, v1[nu,no])."""
+    V = _Views(inp)
+    no, nu = inp.no, inp.nu
+    v1 = np.zeros((nu, no), order="F")
+    etd_parts = []
+    if tuples is None:
+        tuples = all_tuples(no)
+    cache = {}
+
+    def ve(x):
+        if x not in cache:
+            if len(cache) > 3:
+                cache.pop(next(iter(cache)))
+            cache[x] = _trant3_np(expand_vvvo(inp, x), 1)
+        return cache[x]
+
+    for kind, i, j, k in tuples:
+        if kind == 0:
+            w = literal_ijk_w(V, i, j, k, ve(i), ve(j), ve(k))
+            etd_parts.append(literal_reduce(V, i, j, k, w, 1.0, v1))
+        elif kind == 1:
+            w = literal_ijj_w(V, i, j, ve(i), ve(j))
+            etd_parts.append(literal_reduce(V, i, j, k, w, 0.5, v1))
+        else:
+            w = literal_iij_w(V, i, k, ve(i), ve(k))
+            etd_parts.append(literal_reduce(V, i, j, k, w, 0.5, v1))
+    etd = math.fsum(etd_parts)
+    ets = 2.0 * float(np.sum(V.t1.T * v1))
+    return ets, etd, v1
+
+
+def all_tuples(no: int):
+    """Every tuple with work: i>j>k in DDCC_T_TASK order, then for i, j<i the
+    (i,j,j) and (i,i,j) tuples (triples-abc/triples.f90:232-313).  0-based."""
+    out = []
+    for i in range(no):
+        for j in range(i):
+            for k in range(j):
+                out.append((0, i, j, k))
+    for i in range(no):
+        for j in range(i):
+            out.append((1, i, j, j))
+            out.append((2, i, i, j))
+    return out
+
+
+# --------------------------------------------------------------------------- closed form
+
+def closed_w(V: _Views, i, j, k, veo) -> np.ndarray:
+    """W_abc of tuple (i,j,k) from the twelve reference terms in closed form.
+    ``veo[x]`` is VEo_x(a,b,c) = (ab|c x).  Term labels follow ijk_tuple.f90:56-80.
+    With a repeated occupied index the same expression gives the symmetrised W of
+    the degenerate pipelines (SYMT311 after ijj/iij_tuple_formv3), W_aaa = 0."""
+    E = np.einsum
+    T2 = V.T2f
+    VM = V.VM
+    w = -E("abl,lc->abc", T2[:, :, :, i], VM[:, :, k, j])      # 0
+    w += E("dba,cd->abc", veo[i], T2[:, :, j, k])             # 11
+    w += E("ad,dcb->abc", T2[:, :, k, i], veo[j])             # 8
+    w -= E("la,bcl->abc", VM[:, :, i, k], T2[:, :, :, j])      # 3
+    w -= E("acl,lb->abc", T2[:, :, :, i], VM[:, :, j, k])      # 1
+    w += E("dca,bd->abc", veo[i], T2[:, :, k, j])             # 10
+    w += E("ad,dbc->abc", T2[:, :, j, i], veo[k])             # 6
+    w -= E("la,cbl->abc", VM[:, :, i, j], T2[:, :, :, k])      # 5
+    w -= E("bal,lc->abc", T2[:, :, :, j], VM[:, :, k, i])      # 2
+    w += E("dab,cd->abc", veo[j], T2[:, :, i, k])             # 9
+    w -= E("lb,cal->abc", VM[:, :, j, i], T2[:, :, :, k])      # 4
+    w += E("bd,dac->abc", T2[:, :, i, j], veo[k])             # 7
+    w = np.asfortranarray(w)
+    r = np.arange(V.nu)
+    w[r, r, r] = 0.0
+    return w
+
+
+def closed_reduce(V: _Views, i, j, k, w: np.ndarray, weight: float, v1: np.ndarray) -> float:
+    """E[4] and the v1 update in the fused full-sum form of t1wt3.f90:46-95:
+    v1(a,i) += sum_bc [Z1 VOE(b,c,j,k) + Z2 VOE(b,c,k,j)] / D, etc."""
+    nu = V.nu
+    d = _dinv(V, i, j, k)
+    P = lambda s: _perm(w, s)
+    wabc, wacb, wbac, wbca, wcab, wcba = w, P("acb"), P("bac"), P("bca"), P("cab"), P("cba")
+    x3 = float(np.sum((8 * wabc - 4 * (wacb + wcba + wbac) + 2 * (wbca + wcab)) * wabc * d))
+    z1 = (wabc - wbac) * 2 - wacb + wbca
+    z2 = (wacb - wbca) * 2 - wabc + wbac
+    z3 = (wbac - wabc) * 2 - wcab + wcba
+    z4 = (wbca - wacb) * 2 - wcba + wcab
+    z5 = (wcab - wcba) * 2 - wbac + wabc
+    z6 = (wcba - wcab) * 2 - wbca + wacb
+    VOE = V.VOE.reshape((nu, nu, V.no, V.no), order="F")
+    red = lambda z, x, y: np.einsum("abc,bc->a", z * d, VOE[:, :, x, y])
+    v1[:, i] += weight * (red(z1, j, k) + red(z2, k, j))
+    v1[:, j] += weight * (red(z3, i, k) + red(z5, k, i))
+    v1[:, k] += weight * (red(z4, i, j) + red(z6, j, i))
+    return weight * x3
+
+
+def closed_cc_triples(inp, tuples=None):
+    """(T) with closed-form W and the fused reduction for every tuple kind
+    (weight 1/2 for degenerate tuples).  Returns (ets, etd, v1[nu,no])."""
+    V = _Views(inp)
+    no, nu = inp.no, inp.nu
+    v1 = np.zeros((nu, no), order="F")
+    etd = 0.0
+    veo = {x: expand_vvvo(inp, x) for x in range(no)}
+    for kind, i, j, k in (tuples or all_tuples(no)):
+        w = closed_w(V, i, j, k, veo)
+        etd += closed_reduce(V, i, j, k, w, 1.0 if kind == 0 else 0.5, v1)
+    ets = 2.0 * float(np.sum(V.t1.T * v1))
+    return ets, etd, v1
+
+
+def cpu_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)

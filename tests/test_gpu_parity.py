@@ -1,0 +1,170 @@
+"""GPU parity of the FP64 (T) path against the oracle, through the C ABI."""
+import json
+import pathlib
+
+import numpy as np
+import pytest
+
+from libcc_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((pathlib.Path(__file__).parent / "golden" / "energies.json").read_text())
+
+
+def tol(e_ref: float, abs_tol: float = 1e-10, rel_tol: float = 2e-14) -> float:
+    """FP64 parity bar: 1e-10 Eh, or 2e-14 relative for the large synthetic energies
+    where 1e-10 Eh is below the summation round-off of any FP64 evaluation order."""
+    return max(abs_tol, rel_tol * abs(e_ref))
+
+
+@pytest.fixture(scope="module")
+def api():
+    from libcc_b200 import api as A
+    return A
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    from oracle import oracle as O
+    return O
+
+
+@pytest.mark.parametrize("no,nu,seed", [(2, 5, 1), (3, 4, 2), (4, 36, 0), (5, 9, 3), (6, 13, 5), (7, 33, 9),
+                                        (5, 71, 4), (3, 130, 8)])
+def test_fp64_matches_oracle(api, oracle, no, nu, seed):
+    inp = S.generate(no, nu, seed)
+    ets_o, etd_o, v1_o = oracle.c_cc_triples(inp)
+    with api.TriplesPlan(no, nu) as plan:
+        plan.set_system(inp)
+        ets, etd, v1 = plan.forward()
+    assert abs(etd - etd_o) <= tol(etd_o)
+    assert abs(ets - ets_o) <= tol(ets_o)
+    assert np.abs(v1 - v1_o).max() <= 1e-12 * max(1.0, np.abs(v1_o).max())
+
+
+def test_water_avdz_golden(api):
+    g = GOLDEN["water-avdz"]
+    inp = S.workload("water-avdz")
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        ets, etd, v1 = plan.forward()
+    assert abs(ets + etd - g["e_t"]) <= tol(g["e_t"])
+    assert abs(etd - g["etd"]) <= tol(g["etd"])
+    assert abs(np.linalg.norm(v1) - g["v1_norm"]) <= 1e-12 * g["v1_norm"]
+
+
+def test_no12_nu120_golden(api):
+    g = GOLDEN["no12-nu120"]
+    inp = S.workload("no12-nu120")
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        ets, etd, v1 = plan.forward()
+    assert abs(etd - g["etd"]) <= tol(g["etd"])
+    assert abs(ets - g["ets"]) <= tol(g["ets"], rel_tol=1e-12)
+
+
+def test_tuple_kinds_one_at_a_time(api, oracle):
+    """Every tuple of every kind alone, against the reference pipeline of that kind."""
+    no, nu = 5, 11
+    inp = S.generate(no, nu, 21)
+    tuples = oracle.all_tuples(no)
+    with api.TriplesPlan(no, nu) as plan:
+        plan.set_system(inp)
+        for t, (kind, i, j, k) in enumerate(tuples):
+            e_ref, v1_ref = oracle.c_tuple(inp, kind, i, j, k)
+            _, etd, v1 = plan.forward(t, t + 1)
+            assert abs(etd - e_ref) <= tol(e_ref), (kind, i, j, k)
+            assert np.abs(v1 - v1_ref).max() <= 1e-13 * max(1.0, np.abs(v1_ref).max()), (kind, i, j, k)
+
+
+def test_shards_sum_to_whole(api):
+    inp = S.generate(6, 17, 7)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        ets, etd, v1 = plan.forward()
+        n = plan.num_tuples
+        cuts = [0, 7, 23, n]
+        parts = [plan.forward(a, b) for a, b in zip(cuts[:-1], cuts[1:])]
+    assert abs(sum(p[1] for p in parts) - etd) <= tol(etd)
+    assert abs(sum(p[0] for p in parts) - ets) <= tol(ets)
+    assert np.abs(sum(p[2] for p in parts) - v1).max() <= 1e-13
+
+
+def test_bitwise_deterministic(api):
+    inp = S.generate(5, 40, 12)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        a = plan.forward()
+        b = plan.forward()
+    assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
+
+
+def test_device_inputs_match_host_inputs(api):
+    torch = pytest.importorskip("torch")
+    inp = S.generate(4, 23, 13)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        host = plan.forward()
+        dev = [torch.from_numpy(a).cuda() for a in inp.arrays()]
+        plan.set_inputs(*dev)
+        devr = plan.forward()
+    assert host[0] == devr[0] and host[1] == devr[1]
+
+
+def test_cc_triples_entry_matches_plan(api, oracle):
+    inp = S.generate(4, 19, 17)
+    ets, etd, v1 = api.cc_triples(inp.no, inp.nu, *inp.arrays())
+    ets_o, etd_o, v1_o = oracle.c_cc_triples(inp)
+    assert abs(etd - etd_o) <= tol(etd_o) and abs(ets - ets_o) <= tol(ets_o)
+    assert np.abs(v1 - v1_o).max() <= 1e-12
+
+
+def test_legacy_ijk_hooks(api, oracle):
+    """ijk_gpu_init/driver/finalize over the i>j>k tuples, packed slices as ddi_get returns them."""
+    no, nu = 5, 14
+    inp = S.generate(no, nu, 23)
+    hooks = api.IjkGpuHooks(no, nu, inp.eh, inp.ep, inp.t2, inp.vm, inp.voe)
+    e_ref = 0.0
+    v1_ref = np.zeros(nu * no)
+    for kind, i, j, k in oracle.all_tuples(no):
+        if kind != 0:
+            continue
+        cols = [api.packed_columns(inp.vvvo, no, nu, x) for x in (i, j, k)]
+        hooks.driver(i + 1, j + 1, k + 1, *cols)
+        e, v = oracle.c_tuple(inp, kind, i, j, k)
+        e_ref += e
+        v1_ref += v
+    etd = hooks.finalize()
+    assert abs(etd - e_ref) <= tol(e_ref)
+    assert np.abs(hooks.v1 - v1_ref).max() <= 1e-12
+
+
+def test_rejects_nonfinite_input(api):
+    from libcc_b200._native import CctError
+    inp = S.generate(4, 9, 1)
+    inp.t2[5] = np.nan
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        with pytest.raises(CctError) as e:
+            plan.set_system(inp)
+        assert e.value.status == 4
+
+
+def test_rejects_nonnegative_denominator(api):
+    from libcc_b200._native import CctError
+    inp = S.generate(4, 9, 1)
+    inp.ep[0] = -5.0
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        with pytest.raises(CctError) as e:
+            plan.set_system(inp)
+        assert e.value.status == 5
+
+
+def test_forward_before_inputs_is_state_error(api):
+    from libcc_b200._native import CctError
+    with api.TriplesPlan(4, 9) as plan:
+        with pytest.raises(CctError) as e:
+            plan.forward()
+        assert e.value.status == 6
+        with pytest.raises(CctError):
+            plan.forward(5, 2)
