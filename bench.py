@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""(T) benchmark: time to E(T) and TFLOP/s on B200.
+
+One step is one full (T) evaluation -- every tuple of the workload, including
+the degenerate (i,j,j)/(i,i,j) tuples -- through the library's plan API, with
+inputs already resident in HBM.  ``e2e`` repeats the step through the public C
+entry ``cc_triples_b200_`` from pinned host buffers (host->device upload,
+operand build, all tuples, v1/energy read-back).
+
+Under torchrun (N>1) the tuple list is split into cost-balanced contiguous
+shards, one per rank; the partial (ets, etd) are summed with one NCCL
+all-reduce, the only exchange step (the reference's ddi_gsumf).
+
+``--impl reference`` times the CPU stand-in for the reference's triples.x (the
+literal 12-DGEMM/trant3/DRT1WT3 restatement with OpenBLAS) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "(T) time & TFLOP/s: emulated vs native FP64 on 1 B200 at |ΔE(T)|≤1e-8 Eh"
+DEFAULT_WORKLOAD = "no24-nu320"
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_desc(inp, dist):
+    d = f"{inp.name} (no={inp.no}, nu={inp.nu}, seed {inp.seed}, "
+    d += "log-uniform |x| in [1e-6,1] integrals and T2 numerators)" if dist == "log" else "normal integrals)"
+    return d
+
+
+def shard_bounds(tuples_cost, nranks):
+    """Contiguous shards of the tuple list with near-equal summed cost."""
+    total = sum(tuples_cost)
+    bounds, acc, r = [0], 0.0, 1
+    for t, c in enumerate(tuples_cost):
+        acc += c
+        if r < nranks and acc >= total * r / nranks:
+            bounds.append(t + 1)
+            r += 1
+    while len(bounds) < nranks:
+        bounds.append(len(tuples_cost))
+    bounds.append(len(tuples_cost))
+    return bounds
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_bench_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(f[1]), smax=float(f[2]), power=float(f[3]), hw=f[5], hwt=f[6], swt=f[7],
+                                 swp=f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        pmax = max(r["power"] for r in rows)
+        loaded = [r for r in rows if r["power"] >= 0.5 * pmax] or rows
+        reasons = []
+        for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                          ("swp", "sw_power_cap")):
+            if any(r[key].lower().startswith("active") for r in loaded):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in loaded), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": reasons, "samples": len(loaded), "power_w_max": pmax}
+
+
+def read_traffic(workload: str):
+    """DRAM bytes per W-build launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / f"wbuild_f64_{workload}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def golden(workload: str):
+    f = ROOT / "tests" / "golden" / "energies.json"
+    if not f.exists():
+        return None
+    return json.loads(f.read_text()).get(workload)
+
+
+def cpu_sample(inp, budget_s: float = 12.0):
+    """Time the literal CPU restatement on i>j>k tuples of the workload until the
+    budget is spent (at least one tuple).  Returns (TFLOP/s, tuples, seconds, threads)."""
+    from oracle import oracle as O
+    tuples = [t for t in O.all_tuples(inp.no) if t[0] == 0]
+    flop_per = 12.0 * inp.nu ** 3 * (inp.no + inp.nu)
+    O.literal_cc_triples(inp, tuples=tuples[:1])  # page in, build caches
+    done, t0 = 0, time.perf_counter()
+    while done < len(tuples):
+        O.literal_cc_triples(inp, tuples=tuples[done:done + 1])
+        done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return flop_per * done / dt / 1e12, done, dt, O.cpu_threads()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from libcc_b200 import synthetic as S
+    from oracle import oracle as O
+    cfg = S.WORKLOADS[args.workload]
+    inp = S.workload(args.workload)
+    tuples = [t for t in O.all_tuples(inp.no) if t[0] == 0]
+    flop_per = 12.0 * inp.nu ** 3 * (inp.no + inp.nu)
+    per_step = 1
+    for w in range(args.warmup):
+        O.literal_cc_triples(inp, tuples=tuples[w % len(tuples):w % len(tuples) + per_step])
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        a = (args.warmup + s) % len(tuples)
+        O.literal_cc_triples(inp, tuples=tuples[a:a + per_step])
+    dt = time.perf_counter() - t0
+    tf = flop_per * per_step * args.steps / dt / 1e12
+    full_ms = S.flops(inp.no, inp.nu) / (tf * 1e12) * 1e3
+    sample = (f"{per_step} i>j>k tuple per step of {inp.name}; literal 12-DGEMM + trant3 + T3SQUA/ADT3DEN/DRT1WT3 "
+              f"restatement (oracle/oracle.py) with OpenBLAS DGEMM, {O.cpu_threads()} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": tf, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(inp, cfg["dist"]), "form": "cpu-literal-port"},
+            "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": O.cpu_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "ms_per_step extrapolates the sampled tuples/s to all tuples of the workload"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import datetime
+
+    import numpy as np
+    import torch
+
+    from libcc_b200 import api as A
+    from libcc_b200 import synthetic as S
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    cfg = S.WORKLOADS[args.workload]
+    inp = S.workload(args.workload)
+    no, nu = inp.no, inp.nu
+    # tuple list order (ccT_forward): C(no,3) i>j>k tuples, then no(no-1) degenerate ones at half cost
+    n_ijk_all = no * (no - 1) * (no - 2) // 6
+    costs = [1.0] * n_ijk_all + [0.5] * (no * (no - 1))
+    bounds = shard_bounds(costs, world)
+    begin, end = bounds[rank], bounds[rank + 1]
+    flop_step = S.flops(no, nu)
+
+    plan = A.TriplesPlan(no, nu, device=local)
+    dev_inputs = [torch.from_numpy(a).to(f"cuda:{local}") for a in inp.arrays()]
+    plan.set_inputs(*dev_inputs)
+    stream = torch.cuda.current_stream()
+    plan.set_stream(stream.cuda_stream)
+
+    def step():
+        ets, etd, _ = plan.forward(begin, end, want_v1=False)
+        if dist is not None:
+            t = torch.tensor([ets, etd], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t)
+            ets, etd = t.tolist()
+        return ets, etd
+
+    for _ in range(args.warmup):
+        step()
+
+    plan.set_profiling(True)
+    launches = 0
+    wb_ms, wb_n = 0.0, 0
+    with ClockSampler(local) as clocks:
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ets, etd = step()
+            launches += plan.last_forward_launches
+            prof = plan.kernel_profile()
+            wb_ms += prof["wbuild"][0]
+            wb_n += prof["wbuild"][1]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+    plan.set_profiling(False)
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+    ms_step = ms / args.steps
+    tflops = flop_step / (ms_step * 1e-3) / 1e12
+
+    # roofline of the dominant kernel (W-build GEMM), from the timed region's launches
+    n_ijk = no * (no - 1) * (no - 2) // 6
+    my_flop_wb = sum(12.0 * nu ** 3 * (no + nu) * c for c in costs[begin:end]) * args.steps
+    wb_achieved = my_flop_wb / (wb_ms * 1e-3) / 1e12 if wb_ms > 0 else None
+    peak = plan_peak = A.N.load().ccT_measure_fp64_peak(local)
+    traffic = read_traffic(args.workload)
+    roofline = {"bound": "tensor", "kernel": "wbuild_f64_kernel (mma.sync m16n8k4 f64)",
+                "achieved": wb_achieved, "peak": plan_peak, "unit": "TFLOP/s",
+                "frac": (wb_achieved / peak) if (wb_achieved and peak) else None, "traffic": traffic,
+                "peak_source": "measured in this run: mma.sync f64 throughput microbenchmark "
+                               "(ccT_measure_fp64_peak); MEASURED_PEAKS.json has no FP64 entry",
+                "launches": wb_n, "avg_launch_ms": wb_ms / max(wb_n, 1),
+                "flop_per_launch": f"12 nu^3 (no+nu) = {12.0 * nu ** 3 * (no + nu):.4g} for an i>j>k tuple, half "
+                                   "for a degenerate tuple",
+                "share_of_step": wb_ms / ms if ms > 0 else None}
+
+    # accuracy against the oracle fixture
+    acc = None
+    g = golden(args.workload)
+    if g is not None:
+        acc = {"e_t": ets + etd, "oracle_e_t": g["e_t"], "abs_err": abs(ets + etd - g["e_t"]),
+               "rel_err": abs(ets + etd - g["e_t"]) / abs(g["e_t"])}
+
+    # end to end through the C entry, pinned host inputs
+    e2e = None
+    if not args.no_e2e:
+        pinned = []
+        for a in inp.arrays():
+            t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = a
+            pinned.append(t.numpy())
+        h2d = sum(a.nbytes for a in pinned)
+        d2h = nu * no * 8 + 2 * 8
+        plan.close()
+        del dev_inputs
+        torch.cuda.empty_cache()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if world == 1:
+            r = A.cc_triples(no, nu, *pinned)
+            e2e_e = r[0] + r[1]
+        else:
+            with A.TriplesPlan(no, nu, device=local) as p2:
+                p2.set_inputs(*pinned)
+                r = p2.forward(begin, end)
+            t = torch.tensor([r[0], r[1]], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t)
+            e2e_e = float(t.sum())
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = t.item()
+        e2e = {"value": flop_step / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "steps": 1,
+               "path": "cc_triples_b200_ (C ABI) from pinned host buffers" if world == 1 else
+               "ccT_plan_create/ccT_set_inputs(host)/ccT_forward(shard) + NCCL all-reduce",
+               "e_t": e2e_e}
+    else:
+        plan.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        tf_cpu, ntup, sec, thr = cpu_sample(inp)
+        cpu = {"value": tf_cpu, "unit": "TFLOP/s", "cores": thr, "kind": "port",
+               "sample": f"{ntup} i>j>k tuples of {inp.name} in {sec:.1f} s; literal 12-DGEMM + trant3 + "
+                         "T3SQUA/ADT3DEN/DRT1WT3 restatement with OpenBLAS DGEMM"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": tflops, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, libcc_b200/synthetic.py)",
+                "config": {"workload": workload_desc(inp, cfg["dist"]), "form": "fp64 (mma.sync f64)",
+                           "tuples": len(costs), "tuples_ijk": n_ijk, "flop_per_step": flop_step,
+                           "tuples_per_s": len(costs) / (ms_step * 1e-3),
+                           "l2": "inputs larger than L2 (E operand "
+                                 f"{no * nu * nu * (nu + no) * 8 / 1e9:.1f} GB re-streamed per tuple)",
+                           "parallelism": f"tuple shards x{world}" if world > 1 else "1 GPU"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks.summary(), "energies": {"ets": ets, "etd": etd, "e_t": ets + etd},
+                "accuracy_vs_oracle": acc}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

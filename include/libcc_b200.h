@@ -81,6 +81,25 @@ int64_t ccT_num_tuples(int64_t no);
  * ets/etd/v1 sum linearly with the other shards. */
 int ccT_forward(ccT_plan *plan, int64_t begin, int64_t end, double *ets, double *etd, double *v1_out);
 
+/* Launch the plan's kernels on a caller-provided CUDA stream (a cudaStream_t
+ * passed as void*); NULL restores the plan's own stream. */
+int ccT_set_stream(ccT_plan *plan, void *cuda_stream);
+
+/* Time `reps` back-to-back launches of the W-build contraction of one tuple
+ * with CUDA events on the plan's stream; *ms_per_launch gets the mean. */
+int ccT_time_wbuild(ccT_plan *plan, int64_t tuple, int32_t reps, double *ms_per_launch);
+
+/* Per-kernel timing of later ccT_forward calls: on != 0 records a CUDA event
+ * pair around every launch of each kernel class on the plan's stream. */
+int ccT_set_profiling(ccT_plan *plan, int32_t on);
+
+/* Kernel classes for ccT_last_kernel_ms. */
+enum { CCT_KERNEL_WBUILD = 0, CCT_KERNEL_REDUCE = 1 };
+
+/* Summed device milliseconds and launch count of one kernel class in the last
+ * profiled ccT_forward. */
+int ccT_last_kernel_ms(const ccT_plan *plan, int32_t kernel_class, double *total_ms, int64_t *launches);
+
 /* Milliseconds of device time the last ccT_forward spent, measured by CUDA
  * events around its kernels (excludes input upload). */
 double ccT_last_forward_ms(const ccT_plan *plan);

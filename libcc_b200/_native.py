@@ -21,7 +21,7 @@ CCT_MEM_HOST, CCT_MEM_DEVICE = 0, 1
 # every symbol include/libcc_b200.h declares
 EXPORTS = [
     "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
-    "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
+    "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
     "ccT_last_error", "ccT_measure_fp64_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
     "cc_triples_b200_",
 ]
@@ -67,6 +67,14 @@ def load():
     lib.ccT_num_tuples.restype = i64
     lib.ccT_forward.argtypes = [vp, i64, i64, dp, dp, vp]
     lib.ccT_forward.restype = ctypes.c_int
+    lib.ccT_set_stream.argtypes = [vp, vp]
+    lib.ccT_set_stream.restype = ctypes.c_int
+    lib.ccT_time_wbuild.argtypes = [vp, i64, i32, dp]
+    lib.ccT_time_wbuild.restype = ctypes.c_int
+    lib.ccT_set_profiling.argtypes = [vp, i32]
+    lib.ccT_set_profiling.restype = ctypes.c_int
+    lib.ccT_last_kernel_ms.argtypes = [vp, i32, dp, i64p]
+    lib.ccT_last_kernel_ms.restype = ctypes.c_int
     lib.ccT_last_forward_ms.argtypes = [vp]
     lib.ccT_last_forward_ms.restype = ctypes.c_double
     lib.ccT_last_forward_launches.argtypes = [vp]

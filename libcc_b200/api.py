@@ -110,6 +110,17 @@ class TriplesPlan:
         N.check(N.load().ccT_forward(self._h, begin, end, ctypes.byref(ets), ctypes.byref(etd), vptr), "ccT_forward")
         return ets.value, etd.value, v1
 
+    def set_stream(self, stream_handle: int | None):
+        """Run on a caller's CUDA stream (an integer cudaStream_t, e.g.
+        ``torch.cuda.current_stream().cuda_stream``); None restores the plan's own."""
+        N.check(N.load().ccT_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)), "ccT_set_stream")
+
+    def time_wbuild(self, tuple_index: int = 0, reps: int = 3) -> float:
+        """Mean milliseconds of one W-build launch of the given tuple (CUDA events)."""
+        ms = ctypes.c_double()
+        N.check(N.load().ccT_time_wbuild(self._h, tuple_index, reps, ctypes.byref(ms)), "ccT_time_wbuild")
+        return ms.value
+
     @property
     def last_forward_ms(self) -> float:
         return float(N.load().ccT_last_forward_ms(self._h))
@@ -168,3 +179,21 @@ class IjkGpuHooks:
         c = lambda v: ctypes.byref(ctypes.c_int64(v))
         N.load().ijk_gpu_finalize_(c(self.no), c(self.nu), ctypes.byref(self.etd))
         return self.etd.value
+
+
+def _kernel_profile(plan: TriplesPlan):
+    """{class: (total_ms, launches)} of the last profiled forward."""
+    out = {}
+    for cls, name in ((0, "wbuild"), (1, "reduce")):
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        N.check(N.load().ccT_last_kernel_ms(plan._h, cls, ctypes.byref(ms), ctypes.byref(n)), "ccT_last_kernel_ms")
+        out[name] = (ms.value, n.value)
+    return out
+
+
+def _set_profiling(plan: TriplesPlan, on: bool):
+    N.check(N.load().ccT_set_profiling(plan._h, 1 if on else 0), "ccT_set_profiling")
+
+
+TriplesPlan.kernel_profile = _kernel_profile
+TriplesPlan.set_profiling = _set_profiling

@@ -31,10 +31,23 @@ const char *last_error();
   } while (0)
 
 // ----------------------------------------------------------------------------- tiling
-// W-build GEMM tile (FP64 DMMA kernel).  K is padded to KB, the single-index
-// dimension N to BN.
+// W-build GEMM tile (FP64 DMMA kernel).  K is padded to KB; the single-index
+// dimension N is tiled by BN, one of kBNChoices, picked per system to minimise
+// the padding of nu (choose_bn).
 constexpr int kKB = 16;
-constexpr int kBN = 64;
+constexpr int kBNChoices[] = {64, 56, 48, 40, 32};
+inline int choose_bn(int64_t nu) {
+  int best = 64;
+  int64_t best_np = (nu + 63) / 64 * 64;
+  for (int bn : kBNChoices) {
+    const int64_t np = (nu + bn - 1) / bn * bn;
+    if (np < best_np) {
+      best = bn;
+      best_np = np;
+    }
+  }
+  return best;
+}
 // Reduction block edge (elements of a, b, c per block).
 constexpr int kRB = 8;
 
@@ -66,7 +79,8 @@ struct GemmJob {
 struct Dims {
   int no, nu;
   int64_t KP;   // padded contraction length of one half: round_up(nu+no, kKB)
-  int64_t NP;   // padded single-index length: round_up(nu, kBN)
+  int BN;       // N tile of the W-build GEMM (choose_bn)
+  int64_t NP;   // padded single-index length: round_up(nu, BN)
   int nb;       // reduction blocks per index: ceil(nu / kRB)
   int64_t ncta; // canonical block triples: nb(nb+1)(nb+2)/6
 };

@@ -43,7 +43,8 @@ struct ccT_plan {
   int device = 0;
   ccT_options opt{};
   Dims d{};
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream the kernels run on
+  cudaStream_t own_stream = nullptr;  // the plan's own stream
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // inputs (device copies, reference layouts)
   double *eh = nullptr, *ep = nullptr, *t1 = nullptr, *t2 = nullptr, *vm = nullptr, *voe = nullptr;
@@ -62,6 +63,12 @@ struct ccT_plan {
   float last_ms = 0.f;
   int64_t last_launches = 0;
   std::vector<double> host_eh, host_ep;
+  // opt-in per-kernel profiling: event pairs per launch, grouped by kernel class
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;
+  std::vector<int> prof_class;  // class of each recorded pair
+  double kernel_ms[2] = {0.0, 0.0};
+  int64_t kernel_launches[2] = {0, 0};
 };
 
 namespace {
@@ -135,10 +142,50 @@ int check_denominators(ccT_plan *p) {
   return CCT_OK;
 }
 
+// Records one event of a profiled launch pair: cls >= 0 opens pair number
+// prof_class.size() (event 2q), cls < 0 closes the last opened pair (event 2q+1).
+int prof_mark(ccT_plan *p, int cls) {
+  if (!p->profiling) return CCT_OK;
+  size_t n;
+  if (cls >= 0) {
+    n = p->prof_class.size() * 2;
+  } else {
+    if (p->prof_class.empty()) {
+      set_error("profiling: close without open");
+      return CCT_ERR_STATE;
+    }
+    n = p->prof_class.size() * 2 - 1;
+  }
+  while (p->prof_events.size() <= n) {
+    cudaEvent_t e;
+    CCT_CUDA(cudaEventCreate(&e));
+    p->prof_events.push_back(e);
+  }
+  CCT_CUDA(cudaEventRecord(p->prof_events[n], p->stream));
+  if (cls >= 0) p->prof_class.push_back(cls);
+  return CCT_OK;
+}
+
+int prof_collect(ccT_plan *p) {
+  p->kernel_ms[0] = p->kernel_ms[1] = 0.0;
+  p->kernel_launches[0] = p->kernel_launches[1] = 0;
+  if (!p->profiling) return CCT_OK;
+  for (size_t q = 0; q < p->prof_class.size(); q++) {
+    float ms = 0.f;
+    CCT_CUDA(cudaEventElapsedTime(&ms, p->prof_events[2 * q], p->prof_events[2 * q + 1]));
+    p->kernel_ms[p->prof_class[q]] += ms;
+    p->kernel_launches[p->prof_class[q]] += 1;
+  }
+  p->prof_class.clear();
+  return CCT_OK;
+}
+
 int run_tuple(ccT_plan *p, int64_t tix) {
   const Tuple &t = p->tuples[tix];
   const int njobs = t.kind == kIJK ? 3 : 2;
+  CCT_TRY(prof_mark(p, CCT_KERNEL_WBUILD));
   CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tix, njobs, p->stream));
+  CCT_TRY(prof_mark(p, -1));
   TupleDev td;
   td.x[0] = p->X[0];
   td.x[1] = p->X[1];
@@ -148,8 +195,10 @@ int run_tuple(ccT_plan *p, int64_t tix) {
   td.j = t.j;
   td.k = t.k;
   td.weight = t.kind == kIJK ? 1.0 : 0.5;
+  CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE));
   CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->stream));
   CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->stream));
+  CCT_TRY(prof_mark(p, -1));
   p->last_launches += 3;
   return CCT_OK;
 }
@@ -234,7 +283,8 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   d.no = (int)no;
   d.nu = (int)nu;
   d.KP = round_up(nu + no, kKB);
-  d.NP = round_up(nu, kBN);
+  d.BN = choose_bn(nu);
+  d.NP = round_up(nu, d.BN);
   d.nb = (int)((nu + kRB - 1) / kRB);
   d.ncta = (int64_t)d.nb * (d.nb + 1) * (d.nb + 2) / 6;
   p->tuples = tuple_list((int)no);
@@ -243,7 +293,8 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     return s;
   };
   int s;
-  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  p->stream = p->own_stream;
   if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) return fail(CCT_ERR_CUDA);
   const int64_t nu2 = nu * nu;
   if ((s = dalloc(&p->eh, no)) || (s = dalloc(&p->ep, nu)) || (s = dalloc(&p->t1, no * nu)) ||
@@ -365,12 +416,70 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
     CCT_CUDA(cudaMemcpyAsync(v1_out, v1_acc(p), (int64_t)d.nu * d.no * 8, cudaMemcpyDeviceToHost, p->stream));
   CCT_CUDA(cudaStreamSynchronize(p->stream));
   CCT_CUDA(cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1));
+  CCT_TRY(prof_collect(p));
   if (ets) *ets = out3[0];
   if (etd) *etd = out3[1];
   if (!std::isfinite(out3[0]) || !std::isfinite(out3[1])) {
     set_error("E(T) is not finite");
     return CCT_ERR_NONFINITE;
   }
+  return CCT_OK;
+}
+
+int ccT_set_stream(ccT_plan *p, void *cuda_stream) {
+  if (!p) {
+    set_error("plan is NULL");
+    return CCT_ERR_INVALID;
+  }
+  DeviceGuard guard(p->device);
+  CCT_CUDA(cudaStreamSynchronize(p->stream));
+  p->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : p->own_stream;
+  return CCT_OK;
+}
+
+int ccT_time_wbuild(ccT_plan *p, int64_t tuple, int32_t reps, double *ms_per_launch) {
+  if (!p || !ms_per_launch || reps < 1) {
+    set_error("need a plan, an output pointer and reps >= 1");
+    return CCT_ERR_INVALID;
+  }
+  if (!p->inputs_ready) {
+    set_error("ccT_time_wbuild before ccT_set_inputs");
+    return CCT_ERR_STATE;
+  }
+  if (tuple < 0 || tuple >= (int64_t)p->tuples.size()) {
+    set_error("tuple index out of range");
+    return CCT_ERR_INVALID;
+  }
+  DeviceGuard guard(p->device);
+  const int njobs = p->tuples[tuple].kind == kIJK ? 3 : 2;
+  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->stream));  // warm
+  CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
+  for (int r = 0; r < reps; r++) CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->stream));
+  CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
+  CCT_CUDA(cudaEventSynchronize(p->ev1));
+  float ms = 0.f;
+  CCT_CUDA(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
+  *ms_per_launch = ms / reps;
+  return CCT_OK;
+}
+
+int ccT_set_profiling(ccT_plan *p, int32_t on) {
+  if (!p) {
+    set_error("plan is NULL");
+    return CCT_ERR_INVALID;
+  }
+  p->profiling = on != 0;
+  p->prof_class.clear();
+  return CCT_OK;
+}
+
+int ccT_last_kernel_ms(const ccT_plan *p, int32_t cls, double *total_ms, int64_t *launches) {
+  if (!p || cls < 0 || cls > 1) {
+    set_error("need a plan and kernel class 0 or 1");
+    return CCT_ERR_INVALID;
+  }
+  if (total_ms) *total_ms = p->kernel_ms[cls];
+  if (launches) *launches = p->kernel_launches[cls];
   return CCT_OK;
 }
 
@@ -390,7 +499,8 @@ int ccT_plan_destroy(ccT_plan *p) {
   if (p->flags) cudaFree(p->flags);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
-  if (p->stream) cudaStreamDestroy(p->stream);
+  for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
+  if (p->own_stream) cudaStreamDestroy(p->own_stream);
   delete p;
   return CCT_OK;
 }

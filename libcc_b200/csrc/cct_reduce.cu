@@ -29,146 +29,172 @@ __device__ __forceinline__ int soff(int l0, int l1, int l2) { return l0 + 9 * l1
 // the six permutations of three positions, in a fixed order
 __constant__ int c_perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
 
+// W assembly per tuple kind: W(x0,x1,x2) += X_g(x_al0, x_al1, x_al2); {g, al0, al1, al2}
+//   i>j>k : X0(a,b,c) + X1(a,c,b) + X2(b,c,a)
+//   (i,j,j): X0(a,b,c) + X0(a,c,b) + X1(b,c,a) + X1(c,b,a)
+//   (i,i,k): X0(a,b,c) + X0(b,a,c) + X1(a,c,b) + X1(b,c,a)
+__constant__ int c_terms[3][4][4] = {
+    {{0, 0, 1, 2}, {1, 0, 2, 1}, {2, 1, 2, 0}, {0, 0, 0, 0}},
+    {{0, 0, 1, 2}, {0, 0, 2, 1}, {1, 1, 2, 0}, {1, 2, 1, 0}},
+    {{0, 0, 1, 2}, {0, 1, 0, 2}, {1, 0, 2, 1}, {1, 1, 2, 0}}};
+
 __device__ __forceinline__ int perm_index(int p0, int p1) {
   // index of the permutation whose first two entries are (p0, p1)
   return p0 * 2 + ((p1 > p0 ? p1 - 1 : p1));
 }
 
+constexpr int VSL = 6 * 64;  // staged VOE values per slot: 6 planes x 64 (b,c) pairs
+
 __global__ void __launch_bounds__(RT) reduce_kernel(int nu, int no, int64_t NP, TupleDev t,
                                                    const double *__restrict__ eh, const double *__restrict__ ep,
                                                    const double *__restrict__ voe, const int16_t *__restrict__ table,
                                                    double *__restrict__ xpart, double *__restrict__ vpart) {
-  __shared__ double Wsm[6 * SL];
+  extern __shared__ __align__(16) double dyn_smem[];  // REDUCE_SMEM bytes
+  double *Wsm = dyn_smem;                             // [6][SL]
+  double *Vsm = dyn_smem + 6 * SL;                    // [6][VSL]
   __shared__ double vloc[3][RB][3];
-  __shared__ double red[RT];
-  __shared__ int slot_of[6];      // perm sigma -> slot holding block O_sigma
-  __shared__ int pos_of[3];       // position m -> first position with the same block
+  __shared__ double red[RT / 32];
+  __shared__ int slot_of[6];  // perm sigma -> slot holding block O_sigma
+  __shared__ int pos_of[3];   // position m -> first position with the same block
 
   const int tid = threadIdx.x;
   const int64_t cta = blockIdx.x;
   const int S[3] = {table[3 * cta], table[3 * cta + 1], table[3 * cta + 2]};
+  // slots are uniform across the CTA: compute them in registers everywhere
+  int slot[6];
+#pragma unroll
+  for (int sg = 0; sg < 6; sg++) {
+    slot[sg] = sg;
+#pragma unroll
+    for (int s2 = 0; s2 < 6; s2++) {
+      if (s2 < sg && slot[sg] == sg && S[c_perm[s2][0]] == S[c_perm[sg][0]] && S[c_perm[s2][1]] == S[c_perm[sg][1]] &&
+          S[c_perm[s2][2]] == S[c_perm[sg][2]])
+        slot[sg] = s2;
+    }
+  }
+  if (tid < 6) slot_of[tid] = slot[tid];
+  if (tid < 3) pos_of[tid] = (S[0] == S[tid]) ? 0 : ((S[1] == S[tid]) ? 1 : 2);
+  if (tid < 3 * RB * 3) (&vloc[0][0][0])[tid] = 0.0;
 
-  if (tid < 6) {
-    const int *sg = c_perm[tid];
-    int slot = tid;
-    for (int s2 = 0; s2 < tid; s2++) {
-      const int *o = c_perm[s2];
-      if (S[o[0]] == S[sg[0]] && S[o[1]] == S[sg[1]] && S[o[2]] == S[sg[2]]) {
-        slot = s2;
-        break;
+  const int nterm = t.kind == kIJK ? 3 : 4;
+  const int64_t nu2 = (int64_t)nu * nu;
+  const double *planes[6] = {
+      voe + ((int64_t)t.k * no + t.j) * nu2, voe + ((int64_t)t.j * no + t.k) * nu2,   // jk, kj
+      voe + ((int64_t)t.k * no + t.i) * nu2, voe + ((int64_t)t.i * no + t.k) * nu2,   // ik, ki
+      voe + ((int64_t)t.j * no + t.i) * nu2, voe + ((int64_t)t.i * no + t.j) * nu2};  // ij, ji
+
+  // ---- phase 1: issue every global load of this CTA (X terms, staged VOE)
+  double xv[6][4][2];
+  double vv[6][2];
+#pragma unroll
+  for (int sg = 0; sg < 6; sg++) {
+    const bool live = slot[sg] == sg;
+    const int O[3] = {S[c_perm[sg][0]], S[c_perm[sg][1]], S[c_perm[sg][2]]};
+#pragma unroll
+    for (int term = 0; term < 4; term++) {
+      const int *tm = c_terms[t.kind][term];
+      const double *X = t.x[tm[0]];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int idx = tid + RT * e;
+        const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;  // u2: X's contiguous index
+        const int xp = RB * O[tm[1]] + u0, xq = RB * O[tm[2]] + u1, xs = RB * O[tm[3]] + u2;
+        double v = 0.0;
+        if (live && term < nterm && xp < nu && xq < nu && xs < nu) v = X[((int64_t)xp * nu + xq) * NP + xs];
+        xv[sg][term][e] = v;
       }
     }
-    slot_of[tid] = slot;
-  }
-  if (tid < 3) {
-    int p = tid;
-    for (int m = 0; m < tid; m++)
-      if (S[m] == S[tid]) {
-        p = m;
-        break;
-      }
-    pos_of[tid] = p;
-  }
-  if (tid < 3 * RB * 3) (&vloc[0][0][0])[tid] = 0.0;
-  __syncthreads();
-
-  // ---- assemble W on each distinct ordered block of the orbit
-  // terms: W(x0,x1,x2) += X_g(x_al0, x_al1, x_al2)
-  int nterm;
-  int tg[4], tal[4][3];
-  if (t.kind == kIJK) {  // X0(a,b,c) + X1(a,c,b) + X2(b,c,a)
-    nterm = 3;
-    tg[0] = 0; tal[0][0] = 0; tal[0][1] = 1; tal[0][2] = 2;
-    tg[1] = 1; tal[1][0] = 0; tal[1][1] = 2; tal[1][2] = 1;
-    tg[2] = 2; tal[2][0] = 1; tal[2][1] = 2; tal[2][2] = 0;
-  } else if (t.kind == kIJJ) {  // X0(a,b,c) + X0(a,c,b) + X1(b,c,a) + X1(c,b,a)
-    nterm = 4;
-    tg[0] = 0; tal[0][0] = 0; tal[0][1] = 1; tal[0][2] = 2;
-    tg[1] = 0; tal[1][0] = 0; tal[1][1] = 2; tal[1][2] = 1;
-    tg[2] = 1; tal[2][0] = 1; tal[2][1] = 2; tal[2][2] = 0;
-    tg[3] = 1; tal[3][0] = 2; tal[3][1] = 1; tal[3][2] = 0;
-  } else {  // kIIJ: X0(a,b,c) + X0(b,a,c) + X1(a,c,b) + X1(b,c,a)
-    nterm = 4;
-    tg[0] = 0; tal[0][0] = 0; tal[0][1] = 1; tal[0][2] = 2;
-    tg[1] = 0; tal[1][0] = 1; tal[1][1] = 0; tal[1][2] = 2;
-    tg[2] = 1; tal[2][0] = 0; tal[2][1] = 2; tal[2][2] = 1;
-    tg[3] = 1; tal[3][0] = 1; tal[3][1] = 2; tal[3][2] = 0;
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int q = tid + RT * e;  // < 512; only q < VSL used
+      const int plane = q >> 6, pair = q & 63;
+      const int b = RB * O[1] + (pair & 7), c = RB * O[2] + (pair >> 3);
+      double v = 0.0;
+      if (live && q < VSL && b < nu && c < nu) v = planes[plane][b + (int64_t)nu * c];
+      vv[sg][e] = v;
+    }
   }
 
-  for (int sg = 0; sg < 6; sg++) {
-    if (slot_of[sg] != sg) continue;
-    const int O[3] = {S[c_perm[sg][0]], S[c_perm[sg][1]], S[c_perm[sg][2]]};
-    double *wb = Wsm + sg * SL;
-    for (int term = 0; term < nterm; term++) {
-      const double *X = t.x[tg[term]];
-      const int *al = tal[term];
-      for (int idx = tid; idx < RB * RB * RB; idx += RT) {
-        // u2 fastest: the X index that is contiguous in memory (s)
-        const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
-        int l[3];
-        l[al[0]] = u0;
-        l[al[1]] = u1;
-        l[al[2]] = u2;
-        const int xp = RB * O[al[0]] + u0, xq = RB * O[al[1]] + u1, xs = RB * O[al[2]] + u2;
-        double v = 0.0;
-        if (xp < nu && xq < nu && xs < nu) v = X[((int64_t)xp * nu + xq) * NP + xs];
-        const int so = soff(l[0], l[1], l[2]);
-        if (term == 0)
-          wb[so] = v;
-        else
-          wb[so] += v;
+  // ---- phase 2: assemble W in shared memory, one term at a time (fixed order)
+#pragma unroll
+  for (int term = 0; term < 4; term++) {
+    if (term < nterm) {
+#pragma unroll
+      for (int sg = 0; sg < 6; sg++) {
+        if (slot[sg] != sg) continue;
+        const int *tm = c_terms[t.kind][term];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int idx = tid + RT * e;
+          const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
+          int l[3];
+          l[tm[1]] = u0;
+          l[tm[2]] = u1;
+          l[tm[3]] = u2;
+          double *w = Wsm + sg * SL + soff(l[0], l[1], l[2]);
+          if (term == 0)
+            *w = xv[sg][term][e];
+          else
+            *w += xv[sg][term][e];
+        }
       }
       __syncthreads();
     }
-    // W_aaa = 0 (ZEROT3)
-    if (O[0] == O[1] && O[1] == O[2] && tid < RB) wb[soff(tid, tid, tid)] = 0.0;
   }
+#pragma unroll
+  for (int sg = 0; sg < 6; sg++) {
+    if (slot[sg] != sg) continue;
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int q = tid + RT * e;
+      if (q < VSL) Vsm[sg * VSL + q] = vv[sg][e];
+    }
+  }
+  // W_aaa = 0 (ZEROT3): only the all-equal block triple holds diagonal elements
+  if (S[0] == S[1] && S[1] == S[2] && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;
   __syncthreads();
 
-  // ---- energy and v1 contributions
+  // ---- phase 3: energy and v1 contributions, all from shared memory
   const int warp = tid >> 5, lane = tid & 31;
   const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
-  const int64_t nu2 = (int64_t)nu * nu;
-  const double *voe_jk = voe + ((int64_t)t.k * no + t.j) * nu2, *voe_kj = voe + ((int64_t)t.j * no + t.k) * nu2;
-  const double *voe_ik = voe + ((int64_t)t.k * no + t.i) * nu2, *voe_ki = voe + ((int64_t)t.i * no + t.k) * nu2;
-  const double *voe_ij = voe + ((int64_t)t.j * no + t.i) * nu2, *voe_ji = voe + ((int64_t)t.i * no + t.j) * nu2;
   double x3 = 0.0;
-
   for (int sg = 0; sg < 6; sg++) {
     if (slot_of[sg] != sg) continue;
     const int *sp = c_perm[sg];
     const int O[3] = {S[sp[0]], S[sp[1]], S[sp[2]]};
     const int l0 = warp;
     const int a = RB * O[0] + l0;
+    const double epa = a < nu ? ep[a] : 0.0;
     double ci = 0.0, cj = 0.0, ck = 0.0;
+#pragma unroll
     for (int h = 0; h < 2; h++) {
       const int pi = lane + 32 * h;
       const int l1 = pi & 7, l2 = pi >> 3;
       const int b = RB * O[1] + l1, c = RB * O[2] + l2;
-      if (a >= nu || b >= nu || c >= nu) continue;
-      const int lc[3] = {l0, l1, l2};
-      double w[6];
+      if (a < nu && b < nu && c < nu) {
+        const int lc[3] = {l0, l1, l2};
+        double w[6];
 #pragma unroll
-      for (int pp = 0; pp < 6; pp++) {
-        const int *pi3 = c_perm[pp];
-        // block of the permuted element: O_{sigma o pi}
-        const int comp = perm_index(sp[pi3[0]], sp[pi3[1]]);
-        w[pp] = Wsm[slot_of[comp] * SL + soff(lc[pi3[0]], lc[pi3[1]], lc[pi3[2]])];
+        for (int pp = 0; pp < 6; pp++) {
+          const int *pi3 = c_perm[pp];
+          const int comp = perm_index(sp[pi3[0]], sp[pi3[1]]);  // block of the permuted element
+          w[pp] = Wsm[slot_of[comp] * SL + soff(lc[pi3[0]], lc[pi3[1]], lc[pi3[2]])];
+        }
+        // w[0]=abc w[1]=acb w[2]=bac w[3]=bca w[4]=cab w[5]=cba
+        const double wabc = w[0], wacb = w[1], wbac = w[2], wbca = w[3], wcab = w[4], wcba = w[5];
+        const double dinv = 1.0 / (dijk - (epa + ep[b] + ep[c]));
+        x3 += wabc * (8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab)) * dinv;
+        const double z1 = (wabc - wbac) * 2.0 - wacb + wbca;
+        const double z2 = (wacb - wbca) * 2.0 - wabc + wbac;
+        const double z3 = (wbac - wabc) * 2.0 - wcab + wcba;
+        const double z4 = (wbca - wacb) * 2.0 - wcba + wcab;
+        const double z5 = (wcab - wcba) * 2.0 - wbac + wabc;
+        const double z6 = (wcba - wcab) * 2.0 - wbca + wacb;
+        const double *vs = Vsm + sg * VSL + pi;
+        ci += (z1 * vs[0] + z2 * vs[64]) * dinv;
+        cj += (z3 * vs[128] + z5 * vs[192]) * dinv;
+        ck += (z4 * vs[256] + z6 * vs[320]) * dinv;
       }
-      // w[0]=abc w[1]=acb w[2]=bac w[3]=bca w[4]=cab w[5]=cba
-      const double wabc = w[0], wacb = w[1], wbac = w[2], wbca = w[3], wcab = w[4], wcba = w[5];
-      const double dinv = 1.0 / (dijk - (ep[a] + ep[b] + ep[c]));
-      x3 += wabc * (8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab)) * dinv;
-      const double z1 = (wabc - wbac) * 2.0 - wacb + wbca;
-      const double z2 = (wacb - wbca) * 2.0 - wabc + wbac;
-      const double z3 = (wbac - wabc) * 2.0 - wcab + wcba;
-      const double z4 = (wbca - wacb) * 2.0 - wcba + wcab;
-      const double z5 = (wcab - wcba) * 2.0 - wbac + wabc;
-      const double z6 = (wcba - wcab) * 2.0 - wbca + wacb;
-      const int64_t bc = b + (int64_t)nu * c;
-      ci += (z1 * voe_jk[bc] + z2 * voe_kj[bc]) * dinv;
-      cj += (z3 * voe_ik[bc] + z5 * voe_ki[bc]) * dinv;
-      ck += (z4 * voe_ij[bc] + z6 * voe_ji[bc]) * dinv;
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -184,22 +210,27 @@ __global__ void __launch_bounds__(RT) reduce_kernel(int nu, int no, int64_t NP, 
     }
   }
 
-  // ---- CTA partials (fixed-order tree for x3)
-  red[tid] = x3;
+  // ---- CTA partials: warp trees then a fixed-order sum of the 8 warp values
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) x3 += __shfl_down_sync(0xffffffffu, x3, off);
+  if (lane == 0) red[warp] = x3;
   __syncthreads();
-  for (int s = RT / 2; s > 0; s >>= 1) {
-    if (tid < s) red[tid] += red[tid + s];
-    __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int w = 0; w < RT / 32; w++) s += red[w];
+    xpart[cta] = s;
   }
-  if (tid == 0) xpart[cta] = red[0];
   if (tid < 3 * RB * 3) vpart[cta * 72 + tid] = (&vloc[0][0][0])[tid];
 }
 
 // etd_acc[0..1]: Neumaier (sum, compensation); v1_acc(nu, no).
+// Block 0 sums the per-CTA x3 partials; every other warp owns one virtual
+// index a and sums its v1 partials over all block triples containing a.
 __global__ void finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t, const double *__restrict__ xpart,
                                 const double *__restrict__ vpart, double *__restrict__ etd_acc,
                                 double *__restrict__ v1_acc) {
   const int tid = threadIdx.x;
+  const int lane = tid & 31;
   if (blockIdx.x == 0) {
     __shared__ double red[256];
     double s = 0.0;
@@ -220,12 +251,14 @@ __global__ void finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t, const 
     }
     return;
   }
-  const int a = (blockIdx.x - 1) * blockDim.x + tid;
+  const int a = ((blockIdx.x - 1) * blockDim.x + tid) >> 5;
   if (a >= nu) return;
   const int X = a / RB, la = a - (a / RB) * RB;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  int q = 0;
   for (int Y = 0; Y < nb; Y++) {
-    for (int Z = Y; Z < nb; Z++) {
+    for (int Z = Y; Z < nb; Z++, q++) {
+      if ((q & 31) != lane) continue;
       int A, B, C;
       if (X <= Y) {
         A = X; B = Y; C = Z;
@@ -242,9 +275,17 @@ __global__ void finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t, const 
       s2 += vp[2];
     }
   }
-  v1_acc[a + (int64_t)nu * t.i] += t.weight * s0;
-  v1_acc[a + (int64_t)nu * t.j] += t.weight * s1;
-  v1_acc[a + (int64_t)nu * t.k] += t.weight * s2;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    s0 += __shfl_down_sync(0xffffffffu, s0, off);
+    s1 += __shfl_down_sync(0xffffffffu, s1, off);
+    s2 += __shfl_down_sync(0xffffffffu, s2, off);
+  }
+  if (lane == 0) {
+    v1_acc[a + (int64_t)nu * t.i] += t.weight * s0;
+    v1_acc[a + (int64_t)nu * t.j] += t.weight * s1;
+    v1_acc[a + (int64_t)nu * t.k] += t.weight * s2;
+  }
 }
 
 // out3 = {ets, etd, ets+etd}; ets = 2 sum_{i,a} t1(i,a) v1(a,i) (triples.F90:311-316)
@@ -277,14 +318,22 @@ __global__ void ets_kernel(int no, int nu, const double *__restrict__ t1, const 
 
 int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
                   const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
-  reduce_kernel<<<(unsigned)d.ncta, RT, 0, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart, vpart);
+  constexpr int smem = (6 * SL + 6 * VSL) * 8;
+  static int configured_device = -1;
+  int dev = 0;
+  CCT_CUDA(cudaGetDevice(&dev));
+  if (configured_device != dev) {
+    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured_device = dev;
+  }
+  reduce_kernel<<<(unsigned)d.ncta, RT, smem, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart, vpart);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
 
 int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const double *vpart, double *etd_acc,
                     double *v1_acc, cudaStream_t s) {
-  const int vblocks = (d.nu + 255) / 256;
+  const int vblocks = (d.nu * 32 + 255) / 256;  // one warp per virtual index
   finalize_kernel<<<1 + vblocks, 256, 0, s>>>(d.nu, d.nb, d.ncta, t, xpart, vpart, etd_acc, v1_acc);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;

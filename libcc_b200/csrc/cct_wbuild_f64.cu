@@ -12,22 +12,28 @@
 // disappear into the row addressing of the A operand (row (q,p) for the second
 // half) and into the reduction's reads; nothing is transposed in HBM.
 //
-// Kernel: one CTA per 128 x 64 output tile of one job; 4 warps, each 64 x 32;
-// mma.sync.m16n8k4.f64; a 3-stage cp.async ring of 128x16 / 64x16 tiles with
-// 16-byte-aligned rows padded to 20 doubles (conflict-free fragment loads).
+// Kernel: one CTA per 128 x BN output tile of one job (BN in {32..64}, chosen
+// per system so nu needs little padding); 4 warps stacked along M, each
+// 32 x BN; mma.sync.m16n8k4.f64; a 3-stage cp.async ring of 128x16 / BNx16
+// tiles with 16-byte-aligned rows padded to 20 doubles (conflict-free
+// fragment loads); two CTAs per SM.
 #include "cct_internal.cuh"
 
 namespace cct {
 namespace {
 
-constexpr int BM = 128, BN = kBN, BK = kKB;
-constexpr int WM = 64, WN = 32;
-constexpr int NWARP_M = BM / WM, NWARP_N = BN / WN;
-constexpr int NT = NWARP_M * NWARP_N * 32;
-constexpr int STAGES = 3;  // 3 x 46 KB ring: two CTAs per SM
+constexpr int BM = 128, BK = kKB;
+constexpr int WM = 32;
+constexpr int NWARP = BM / WM;
+constexpr int NT = NWARP * 32;
+constexpr int STAGES = 3;
 constexpr int LDS = BK + 4;  // padded smem row (doubles)
-constexpr int MF = WM / 16, NF = WN / 8;
-constexpr int SMEM_BYTES = STAGES * (BM + BN) * LDS * 8 + BM * 2 * 4;
+constexpr int MF = WM / 16;
+
+template <int BN>
+constexpr int smem_bytes() {
+  return STAGES * (BM + BN) * LDS * 8 + BM * 2 * 4;
+}
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -46,8 +52,10 @@ __device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, dou
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-__global__ void __launch_bounds__(NT) wbuild_f64_kernel(const GemmJob *__restrict__ jobs, int nu, int64_t KP,
-                                                        int64_t NP, int tiles_n) {
+template <int BN>
+__global__ void __launch_bounds__(NT, 2) wbuild_f64_kernel(const GemmJob *__restrict__ jobs, int nu, int64_t KP,
+                                                           int64_t NP, int tiles_n) {
+  constexpr int NF = BN / 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + STAGES * BM * LDS;
@@ -98,7 +106,6 @@ __global__ void __launch_bounds__(NT) wbuild_f64_kernel(const GemmJob *__restric
   };
 
   const int warp = tid >> 5, lane = tid & 31;
-  const int wm = warp / NWARP_N, wn = warp - (warp / NWARP_N) * NWARP_N;
   const int g = lane >> 2, t = lane & 3;
 
   double acc[MF][NF][4];
@@ -123,8 +130,8 @@ __global__ void __launch_bounds__(NT) wbuild_f64_kernel(const GemmJob *__restric
       if (nk < ktiles) load_stage(nk % STAGES, nk);
       cp_async_commit();
     }
-    const double *as = As + (kt % STAGES) * BM * LDS + (wm * WM) * LDS;
-    const double *bs = Bs + (kt % STAGES) * BN * LDS + (wn * WN) * LDS;
+    const double *as = As + (kt % STAGES) * BM * LDS + (warp * WM) * LDS;
+    const double *bs = Bs + (kt % STAGES) * BN * LDS;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       double af[MF][2], bf[NF];
@@ -148,9 +155,9 @@ __global__ void __launch_bounds__(NT) wbuild_f64_kernel(const GemmJob *__restric
   for (int i = 0; i < MF; i++) {
 #pragma unroll
     for (int half = 0; half < 2; half++) {
-      const int64_t m = m0 + wm * WM + i * 16 + g + half * 8;
+      const int64_t m = m0 + warp * WM + i * 16 + g + half * 8;
       if (m >= M) continue;
-      double *orow = job.out + m * NP + n0 + wn * WN + 2 * t;
+      double *orow = job.out + m * NP + n0 + 2 * t;
 #pragma unroll
       for (int j = 0; j < NF; j++) {
         double2 v = make_double2(acc[i][j][2 * half], acc[i][j][2 * half + 1]);
@@ -160,21 +167,38 @@ __global__ void __launch_bounds__(NT) wbuild_f64_kernel(const GemmJob *__restric
   }
 }
 
-}  // namespace
-
-int launch_wbuild_f64(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    CCT_CUDA(cudaFuncSetAttribute(wbuild_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    configured = true;
+template <int BN>
+int launch_bn(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStream_t s) {
+  constexpr int smem = smem_bytes<BN>();
+  static int configured_device = -1;
+  int dev = 0;
+  CCT_CUDA(cudaGetDevice(&dev));
+  if (configured_device != dev) {
+    CCT_CUDA(cudaFuncSetAttribute(wbuild_f64_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    configured_device = dev;
   }
   const int64_t M = (int64_t)d.nu * d.nu;
   const int tiles_m = (int)((M + BM - 1) / BM);
   const int tiles_n = (int)(d.NP / BN);
   dim3 grid(tiles_m * tiles_n, njobs);
-  wbuild_f64_kernel<<<grid, NT, SMEM_BYTES, s>>>(jobs_dev, d.nu, d.KP, d.NP, tiles_n);
+  wbuild_f64_kernel<BN><<<grid, NT, smem, s>>>(jobs_dev, d.nu, d.KP, d.NP, tiles_n);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
+}
+
+}  // namespace
+
+int launch_wbuild_f64(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStream_t s) {
+  switch (d.BN) {
+    case 64: return launch_bn<64>(d, jobs_dev, njobs, s);
+    case 56: return launch_bn<56>(d, jobs_dev, njobs, s);
+    case 48: return launch_bn<48>(d, jobs_dev, njobs, s);
+    case 40: return launch_bn<40>(d, jobs_dev, njobs, s);
+    case 32: return launch_bn<32>(d, jobs_dev, njobs, s);
+    default:
+      set_error("unsupported W-build N tile " + std::to_string(d.BN));
+      return CCT_ERR_INVALID;
+  }
 }
 
 }  // namespace cct

@@ -69,6 +69,7 @@ def lib():
         _lib.orc_task.argtypes = [i64, i64, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]
         _lib.orc_div_even.argtypes = [i64, i64, i64, ctypes.POINTER(i64), ctypes.POINTER(i64)]
         _lib.orc_tuple.argtypes = [ctypes.c_int] + [i64] * 5 + [dp] * 11 + [dp]
+        _lib.orc_reduce_tuple.argtypes = [ctypes.c_int] + [i64] * 5 + [dp] * 7
     return _lib
 
 
@@ -213,6 +214,15 @@ class _Views:
 
 # --------------------------------------------------------------------------- literal numpy pipeline
 
+def _dgemm(ta: str, tb: str, alpha: float, a: np.ndarray, b: np.ndarray, beta: float, c: np.ndarray):
+    """C := alpha op(A) op(B) + beta C in place, through the BLAS DGEMM the
+    reference calls (scipy's handle on the image's OpenBLAS)."""
+    from scipy.linalg.blas import dgemm
+    out = dgemm(alpha, a, b, beta=beta, c=c, trans_a=int(ta == "t"), trans_b=int(tb == "t"), overwrite_c=1)
+    if out is not c and not np.shares_memory(out, c):
+        c[...] = out
+
+
 def literal_ijk_w(V: _Views, i, j, k, ve_i, ve_j, ve_k) -> np.ndarray:
     """ijk_tuple_formv3 (triples-abc/ijk_tuple.f90:1-53) with BLAS DGEMMs; ve_x are the
     swapped slices ve_x(a,b,c) = (ac|b x).  Returns W (nu,nu,nu) Fortran order."""
@@ -222,21 +232,21 @@ def literal_ijk_w(V: _Views, i, j, k, ve_i, ve_j, ve_k) -> np.ndarray:
     m2 = lambda v: v.reshape((nu2, nu), order="F")
     m1 = lambda v: v.reshape((nu, nu2), order="F")
     vi, vj, vk = m1(ve_i), m1(ve_j), m1(ve_k)
-    m2(v3)[...] = -(V.t2x(i) @ V.vmxy(k, j))                           # #0
-    m2(v3)[...] += vi.T @ V.t2xy(k, j).T                               # #11
-    m1(v3)[...] += V.t2xy(i, k) @ vj                                   # #8
-    m1(v3)[...] -= V.vmxy(i, k).T @ V.t2x(j).T                         # #3
+    _dgemm("n", "n", -1.0, V.t2x(i), V.vmxy(k, j), 0.0, m2(v3))      # #0
+    _dgemm("t", "t", 1.0, vi, V.t2xy(k, j), 1.0, m2(v3))            # #11
+    _dgemm("n", "n", 1.0, V.t2xy(i, k), vj, 1.0, m1(v3))            # #8
+    _dgemm("t", "t", -1.0, V.vmxy(i, k), V.t2x(j), 1.0, m1(v3))     # #3
     v3 = _trant3_np(v3, 1)
-    m2(v3)[...] -= V.t2x(i) @ V.vmxy(j, k)                             # #1
-    m2(v3)[...] += vi.T @ V.t2xy(j, k).T                               # #10
-    m1(v3)[...] += V.t2xy(i, j) @ vk                                   # #6
-    m1(v3)[...] -= V.vmxy(i, j).T @ V.t2x(k).T                         # #5
+    _dgemm("n", "n", -1.0, V.t2x(i), V.vmxy(j, k), 1.0, m2(v3))     # #1
+    _dgemm("t", "t", 1.0, vi, V.t2xy(j, k), 1.0, m2(v3))            # #10
+    _dgemm("n", "n", 1.0, V.t2xy(i, j), vk, 1.0, m1(v3))            # #6
+    _dgemm("t", "t", -1.0, V.vmxy(i, j), V.t2x(k), 1.0, m1(v3))     # #5
     v3 = _trant3_np(v3, 4)
-    m2(v3)[...] -= V.t2x(j) @ V.vmxy(k, i)                             # #2
-    m2(v3)[...] += vj.T @ V.t2xy(k, i).T                               # #9
+    _dgemm("n", "n", -1.0, V.t2x(j), V.vmxy(k, i), 1.0, m2(v3))     # #2
+    _dgemm("t", "t", 1.0, vj, V.t2xy(k, i), 1.0, m2(v3))            # #9
     v3 = _trant3_np(v3, 1)
-    m1(v3)[...] -= V.vmxy(j, i).T @ V.t2x(k).T                         # #4
-    m1(v3)[...] += V.t2xy(j, i) @ vk                                   # #7
+    _dgemm("t", "t", -1.0, V.vmxy(j, i), V.t2x(k), 1.0, m1(v3))     # #4
+    _dgemm("n", "n", 1.0, V.t2xy(j, i), vk, 1.0, m1(v3))            # #7
     v3 = _trant3_np(v3, 4)
     r = np.arange(nu)
     v3[r, r, r] = 0.0                                                  # ZEROT3
@@ -250,17 +260,17 @@ def literal_ijj_w(V: _Views, i, j, ve_i, ve_j) -> np.ndarray:
     m2 = lambda v: v.reshape((nu2, nu), order="F")
     m1 = lambda v: v.reshape((nu, nu2), order="F")
     v3 = np.zeros((nu, nu, nu), order="F")
-    m2(v3)[...] = -(V.t2x(i) @ V.vmxy(j, j))
+    _dgemm("n", "n", -1.0, V.t2x(i), V.vmxy(j, j), 0.0, m2(v3))
     v3 = _trant3_np(v3, 2)
-    m2(v3)[...] -= V.t2x(j) @ V.vmxy(j, i)
+    _dgemm("n", "n", -1.0, V.t2x(j), V.vmxy(j, i), 1.0, m2(v3))
     v3 = _trant3_np(v3, 1)
-    m2(v3)[...] -= V.t2x(j) @ V.vmxy(i, j)
+    _dgemm("n", "n", -1.0, V.t2x(j), V.vmxy(i, j), 1.0, m2(v3))
     v3 = _trant3_np(v3, 4)
-    m1(v3)[...] += V.t2xy(i, j) @ m1(ve_j)
+    _dgemm("n", "n", 1.0, V.t2xy(i, j), m1(ve_j), 1.0, m1(v3))
     v3 = _trant3_np(v3, 3)
-    m1(v3)[...] += V.t2xy(j, i) @ m1(ve_j)
+    _dgemm("n", "n", 1.0, V.t2xy(j, i), m1(ve_j), 1.0, m1(v3))
     v3 = _trant3_np(v3, 1)
-    m1(v3)[...] += V.t2xy(j, j) @ m1(ve_i)
+    _dgemm("n", "n", 1.0, V.t2xy(j, j), m1(ve_i), 1.0, m1(v3))
     v3 = _trant3_np(v3, 2)
     v3 = np.asfortranarray(v3 + _perm(v3, "acb"))
     r = np.arange(nu)
@@ -275,17 +285,17 @@ def literal_iij_w(V: _Views, i, k, ve_i, ve_k) -> np.ndarray:
     m2 = lambda v: v.reshape((nu2, nu), order="F")
     m1 = lambda v: v.reshape((nu, nu2), order="F")
     v3 = np.zeros((nu, nu, nu), order="F")
-    m2(v3)[...] = -(V.t2x(i) @ V.vmxy(k, i))
+    _dgemm("n", "n", -1.0, V.t2x(i), V.vmxy(k, i), 0.0, m2(v3))
     v3 = _trant3_np(v3, 1)
-    m2(v3)[...] -= V.t2x(i) @ V.vmxy(i, k)
+    _dgemm("n", "n", -1.0, V.t2x(i), V.vmxy(i, k), 1.0, m2(v3))
     v3 = _trant3_np(v3, 2)
-    m2(v3)[...] -= V.t2x(k) @ V.vmxy(i, i)
+    _dgemm("n", "n", -1.0, V.t2x(k), V.vmxy(i, i), 1.0, m2(v3))
     v3 = _trant3_np(v3, 2)
-    m1(v3)[...] += V.t2xy(i, i) @ m1(ve_k)
+    _dgemm("n", "n", 1.0, V.t2xy(i, i), m1(ve_k), 1.0, m1(v3))
     v3 = _trant3_np(v3, 1)
-    m1(v3)[...] += V.t2xy(i, k) @ m1(ve_i)
+    _dgemm("n", "n", 1.0, V.t2xy(i, k), m1(ve_i), 1.0, m1(v3))
     v3 = _trant3_np(v3, 3)
-    m1(v3)[...] += V.t2xy(k, i) @ m1(ve_i)
+    _dgemm("n", "n", 1.0, V.t2xy(k, i), m1(ve_i), 1.0, m1(v3))
     v3 = _trant3_np(v3, 3)
     v3 = np.asfortranarray(v3 + _perm(v3, "bac"))
     r = np.arange(nu)
@@ -325,9 +335,8 @@ def literal_cc_triples(inp, tuples=None, threads=None):
     """(T) through the literal numpy pipeline.  ``tuples`` optionally restricts the
     work to a list of (kind, i, j, k) (kind 0: i>j>k, 1: (i,j,j), 2: (i,i,k));
     degenerate tuples go through the literal ijj/iij_tuple_formv3 sequences with
-    SYMT311, and the DRT1WT3 reduction with weight 1/2 (tests/test_oracle.py ties
-    that to the reference's DRT1WT3IJ/JK).  Tuple energies are summed with
-    math.fsum.  Returns (ets, etd, v1[nu,no])."""
+    SYMT311; every tuple then goes through the C restatement of T3SQUA, ADT3DEN
+    and DRT1WT3IJK/IJ/JK.  Tuple energies are summed with math.fsum.  Returns (ets, etd, v1[nu,no])."""
     V = _Views(inp)
     no, nu = inp.no, inp.nu
     v1 = np.zeros((nu, no), order="F")
@@ -343,17 +352,22 @@ def literal_cc_triples(inp, tuples=None, threads=None):
             cache[x] = _trant3_np(expand_vvvo(inp, x), 1)
         return cache[x]
 
+    v1c = np.zeros(nu * no)
+    t3 = np.zeros(nu ** 3)
     for kind, i, j, k in tuples:
         if kind == 0:
             w = literal_ijk_w(V, i, j, k, ve(i), ve(j), ve(k))
-            etd_parts.append(literal_reduce(V, i, j, k, w, 1.0, v1))
         elif kind == 1:
             w = literal_ijj_w(V, i, j, ve(i), ve(j))
-            etd_parts.append(literal_reduce(V, i, j, k, w, 0.5, v1))
         else:
             w = literal_iij_w(V, i, k, ve(i), ve(k))
-            etd_parts.append(literal_reduce(V, i, j, k, w, 0.5, v1))
+        wf = np.ascontiguousarray(w.ravel(order="F"))
+        e = ctypes.c_double(0.0)
+        lib().orc_reduce_tuple(kind, no, nu, i, j, k, _p(wf), _p(t3), _p(inp.voe), _p(inp.eh), _p(inp.ep),
+                               _p(v1c), ctypes.byref(e))
+        etd_parts.append(e.value)
     etd = math.fsum(etd_parts)
+    v1[...] = v1c.reshape((nu, no), order="F")
     ets = 2.0 * float(np.sum(V.t1.T * v1))
     return ets, etd, v1
 

@@ -46,6 +46,7 @@ void orc_trant3(double *v, i64 nu, int id)
     double x;
     switch (id) {
     case 1: /* trant3.f:13-24 */
+#pragma omp parallel for private(a, c, x) schedule(dynamic, 4)
         for (b = 0; b < nu; b++)
             for (c = 0; c <= b; c++)
                 for (a = 0; a < nu; a++) {
@@ -55,6 +56,7 @@ void orc_trant3(double *v, i64 nu, int id)
                 }
         break;
     case 2: /* trant3.f:25-36 */
+#pragma omp parallel for private(a, b, x) schedule(dynamic, 4)
         for (c = 0; c < nu; c++)
             for (a = 0; a < nu; a++)
                 for (b = 0; b <= a; b++) {
@@ -64,6 +66,7 @@ void orc_trant3(double *v, i64 nu, int id)
                 }
         break;
     case 3: /* trant3.f:37-48 */
+#pragma omp parallel for private(a, c, x) schedule(dynamic, 4)
         for (b = 0; b < nu; b++)
             for (a = 0; a < nu; a++)
                 for (c = 0; c <= a; c++) {
@@ -72,7 +75,8 @@ void orc_trant3(double *v, i64 nu, int id)
                     V3(v, c, b, a) = x;
                 }
         break;
-    case 4: /* trant3.f:49-66 */
+    case 4: /* trant3.f:49-66 (the reference splits b over SMP ranks) */
+#pragma omp parallel for private(a, c, x) schedule(dynamic, 4)
         for (b = 0; b < nu; b++)
             for (c = 0; c <= b; c++)
                 for (a = 0; a <= c; a++) {
@@ -87,7 +91,8 @@ void orc_trant3(double *v, i64 nu, int id)
                     V3(v, c, b, a) = x;
                 }
         break;
-    case 5: /* trant3.f:67-80 */
+    case 5: /* trant3.f:67-80 (the reference splits a over SMP ranks) */
+#pragma omp parallel for private(c, d, x) schedule(dynamic, 4)
         for (a = 0; a < nu; a++)
             for (c = 0; c <= a; c++)
                 for (d = 0; d <= c; d++) {
@@ -279,6 +284,7 @@ double orc_t3squa(i64 no, i64 nu, i64 i, i64 j, i64 k, const double *t3, const d
     (void)no;
     double dijk = eh[i] + eh[j] + eh[k];
     double x3 = 0.0;
+#pragma omp parallel for reduction(+ : x3) schedule(static)
     for (i64 c = 0; c < nu; c++)
         for (i64 b = 0; b < nu; b++)
             for (i64 a = 0; a < nu; a++) {
@@ -297,6 +303,7 @@ double orc_t3squa(i64 no, i64 nu, i64 i, i64 j, i64 k, const double *t3, const d
 /* ADT3DEN_SMP (triples-abc/ddcc_aux.f:97-115): V3(c,b,a) /= DEH - e_a - e_b - e_c. */
 void orc_adt3den(i64 nu, double deh, double *t3, const double *ep)
 {
+#pragma omp parallel for schedule(static)
     for (i64 a = 0; a < nu; a++)
         for (i64 b = 0; b < nu; b++)
             for (i64 c = 0; c < nu; c++) V3(t3, c, b, a) /= (deh - ep[a] - ep[b] - ep[c]);
@@ -305,6 +312,7 @@ void orc_adt3den(i64 nu, double deh, double *t3, const double *ep)
 /* SMT3FOUR_SMP (triples-abc/ddcc_aux.f:189-214). */
 static void orc_smt3four(i64 nu, double *t3, const double *v3)
 {
+#pragma omp parallel for schedule(static)
     for (i64 c = 0; c < nu; c++) {
         for (i64 b = 0; b < nu; b++) V3(t3, b, b, c) = 0.0;
         for (i64 b = 1; b < nu; b++)
@@ -321,7 +329,15 @@ static void orc_t1wt3ijk(i64 i, i64 j, i64 k, i64 no, i64 nu, double *v1, const 
 {
     const i64 nu2 = nu * nu;
     orc_smt3four(nu, t3, ti);
-    orc_dgemm('n', 'n', nu, 1, nu2, 1.0, t3, nu, voe + k * nu2 * no + j * nu2, nu2, 1.0, v1 + i * nu, nu);
+    /* DGEMM('N','N',NU,1,NU2,...): v1(a,I) += sum_bc T3(a,bc) VOE(bc,J,K) */
+    const double *x = voe + k * nu2 * no + j * nu2;
+    double *y = v1 + i * nu;
+#pragma omp parallel for schedule(static)
+    for (i64 a = 0; a < nu; a++) {
+        double s = 0.0;
+        for (i64 bc = 0; bc < nu2; bc++) s += t3[a + nu * bc] * x[bc];
+        y[a] += s;
+    }
 }
 
 /* DRT1WT3IJK_SMP (triples-abc/ddcc_aux.f:146-169). */
@@ -518,4 +534,20 @@ int orc_cc_triples(i64 no, i64 nu, const double *eh, const double *ep, const dou
     *etd = e;
     free(v3); free(t3); free(ve_i); free(ve_j); free(ve_k);
     return 0;
+}
+
+/* The reduction half of one tuple (T3SQUA, ADT3DEN, DRT1WT3IJK/IJ/JK) on a W
+ * already formed (and, for degenerate tuples, symmetrised) by the caller.
+ * kind/(i,j,k) as in orc_tuple.  v3 is divided in place; t3 is scratch. */
+void orc_reduce_tuple(int kind, i64 no, i64 nu, i64 i, i64 j, i64 k, double *v3, double *t3,
+                      const double *voe, const double *eh, const double *ep, double *v1, double *etd)
+{
+    *etd += orc_t3squa(no, nu, i, j, k, v3, eh, ep);
+    orc_adt3den(nu, eh[i] + eh[j] + eh[k], v3, ep);
+    if (kind == 0)
+        orc_drt1wt3ijk(i, j, k, no, nu, v1, voe, v3, t3);
+    else if (kind == 1)
+        orc_drt1wt3ij(i, j, no, nu, v1, voe, v3, t3);
+    else
+        orc_drt1wt3jk(i, k, no, nu, v1, voe, v3, t3);
 }

@@ -168,3 +168,33 @@ def test_forward_before_inputs_is_state_error(api):
         assert e.value.status == 6
         with pytest.raises(CctError):
             plan.forward(5, 2)
+
+
+def test_kernel_profiling_counts(api):
+    inp = S.generate(4, 21, 31)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        plain = plan.forward()
+        plan.set_profiling(True)
+        prof_run = plan.forward()
+        prof = plan.kernel_profile()
+        plan.set_profiling(False)
+        again = plan.forward()
+    n = plan.num_tuples
+    assert prof["wbuild"][1] == n and prof["reduce"][1] == n
+    assert prof["wbuild"][0] > 0 and prof["reduce"][0] > 0
+    assert plain[1] == prof_run[1] == again[1]
+
+
+def test_caller_stream(api):
+    torch = pytest.importorskip("torch")
+    inp = S.generate(4, 15, 32)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        a = plan.forward()
+        s = torch.cuda.Stream()
+        plan.set_stream(s.cuda_stream)
+        b = plan.forward()
+        plan.set_stream(None)
+        c = plan.forward()
+    assert a[1] == b[1] == c[1]
