@@ -117,6 +117,34 @@ const char *ccT_last_error(void);
  * microbenchmark; the denominator of the FP64 roofline). */
 double ccT_measure_fp64_peak(int32_t device);
 
+/* ------------------------------------------------------------------ allocation-free reduction
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory: codes that reserve one arena for all their GPU
+ * buffers up front, and drivers that must not risk the implicit device
+ * synchronisation of cudaMalloc/cudaFree in the middle of their own
+ * asynchronous work.
+ *
+ * Adds the E[4] and E[5] contributions of one tuple (i,j,k), 0-based with
+ * i >= j >= k not all equal (weight 1/2 when two are equal), computed from a
+ * W_abc the caller already holds on the device (w(a,b,c) at a + nu*(b + nu*c);
+ * w(a,a,a) is treated as 0), into the caller's device accumulators:
+ * etd_acc[0..1] (sum and compensation term; etd = etd_acc[0] + etd_acc[1]) and
+ * v1_acc(nu,no).  eh, ep, voe are device arrays in the reference layouts.
+ * Kernels run on cuda_stream (a cudaStream_t as void*, NULL = default stream).
+ *
+ * It allocates nothing: its per-block partial sums live in one fixed array in
+ * the library's device memory, sized for nu <= CCT_NOALLOC_MAX_NU (6.4 MiB,
+ * held by every GPU that loads the library until the process exits).  Larger
+ * nu is rejected with CCT_ERR_INVALID.  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress) with the device current,
+ * so make the first call before any stream capture.  All calls share the
+ * array: calls whose kernels overlap on the GPU (different streams with no
+ * ordering between them) race; calls ordered on one stream are safe. */
+#define CCT_NOALLOC_MAX_NU 320
+int ccT_reduce_w_noalloc(int64_t no, int64_t nu, int64_t i, int64_t j, int64_t k, const double *w,
+                         const double *eh, const double *ep, const double *voe, double *etd_acc,
+                         double *v1_acc, void *cuda_stream);
+
 /* ------------------------------------------------------------------ legacy hooks
  * ijk_gpu_init_    replaces the call at src/triples-ijk/triples_cpu.F90:363
  * ijk_gpu_driver_  replaces src/triples-ijk/ddcc_t_ijk_big_cuda.f:12-14

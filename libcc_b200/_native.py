@@ -23,7 +23,7 @@ EXPORTS = [
     "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
     "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
     "ccT_last_error", "ccT_measure_fp64_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
-    "cc_triples_b200_",
+    "cc_triples_b200_", "ccT_reduce_w_noalloc",
 ]
 
 
@@ -95,6 +95,8 @@ def load():
     lib.ijk_gpu_finalize_.restype = None
     lib.cc_triples_b200_.argtypes = [i64p, i64p] + [dp] * 10
     lib.cc_triples_b200_.restype = None
+    lib.ccT_reduce_w_noalloc.argtypes = [i64] * 5 + [vp] * 6 + [vp]
+    lib.ccT_reduce_w_noalloc.restype = ctypes.c_int
     _lib = lib
     return lib
 
