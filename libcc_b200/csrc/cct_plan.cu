@@ -44,17 +44,22 @@ struct ccT_plan {
   ccT_options opt{};
   Dims d{};
   cudaStream_t stream = nullptr;      // stream the kernels run on
-  cudaStream_t own_stream = nullptr;  // the plan's own stream
+  cudaStream_t own_stream = nullptr;  // the plan's own stream (ordering, ets)
+  cudaStream_t gemm_stream = nullptr; // W-build GEMMs, highest priority
+  cudaStream_t red_stream = nullptr;  // reductions, lowest priority: they fill GEMM tail waves
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_gemm[2] = {nullptr, nullptr}, ev_red[2] = {nullptr, nullptr};
+  int64_t tick = 0;                   // tuples issued so far: selects the X buffer
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // inputs (device copies, reference layouts)
   double *eh = nullptr, *ep = nullptr, *t1 = nullptr, *t2 = nullptr, *vm = nullptr, *voe = nullptr;
   // derived operands
   double *E = nullptr, *F = nullptr;
-  double *X[3] = {nullptr, nullptr, nullptr};
+  double *X[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // double-buffered GEMM outputs
   double *xpart = nullptr, *vpart = nullptr;
   int16_t *cta_table = nullptr;
   double *acc = nullptr;  // [etd_sum, etd_comp, out3[3], v1(nu*no)]
-  GemmJob *jobs = nullptr;  // 3 per tuple
+  GemmJob *jobs = nullptr;  // [buffer][tuple][3]
   int *flags = nullptr;
   double *stage = nullptr;  // packed-slice staging for the legacy hook
   std::vector<Tuple> tuples;
@@ -97,14 +102,16 @@ int build_jobs(ccT_plan *p) {
   const int64_t nu2 = (int64_t)d.nu * d.nu;
   auto Ex = [&](int x) { return p->E + (int64_t)x * nu2 * d.KP; };
   auto Fyz = [&](int y, int z) { return p->F + ((int64_t)y * d.no + z) * d.NP * d.KP; };
+  int buf = 0;
   auto G = [&](int x1, int x2, int x3, int slot) {
-    return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[slot], 2, 0};
+    return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][slot], 2, 0};
   };
   auto H = [&](int x1, int x2, int x3, int slot) {
-    return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[slot], 1, 0};
+    return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 0};
   };
   std::vector<GemmJob> jobs;
-  jobs.reserve(p->tuples.size() * 3);
+  jobs.reserve(p->tuples.size() * 6);
+  for (buf = 0; buf < 2; buf++)
   for (const Tuple &t : p->tuples) {
     if (t.kind == kIJK) {
       jobs.push_back(G(t.i, t.j, t.k, 0));
@@ -144,7 +151,7 @@ int check_denominators(ccT_plan *p) {
 
 // Records one event of a profiled launch pair: cls >= 0 opens pair number
 // prof_class.size() (event 2q), cls < 0 closes the last opened pair (event 2q+1).
-int prof_mark(ccT_plan *p, int cls) {
+int prof_mark(ccT_plan *p, int cls, cudaStream_t st) {
   if (!p->profiling) return CCT_OK;
   size_t n;
   if (cls >= 0) {
@@ -161,7 +168,7 @@ int prof_mark(ccT_plan *p, int cls) {
     CCT_CUDA(cudaEventCreate(&e));
     p->prof_events.push_back(e);
   }
-  CCT_CUDA(cudaEventRecord(p->prof_events[n], p->stream));
+  CCT_CUDA(cudaEventRecord(p->prof_events[n], st));
   if (cls >= 0) p->prof_class.push_back(cls);
   return CCT_OK;
 }
@@ -180,25 +187,52 @@ int prof_collect(ccT_plan *p) {
   return CCT_OK;
 }
 
+// Orders the plan's GEMM and reduction streams after everything already issued
+// on p->stream.
+int fork_streams(ccT_plan *p) {
+  CCT_CUDA(cudaEventRecord(p->ev_fork, p->stream));
+  CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_fork, 0));
+  CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_fork, 0));
+  return CCT_OK;
+}
+
+// Orders p->stream after every GEMM and reduction issued so far (each GEMM is
+// already waited on by the reduction that follows it).
+int join_streams(ccT_plan *p) {
+  CCT_CUDA(cudaEventRecord(p->ev_join, p->red_stream));
+  CCT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_join, 0));
+  return CCT_OK;
+}
+
+// W-build of tuple tix into X buffer b on the GEMM stream, then its reduction on
+// the reduction stream.  The GEMM waits until the reduction that last read
+// buffer b (two tuples earlier) is done; the reduction waits for its GEMM.
 int run_tuple(ccT_plan *p, int64_t tix) {
   const Tuple &t = p->tuples[tix];
   const int njobs = t.kind == kIJK ? 3 : 2;
-  CCT_TRY(prof_mark(p, CCT_KERNEL_WBUILD));
-  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tix, njobs, p->stream));
-  CCT_TRY(prof_mark(p, -1));
+  const int b = (int)(p->tick & 1);
+  p->tick++;
+  const int64_t ntup = (int64_t)p->tuples.size();
+  CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[b], 0));
+  CCT_TRY(prof_mark(p, CCT_KERNEL_WBUILD, p->gemm_stream));
+  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, p->gemm_stream));
+  CCT_TRY(prof_mark(p, -1, p->gemm_stream));
+  CCT_CUDA(cudaEventRecord(p->ev_gemm[b], p->gemm_stream));
+  CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_gemm[b], 0));
   TupleDev td;
-  td.x[0] = p->X[0];
-  td.x[1] = p->X[1];
-  td.x[2] = p->X[2];
+  td.x[0] = p->X[b][0];
+  td.x[1] = p->X[b][1];
+  td.x[2] = p->X[b][2];
   td.kind = t.kind;
   td.i = t.i;
   td.j = t.j;
   td.k = t.k;
   td.weight = t.kind == kIJK ? 1.0 : 0.5;
-  CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE));
-  CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->stream));
-  CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->stream));
-  CCT_TRY(prof_mark(p, -1));
+  CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE, p->red_stream));
+  CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->red_stream));
+  CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->red_stream));
+  CCT_TRY(prof_mark(p, -1, p->red_stream));
+  CCT_CUDA(cudaEventRecord(p->ev_red[b], p->red_stream));
   p->last_launches += 3;
   return CCT_OK;
 }
@@ -293,18 +327,27 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     return s;
   };
   int s;
-  if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  int prio_least = 0, prio_greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&p->gemm_stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&p->red_stream, cudaStreamNonBlocking, prio_least) != cudaSuccess)
+    return fail(CCT_ERR_CUDA);
   p->stream = p->own_stream;
+  for (cudaEvent_t *e : {&p->ev_fork, &p->ev_join, &p->ev_gemm[0], &p->ev_gemm[1], &p->ev_red[0], &p->ev_red[1]})
+    if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return fail(CCT_ERR_CUDA);
   if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) return fail(CCT_ERR_CUDA);
   const int64_t nu2 = nu * nu;
   if ((s = dalloc(&p->eh, no)) || (s = dalloc(&p->ep, nu)) || (s = dalloc(&p->t1, no * nu)) ||
       (s = dalloc(&p->t2, nu2 * no * no)) || (s = dalloc(&p->vm, no * nu * no * no)) ||
       (s = dalloc(&p->voe, nu2 * no * no)) || (s = dalloc(&p->E, no * nu2 * d.KP)) ||
-      (s = dalloc(&p->F, no * no * d.NP * d.KP)) || (s = dalloc(&p->X[0], nu2 * d.NP)) ||
-      (s = dalloc(&p->X[1], nu2 * d.NP)) || (s = dalloc(&p->X[2], nu2 * d.NP)) ||
-      (s = dalloc(&p->xpart, d.ncta)) || (s = dalloc(&p->vpart, d.ncta * 72)) ||
+      (s = dalloc(&p->F, no * no * d.NP * d.KP)) || (s = dalloc(&p->X[0][0], nu2 * d.NP)) ||
+      (s = dalloc(&p->X[0][1], nu2 * d.NP)) || (s = dalloc(&p->X[0][2], nu2 * d.NP)) ||
+      (s = dalloc(&p->X[1][0], nu2 * d.NP)) || (s = dalloc(&p->X[1][1], nu2 * d.NP)) ||
+      (s = dalloc(&p->X[1][2], nu2 * d.NP)) ||
+      (s = dalloc(&p->xpart, d.ncta)) || (s = dalloc(&p->vpart, (int64_t)12 * d.nb * d.nb * (d.nb + 1))) ||
       (s = dalloc(&p->cta_table, d.ncta * 3)) || (s = dalloc(&p->acc, 5 + nu * no)) ||
-      (s = dalloc(&p->jobs, p->tuples.size() * 3)) || (s = dalloc(&p->flags, 4)))
+      (s = dalloc(&p->jobs, p->tuples.size() * 6)) || (s = dalloc(&p->flags, 4)))
     return fail(s);
   std::vector<int16_t> table(d.ncta * 3);
   int64_t idx = 0;
@@ -406,7 +449,9 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   p->last_launches = 0;
   CCT_CUDA(cudaMemsetAsync(p->acc, 0, (5 + (int64_t)d.nu * d.no) * 8, p->stream));
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
+  CCT_TRY(fork_streams(p));
   for (int64_t t = begin; t < end; t++) CCT_TRY(run_tuple(p, t));
+  CCT_TRY(join_streams(p));
   CCT_TRY(launch_ets(d, p->t1, v1_acc(p), p->acc, p->acc + 2, p->stream));
   p->last_launches += 1;
   CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
@@ -452,10 +497,13 @@ int ccT_time_wbuild(ccT_plan *p, int64_t tuple, int32_t reps, double *ms_per_lau
   }
   DeviceGuard guard(p->device);
   const int njobs = p->tuples[tuple].kind == kIJK ? 3 : 2;
-  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->stream));  // warm
-  CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
-  for (int r = 0; r < reps; r++) CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->stream));
-  CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
+  CCT_TRY(fork_streams(p));
+  CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[0], 0));
+  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream));  // warm
+  CCT_CUDA(cudaEventRecord(p->ev0, p->gemm_stream));
+  for (int r = 0; r < reps; r++) CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream));
+  CCT_CUDA(cudaEventRecord(p->ev1, p->gemm_stream));
+  CCT_CUDA(cudaEventRecord(p->ev_red[0], p->gemm_stream));  // later writers of buffer 0 follow these
   CCT_CUDA(cudaEventSynchronize(p->ev1));
   float ms = 0.f;
   CCT_CUDA(cudaEventElapsedTime(&ms, p->ev0, p->ev1));
@@ -489,9 +537,11 @@ int64_t ccT_last_forward_launches(const ccT_plan *p) { return p ? p->last_launch
 int ccT_plan_destroy(ccT_plan *p) {
   if (!p) return CCT_OK;
   DeviceGuard guard(p->device);
-  if (p->stream) cudaStreamSynchronize(p->stream);
-  double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->X[0], p->X[1], p->X[2],
-                    p->xpart, p->vpart, p->acc, p->stage};
+  for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream})
+    if (st) cudaStreamSynchronize(st);
+  double *bufs[] = {p->eh,      p->ep,      p->t1,      p->t2,      p->vm,      p->voe,  p->E,     p->F,
+                    p->X[0][0], p->X[0][1], p->X[0][2], p->X[1][0], p->X[1][1], p->X[1][2], p->xpart, p->vpart,
+                    p->acc,     p->stage};
   for (double *b : bufs)
     if (b) cudaFree(b);
   if (p->cta_table) cudaFree(p->cta_table);
@@ -500,6 +550,10 @@ int ccT_plan_destroy(ccT_plan *p) {
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
+  for (cudaEvent_t e : {p->ev_fork, p->ev_join, p->ev_gemm[0], p->ev_gemm[1], p->ev_red[0], p->ev_red[1]})
+    if (e) cudaEventDestroy(e);
+  if (p->gemm_stream) cudaStreamDestroy(p->gemm_stream);
+  if (p->red_stream) cudaStreamDestroy(p->red_stream);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
   delete p;
   return CCT_OK;
@@ -575,7 +629,8 @@ void ijk_gpu_driver_(const int64_t *nu, const int64_t *no, const int64_t *i, con
   }
   // index of (I,J,K) in the tuple list: DDCC_T_TASK order
   const int64_t tix = I * (I - 1) * (I - 2) / 6 + J * (J - 1) / 2 + K;
-  int s = run_tuple(p, tix);
+  int s = fork_streams(p);
+  if (!s) s = run_tuple(p, tix);
   if (s) legacy_stop("ijk_gpu_driver", s);
 }
 
@@ -588,7 +643,8 @@ void ijk_gpu_finalize_(const int64_t *no, const int64_t *nu, double *etd) {
   const int64_t n = (int64_t)p->d.nu * p->d.no;
   std::vector<double> v1(n);
   double e[2];
-  if (cudaMemcpyAsync(e, p->acc, 16, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess ||
+  if (join_streams(p) != CCT_OK ||
+      cudaMemcpyAsync(e, p->acc, 16, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess ||
       cudaMemcpyAsync(v1.data(), v1_acc(p), n * 8, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess ||
       cudaStreamSynchronize(p->stream) != cudaSuccess)
     legacy_stop("ijk_gpu_finalize", CCT_ERR_CUDA);

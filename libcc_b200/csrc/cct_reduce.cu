@@ -21,206 +21,254 @@
 namespace cct {
 namespace {
 
-constexpr int RB = kRB;             // 8
-constexpr int RT = 256;             // threads per reduction CTA
-constexpr int SL = 640;             // doubles per padded 8x8x8 block in smem
-__device__ __forceinline__ int soff(int l0, int l1, int l2) { return l0 + 9 * l1 + 81 * l2; }
+constexpr int RB = kRB;  // 8
+constexpr int RT = 256;  // threads per reduction CTA
+constexpr int SL = 640;  // doubles per padded 8x8x8 block in smem
+__host__ __device__ constexpr int soff(int l0, int l1, int l2) { return l0 + 9 * l1 + 81 * l2; }
 
-// the six permutations of three positions, in a fixed order
-__constant__ int c_perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+// The six permutations of three positions, in a fixed order:
+// 0:(0,1,2)=abc 1:(0,2,1)=acb 2:(1,0,2)=bac 3:(1,2,0)=bca 4:(2,0,1)=cab 5:(2,1,0)=cba
+__host__ __device__ constexpr int pm(int p, int m) {
+  return p == 0 ? m : p == 1 ? (m == 0 ? 0 : m == 1 ? 2 : 1) : p == 2 ? (m == 0 ? 1 : m == 1 ? 0 : 2)
+       : p == 3 ? (m == 0 ? 1 : m == 1 ? 2 : 0) : p == 4 ? (m == 0 ? 2 : m == 1 ? 0 : 1)
+                : (m == 0 ? 2 : m == 1 ? 1 : 0);
+}
+__host__ __device__ constexpr int pidx(int p0, int p1) { return p0 * 2 + (p1 > p0 ? p1 - 1 : p1); }
+// perm value of role r for element pi(x): W(x_{pi(r(0))}, ...) -> index of pi o r
+__host__ __device__ constexpr int compose(int pi, int r) { return pidx(pm(pi, pm(r, 0)), pm(pi, pm(r, 1))); }
 
 // W assembly per tuple kind: W(x0,x1,x2) += X_g(x_al0, x_al1, x_al2); {g, al0, al1, al2}
 //   i>j>k : X0(a,b,c) + X1(a,c,b) + X2(b,c,a)
 //   (i,j,j): X0(a,b,c) + X0(a,c,b) + X1(b,c,a) + X1(c,b,a)
 //   (i,i,k): X0(a,b,c) + X0(b,a,c) + X1(a,c,b) + X1(b,c,a)
-__constant__ int c_terms[3][4][4] = {
-    {{0, 0, 1, 2}, {1, 0, 2, 1}, {2, 1, 2, 0}, {0, 0, 0, 0}},
-    {{0, 0, 1, 2}, {0, 0, 2, 1}, {1, 1, 2, 0}, {1, 2, 1, 0}},
-    {{0, 0, 1, 2}, {0, 1, 0, 2}, {1, 0, 2, 1}, {1, 1, 2, 0}}};
+__host__ __device__ constexpr int term_entry(int kind, int term, int f) {
+  constexpr int tab[3][4][4] = {{{0, 0, 1, 2}, {1, 0, 2, 1}, {2, 1, 2, 0}, {0, 0, 0, 0}},
+                                {{0, 0, 1, 2}, {0, 0, 2, 1}, {1, 1, 2, 0}, {1, 2, 1, 0}},
+                                {{0, 0, 1, 2}, {0, 1, 0, 2}, {1, 0, 2, 1}, {1, 1, 2, 0}}};
+  return tab[kind][term][f];
+}
+__host__ __device__ constexpr int kstride(int m) { return m == 0 ? 1 : (m == 1 ? 9 : 81); }
 
-__device__ __forceinline__ int perm_index(int p0, int p1) {
-  // index of the permutation whose first two entries are (p0, p1)
-  return p0 * 2 + ((p1 > p0 ? p1 - 1 : p1));
+template <typename T>
+__device__ __forceinline__ T sel3(int m, T v0, T v1, T v2) {
+  return m == 0 ? v0 : (m == 1 ? v1 : v2);
 }
 
-constexpr int VSL = 6 * 64;  // staged VOE values per slot: 6 planes x 64 (b,c) pairs
+// VOE staging: three block pairs x six planes x 64: pair 0 (b,c), 1 (a,c), 2 (a,b);
+// planes 0..5 = (j,k) (k,j) (i,k) (k,i) (i,j) (j,i); plane ^ 1 swaps the pair's order.
+constexpr int VPAIR = 6 * 64;
+__device__ __forceinline__ int nb_of(int nu) { return (nu + RB - 1) / RB; }
+constexpr int REDUCE_SMEM = (6 * SL + 3 * VPAIR) * 8;
 
-__global__ void __launch_bounds__(RT) reduce_kernel(int nu, int no, int64_t NP, TupleDev t,
-                                                   const double *__restrict__ eh, const double *__restrict__ ep,
-                                                   const double *__restrict__ voe, const int16_t *__restrict__ table,
-                                                   double *__restrict__ xpart, double *__restrict__ vpart) {
-  extern __shared__ __align__(16) double dyn_smem[];  // REDUCE_SMEM bytes
-  double *Wsm = dyn_smem;                             // [6][SL]
-  double *Vsm = dyn_smem + 6 * SL;                    // [6][VSL]
-  __shared__ double vloc[3][RB][3];
+// One CTA per unordered block triple {A<=B<=C}.  Phase A assembles W on every
+// distinct ordered block of the orbit in shared memory (term by term, fixed
+// order).  Phase B: each thread evaluates orbits -- the six index permutations
+// of one (a,b,c) of block (A,B,C) share six W values and one denominator --
+// and accumulates E[4] and the v1 updates of all six elements.  Phase C sums
+// the per-thread v1 partials in a fixed order.
+template <int KIND>
+__global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t NP, TupleDev t,
+                                                      const double *__restrict__ eh, const double *__restrict__ ep,
+                                                      const double *__restrict__ voe,
+                                                      const int16_t *__restrict__ table, double *__restrict__ xpart,
+                                                      double *__restrict__ vpart) {
+  constexpr int NTERM = KIND == kIJK ? 3 : 4;
+  extern __shared__ __align__(16) double dyn_smem[];
+  double *Wsm = dyn_smem;             // [6][SL]
+  double *Vsm = Wsm + 6 * SL;         // [3][6][64]
   __shared__ double red[RT / 32];
-  __shared__ int slot_of[6];  // perm sigma -> slot holding block O_sigma
-  __shared__ int pos_of[3];   // position m -> first position with the same block
+  __shared__ double warpA[RT / 32][RB][3], warpB[RT / 32][4][3], warpC[RT / 32][2][3];
 
   const int tid = threadIdx.x;
   const int64_t cta = blockIdx.x;
-  const int S[3] = {table[3 * cta], table[3 * cta + 1], table[3 * cta + 2]};
-  // slots are uniform across the CTA: compute them in registers everywhere
+  const int S0 = table[3 * cta], S1 = table[3 * cta + 1], S2 = table[3 * cta + 2];
+  auto Sm = [&](int m) { return sel3(m, S0, S1, S2); };
+  // slot[p]: first permutation whose ordered block triple equals O_p (uniform)
   int slot[6];
 #pragma unroll
-  for (int sg = 0; sg < 6; sg++) {
-    slot[sg] = sg;
+  for (int p = 0; p < 6; p++) {
+    slot[p] = p;
 #pragma unroll
-    for (int s2 = 0; s2 < 6; s2++) {
-      if (s2 < sg && slot[sg] == sg && S[c_perm[s2][0]] == S[c_perm[sg][0]] && S[c_perm[s2][1]] == S[c_perm[sg][1]] &&
-          S[c_perm[s2][2]] == S[c_perm[sg][2]])
-        slot[sg] = s2;
-    }
+    for (int q = 5; q >= 0; q--)
+      if (q < p && Sm(pm(q, 0)) == Sm(pm(p, 0)) && Sm(pm(q, 1)) == Sm(pm(p, 1)) && Sm(pm(q, 2)) == Sm(pm(p, 2)))
+        slot[p] = q;
   }
-  if (tid < 6) slot_of[tid] = slot[tid];
-  if (tid < 3) pos_of[tid] = (S[0] == S[tid]) ? 0 : ((S[1] == S[tid]) ? 1 : 2);
-  if (tid < 3 * RB * 3) (&vloc[0][0][0])[tid] = 0.0;
 
-  const int nterm = t.kind == kIJK ? 3 : 4;
-  const int64_t nu2 = (int64_t)nu * nu;
-  const double *planes[6] = {
-      voe + ((int64_t)t.k * no + t.j) * nu2, voe + ((int64_t)t.j * no + t.k) * nu2,   // jk, kj
-      voe + ((int64_t)t.k * no + t.i) * nu2, voe + ((int64_t)t.i * no + t.k) * nu2,   // ik, ki
-      voe + ((int64_t)t.j * no + t.i) * nu2, voe + ((int64_t)t.i * no + t.j) * nu2};  // ij, ji
-
-  // ---- phase 1: issue every global load of this CTA (X terms, staged VOE)
-  double xv[6][4][2];
-  double vv[6][2];
+  // ---- phase A: W on the orbit blocks, one X term at a time
 #pragma unroll
-  for (int sg = 0; sg < 6; sg++) {
-    const bool live = slot[sg] == sg;
-    const int O[3] = {S[c_perm[sg][0]], S[c_perm[sg][1]], S[c_perm[sg][2]]};
+  for (int term = 0; term < NTERM; term++) {
+    constexpr int dummy = 0;
+    (void)dummy;
+    const int g = term_entry(KIND, term, 0);
+    const int al0 = term_entry(KIND, term, 1), al1 = term_entry(KIND, term, 2), al2 = term_entry(KIND, term, 3);
+    const double *X = t.x[0];
+    if (g == 1) X = t.x[1];
+    if (g == 2) X = t.x[2];
+    double xv[6][2];
 #pragma unroll
-    for (int term = 0; term < 4; term++) {
-      const int *tm = c_terms[t.kind][term];
-      const double *X = t.x[tm[0]];
+    for (int p = 0; p < 6; p++) {
+      const bool live = slot[p] == p;
+      const int O0 = Sm(pm(p, 0)), O1 = Sm(pm(p, 1)), O2 = Sm(pm(p, 2));
+      const int Oa0 = sel3(al0, O0, O1, O2), Oa1 = sel3(al1, O0, O1, O2), Oa2 = sel3(al2, O0, O1, O2);
 #pragma unroll
       for (int e = 0; e < 2; e++) {
         const int idx = tid + RT * e;
-        const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;  // u2: X's contiguous index
-        const int xp = RB * O[tm[1]] + u0, xq = RB * O[tm[2]] + u1, xs = RB * O[tm[3]] + u2;
+        const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;  // u2: contiguous X index
+        const int xp = RB * Oa0 + u0, xq = RB * Oa1 + u1, xs = RB * Oa2 + u2;
         double v = 0.0;
-        if (live && term < nterm && xp < nu && xq < nu && xs < nu) v = X[((int64_t)xp * nu + xq) * NP + xs];
-        xv[sg][term][e] = v;
+        if (live && xp < nu && xq < nu && xs < nu) v = __ldg(X + ((int64_t)xp * nu + xq) * NP + xs);
+        xv[p][e] = v;
       }
     }
 #pragma unroll
-    for (int e = 0; e < 2; e++) {
-      const int q = tid + RT * e;  // < 512; only q < VSL used
-      const int plane = q >> 6, pair = q & 63;
-      const int b = RB * O[1] + (pair & 7), c = RB * O[2] + (pair >> 3);
+    for (int p = 0; p < 6; p++) {
+      if (slot[p] != p) continue;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int idx = tid + RT * e;
+        const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
+        const int so = u0 * kstride(al0) + u1 * kstride(al1) + u2 * kstride(al2);
+        double *w = Wsm + p * SL + so;
+        if (term == 0)
+          *w = xv[p][e];
+        else
+          *w += xv[p][e];
+      }
+    }
+    __syncthreads();
+  }
+  {
+    const int64_t nu2 = (int64_t)nu * nu;
+    for (int q = tid; q < 3 * VPAIR; q += RT) {
+      const int pr = q / VPAIR, plane = (q / 64) % 6, r = q & 63;
+      const int B1 = pr == 0 ? S1 : S0, B2 = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
+      const int f = RB * B1 + (r & 7), s2 = RB * B2 + (r >> 3);
+      const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
+      const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
       double v = 0.0;
-      if (live && q < VSL && b < nu && c < nu) v = planes[plane][b + (int64_t)nu * c];
-      vv[sg][e] = v;
+      if (f < nu && s2 < nu) v = voe[((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2];
+      Vsm[q] = v;
     }
   }
-
-  // ---- phase 2: assemble W in shared memory, one term at a time (fixed order)
-#pragma unroll
-  for (int term = 0; term < 4; term++) {
-    if (term < nterm) {
-#pragma unroll
-      for (int sg = 0; sg < 6; sg++) {
-        if (slot[sg] != sg) continue;
-        const int *tm = c_terms[t.kind][term];
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int idx = tid + RT * e;
-          const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
-          int l[3];
-          l[tm[1]] = u0;
-          l[tm[2]] = u1;
-          l[tm[3]] = u2;
-          double *w = Wsm + sg * SL + soff(l[0], l[1], l[2]);
-          if (term == 0)
-            *w = xv[sg][term][e];
-          else
-            *w += xv[sg][term][e];
-        }
-      }
-      __syncthreads();
-    }
-  }
-#pragma unroll
-  for (int sg = 0; sg < 6; sg++) {
-    if (slot[sg] != sg) continue;
-#pragma unroll
-    for (int e = 0; e < 2; e++) {
-      const int q = tid + RT * e;
-      if (q < VSL) Vsm[sg * VSL + q] = vv[sg][e];
-    }
-  }
-  // W_aaa = 0 (ZEROT3): only the all-equal block triple holds diagonal elements
-  if (S[0] == S[1] && S[1] == S[2] && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;
+  if (S0 == S1 && S1 == S2 && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;  // W_aaa = 0 (ZEROT3)
   __syncthreads();
 
-  // ---- phase 3: energy and v1 contributions, all from shared memory
-  const int warp = tid >> 5, lane = tid & 31;
+  // ---- phase B: orbits
   const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
   double x3 = 0.0;
-  for (int sg = 0; sg < 6; sg++) {
-    if (slot_of[sg] != sg) continue;
-    const int *sp = c_perm[sg];
-    const int O[3] = {S[sp[0]], S[sp[1]], S[sp[2]]};
-    const int l0 = warp;
-    const int a = RB * O[0] + l0;
-    const double epa = a < nu ? ep[a] : 0.0;
-    double ci = 0.0, cj = 0.0, ck = 0.0;
+  double accA[3] = {0.0, 0.0, 0.0}, accB[3] = {0.0, 0.0, 0.0}, accC[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  const int l0 = tid & 7, l1 = (tid >> 3) & 7;
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int pi = lane + 32 * h;
-      const int l1 = pi & 7, l2 = pi >> 3;
-      const int b = RB * O[1] + l1, c = RB * O[2] + l2;
-      if (a < nu && b < nu && c < nu) {
-        const int lc[3] = {l0, l1, l2};
-        double w[6];
+  for (int e = 0; e < 2; e++) {
+    const int l2 = (tid >> 6) + 4 * e;
+    const int a = RB * S0 + l0, b = RB * S1 + l1, c = RB * S2 + l2;
+    bool take = a < nu && b < nu && c < nu && !(a == b && b == c);
+    if (S0 == S1 && l0 > l1) take = false;  // the orbit is counted from its a<=b member
+    if (S1 == S2 && l1 > l2) take = false;  // ... and from its b<=c member
+    if (!take) continue;
+    const double mult = (a == b || b == c) ? 0.5 : 1.0;  // three distinct elements, each met twice
+    const int lc[3] = {l0, l1, l2};
+    double w[6];
 #pragma unroll
-        for (int pp = 0; pp < 6; pp++) {
-          const int *pi3 = c_perm[pp];
-          const int comp = perm_index(sp[pi3[0]], sp[pi3[1]]);  // block of the permuted element
-          w[pp] = Wsm[slot_of[comp] * SL + soff(lc[pi3[0]], lc[pi3[1]], lc[pi3[2]])];
-        }
-        // w[0]=abc w[1]=acb w[2]=bac w[3]=bca w[4]=cab w[5]=cba
-        const double wabc = w[0], wacb = w[1], wbac = w[2], wbca = w[3], wcab = w[4], wcba = w[5];
-        const double dinv = 1.0 / (dijk - (epa + ep[b] + ep[c]));
-        x3 += wabc * (8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab)) * dinv;
-        const double z1 = (wabc - wbac) * 2.0 - wacb + wbca;
-        const double z2 = (wacb - wbca) * 2.0 - wabc + wbac;
-        const double z3 = (wbac - wabc) * 2.0 - wcab + wcba;
-        const double z4 = (wbca - wacb) * 2.0 - wcba + wcab;
-        const double z5 = (wcab - wcba) * 2.0 - wbac + wabc;
-        const double z6 = (wcba - wcab) * 2.0 - wbca + wacb;
-        const double *vs = Vsm + sg * VSL + pi;
-        ci += (z1 * vs[0] + z2 * vs[64]) * dinv;
-        cj += (z3 * vs[128] + z5 * vs[192]) * dinv;
-        ck += (z4 * vs[256] + z6 * vs[320]) * dinv;
+    for (int p = 0; p < 6; p++)
+      w[p] = Wsm[slot[p] * SL + soff(lc[pm(p, 0)], lc[pm(p, 1)], lc[pm(p, 2)])];
+    const double dinv = mult * __drcp_rn(dijk - (ep[a] + ep[b] + ep[c]));
+    // VOE values of the three index pairs, all six planes
+    double vo[3][6];
+    const int rp[3] = {l1 + 8 * l2, l0 + 8 * l2, l0 + 8 * l1};
+#pragma unroll
+    for (int pr = 0; pr < 3; pr++)
+#pragma unroll
+      for (int pl = 0; pl < 6; pl++) vo[pr][pl] = Vsm[pr * VPAIR + pl * 64 + rp[pr]];
+#pragma unroll
+    for (int pi = 0; pi < 6; pi++) {
+      // element pi(x); its role values: abc acb bac bca cab cba
+      const double wabc = w[compose(pi, 0)], wacb = w[compose(pi, 1)], wbac = w[compose(pi, 2)];
+      const double wbca = w[compose(pi, 3)], wcab = w[compose(pi, 4)], wcba = w[compose(pi, 5)];
+      x3 += wabc * (8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab)) * dinv;
+      const double z1 = (wabc - wbac) * 2.0 - wacb + wbca;
+      const double z2 = (wacb - wbca) * 2.0 - wabc + wbac;
+      const double z3 = (wbac - wabc) * 2.0 - wcab + wcba;
+      const double z4 = (wbca - wacb) * 2.0 - wcba + wcab;
+      const double z5 = (wcab - wcba) * 2.0 - wbac + wabc;
+      const double z6 = (wcba - wcab) * 2.0 - wbca + wacb;
+      // the element's first index is x_{pm(pi,0)}; its (second, third) pair is the
+      // other two coordinates, in order (pm(pi,1), pm(pi,2))
+      const int first = pm(pi, 0);
+      const int pr = first;                         // pair index = the coordinate left out
+      const int flip = pm(pi, 1) > pm(pi, 2) ? 1 : 0;
+      const double *v = vo[pr];
+      const double ci = (z1 * v[0 ^ flip] + z2 * v[1 ^ flip]) * dinv;
+      const double cj = (z3 * v[2 ^ flip] + z5 * v[3 ^ flip]) * dinv;
+      const double ck = (z4 * v[4 ^ flip] + z6 * v[5 ^ flip]) * dinv;
+      if (first == 0) {
+        accA[0] += ci; accA[1] += cj; accA[2] += ck;
+      } else if (first == 1) {
+        accB[0] += ci; accB[1] += cj; accB[2] += ck;
+      } else {
+        accC[e][0] += ci; accC[e][1] += cj; accC[e][2] += ck;
       }
     }
+  }
+  // ---- phase C: fixed-order sums.  Lane layout: l0 = lane & 7,
+  // l1 = (lane >> 3) + 4 (warp & 1), l2 = (warp >> 1) + 4 e.
+  const int warp = tid >> 5, lane = tid & 31;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      ci += __shfl_down_sync(0xffffffffu, ci, off);
-      cj += __shfl_down_sync(0xffffffffu, cj, off);
-      ck += __shfl_down_sync(0xffffffffu, ck, off);
+  for (int q = 0; q < 3; q++) {
+    double va = accA[q], vb = accB[q], vc0 = accC[0][q], vc1 = accC[1][q];
+    va += __shfl_xor_sync(0xffffffffu, va, 8);
+    va += __shfl_xor_sync(0xffffffffu, va, 16);  // sum over lanes with equal l0
+    vb += __shfl_xor_sync(0xffffffffu, vb, 1);
+    vb += __shfl_xor_sync(0xffffffffu, vb, 2);
+    vb += __shfl_xor_sync(0xffffffffu, vb, 4);   // sum over lanes with equal l1
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      vc0 += __shfl_xor_sync(0xffffffffu, vc0, off);
+      vc1 += __shfl_xor_sync(0xffffffffu, vc1, off);
     }
+    if (lane < RB) warpA[warp][lane][q] = va;
+    if ((lane & 7) == 0) warpB[warp][lane >> 3][q] = vb;
     if (lane == 0) {
-      const int pos = pos_of[sp[0]];
-      vloc[pos][l0][0] += ci;
-      vloc[pos][l0][1] += cj;
-      vloc[pos][l0][2] += ck;
+      warpC[warp][0][q] = vc0;
+      warpC[warp][1][q] = vc1;
     }
   }
-
-  // ---- CTA partials: warp trees then a fixed-order sum of the 8 warp values
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) x3 += __shfl_down_sync(0xffffffffu, x3, off);
   if (lane == 0) red[warp] = x3;
   __syncthreads();
+
   if (tid == 0) {
-    double s = 0.0;
-    for (int w = 0; w < RT / 32; w++) s += red[w];
-    xpart[cta] = s;
+    double sum = 0.0;
+    for (int w2 = 0; w2 < RT / 32; w2++) sum += red[w2];
+    xpart[cta] = sum;
   }
-  if (tid < 3 * RB * 3) vpart[cta * 72 + tid] = (&vloc[0][0][0])[tid];
+  // v1 partials: position pos (first of equal blocks) collects every coordinate m
+  // whose block equals it; written to vslab[X][l][col][q], q = the pair of the
+  // other two blocks, so every (block, pair) slot has exactly one writer.
+  if (tid < 72) {
+    const int pos = tid / 24, l = (tid / 3) % 8, col = tid % 3;
+    const int posm[3] = {0, S1 == S0 ? 0 : 1, S2 == S0 ? 0 : (S2 == S1 ? 1 : 2)};
+    if (posm[pos] == pos) {
+      double v = 0.0;
+#pragma unroll
+      for (int m = 0; m < 3; m++) {
+        if (posm[m] != pos) continue;
+        if (m == 0) {
+          for (int w2 = 0; w2 < RT / 32; w2++) v += warpA[w2][l][col];
+        } else if (m == 1) {
+          for (int w2 = (l >> 2); w2 < RT / 32; w2 += 2) v += warpB[w2][l & 3][col];
+        } else {
+          for (int w2 = 2 * (l & 3); w2 < 2 * (l & 3) + 2; w2++) v += warpC[w2][l >> 2][col];
+        }
+      }
+      const int X = pos == 0 ? S0 : (pos == 1 ? S1 : S2);
+      const int Y = pos == 0 ? S1 : S0, Z = pos == 2 ? S1 : S2;  // the other two, Y <= Z
+      const int64_t npairs = (int64_t)nb_of(nu) * (nb_of(nu) + 1) / 2;
+      const int64_t q = (int64_t)Z * (Z + 1) / 2 + Y;
+      vpart[(((int64_t)X * RB + l) * 3 + col) * npairs + q] = v;
+    }
+  }
 }
 
 // etd_acc[0..1]: Neumaier (sum, compensation); v1_acc(nu, no).
@@ -254,37 +302,21 @@ __global__ void finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t, const 
   const int a = ((blockIdx.x - 1) * blockDim.x + tid) >> 5;
   if (a >= nu) return;
   const int X = a / RB, la = a - (a / RB) * RB;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  int q = 0;
-  for (int Y = 0; Y < nb; Y++) {
-    for (int Z = Y; Z < nb; Z++, q++) {
-      if ((q & 31) != lane) continue;
-      int A, B, C;
-      if (X <= Y) {
-        A = X; B = Y; C = Z;
-      } else if (X <= Z) {
-        A = Y; B = X; C = Z;
-      } else {
-        A = Y; B = Z; C = X;
-      }
-      const int64_t idx = (int64_t)C * (C + 1) * (C + 2) / 6 + (int64_t)B * (B + 1) / 2 + A;
-      const int pos = (A == X) ? 0 : ((B == X) ? 1 : 2);
-      const double *vp = vpart + idx * 72 + pos * 24 + la * 3;
-      s0 += vp[0];
-      s1 += vp[1];
-      s2 += vp[2];
-    }
-  }
+  const int64_t npairs = (int64_t)nb * (nb + 1) / 2;
+  const double *slab = vpart + ((int64_t)X * RB + la) * 3 * npairs;
+  double sc[3];
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    s0 += __shfl_down_sync(0xffffffffu, s0, off);
-    s1 += __shfl_down_sync(0xffffffffu, s1, off);
-    s2 += __shfl_down_sync(0xffffffffu, s2, off);
+  for (int col = 0; col < 3; col++) {
+    double v = 0.0;
+    for (int64_t q = lane; q < npairs; q += 32) v += slab[col * npairs + q];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    sc[col] = v;
   }
   if (lane == 0) {
-    v1_acc[a + (int64_t)nu * t.i] += t.weight * s0;
-    v1_acc[a + (int64_t)nu * t.j] += t.weight * s1;
-    v1_acc[a + (int64_t)nu * t.k] += t.weight * s2;
+    v1_acc[a + (int64_t)nu * t.i] += t.weight * sc[0];
+    v1_acc[a + (int64_t)nu * t.j] += t.weight * sc[1];
+    v1_acc[a + (int64_t)nu * t.k] += t.weight * sc[2];
   }
 }
 
@@ -316,19 +348,27 @@ __global__ void ets_kernel(int no, int nu, const double *__restrict__ t1, const 
 
 }  // namespace
 
-int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
-                  const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
-  constexpr int smem = (6 * SL + 6 * VSL) * 8;
+template <int KIND>
+int launch_reduce_kind(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
+                       const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
   static int configured_device = -1;
   int dev = 0;
   CCT_CUDA(cudaGetDevice(&dev));
   if (configured_device != dev) {
-    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, REDUCE_SMEM));
     configured_device = dev;
   }
-  reduce_kernel<<<(unsigned)d.ncta, RT, smem, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart, vpart);
+  reduce_kernel<KIND><<<(unsigned)d.ncta, RT, REDUCE_SMEM, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart,
+                                                               vpart);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
+}
+
+int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
+                  const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
+  if (t.kind == kIJK) return launch_reduce_kind<kIJK>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+  if (t.kind == kIJJ) return launch_reduce_kind<kIJJ>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+  return launch_reduce_kind<kIIJ>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
 }
 
 int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const double *vpart, double *etd_acc,
