@@ -1,6 +1,7 @@
 // Internal declarations shared by the libcc_b200 translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -91,6 +92,42 @@ struct TupleDev {
   int kind, i, j, k;
   double weight;        // 1 for i>j>k, 1/2 for degenerate tuples
 };
+
+// ----------------------------------------------------------------------------- INT8 emulation
+// Digit count of the split-integer operands (7 bits each).  Measured on the
+// no=24/nu=320 workload: |dE|/|E| = 1.7e-7 (4 digits), 1.6e-9 (5), 1.4e-13 (7).
+constexpr int kEmuMinSlices = 4, kEmuMaxSlices = 7, kEmuDefaultSlices = 5;
+constexpr int kEmuBN = 64;  // N tile of the emulated W-build
+
+// One emulated W-build GEMM: half h multiplies E-digit rows (half 0: E[x1] rows
+// (p,q); half 1: E^T[x2] rows (p,q) = E[x2] rows (q,p)) with F-digit rows of
+// F[fyz[h] / no][fyz[h] % no].
+struct EmuJob {
+  int x1, x2;
+  int fyz[2];
+  double *out;
+  int nhalves;
+  int x3;  // the index both halves' F rows share: fyz[h] = (x2|x1) * no + x3
+};
+
+// Split-integer operands of one plan.
+struct EmuOperands {
+  int slices = kEmuDefaultSlices;
+  int64_t KP8 = 0;                           // digit row length: round_up(nu+no, 32)
+  int8_t *E8 = nullptr, *E8T = nullptr;      // [slice][x][r1][r2][KP8], and r1<->r2
+  int8_t *F8 = nullptr;                      // [slice][y][z][NP][KP8]
+  // Digit scales shared by both halves of a GEMM, so one set of diagonal
+  // accumulators serves the whole contraction: expE[p*nu+q] (symmetric) is the
+  // largest row exponent of E[x][p][q] and E[x][q][p] over all x; expF[z*NP+n]
+  // the largest of F[y][z][n] over all y.  expET and expRowF hold the per-row
+  // exponents they are reduced from.
+  int16_t *expE = nullptr, *expET = nullptr, *expF = nullptr, *expRowF = nullptr;
+  CUtensorMap mapE, mapET, mapF;
+};
+
+int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOperands *o, cudaStream_t s);
+int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
+                      cudaStream_t s);
 
 // ----------------------------------------------------------------------------- launchers
 // layout.cu

@@ -39,6 +39,10 @@ std::vector<Tuple> tuple_list(int no) {
 
 using namespace cct;
 
+// X buffer sets: the W-build of tuple t may run while the reductions of
+// tuples t-1 .. t-kNBuf+1 are still reading theirs.
+constexpr int kNBuf = 3;
+
 struct ccT_plan {
   int device = 0;
   ccT_options opt{};
@@ -48,18 +52,21 @@ struct ccT_plan {
   cudaStream_t gemm_stream = nullptr; // W-build GEMMs, highest priority
   cudaStream_t red_stream = nullptr;  // reductions, lowest priority: they fill GEMM tail waves
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaEvent_t ev_gemm[2] = {nullptr, nullptr}, ev_red[2] = {nullptr, nullptr};
+  cudaEvent_t ev_gemm[kNBuf] = {}, ev_red[kNBuf] = {};
   int64_t tick = 0;                   // tuples issued so far: selects the X buffer
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // inputs (device copies, reference layouts)
   double *eh = nullptr, *ep = nullptr, *t1 = nullptr, *t2 = nullptr, *vm = nullptr, *voe = nullptr;
   // derived operands
   double *E = nullptr, *F = nullptr;
-  double *X[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // double-buffered GEMM outputs
+  double *X[kNBuf][3] = {};  // GEMM outputs, kNBuf tuples in flight
   double *xpart = nullptr, *vpart = nullptr;
   int16_t *cta_table = nullptr;
   double *acc = nullptr;  // [etd_sum, etd_comp, out3[3], v1(nu*no)]
   GemmJob *jobs = nullptr;  // [buffer][tuple][3]
+  bool emulated = false;    // INT8 split-integer W-build
+  EmuOperands emu;
+  EmuJob *emu_jobs = nullptr;  // [buffer][tuple][3]
   int *flags = nullptr;
   double *stage = nullptr;  // packed-slice staging for the legacy hook
   std::vector<Tuple> tuples;
@@ -110,8 +117,8 @@ int build_jobs(ccT_plan *p) {
     return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 0};
   };
   std::vector<GemmJob> jobs;
-  jobs.reserve(p->tuples.size() * 6);
-  for (buf = 0; buf < 2; buf++)
+  jobs.reserve(p->tuples.size() * 3 * kNBuf);
+  for (buf = 0; buf < kNBuf; buf++)
   for (const Tuple &t : p->tuples) {
     if (t.kind == kIJK) {
       jobs.push_back(G(t.i, t.j, t.k, 0));
@@ -128,6 +135,24 @@ int build_jobs(ccT_plan *p) {
     }
   }
   CCT_CUDA(cudaMemcpy(p->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
+  if (p->emulated) {
+    // same jobs for the split-integer kernel: half 0 E[x1] x F[x2][x3], half 1 E^T[x2] x F[x1][x3]
+    std::vector<EmuJob> ej(jobs.size());
+    for (size_t q = 0; q < jobs.size(); q++) {
+      const GemmJob &g = jobs[q];
+      const int64_t slab = nu2 * d.KP, fslab = d.NP * d.KP;
+      EmuJob e{};
+      e.x1 = (int)((g.a0 - p->E) / slab);
+      e.x2 = (int)((g.a1 - p->E) / slab);
+      e.fyz[0] = (int)((g.b0 - p->F) / fslab);
+      e.fyz[1] = (int)((g.b1 - p->F) / fslab);
+      e.out = g.out;
+      e.nhalves = g.nhalves;
+      e.x3 = e.fyz[0] % d.no;  // half 0 reads F[x2][x3], half 1 F[x1][x3]
+      ej[q] = e;
+    }
+    CCT_CUDA(cudaMemcpy(p->emu_jobs, ej.data(), ej.size() * sizeof(EmuJob), cudaMemcpyHostToDevice));
+  }
   return CCT_OK;
 }
 
@@ -210,12 +235,16 @@ int join_streams(ccT_plan *p) {
 int run_tuple(ccT_plan *p, int64_t tix) {
   const Tuple &t = p->tuples[tix];
   const int njobs = t.kind == kIJK ? 3 : 2;
-  const int b = (int)(p->tick & 1);
+  const int b = (int)(p->tick % kNBuf);
   p->tick++;
   const int64_t ntup = (int64_t)p->tuples.size();
   CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[b], 0));
   CCT_TRY(prof_mark(p, CCT_KERNEL_WBUILD, p->gemm_stream));
-  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, p->gemm_stream));
+  if (p->emulated)
+    CCT_TRY(launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1,
+                              p->gemm_stream));
+  else
+    CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, p->gemm_stream));
   CCT_TRY(prof_mark(p, -1, p->gemm_stream));
   CCT_CUDA(cudaEventRecord(p->ev_gemm[b], p->gemm_stream));
   CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_gemm[b], 0));
@@ -299,9 +328,11 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     set_error("unknown precision");
     return CCT_ERR_INVALID;
   }
-  if (o.precision == CCT_PREC_INT8_EMU) {
-    set_error("INT8-emulated precision is not built in this library version");
-    return CCT_ERR_UNSUPPORTED;
+  if (o.precision == CCT_PREC_INT8_EMU &&
+      o.emu_slices != 0 && (o.emu_slices < kEmuMinSlices || o.emu_slices > kEmuMaxSlices)) {
+    set_error("emu_slices must be 0 (default) or in [" + std::to_string(kEmuMinSlices) + ", " +
+              std::to_string(kEmuMaxSlices) + "]");
+    return CCT_ERR_INVALID;
   }
   int ndev = 0;
   CCT_CUDA(cudaGetDeviceCount(&ndev));
@@ -317,7 +348,8 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   d.no = (int)no;
   d.nu = (int)nu;
   d.KP = round_up(nu + no, kKB);
-  d.BN = choose_bn(nu);
+  p->emulated = o.precision == CCT_PREC_INT8_EMU;
+  d.BN = p->emulated ? kEmuBN : choose_bn(nu);
   d.NP = round_up(nu, d.BN);
   d.nb = (int)((nu + kRB - 1) / kRB);
   d.ncta = (int64_t)d.nb * (d.nb + 1) * (d.nb + 2) / 6;
@@ -331,24 +363,39 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) return fail(CCT_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithPriority(&p->gemm_stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess ||
-      cudaStreamCreateWithPriority(&p->red_stream, cudaStreamNonBlocking, prio_least) != cudaSuccess)
+      cudaStreamCreateWithPriority(&p->red_stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess)
     return fail(CCT_ERR_CUDA);
   p->stream = p->own_stream;
-  for (cudaEvent_t *e : {&p->ev_fork, &p->ev_join, &p->ev_gemm[0], &p->ev_gemm[1], &p->ev_red[0], &p->ev_red[1]})
+  for (cudaEvent_t *e : {&p->ev_fork, &p->ev_join})
     if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return fail(CCT_ERR_CUDA);
+  for (int b = 0; b < kNBuf; b++)
+    if (cudaEventCreateWithFlags(&p->ev_gemm[b], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_red[b], cudaEventDisableTiming) != cudaSuccess)
+      return fail(CCT_ERR_CUDA);
   if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) return fail(CCT_ERR_CUDA);
   const int64_t nu2 = nu * nu;
   if ((s = dalloc(&p->eh, no)) || (s = dalloc(&p->ep, nu)) || (s = dalloc(&p->t1, no * nu)) ||
       (s = dalloc(&p->t2, nu2 * no * no)) || (s = dalloc(&p->vm, no * nu * no * no)) ||
       (s = dalloc(&p->voe, nu2 * no * no)) || (s = dalloc(&p->E, no * nu2 * d.KP)) ||
-      (s = dalloc(&p->F, no * no * d.NP * d.KP)) || (s = dalloc(&p->X[0][0], nu2 * d.NP)) ||
-      (s = dalloc(&p->X[0][1], nu2 * d.NP)) || (s = dalloc(&p->X[0][2], nu2 * d.NP)) ||
-      (s = dalloc(&p->X[1][0], nu2 * d.NP)) || (s = dalloc(&p->X[1][1], nu2 * d.NP)) ||
-      (s = dalloc(&p->X[1][2], nu2 * d.NP)) ||
+      (s = dalloc(&p->F, no * no * d.NP * d.KP)) ||
       (s = dalloc(&p->xpart, d.ncta)) || (s = dalloc(&p->vpart, (int64_t)12 * d.nb * d.nb * (d.nb + 1))) ||
       (s = dalloc(&p->cta_table, d.ncta * 3)) || (s = dalloc(&p->acc, 5 + nu * no)) ||
-      (s = dalloc(&p->jobs, p->tuples.size() * 6)) || (s = dalloc(&p->flags, 4)))
+      (s = dalloc(&p->jobs, p->tuples.size() * 3 * kNBuf)) || (s = dalloc(&p->flags, 4)))
     return fail(s);
+  for (int b = 0; b < kNBuf; b++)
+    for (int g = 0; g < 3; g++)
+      if ((s = dalloc(&p->X[b][g], nu2 * d.NP))) return fail(s);
+  if (p->emulated) {
+    EmuOperands &e = p->emu;
+    e.slices = o.emu_slices ? o.emu_slices : kEmuDefaultSlices;
+    e.KP8 = round_up(nu + no, 32);
+    const int64_t rowsE = no * nu2, rowsF = no * no * d.NP;
+    if ((s = dalloc(&e.E8, e.slices * rowsE * e.KP8)) || (s = dalloc(&e.E8T, e.slices * rowsE * e.KP8)) ||
+        (s = dalloc(&e.F8, e.slices * rowsF * e.KP8)) || (s = dalloc(&e.expE, rowsE)) ||
+        (s = dalloc(&e.expET, rowsE)) || (s = dalloc(&e.expF, rowsF)) || (s = dalloc(&e.expRowF, rowsF)) ||
+        (s = dalloc(&p->emu_jobs, p->tuples.size() * 3 * kNBuf)))
+      return fail(s);
+  }
   std::vector<int16_t> table(d.ncta * 3);
   int64_t idx = 0;
   for (int C = 0; C < d.nb; C++)
@@ -408,6 +455,7 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   }
   if (s == CCT_OK) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
+  if (s == CCT_OK && p->emulated) s = emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
   if (staged) cudaFreeAsync(staged, p->stream);
   if (s != CCT_OK) return s;
   p->host_eh.resize(no);
@@ -448,6 +496,7 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   const Dims &d = p->d;
   p->last_launches = 0;
   CCT_CUDA(cudaMemsetAsync(p->acc, 0, (5 + (int64_t)d.nu * d.no) * 8, p->stream));
+  CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
   CCT_TRY(fork_streams(p));
   for (int64_t t = begin; t < end; t++) CCT_TRY(run_tuple(p, t));
@@ -456,6 +505,8 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   p->last_launches += 1;
   CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
   double out3[3];
+  int werr = 0;
+  CCT_CUDA(cudaMemcpyAsync(&werr, p->flags + 1, 4, cudaMemcpyDeviceToHost, p->stream));
   CCT_CUDA(cudaMemcpyAsync(out3, p->acc + 2, 3 * 8, cudaMemcpyDeviceToHost, p->stream));
   if (v1_out)
     CCT_CUDA(cudaMemcpyAsync(v1_out, v1_acc(p), (int64_t)d.nu * d.no * 8, cudaMemcpyDeviceToHost, p->stream));
@@ -464,6 +515,10 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   CCT_TRY(prof_collect(p));
   if (ets) *ets = out3[0];
   if (etd) *etd = out3[1];
+  if (werr) {
+    set_error("an emulated W-build kernel ran out its bounded wait and unwound");
+    return CCT_ERR_TIMEOUT;
+  }
   if (!std::isfinite(out3[0]) || !std::isfinite(out3[1])) {
     set_error("E(T) is not finite");
     return CCT_ERR_NONFINITE;
@@ -499,9 +554,13 @@ int ccT_time_wbuild(ccT_plan *p, int64_t tuple, int32_t reps, double *ms_per_lau
   const int njobs = p->tuples[tuple].kind == kIJK ? 3 : 2;
   CCT_TRY(fork_streams(p));
   CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[0], 0));
-  CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream));  // warm
+  auto launch = [&]() {
+    return p->emulated ? launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * tuple, njobs, p->flags + 1, p->gemm_stream)
+                       : launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream);
+  };
+  CCT_TRY(launch());  // warm
   CCT_CUDA(cudaEventRecord(p->ev0, p->gemm_stream));
-  for (int r = 0; r < reps; r++) CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream));
+  for (int r = 0; r < reps; r++) CCT_TRY(launch());
   CCT_CUDA(cudaEventRecord(p->ev1, p->gemm_stream));
   CCT_CUDA(cudaEventRecord(p->ev_red[0], p->gemm_stream));  // later writers of buffer 0 follow these
   CCT_CUDA(cudaEventSynchronize(p->ev1));
@@ -539,19 +598,27 @@ int ccT_plan_destroy(ccT_plan *p) {
   DeviceGuard guard(p->device);
   for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream})
     if (st) cudaStreamSynchronize(st);
-  double *bufs[] = {p->eh,      p->ep,      p->t1,      p->t2,      p->vm,      p->voe,  p->E,     p->F,
-                    p->X[0][0], p->X[0][1], p->X[0][2], p->X[1][0], p->X[1][1], p->X[1][2], p->xpart, p->vpart,
-                    p->acc,     p->stage};
+  double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->xpart, p->vpart, p->acc, p->stage};
   for (double *b : bufs)
     if (b) cudaFree(b);
+  for (int b = 0; b < kNBuf; b++)
+    for (int g = 0; g < 3; g++)
+      if (p->X[b][g]) cudaFree(p->X[b][g]);
   if (p->cta_table) cudaFree(p->cta_table);
   if (p->jobs) cudaFree(p->jobs);
   if (p->flags) cudaFree(p->flags);
+  for (void *b : {(void *)p->emu.E8, (void *)p->emu.E8T, (void *)p->emu.F8, (void *)p->emu.expE,
+                  (void *)p->emu.expET, (void *)p->emu.expF, (void *)p->emu.expRowF, (void *)p->emu_jobs})
+    if (b) cudaFree(b);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);
-  for (cudaEvent_t e : {p->ev_fork, p->ev_join, p->ev_gemm[0], p->ev_gemm[1], p->ev_red[0], p->ev_red[1]})
+  for (cudaEvent_t e : {p->ev_fork, p->ev_join})
     if (e) cudaEventDestroy(e);
+  for (int b = 0; b < kNBuf; b++) {
+    if (p->ev_gemm[b]) cudaEventDestroy(p->ev_gemm[b]);
+    if (p->ev_red[b]) cudaEventDestroy(p->ev_red[b]);
+  }
   if (p->gemm_stream) cudaStreamDestroy(p->gemm_stream);
   if (p->red_stream) cudaStreamDestroy(p->red_stream);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);

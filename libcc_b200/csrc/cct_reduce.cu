@@ -356,6 +356,8 @@ int launch_reduce_kind(const Dims &d, const TupleDev &t, const double *eh, const
   CCT_CUDA(cudaGetDevice(&dev));
   if (configured_device != dev) {
     CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, REDUCE_SMEM));
+    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
     configured_device = dev;
   }
   reduce_kernel<KIND><<<(unsigned)d.ncta, RT, REDUCE_SMEM, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart,

@@ -1,0 +1,78 @@
+"""INT8 split-integer emulated FP64 W-build (tcgen05 kind::i8) against the oracle."""
+import numpy as np
+import pytest
+
+from libcc_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _plan(api, inp, slices):
+    from libcc_b200 import _native as N
+    import ctypes
+    lib = N.load()
+    opt = N.Options()
+    lib.ccT_options_default(ctypes.byref(opt))
+    opt.precision = N.CCT_PREC_INT8_EMU
+    opt.emu_slices = slices
+    h = ctypes.c_void_p()
+    N.check(lib.ccT_plan_create(ctypes.byref(h), inp.no, inp.nu, ctypes.byref(opt)), "ccT_plan_create")
+    plan = api.TriplesPlan.__new__(api.TriplesPlan)
+    plan._h, plan.no, plan.nu, plan.precision, plan.device = h, inp.no, inp.nu, "int8", 0
+    plan.num_tuples = int(lib.ccT_num_tuples(inp.no))
+    return plan
+
+
+@pytest.fixture(scope="module")
+def api():
+    from libcc_b200 import api as A
+    return A
+
+
+@pytest.mark.parametrize("no,nu,seed", [(3, 7, 1), (4, 36, 0), (5, 64, 3), (6, 70, 5)])
+def test_emulated_seven_slices_match_oracle(api, no, nu, seed):
+    from oracle import oracle as O
+    inp = S.generate(no, nu, seed)
+    ets_o, etd_o, v1_o = O.c_cc_triples(inp)
+    plan = api.TriplesPlan(no, nu, precision="int8")
+    with plan:
+        plan.set_system(inp)
+        ets, etd, v1 = plan.forward()
+    assert abs(etd - etd_o) <= 1e-11 * abs(etd_o), (etd, etd_o)
+    assert abs(ets - ets_o) <= 1e-9 * abs(ets_o) + 1e-12
+    assert np.abs(v1 - v1_o).max() <= 1e-9 * np.abs(v1_o).max()
+
+
+@pytest.mark.parametrize("slices,rel", [(4, 3e-6), (5, 3e-8), (6, 3e-10), (7, 1e-11)])
+def test_error_falls_with_slice_count(api, slices, rel):
+    inp = S.generate(5, 48, 9, dist="log")
+    with api.TriplesPlan(inp.no, inp.nu) as ref:
+        ref.set_system(inp)
+        _, etd_ref, _ = ref.forward()
+    with _plan(api, inp, slices) as plan:
+        plan.set_system(inp)
+        _, etd, _ = plan.forward()
+    assert abs(etd - etd_ref) <= rel * abs(etd_ref), (slices, etd, etd_ref)
+
+
+def test_emulated_tuple_kinds_and_shards(api):
+    from oracle import oracle as O
+    no, nu = 5, 17
+    inp = S.generate(no, nu, 21)
+    tuples = O.all_tuples(no)
+    with api.TriplesPlan(no, nu, precision="int8") as plan:
+        plan.set_system(inp)
+        for t in (0, 9, 10, 11, len(tuples) - 1):
+            kind, i, j, k = tuples[t]
+            e_ref, v1_ref = O.c_tuple(inp, kind, i, j, k)
+            _, etd, v1 = plan.forward(t, t + 1)
+            assert abs(etd - e_ref) <= 1e-11 * abs(e_ref), (kind, i, j, k)
+
+
+def test_emulated_deterministic(api):
+    inp = S.generate(4, 40, 12)
+    with api.TriplesPlan(inp.no, inp.nu, precision="int8") as plan:
+        plan.set_system(inp)
+        a = plan.forward()
+        b = plan.forward()
+    assert a[1] == b[1] and np.array_equal(a[2], b[2])
