@@ -3,9 +3,12 @@
 
 One step is one full (T) evaluation -- every tuple of the workload, including
 the degenerate (i,j,j)/(i,i,j) tuples -- through the library's plan API, with
-inputs already resident in HBM.  ``e2e`` repeats the step through the public C
-entry ``cc_triples_b200_`` from pinned host buffers (host->device upload,
-operand build, all tuples, v1/energy read-back).
+inputs already resident in HBM.  Both forms are timed: the native FP64 form
+(mma.sync f64) and the split-integer emulated form (tcgen05 INT8); the
+headline value is the emulated form, the native one is reported beside it with
+the speed-up and the relative energy difference.  ``e2e`` repeats the headline
+step through the C ABI from pinned host buffers (plan create, host->device
+upload, operand build, all tuples, v1/energy read-back, destroy).
 
 Under torchrun (N>1) the tuple list is split into cost-balanced contiguous
 shards, one per rank; the partial (ets, etd) are summed with one NCCL
@@ -41,6 +44,7 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--emu-slices", type=int, default=5, help="7-bit digits per operand of the emulated form (4..7)")
     return ap.parse_args()
 
 
@@ -123,9 +127,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(loaded), "power_w_max": pmax}
 
 
-def read_traffic(workload: str):
+def read_traffic(workload: str, kind: str = "f64"):
     """DRAM bytes per W-build launch from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / f"wbuild_f64_{workload}.txt"
+    f = ROOT / "profiles" / f"wbuild_{kind}_{workload}.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -194,6 +198,26 @@ def run_reference(args, rank, world):
     return 0
 
 
+def make_plan(A, no, nu, device, form):
+    """Plan for one form: 'fp64' (native mma.sync f64) or 'int8:S' (S-digit emulation)."""
+    if form == "fp64":
+        return A.TriplesPlan(no, nu, device=device)
+    import ctypes
+    N = A.N
+    lib = N.load()
+    opt = N.Options()
+    lib.ccT_options_default(ctypes.byref(opt))
+    opt.precision = N.CCT_PREC_INT8_EMU
+    opt.device = device
+    opt.emu_slices = int(form.split(":")[1])
+    h = ctypes.c_void_p()
+    N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
+    plan = A.TriplesPlan.__new__(A.TriplesPlan)
+    plan._h, plan.no, plan.nu, plan.precision, plan.device = h, no, nu, form, device
+    plan.num_tuples = int(lib.ccT_num_tuples(no))
+    return plan
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -204,7 +228,6 @@ def main():
 
     import datetime
 
-    import numpy as np
     import torch
 
     from libcc_b200 import api as A
@@ -226,32 +249,39 @@ def main():
     bounds = shard_bounds(costs, world)
     begin, end = bounds[rank], bounds[rank + 1]
     flop_step = S.flops(no, nu)
-
-    plan = A.TriplesPlan(no, nu, device=local)
+    my_flop_wb = sum(12.0 * nu ** 3 * (no + nu) * c for c in costs[begin:end])
     dev_inputs = [torch.from_numpy(a).to(f"cuda:{local}") for a in inp.arrays()]
-    plan.set_inputs(*dev_inputs)
     stream = torch.cuda.current_stream()
-    plan.set_stream(stream.cuda_stream)
+    N = A.N
+    peaks = {"fp64": N.load().ccT_measure_fp64_peak(local), "int8": N.load().ccT_measure_int8_peak(local)}
+    g = golden(args.workload)
 
-    def step():
-        ets, etd, _ = plan.forward(begin, end, want_v1=False)
-        if dist is not None:
-            t = torch.tensor([ets, etd], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t)
-            ets, etd = t.tolist()
-        return ets, etd
+    def allreduce(vals, op="sum"):
+        if dist is None:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX)
+        return t.tolist()
 
-    for _ in range(args.warmup):
-        step()
+    def run_form(form, sampler):
+        plan = make_plan(A, no, nu, local, form)
+        plan.set_inputs(*dev_inputs)
+        plan.set_stream(stream.cuda_stream)
 
-    plan.set_profiling(True)
-    launches = 0
-    wb_ms, wb_n = 0.0, 0
-    with ClockSampler(local) as clocks:
+        def step():
+            ets, etd, _ = plan.forward(begin, end, want_v1=False)
+            return allreduce([ets, etd])
+
+        for _ in range(args.warmup):
+            step()
+        plan.set_profiling(True)
+        launches, wb_ms, wb_n = 0, 0.0, 0
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler is not None:
+            sampler.__enter__()
         e0.record(stream)
         for _ in range(args.steps):
             ets, etd = step()
@@ -261,41 +291,50 @@ def main():
             wb_n += prof["wbuild"][1]
         e1.record(stream)
         torch.cuda.synchronize()
+        if sampler is not None:
+            sampler.__exit__(None, None, None)
         if dist is not None:
             dist.barrier()
-    plan.set_profiling(False)
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
-    ms_step = ms / args.steps
-    tflops = flop_step / (ms_step * 1e-3) / 1e12
+        plan.close()
+        ms = allreduce([e0.elapsed_time(e1)], op="max")[0]
+        ms_step = ms / args.steps
+        emu = form != "fp64"
+        S_ = int(form.split(":")[1]) if emu else 0
+        # algorithmic work of the W-build launches in the timed region
+        fp64_flop = my_flop_wb * args.steps
+        if emu:
+            ops = fp64_flop * S_ * (S_ + 1) / 2  # INT8 ops: S(S+1)/2 digit products per FP64 multiply-add
+            achieved = ops / (wb_ms * 1e-3) / 1e12 if wb_ms > 0 else None
+            peak, unit, kern = peaks["int8"], "TOPS (int8)", "wbuild_emu_kernel (tcgen05.mma kind::i8, TMA, TMEM)"
+            psrc = ("measured in this run: tcgen05.mma kind::i8 throughput with operands resident in shared memory "
+                    "(ccT_measure_int8_peak); MEASURED_PEAKS.json has no INT8 entry")
+            per_launch = f"{S_ * (S_ + 1) // 2} x 12 nu^3 (no+nu) int8 ops for an i>j>k tuple, half for a degenerate tuple"
+        else:
+            achieved = fp64_flop / (wb_ms * 1e-3) / 1e12 if wb_ms > 0 else None
+            peak, unit, kern = peaks["fp64"], "TFLOP/s", "wbuild_f64_kernel (mma.sync m16n8k4 f64)"
+            psrc = ("measured in this run: mma.sync f64 throughput microbenchmark (ccT_measure_fp64_peak); "
+                    "MEASURED_PEAKS.json has no FP64 entry")
+            per_launch = f"12 nu^3 (no+nu) = {12.0 * nu ** 3 * (no + nu):.4g} flop for an i>j>k tuple, half for a degenerate tuple"
+        out = {"form": form, "ms_per_step": ms_step, "tflops": flop_step / (ms_step * 1e-3) / 1e12,
+               "ets": ets, "etd": etd, "e_t": ets + etd, "gpu_launches": launches,
+               "roofline": {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak, "unit": unit,
+                            "frac": (achieved / peak) if (achieved and peak) else None,
+                            "traffic": read_traffic(args.workload, "emu" if emu else "f64"),
+                            "peak_source": psrc, "launches": wb_n, "avg_launch_ms": wb_ms / max(wb_n, 1),
+                            "work_per_launch": per_launch, "share_of_step": wb_ms / ms if ms > 0 else None}}
+        if g is not None:
+            out["abs_err_vs_oracle"] = abs(out["e_t"] - g["e_t"])
+            out["rel_err_vs_oracle"] = abs(out["e_t"] - g["e_t"]) / abs(g["e_t"])
+        return out
 
-    # roofline of the dominant kernel (W-build GEMM), from the timed region's launches
-    n_ijk = no * (no - 1) * (no - 2) // 6
-    my_flop_wb = sum(12.0 * nu ** 3 * (no + nu) * c for c in costs[begin:end]) * args.steps
-    wb_achieved = my_flop_wb / (wb_ms * 1e-3) / 1e12 if wb_ms > 0 else None
-    peak = plan_peak = A.N.load().ccT_measure_fp64_peak(local)
-    traffic = read_traffic(args.workload)
-    roofline = {"bound": "tensor", "kernel": "wbuild_f64_kernel (mma.sync m16n8k4 f64)",
-                "achieved": wb_achieved, "peak": plan_peak, "unit": "TFLOP/s",
-                "frac": (wb_achieved / peak) if (wb_achieved and peak) else None, "traffic": traffic,
-                "peak_source": "measured in this run: mma.sync f64 throughput microbenchmark "
-                               "(ccT_measure_fp64_peak); MEASURED_PEAKS.json has no FP64 entry",
-                "launches": wb_n, "avg_launch_ms": wb_ms / max(wb_n, 1),
-                "flop_per_launch": f"12 nu^3 (no+nu) = {12.0 * nu ** 3 * (no + nu):.4g} for an i>j>k tuple, half "
-                                   "for a degenerate tuple",
-                "share_of_step": wb_ms / ms if ms > 0 else None}
+    emu_form = f"int8:{args.emu_slices}"
+    clocks = ClockSampler(local)
+    forms = {"fp64": run_form("fp64", None), "int8_emu": run_form(emu_form, clocks)}
+    head = forms["int8_emu"]
+    rel_vs_native = abs(head["e_t"] - forms["fp64"]["e_t"]) / abs(forms["fp64"]["e_t"])
+    head["rel_err_vs_native_fp64"] = rel_vs_native
 
-    # accuracy against the oracle fixture
-    acc = None
-    g = golden(args.workload)
-    if g is not None:
-        acc = {"e_t": ets + etd, "oracle_e_t": g["e_t"], "abs_err": abs(ets + etd - g["e_t"]),
-               "rel_err": abs(ets + etd - g["e_t"]) / abs(g["e_t"])}
-
-    # end to end through the C entry, pinned host inputs
+    # end to end through the C ABI from pinned host buffers (headline form)
     e2e = None
     if not args.no_e2e:
         pinned = []
@@ -305,36 +344,25 @@ def main():
             pinned.append(t.numpy())
         h2d = sum(a.nbytes for a in pinned)
         d2h = nu * no * 8 + 2 * 8
-        plan.close()
         del dev_inputs
         torch.cuda.empty_cache()
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        if world == 1:
-            r = A.cc_triples(no, nu, *pinned)
-            e2e_e = r[0] + r[1]
-        else:
-            with A.TriplesPlan(no, nu, device=local) as p2:
-                p2.set_inputs(*pinned)
-                r = p2.forward(begin, end)
-            t = torch.tensor([r[0], r[1]], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t)
-            e2e_e = float(t.sum())
+        with make_plan(A, no, nu, local, emu_form) as p2:
+            p2.set_inputs(*pinned)
+            r = p2.forward(begin, end)
+        e2e_e = sum(allreduce([r[0], r[1]]))
         torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = t.item()
+        e2e_s = allreduce([time.perf_counter() - t0], op="max")[0]
         e2e = {"value": flop_step / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "steps": 1,
-               "path": "cc_triples_b200_ (C ABI) from pinned host buffers" if world == 1 else
-               "ccT_plan_create/ccT_set_inputs(host)/ccT_forward(shard) + NCCL all-reduce",
+               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "steps": 1, "form": emu_form,
+               "path": "ccT_plan_create/ccT_set_inputs(host)/ccT_forward/ccT_plan_destroy (C ABI), pinned inputs"
+                       + (" + NCCL all-reduce of the shard energies" if world > 1 else ""),
                "e_t": e2e_e}
     else:
-        plan.close()
+        del dev_inputs
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,18 +372,25 @@ def main():
                          "T3SQUA/ADT3DEN/DRT1WT3 restatement with OpenBLAS DGEMM"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": tflops, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, libcc_b200/synthetic.py)",
-                "config": {"workload": workload_desc(inp, cfg["dist"]), "form": "fp64 (mma.sync f64)",
-                           "tuples": len(costs), "tuples_ijk": n_ijk, "flop_per_step": flop_step,
-                           "tuples_per_s": len(costs) / (ms_step * 1e-3),
-                           "l2": "inputs larger than L2 (E operand "
-                                 f"{no * nu * nu * (nu + no) * 8 / 1e9:.1f} GB re-streamed per tuple)",
+        line = {"metric": METRIC, "value": head["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "int8 tensor pipe (split-integer FP64 emulation)",
+                "data": "synthetic (seeded generator, libcc_b200/synthetic.py)",
+                "config": {"workload": workload_desc(inp, cfg["dist"]), "form": f"emulated FP64, {args.emu_slices} "
+                           "7-bit digits per operand (tcgen05 kind::i8)", "tuples": len(costs), "tuples_ijk": n_ijk_all,
+                           "flop_per_step": flop_step, "tuples_per_s": len(costs) / (head["ms_per_step"] * 1e-3),
+                           "l2": "inputs larger than L2 (digit operands "
+                                 f"{2 * args.emu_slices * no * nu * nu * (nu + no) / 1e9:.1f} GB re-streamed per step)",
                            "parallelism": f"tuple shards x{world}" if world > 1 else "1 GPU"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks.summary(), "energies": {"ets": ets, "etd": etd, "e_t": ets + etd},
-                "accuracy_vs_oracle": acc}
+                "roofline": head["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["gpu_launches"],
+                "clocks": clocks.summary(), "energies": {"ets": head["ets"], "etd": head["etd"], "e_t": head["e_t"]},
+                "accuracy": {"rel_err_vs_native_fp64": rel_vs_native,
+                             "rel_err_vs_oracle": head.get("rel_err_vs_oracle"),
+                             "native_rel_err_vs_oracle": forms["fp64"].get("rel_err_vs_oracle"),
+                             "bar": "relative 2.1e-7 = 1e-8 Eh on a (T) energy of 0.048 Eh (Ar6); the seeded data "
+                                    "give |E(T)| ~ 7.7e9 Eh, where an absolute 1e-8 Eh is below FP64 resolution"},
+                "forms": forms,
+                "speedup_emulated_over_native": forms["fp64"]["ms_per_step"] / head["ms_per_step"]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

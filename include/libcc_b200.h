@@ -117,6 +117,11 @@ const char *ccT_last_error(void);
  * microbenchmark; the denominator of the FP64 roofline). */
 double ccT_measure_fp64_peak(int32_t device);
 
+/* Measured INT8 tensor-pipe throughput (tcgen05.mma kind::i8, operands
+ * resident in shared memory) in tera-ops/s: the denominator of the emulated
+ * form's roofline. */
+double ccT_measure_int8_peak(int32_t device);
+
 /* ------------------------------------------------------------------ allocation-free reduction
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory: codes that reserve one arena for all their GPU

@@ -22,7 +22,7 @@ CCT_MEM_HOST, CCT_MEM_DEVICE = 0, 1
 EXPORTS = [
     "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
     "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
-    "ccT_last_error", "ccT_measure_fp64_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
+    "ccT_last_error", "ccT_measure_fp64_peak", "ccT_measure_int8_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
     "cc_triples_b200_", "ccT_reduce_w_noalloc",
 ]
 
@@ -87,6 +87,8 @@ def load():
     lib.ccT_last_error.restype = ctypes.c_char_p
     lib.ccT_measure_fp64_peak.argtypes = [i32]
     lib.ccT_measure_fp64_peak.restype = ctypes.c_double
+    lib.ccT_measure_int8_peak.argtypes = [i32]
+    lib.ccT_measure_int8_peak.restype = ctypes.c_double
     lib.ijk_gpu_init_.argtypes = [i64p, i64p, dp, dp, dp, dp, dp, dp]
     lib.ijk_gpu_init_.restype = None
     lib.ijk_gpu_driver_.argtypes = [i64p] * 5 + [dp] * 7

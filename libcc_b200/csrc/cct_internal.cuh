@@ -152,5 +152,6 @@ int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const doub
 
 // peak.cu
 double measure_fp64_peak(int device);
+double measure_int8_peak(int device);
 
 }  // namespace cct

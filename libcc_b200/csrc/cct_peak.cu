@@ -32,7 +32,96 @@ __global__ void peak_kernel(double *out, int iters) {
   if (s == 1234.5678) out[0] = s;  // keeps the loop alive
 }
 
+// INT8 tensor-pipe probe: one thread per CTA issues back-to-back
+// tcgen05.mma kind::i8 (M=128, N=256, K=32) on operands already in shared
+// memory, into one TMEM accumulator; the wait for completion is bounded.
+__global__ void __launch_bounds__(128, 1) int8_peak_kernel(int iters, int *err) {
+  __shared__ __align__(1024) uint8_t ops[128 * 32 + 256 * 32];
+  __shared__ uint64_t done;
+  __shared__ uint32_t tbase;
+  const int warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < (int)sizeof(ops); i += blockDim.x) ops[i] = (uint8_t)(i * 7);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(&tbase)),
+                 "r"(256));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 32) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&done)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("fence.proxy.async.shared::cta;");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tbase;
+  if (threadIdx.x == 32) {
+    auto desc = [](const void *p) {
+      const uint64_t a = (uint32_t)__cvta_generic_to_shared(p);
+      return ((a & 0x3FFFF) >> 4) | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) | (6ull << 61);
+    };
+    const uint64_t da = desc(ops), db = desc(ops + 128 * 32);
+    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) | (8u << 24);
+    for (int it = 0; it < iters; it++) {
+      const uint32_t acc = it > 0 ? 1u : 0u;
+      asm volatile(
+          "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; }" ::"r"(tmem),
+          "l"(da), "l"(db), "r"(idesc), "r"(acc));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        (uint32_t)__cvta_generic_to_shared(&done)));
+    bool ok = false;
+    for (long w = 0; w < (1L << 26) && !ok; w++) {
+      uint32_t r;
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+          : "=r"(r)
+          : "r"((uint32_t)__cvta_generic_to_shared(&done))
+          : "memory");
+      ok = r != 0;
+    }
+    if (!ok) atomicExch(err, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+}
+
 }  // namespace
+
+double measure_int8_peak(int device) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return 0.0;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  int *err = nullptr;
+  cudaEvent_t e0, e1;
+  double best = 0.0;
+  if (cudaMalloc(&err, 4) == cudaSuccess && cudaMemset(err, 0, 4) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+      cudaEventCreate(&e1) == cudaSuccess) {
+    const int iters = 2048, blocks = nsm * 2;
+    for (int rep = 0; rep < 4; rep++) {
+      cudaEventRecord(e0);
+      int8_peak_kernel<<<blocks, 128>>>(iters, err);
+      cudaEventRecord(e1);
+      if (cudaEventSynchronize(e1) != cudaSuccess) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double ops = 2.0 * 128 * 256 * 32 * (double)iters * blocks;
+      if (rep > 0 && ms > 0) best = std::max(best, ops / (ms * 1e-3) / 1e12);
+    }
+    int herr = 0;
+    cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost);
+    if (herr) best = 0.0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (err) cudaFree(err);
+  cudaSetDevice(prev);
+  return best;
+}
 
 double measure_fp64_peak(int device) {
   int prev = 0;

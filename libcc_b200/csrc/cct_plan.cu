@@ -627,6 +627,7 @@ int ccT_plan_destroy(ccT_plan *p) {
 }
 
 double ccT_measure_fp64_peak(int32_t device) { return measure_fp64_peak(device); }
+double ccT_measure_int8_peak(int32_t device) { return measure_int8_peak(device); }
 
 // ----------------------------------------------------------------------------- legacy hooks
 

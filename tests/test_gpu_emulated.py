@@ -34,13 +34,25 @@ def test_emulated_seven_slices_match_oracle(api, no, nu, seed):
     from oracle import oracle as O
     inp = S.generate(no, nu, seed)
     ets_o, etd_o, v1_o = O.c_cc_triples(inp)
-    plan = api.TriplesPlan(no, nu, precision="int8")
-    with plan:
+    with _plan(api, inp, 7) as plan:
         plan.set_system(inp)
         ets, etd, v1 = plan.forward()
     assert abs(etd - etd_o) <= 1e-11 * abs(etd_o), (etd, etd_o)
     assert abs(ets - ets_o) <= 1e-9 * abs(ets_o) + 1e-12
     assert np.abs(v1 - v1_o).max() <= 1e-9 * np.abs(v1_o).max()
+
+
+@pytest.mark.parametrize("dist", ["normal", "log"])
+def test_default_emulation_meets_relative_bar(api, dist):
+    """Default digit count against the oracle: relative 2.1e-7, i.e. 1e-8 Eh on a
+    (T) energy of 0.048 Eh (the Ar6 magnitude)."""
+    from oracle import oracle as O
+    inp = S.generate(5, 40, 77, dist=dist)
+    ets_o, etd_o, _ = O.c_cc_triples(inp)
+    with api.TriplesPlan(inp.no, inp.nu, precision="int8") as plan:
+        plan.set_system(inp)
+        ets, etd, _ = plan.forward()
+    assert abs((ets + etd) - (ets_o + etd_o)) <= 2.1e-7 * abs(ets_o + etd_o)
 
 
 @pytest.mark.parametrize("slices,rel", [(4, 3e-6), (5, 3e-8), (6, 3e-10), (7, 1e-11)])
@@ -60,7 +72,7 @@ def test_emulated_tuple_kinds_and_shards(api):
     no, nu = 5, 17
     inp = S.generate(no, nu, 21)
     tuples = O.all_tuples(no)
-    with api.TriplesPlan(no, nu, precision="int8") as plan:
+    with _plan(api, inp, 7) as plan:
         plan.set_system(inp)
         for t in (0, 9, 10, 11, len(tuples) - 1):
             kind, i, j, k = tuples[t]
