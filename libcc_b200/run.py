@@ -1,0 +1,69 @@
+"""Command-line (T) evaluation: ``python -m libcc_b200.run``.
+
+Runs a named synthetic workload or a GAMESS ``triples.restart`` file through the
+library and prints the reference's result line (``ets/etd/ets+etd=``,
+triples.F90:316) with the device time.
+
+    python -m libcc_b200.run --workload no16-nu200 --form fp64
+    python -m libcc_b200.run --restart triples.restart --form int8:5
+    python -m libcc_b200.run --workload no24-nu320 --tuples 4      # first 4 tuples only
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import sys
+import time
+
+
+def make_plan(no: int, nu: int, form: str, device: int = 0):
+    from . import _native as N
+    from .api import TriplesPlan
+    if form == "fp64":
+        return TriplesPlan(no, nu, device=device)
+    if not form.startswith("int8"):
+        raise ValueError("form must be fp64 or int8[:digits]")
+    digits = int(form.split(":")[1]) if ":" in form else 0
+    lib = N.load()
+    opt = N.Options()
+    lib.ccT_options_default(ctypes.byref(opt))
+    opt.precision = N.CCT_PREC_INT8_EMU
+    opt.device = device
+    opt.emu_slices = digits
+    h = ctypes.c_void_p()
+    N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
+    plan = TriplesPlan.__new__(TriplesPlan)
+    plan._h, plan.no, plan.nu, plan.precision, plan.device = h, no, nu, form, device
+    plan.num_tuples = int(lib.ccT_num_tuples(no))
+    return plan
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m libcc_b200.run", description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    src = ap.add_mutually_exclusive_group(required=True)
+    src.add_argument("--workload", help="named synthetic workload (libcc_b200.synthetic.WORKLOADS)")
+    src.add_argument("--restart", help="path of a triples.restart file")
+    ap.add_argument("--form", default="fp64", help="fp64 or int8[:digits] (default fp64)")
+    ap.add_argument("--tuples", type=int, default=0, help="run only the first N tuples (default all)")
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+
+    from . import restart, synthetic
+    from .api import format_energies
+    inp = synthetic.workload(args.workload) if args.workload else restart.read(args.restart)
+    with make_plan(inp.no, inp.nu, args.form, args.device) as plan:
+        t0 = time.perf_counter()
+        plan.set_system(inp)
+        t1 = time.perf_counter()
+        end = args.tuples or plan.num_tuples
+        ets, etd, _ = plan.forward(0, end)
+        print(f" no={inp.no} nu={inp.nu} form={args.form} tuples={end}/{plan.num_tuples}")
+        print(format_energies(ets, etd))
+        print(f" device ms={plan.last_forward_ms:.3f} set_inputs s={t1 - t0:.3f} "
+              f"launches={plan.last_forward_launches}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
