@@ -54,21 +54,6 @@ def workload_desc(inp, dist):
     return d
 
 
-def shard_bounds(tuples_cost, nranks):
-    """Contiguous shards of the tuple list with near-equal summed cost."""
-    total = sum(tuples_cost)
-    bounds, acc, r = [0], 0.0, 1
-    for t, c in enumerate(tuples_cost):
-        acc += c
-        if r < nranks and acc >= total * r / nranks:
-            bounds.append(t + 1)
-            r += 1
-    while len(bounds) < nranks:
-        bounds.append(len(tuples_cost))
-    bounds.append(len(tuples_cost))
-    return bounds
-
-
 class ClockSampler:
     """nvidia-smi clock/throttle samples every 200 ms while running."""
 
@@ -231,6 +216,7 @@ def main():
     import torch
 
     from libcc_b200 import api as A
+    from libcc_b200 import shard
     from libcc_b200 import synthetic as S
 
     torch.cuda.set_device(local)
@@ -245,9 +231,8 @@ def main():
     no, nu = inp.no, inp.nu
     # tuple list order (ccT_forward): C(no,3) i>j>k tuples, then no(no-1) degenerate ones at half cost
     n_ijk_all = no * (no - 1) * (no - 2) // 6
-    costs = [1.0] * n_ijk_all + [0.5] * (no * (no - 1))
-    bounds = shard_bounds(costs, world)
-    begin, end = bounds[rank], bounds[rank + 1]
+    costs = shard.tuple_costs(no)
+    begin, end = shard.shard_of(no, rank, world)
     flop_step = S.flops(no, nu)
     my_flop_wb = sum(12.0 * nu ** 3 * (no + nu) * c for c in costs[begin:end])
     dev_inputs = [torch.from_numpy(a).to(f"cuda:{local}") for a in inp.arrays()]
@@ -269,8 +254,8 @@ def main():
         plan.set_stream(stream.cuda_stream)
 
         def step():
-            ets, etd, _ = plan.forward(begin, end, want_v1=False)
-            return allreduce([ets, etd])
+            ets, etd, _ = shard.sharded_cc_triples(plan, want_v1=False)
+            return ets, etd
 
         for _ in range(args.warmup):
             step()
@@ -352,8 +337,8 @@ def main():
         t0 = time.perf_counter()
         with make_plan(A, no, nu, local, emu_form) as p2:
             p2.set_inputs(*pinned)
-            r = p2.forward(begin, end)
-        e2e_e = sum(allreduce([r[0], r[1]]))
+            r = shard.sharded_cc_triples(p2)
+        e2e_e = r[0] + r[1]
         torch.cuda.synchronize()
         e2e_s = allreduce([time.perf_counter() - t0], op="max")[0]
         e2e = {"value": flop_step / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
