@@ -15,28 +15,56 @@
 // diagonals are scaled and summed in the epilogue.  Digit count S (4..7) is a
 // plan option: about 7S - 2 bits of each operand row survive.
 //
-// Kernel layout (one CTA per 128 x 64 tile of one job):
-//   warp 0      TMA producer: per 32-byte K chunk, S digit slices of the A rows
-//               (128 x 32 B) and of the B rows (64 x 32 B), SWIZZLE_32B, 4-stage ring
-//   warp 1      TMEM owner + MMA issuer (one thread): S(S+1)/2 MMAs per chunk into
-//               S diagonal accumulators (64 int32 columns each), both halves
-//   warps 2..5  drain: tcgen05.ld each diagonal, scale, sum in FP64, write X once
-// With S = 4 the accumulators fit 256 TMEM columns and two CTAs share an SM, so
-// one CTA's drain overlaps the other's MMAs.  Every mbarrier wait is bounded; a
-// timeout sets the error word and the CTA unwinds, freeing its tensor memory.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
-#include <mutex>
-
+// Operands are pre-tiled (EmuOperands): the digits of one 32-byte K chunk of
+// a 128-row A tile, all S slices, are one contiguous S x 4 KB run already in
+// the tensor core's K-major no-swizzle layout, and likewise S x 2 KB for a
+// 64-row B tile.  A pipeline stage is therefore two bulk copies
+// (cp.async.bulk) of large contiguous runs instead of 2S narrow tensor boxes.
+//
+// Persistent kernel, one 192-thread CTA per SM, work items (job, row tile,
+// column tile) taken round-robin with the column tile fastest, so the CTAs
+// in flight share A tiles through L2:
+//   warp 0      producer: per K chunk, one bulk copy of the A digits and one
+//               of the B digits into a ring of stages; it runs ahead across
+//               work items, so the ring never drains between tiles
+//   warp 1      TMEM owner + MMA issuer (one thread): S(S+1)/2 MMAs per chunk
+//               into S diagonal accumulators (64 int32 columns each)
+//   warps 2..5  drain: tcgen05.ld every diagonal, scale, sum in FP64, store X,
+//               then hand the tensor memory back to the issuer (the ring keeps
+//               filling meanwhile, so the next item's MMAs start at once)
+// Every mbarrier wait is bounded and also ends when another role aborted; a
+// timeout sets the error word, the producer waits for its copies in flight,
+// the issuer for its MMAs, and the CTA frees its tensor memory and returns.
 #include "cct_internal.cuh"
 
 namespace cct {
 namespace {
 
-constexpr int EBM = 128, EBN = 64, EKC = 32;  // tile rows, tile cols, K bytes per chunk
-constexpr int ESTAGES = 4;
-constexpr int A_SLICE = EBM * EKC, B_SLICE = EBN * EKC;  // bytes per slice per stage
+constexpr int EBM = kEmuBM, EBN = kEmuBN;
+constexpr int A_BLK = kEmuABlk, B_BLK = kEmuBBlk;
+// A stage holds KS consecutive K chunks (all S digit slices of each), so one
+// barrier round trip feeds KS S(S+1)/2 MMAs.  Ring depth: as many stages as
+// the shared-memory budget holds, between 2 and 8.
+#ifndef CCT_EMU_KS
+#define CCT_EMU_KS 2
+#endif
+#ifndef CCT_EMU_DRAIN_WARPS
+#define CCT_EMU_DRAIN_WARPS 8
+#endif
+#ifndef CCT_EMU_SMEM_BUDGET
+#define CCT_EMU_SMEM_BUDGET (180 * 1024)
+#endif
+constexpr int KS = CCT_EMU_KS;
+constexpr int NDW = CCT_EMU_DRAIN_WARPS;  // drain warps: NDW/4 per TMEM lane quarter
+constexpr int EMU_THREADS = 64 + 32 * NDW;
+template <int S>
+constexpr int emu_stages() {
+  return CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + B_BLK)) > 8   ? 8
+         : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + B_BLK)) < 2 ? 2
+                                                                 : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + B_BLK));
+}
+template <int S>
+constexpr uint32_t emu_tmem_cols() { return S * EBN <= 256 ? 256u : 512u; }
 constexpr long kWaitLimit = 1L << 26;
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -50,39 +78,53 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
 }
-// Bounded wait on a phase parity; false (and *err set) when the limit runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int *err) {
+__device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on a phase parity.  Returns false when another role of the CTA
+// aborted, or when the limit runs out (then the error word and the abort flag
+// are set).
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int *err, volatile int *abort_flag) {
   for (long it = 0; it < kWaitLimit; it++) {
-    uint32_t ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(su32(b)), "r"(parity)
-        : "memory");
-    if (ok) return true;
+    if (mbar_test(b, parity)) return true;
+    if ((it & 63) == 63 && *abort_flag) return false;
   }
   atomicExch(err, 1);
+  *abort_flag = 1;
   return false;
 }
-__device__ __forceinline__ void tma_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1) {
+// Bounded wait that ignores the abort flag (used to let work in flight land).
+__device__ __forceinline__ void mbar_settle(uint64_t *b, uint32_t parity, int *err) {
+  for (long it = 0; it < kWaitLimit; it++)
+    if (mbar_test(b, parity)) return;
+  atomicExch(err, 1);
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
-          su32(dst)),
-      "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1)
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(su32(dst)),
+      "l"(src), "r"(bytes), "r"(su32(bar))
       : "memory");
 }
-// K-major, SWIZZLE_32B: 8-row x 32-byte atoms, atoms 256 B apart along M.
-__device__ __forceinline__ uint64_t desc_sw32(const void *p) {
+// K-major, no swizzle: 8-row x 16-byte core matrices; the two K halves of a
+// 32-byte chunk 128 B apart (leading offset), 8-row groups 256 B apart (stride
+// offset).  Start address and offsets are in 16-byte units.
+__device__ __forceinline__ uint64_t desc_kmajor(const void *p) {
   const uint64_t a = su32(p);
-  return ((a & 0x3FFFF) >> 4) | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) | (6ull << 61);
+  return ((a & 0x3FFFF) >> 4) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46);
 }
 
 struct EmuArgs {
   const EmuJob *jobs;
+  const int8_t *E8, *E8T, *F8;
   const int16_t *expE, *expF;
-  int nu, no, kchunks;
-  int64_t NP, rowsE, rowsF;  // rows per slice in the E/E^T and F tensors
-  int tiles_n;
+  int nu, njobs, kchunks, tiles_m, tiles_n;
+  int64_t NP;
   int *err;
 };
 
@@ -94,30 +136,27 @@ __device__ __forceinline__ double pow2(int e) {
 }
 
 template <int S>
-constexpr int emu_tmem_cols() { return S * kEmuBN <= 256 ? 256 : 512; }
-template <int S>
-constexpr int emu_ctas_per_sm() { return S * kEmuBN <= 256 ? 2 : 1; }
-
-template <int S>
-__global__ void __launch_bounds__(192, emu_ctas_per_sm<S>())
-    wbuild_emu_kernel(const __grid_constant__ CUtensorMap mapE, const __grid_constant__ CUtensorMap mapET,
-                      const __grid_constant__ CUtensorMap mapF, const EmuArgs args) {
+__global__ void __launch_bounds__(EMU_THREADS, 1) wbuild_emu_kernel(const EmuArgs args) {
   constexpr uint32_t TCOLS = emu_tmem_cols<S>();
+  constexpr int ST = emu_stages<S>();
+  constexpr int CA = S * A_BLK, CB = S * B_BLK;    // bytes of one K chunk per operand
+  constexpr int SA = KS * CA, SB = KS * CB;        // bytes of one stage per operand
   extern __shared__ __align__(1024) uint8_t emu_smem[];
   uint8_t *base = (uint8_t *)(((uintptr_t)emu_smem + 1023) & ~(uintptr_t)1023);
-  uint8_t *sA = base;                                   // [stage][S][128][32]
-  uint8_t *sB = base + ESTAGES * S * A_SLICE;           // [stage][S][64][32]
-  __shared__ uint64_t full[ESTAGES], empty[ESTAGES], acc_full;
+  uint8_t *sA = base;            // [stage][chunk][slice][4096]
+  uint8_t *sB = base + ST * SA;  // [stage][chunk][slice][2048]
+  __shared__ uint64_t full[ST], empty[ST], acc_full, tmem_empty, mma_done;
   __shared__ uint32_t tmem_base;
+  __shared__ int abort_word;
+  volatile int *abort_flag = &abort_word;
 
-  const EmuJob job = args.jobs[blockIdx.y];
-  const int tile_m = blockIdx.x / args.tiles_n, tile_n = blockIdx.x - tile_m * args.tiles_n;
-  const int64_t M = (int64_t)args.nu * args.nu;
-  const int64_t m0 = (int64_t)tile_m * EBM;
-  const int n0 = tile_n * EBN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nh = job.nhalves;
-  const int nk = args.kchunks;
+  const int64_t M = (int64_t)args.nu * args.nu;
+  const int per_job = args.tiles_m * args.tiles_n;
+  const int64_t nitems = (int64_t)args.njobs * per_job;
+  const int KC = args.kchunks;
+  const int64_t aslab = (int64_t)args.tiles_m * KC * CA;  // bytes per occupied index
+  const int64_t bslab = (int64_t)args.tiles_n * KC * CB;  // bytes per (y,z)
 
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base)),
@@ -125,11 +164,14 @@ __global__ void __launch_bounds__(192, emu_ctas_per_sm<S>())
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < ESTAGES; s++) {
+    for (int s = 0; s < ST; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     mbar_init(&acc_full, 1);
+    mbar_init(&tmem_empty, NDW);  // one arrival per drain warp
+    mbar_init(&mma_done, 1);
+    abort_word = 0;
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -138,108 +180,158 @@ __global__ void __launch_bounds__(192, emu_ctas_per_sm<S>())
   const uint32_t tmem = tmem_base;
 
   if (warp == 0) {
-    if (lane == 0) {  // ---------------- TMA producer
+    if (lane == 0) {  // ---------------- producer
+      uint32_t g = 0;
       bool ok = true;
-      for (int h = 0; h < nh && ok; h++) {
-        const CUtensorMap *mA = h == 0 ? &mapE : &mapET;
-        const int64_t arow = (int64_t)(h == 0 ? job.x1 : job.x2) * M + m0;
-        const int64_t brow = (int64_t)job.fyz[h] * args.NP + n0;
-        for (int kc = 0; kc < nk; kc++) {
-          const int g = h * nk + kc, st = g % ESTAGES;
-          if (g >= ESTAGES && !mbar_wait(&empty[st], ((g / ESTAGES) - 1) & 1, args.err)) {
-            ok = false;
-            break;
+      for (int64_t it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+        const int jb = (int)(it / per_job);
+        const int rem = (int)(it - (int64_t)jb * per_job);
+        const int tm = rem / args.tiles_n, tn = rem - tm * args.tiles_n;
+        const EmuJob job = args.jobs[jb];
+        for (int h = 0; h < job.nhalves && ok; h++) {
+          const int8_t *A = (h == 0 ? args.E8 + job.x1 * aslab : args.E8T + job.x2 * aslab) + (int64_t)tm * KC * CA;
+          const int8_t *B = args.F8 + job.fyz[h] * bslab + (int64_t)tn * KC * CB;
+          for (int kc = 0; kc < KC; kc += KS, g++) {
+            const int st = (int)(g % ST);
+            const uint32_t nch = KC - kc < KS ? (uint32_t)(KC - kc) : (uint32_t)KS;  // the last stage may be short
+            if (g >= (uint32_t)ST && !mbar_wait(&empty[st], ((g / ST) - 1) & 1, args.err, abort_flag)) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(&full[st], nch * (CA + CB));
+            bulk_load(sA + st * SA, A + (int64_t)kc * CA, nch * CA, &full[st]);
+            bulk_load(sB + st * SB, B + (int64_t)kc * CB, nch * CB, &full[st]);
           }
-          mbar_expect_tx(&full[st], S * (A_SLICE + B_SLICE));
-#pragma unroll
-          for (int t = 0; t < S; t++)
-            tma_2d(sA + (st * S + t) * A_SLICE, mA, &full[st], kc * EKC, (int)(t * args.rowsE + arow));
-#pragma unroll
-          for (int t = 0; t < S; t++)
-            tma_2d(sB + (st * S + t) * B_SLICE, &mapF, &full[st], kc * EKC, (int)(t * args.rowsF + brow));
         }
       }
+      // let every copy still in flight land before the CTA can exit
+      for (uint32_t q = g > (uint32_t)ST ? g - ST : 0; q < g; q++) mbar_settle(&full[q % ST], (q / ST) & 1, args.err);
     }
   } else if (warp == 1) {
-    if (lane == 0) {  // ---------------- MMA issuer: both halves into one set of diagonals
+    if (lane == 0) {  // ---------------- MMA issuer
       // kind::i8, D s32, A/B s8, K-major, M = 128, N = 64
       const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(EBN >> 3) << 17) | (8u << 24);
-      for (int h = 0; h < nh; h++) {
-        bool ok = true;
-        for (int kc = 0; kc < nk; kc++) {
-          const int g = h * nk + kc, st = g % ESTAGES;
-          if (!mbar_wait(&full[st], (g / ESTAGES) & 1, args.err)) {
-            ok = false;
-            break;
-          }
-          asm volatile("tcgen05.fence::after_thread_sync;");
-#pragma unroll
-          for (int t = 0; t < S; t++) {
-            const uint64_t da = desc_sw32(sA + (st * S + t) * A_SLICE);
-#pragma unroll
-            for (int u = 0; u < S - t; u++) {
-              const uint64_t db = desc_sw32(sB + (st * S + u) * B_SLICE);
-              const uint32_t dcol = tmem + (uint32_t)((t + u) * EBN);
-              const uint32_t accum = (h > 0 || kc > 0 || t > 0) ? 1u : 0u;
-              asm volatile(
-                  "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; }" ::"r"(
-                      dcol),
-                  "l"(da), "l"(db), "r"(idesc), "r"(accum));
+      const uint64_t dA0 = desc_kmajor(sA), dB0 = desc_kmajor(sB);
+      uint32_t g = 0, n = 0;
+      bool ok = true;
+      for (int64_t it = blockIdx.x; it < nitems && ok; it += gridDim.x, n++) {
+        // the drain of the previous item has read the accumulators
+        if (n > 0 && !mbar_wait(&tmem_empty, (n - 1) & 1, args.err, abort_flag)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const int nh = args.jobs[it / per_job].nhalves;
+        for (int h = 0; h < nh && ok; h++) {
+          for (int kc = 0; kc < KC; kc += KS, g++) {
+            const int st = (int)(g % ST);
+            const int nch = KC - kc < KS ? KC - kc : KS;
+            if (!mbar_wait(&full[st], (g / ST) & 1, args.err, abort_flag)) {
+              ok = false;
+              break;
             }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+            for (int c = 0; c < KS; c++) {
+              if (c >= nch) break;
+              // descriptor start addresses are linear in 16-byte units
+              const uint64_t dA = dA0 + (uint64_t)((st * SA + c * CA) >> 4);
+              const uint64_t dB = dB0 + (uint64_t)((st * SB + c * CB) >> 4);
+              const uint32_t first = (h == 0 && kc == 0 && c == 0) ? 0u : 1u;  // accumulate flag of the t = 0 row
+#pragma unroll
+              for (int t = 0; t < S; t++) {
+#pragma unroll
+                for (int u = 0; u < S - t; u++) {
+                  asm volatile(
+                      "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; "
+                      "}" ::"r"(tmem + (uint32_t)((t + u) * EBN)),
+                      "l"(dA + (uint64_t)(t * (A_BLK >> 4))), "l"(dB + (uint64_t)(u * (B_BLK >> 4))), "r"(idesc),
+                      "r"(t > 0 ? 1u : first));
+                }
+              }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                su32(&empty[st])));
           }
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              su32(&empty[st])));
         }
         if (!ok) break;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            su32(&acc_full)));
       }
+      // every MMA issued has completed before the tensor memory is freed
       asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&acc_full)));
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&mma_done)));
+      mbar_settle(&mma_done, 0, args.err);
     }
-  } else {  // ---------------- drain (warps 2..5 own TMEM lane quarters 2,3,0,1)
+  } else {  // ---------------- drain: warp w owns TMEM lane quarter w % 4
+    constexpr int CW = EBN / (NDW / 4);  // columns per drain warp
     const int q = warp & 3;
     const int row = q * 32 + lane;
-    const int64_t m = m0 + row;
-    const bool live = m < M;
+    const int cbase = ((warp - 2) / 4) * CW;
     // diagonal d = t + u (0-based digits) carries 2^(-7(d+2))
     double cd[S];
 #pragma unroll
     for (int d = 0; d < S; d++) cd[d] = pow2(-7 * (d + 2));
-    if (mbar_wait(&acc_full, 0, args.err)) {
-      asm volatile("tcgen05.fence::after_thread_sync;");
+    uint32_t n = 0;
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x, n++) {
+      // everything that does not depend on the MMAs is fetched before the wait
+      const int jb = (int)(it / per_job);
+      const int rem = (int)(it - (int64_t)jb * per_job);
+      const int tm = rem / args.tiles_n, tn = rem - tm * args.tiles_n;
+      const EmuJob job = args.jobs[jb];
+      const int64_t m = (int64_t)tm * EBM + row;
+      const bool live = m < M;
       const int eA = live ? args.expE[m] : 0;
-      const int16_t *eB = args.expF + (int64_t)job.x3 * args.NP + n0;
-      double *xrow = job.out + m * args.NP + n0;
-#pragma unroll 1
-      for (int c0 = 0; c0 < EBN; c0 += 16) {
-        double acc[16];
+      const int n0 = tn * EBN + cbase;
+      // warp-uniform decision: the tcgen05.ld below are .sync.aligned
+      if (!__all_sync(0xffffffffu, mbar_wait(&acc_full, n & 1, args.err, abort_flag))) break;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      double acc[CW];
 #pragma unroll
-        for (int j = 0; j < 16; j++) acc[j] = 0.0;
+      for (int c0 = 0; c0 < CW; c0 += 16) {
+        constexpr int DB = S <= 5 ? S : 1;  // diagonals per tcgen05.wait::ld
 #pragma unroll
-        for (int d = 0; d < S; d++) {
-          uint32_t v[16];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                "=r"(v[15])
-              : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(d * EBN + c0)));
+        for (int d0 = 0; d0 < S; d0 += DB) {
+          uint32_t v[DB][16];
+#pragma unroll
+          for (int dd = 0; dd < DB; dd++)
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[dd][0]), "=r"(v[dd][1]), "=r"(v[dd][2]), "=r"(v[dd][3]), "=r"(v[dd][4]), "=r"(v[dd][5]),
+                  "=r"(v[dd][6]), "=r"(v[dd][7]), "=r"(v[dd][8]), "=r"(v[dd][9]), "=r"(v[dd][10]), "=r"(v[dd][11]),
+                  "=r"(v[dd][12]), "=r"(v[dd][13]), "=r"(v[dd][14]), "=r"(v[dd][15])
+                : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((d0 + dd) * EBN + cbase + c0)));
           asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
-          for (int j = 0; j < 16; j++) acc[j] = fma((double)(int32_t)v[j], cd[d], acc[j]);
-        }
-        if (live) {
+          for (int j = 0; j < 16; j++) {
+            double a = d0 == 0 ? 0.0 : acc[c0 + j];
 #pragma unroll
-          for (int j = 0; j < 16; j += 2) {
-            const double s0 = acc[j] * pow2(eA + eB[c0 + j]);
-            const double s1 = acc[j + 1] * pow2(eA + eB[c0 + j + 1]);
-            *reinterpret_cast<double2 *>(xrow + c0 + j) = make_double2(s0, s1);
+            for (int dd = 0; dd < DB; dd++) a = fma((double)(int32_t)v[dd][j], cd[d0 + dd], a);
+            acc[c0 + j] = a;
           }
+        }
+      }
+      // every diagonal is in registers: hand the tensor memory to the next item
+      // before the scaling and the stores
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tmem_empty);
+      if (live) {
+        double *xrow = job.out + m * args.NP + n0;
+        const int16_t *eB = args.expF + (int64_t)job.x3 * args.NP + n0;
+#pragma unroll
+        for (int j = 0; j < CW; j += 2) {
+          const double s0 = acc[j] * pow2(eA + eB[j]);
+          const double s1 = acc[j + 1] * pow2(eA + eB[j + 1]);
+          *reinterpret_cast<double2 *>(xrow + j) = make_double2(s0, s1);
         }
       }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
 }
 
@@ -284,106 +376,119 @@ __global__ void shared_exp_f_kernel(const int16_t *__restrict__ rowexp, int no, 
   }
 }
 
-// Pass 3: S truncated 7-bit digits of value * 2^-e, |value * 2^-e| < 1.
-__device__ __forceinline__ void digits_row(const double *__restrict__ src, int64_t kvalid, int e, int S, int64_t KP8,
-                                           int8_t *dst, int64_t slice_stride, int8_t *dstT) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t k = lane; k < KP8; k += 32) {
-    double y = k < kvalid ? ldexp(src[k], -e) : 0.0;
-    for (int t = 0; t < S; t++) {
-      y *= 128.0;
-      const double a = trunc(y);  // |a| <= 127
-      y -= a;                     // exact
-      dst[t * slice_stride + k] = (int8_t)a;
-      if (dstT) dstT[t * slice_stride + k] = (int8_t)a;
+// Byte offset of (row r, K byte kb) inside one tiled block: 8-row x 16-byte
+// core matrices, K halves 128 B apart, 8-row groups 256 B apart.
+__host__ __device__ constexpr int blk_off(int r, int kb) { return (r >> 3) * 256 + (kb >> 4) * 128 + (r & 7) * 16 + (kb & 15); }
+
+// Pass 3: S truncated 7-bit digits of value * 2^-e, |value * 2^-e| < 1.  A
+// lane takes four consecutive K bytes, so each slice gets one 32-bit store;
+// the four bytes are adjacent in the tiled layout (kb % 4 == 0).
+__device__ __forceinline__ void digits4(const double *__restrict__ src, int64_t k, int64_t kvalid, int e, int S,
+                                        uint32_t *w) {
+  double y[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) y[i] = (k + i) < kvalid ? ldexp(src[k + i], -e) : 0.0;
+  for (int t = 0; t < S; t++) {
+    uint32_t word = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      y[i] *= 128.0;
+      const double a = trunc(y[i]);  // |a| <= 127
+      y[i] -= a;                     // exact
+      word |= (uint32_t)(uint8_t)(int8_t)a << (8 * i);
     }
+    w[t] = word;
   }
 }
 
+// E digits: row (x, m = r1*nu + r2) goes to E8 at row m and to E8T at row
+// r2*nu + r1 of the same occupied index x.
 __global__ void digits_e_kernel(const double *__restrict__ E, int no, int nu, int64_t KP, int64_t KP8, int S,
-                                const int16_t *__restrict__ expE, int8_t *__restrict__ E8, int8_t *__restrict__ E8T) {
+                                int64_t tiles_m, const int16_t *__restrict__ expE, int8_t *__restrict__ E8,
+                                int8_t *__restrict__ E8T) {
   const int64_t nu2 = (int64_t)nu * nu, rows = (int64_t)no * nu2;
+  const int64_t KC = KP8 / kEmuKC;
+  const int lane = threadIdx.x & 31;
   int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (; row < rows; row += stride) {
-    const int64_t x = row / nu2, rem = row - x * nu2;
-    const int64_t r1 = rem / nu, r2 = rem - r1 * nu;
-    const int64_t rowT = x * nu2 + r2 * nu + r1;
-    digits_row(E + row * KP, nu + no, expE[rem], S, KP8, E8 + row * KP8, rows * KP8, E8T + rowT * KP8);
+    const int64_t x = row / nu2, m = row - x * nu2;
+    const int64_t r1 = m / nu, r2 = m - r1 * nu;
+    const int64_t mt = r2 * nu + r1;
+    const int e = expE[m];
+    for (int64_t k = 4 * lane; k < KP8; k += 128) {
+      uint32_t w[kEmuMaxSlices];
+      digits4(E + row * KP, k, nu + no, e, S, w);
+      const int64_t kc = k / kEmuKC;
+      const int kb = (int)(k - kc * kEmuKC);
+      const int64_t ba = ((x * tiles_m + m / kEmuBM) * KC + kc) * S * kEmuABlk + blk_off((int)(m % kEmuBM), kb);
+      const int64_t bt = ((x * tiles_m + mt / kEmuBM) * KC + kc) * S * kEmuABlk + blk_off((int)(mt % kEmuBM), kb);
+      for (int t = 0; t < S; t++) {
+        *reinterpret_cast<uint32_t *>(E8 + ba + (int64_t)t * kEmuABlk) = w[t];
+        *reinterpret_cast<uint32_t *>(E8T + bt + (int64_t)t * kEmuABlk) = w[t];
+      }
+    }
   }
 }
 
 __global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, int64_t NP, int64_t KP, int64_t KP8,
                                 int S, const int16_t *__restrict__ expF, int8_t *__restrict__ F8) {
   const int64_t rows = (int64_t)no * no * NP;
+  const int64_t KC = KP8 / kEmuKC, tiles_n = NP / kEmuBN;
+  const int lane = threadIdx.x & 31;
   int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (; row < rows; row += stride) {
-    const int64_t z = (row / NP) % no, n = row % NP;
-    digits_row(F + row * KP, nu + no, expF[z * NP + n], S, KP8, F8 + row * KP8, rows * KP8, nullptr);
+    const int64_t yz = row / NP, n = row - yz * NP;
+    const int64_t z = yz % no;
+    const int e = expF[z * NP + n];
+    for (int64_t k = 4 * lane; k < KP8; k += 128) {
+      uint32_t w[kEmuMaxSlices];
+      digits4(F + row * KP, k, nu + no, e, S, w);
+      const int64_t kc = k / kEmuKC;
+      const int kb = (int)(k - kc * kEmuKC);
+      const int64_t b = ((yz * tiles_n + n / kEmuBN) * KC + kc) * S * kEmuBBlk + blk_off((int)(n % kEmuBN), kb);
+      for (int t = 0; t < S; t++) *reinterpret_cast<uint32_t *>(F8 + b + (int64_t)t * kEmuBBlk) = w[t];
+    }
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-std::mutex g_encode_mutex;
-
-int get_encode() {
-  std::lock_guard<std::mutex> lock(g_encode_mutex);
-  if (g_encode) return CCT_OK;
-  cudaDriverEntryPointQueryResult qr;
-  void *fn = nullptr;
-  CCT_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr));
-  if (!fn || qr != cudaDriverEntryPointSuccess) {
-    set_error("cuTensorMapEncodeTiled is not available from the driver");
-    return CCT_ERR_UNSUPPORTED;
-  }
-  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  return CCT_OK;
-}
-
-int make_map(CUtensorMap *m, const int8_t *base, int64_t rows, int64_t row_bytes, int box_rows) {
-  cuuint64_t dims[2] = {(cuuint64_t)row_bytes, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
-  cuuint32_t box[2] = {(cuuint32_t)EKC, (cuuint32_t)box_rows};
-  cuuint32_t es[2] = {1, 1};
-  const CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)base, dims, strides, box, es,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
-    return CCT_ERR_CUDA;
-  }
-  return CCT_OK;
-}
+int g_num_sms[64] = {0};
 
 template <int S>
 int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err, cudaStream_t s) {
-  constexpr int smem = ESTAGES * S * (A_SLICE + B_SLICE) + 1024;
+  constexpr int smem = emu_stages<S>() * KS * S * (A_BLK + B_BLK) + 1024;
   static int configured_device = -1;
   int dev = 0;
   CCT_CUDA(cudaGetDevice(&dev));
   if (configured_device != dev) {
     CCT_CUDA(cudaFuncSetAttribute(wbuild_emu_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    // full shared-memory carveout, so reduction CTAs can sit beside a W-build CTA
     CCT_CUDA(cudaFuncSetAttribute(wbuild_emu_kernel<S>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   cudaSharedmemCarveoutMaxShared));
     configured_device = dev;
   }
+  if (dev < 0 || dev >= 64) {
+    set_error("device ordinal out of range");
+    return CCT_ERR_INVALID;
+  }
+  if (g_num_sms[dev] == 0) CCT_CUDA(cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev));
   EmuArgs a;
   a.jobs = jobs_dev;
+  a.E8 = o.E8;
+  a.E8T = o.E8T;
+  a.F8 = o.F8;
   a.expE = o.expE;
   a.expF = o.expF;
   a.nu = d.nu;
-  a.no = d.no;
-  a.kchunks = (int)(o.KP8 / EKC);
-  a.NP = d.NP;
-  a.rowsE = (int64_t)d.no * d.nu * d.nu;
-  a.rowsF = (int64_t)d.no * d.no * d.NP;
+  a.njobs = njobs;
+  a.kchunks = (int)(o.KP8 / kEmuKC);
+  a.tiles_m = (int)o.tiles_m;
   a.tiles_n = (int)(d.NP / EBN);
+  a.NP = d.NP;
   a.err = err;
-  const int64_t M = (int64_t)d.nu * d.nu;
-  dim3 grid((unsigned)(((M + EBM - 1) / EBM) * a.tiles_n), (unsigned)njobs);
-  wbuild_emu_kernel<S><<<grid, 192, smem, s>>>(o.mapE, o.mapET, o.mapF, a);
+  const int64_t items = (int64_t)njobs * a.tiles_m * a.tiles_n;
+  const int grid = (int)(items < g_num_sms[dev] ? items : g_num_sms[dev]);
+  wbuild_emu_kernel<S><<<grid, EMU_THREADS, smem, s>>>(a);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
@@ -396,11 +501,10 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
               std::to_string(kEmuMaxSlices) + "]");
     return CCT_ERR_INVALID;
   }
-  if (d.NP % EBN != 0) {
-    set_error("emulated plan needs NP to be a multiple of 64");
+  if (d.NP % EBN != 0 || o->KP8 % kEmuKC != 0) {
+    set_error("emulated plan needs NP a multiple of 64 and KP8 a multiple of 32");
     return CCT_ERR_INVALID;
   }
-  CCT_TRY(get_encode());
   const int64_t rowsE = (int64_t)d.no * d.nu * d.nu, rowsF = (int64_t)d.no * d.no * d.NP;
   auto grid_rows = [](int64_t rows) {
     int64_t b = (rows * 32 + 255) / 256;
@@ -419,13 +523,15 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
   CCT_CUDA(cudaGetLastError());
   shared_exp_f_kernel<<<grid_flat((int64_t)d.no * d.NP), 256, 0, s>>>(o->expRowF, d.no, d.NP, o->expF);
   CCT_CUDA(cudaGetLastError());
-  digits_e_kernel<<<grid_rows(rowsE), 256, 0, s>>>(E, d.no, d.nu, d.KP, o->KP8, o->slices, o->expE, o->E8, o->E8T);
+  // the rows past nu^2 in the last row tile stay zero
+  const size_t bytesE = (size_t)o->slices * d.no * o->tiles_m * kEmuBM * o->KP8;
+  CCT_CUDA(cudaMemsetAsync(o->E8, 0, bytesE, s));
+  CCT_CUDA(cudaMemsetAsync(o->E8T, 0, bytesE, s));
+  digits_e_kernel<<<grid_rows(rowsE), 256, 0, s>>>(E, d.no, d.nu, d.KP, o->KP8, o->slices, o->tiles_m, o->expE,
+                                                   o->E8, o->E8T);
   CCT_CUDA(cudaGetLastError());
   digits_f_kernel<<<grid_rows(rowsF), 256, 0, s>>>(F, d.no, d.nu, d.NP, d.KP, o->KP8, o->slices, o->expF, o->F8);
   CCT_CUDA(cudaGetLastError());
-  CCT_TRY(make_map(&o->mapE, o->E8, (int64_t)o->slices * rowsE, o->KP8, EBM));
-  CCT_TRY(make_map(&o->mapET, o->E8T, (int64_t)o->slices * rowsE, o->KP8, EBM));
-  CCT_TRY(make_map(&o->mapF, o->F8, (int64_t)o->slices * rowsF, o->KP8, EBN));
   return CCT_OK;
 }
 

@@ -110,19 +110,27 @@ struct EmuJob {
   int x3;  // the index both halves' F rows share: fyz[h] = (x2|x1) * no + x3
 };
 
-// Split-integer operands of one plan.
+// Split-integer operands of one plan, stored pre-tiled in the tensor core's
+// K-major no-swizzle shared-memory layout, so one pipeline stage (one 32-byte
+// K chunk, every digit slice) is a single contiguous bulk copy per operand.
+// A block holds one digit slice of one K chunk of one row tile: 8-row x 16-byte
+// core matrices, row r / byte kb at (r/8)*256 + (kb/16)*128 + (r%8)*16 + kb%16.
+constexpr int kEmuBM = 128;                      // rows per A tile
+constexpr int kEmuKC = 32;                       // K bytes per chunk (one kind::i8 MMA)
+constexpr int kEmuABlk = kEmuBM * kEmuKC;        // 4096 bytes
+constexpr int kEmuBBlk = kEmuBN * kEmuKC;        // 2048 bytes
 struct EmuOperands {
   int slices = kEmuDefaultSlices;
   int64_t KP8 = 0;                           // digit row length: round_up(nu+no, 32)
-  int8_t *E8 = nullptr, *E8T = nullptr;      // [slice][x][r1][r2][KP8], and r1<->r2
-  int8_t *F8 = nullptr;                      // [slice][y][z][NP][KP8]
+  int64_t tiles_m = 0;                       // ceil(nu^2 / 128) row tiles per occupied index
+  int8_t *E8 = nullptr, *E8T = nullptr;      // [x][tile_m][kchunk][slice][4096]; E8T rows (q,p)
+  int8_t *F8 = nullptr;                      // [y*no+z][tile_n][kchunk][slice][2048]
   // Digit scales shared by both halves of a GEMM, so one set of diagonal
   // accumulators serves the whole contraction: expE[p*nu+q] (symmetric) is the
   // largest row exponent of E[x][p][q] and E[x][q][p] over all x; expF[z*NP+n]
   // the largest of F[y][z][n] over all y.  expET and expRowF hold the per-row
   // exponents they are reduced from.
   int16_t *expE = nullptr, *expET = nullptr, *expF = nullptr, *expRowF = nullptr;
-  CUtensorMap mapE, mapET, mapF;
 };
 
 int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOperands *o, cudaStream_t s);

@@ -388,9 +388,11 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   if (p->emulated) {
     EmuOperands &e = p->emu;
     e.slices = o.emu_slices ? o.emu_slices : kEmuDefaultSlices;
-    e.KP8 = round_up(nu + no, 32);
+    e.KP8 = round_up(nu + no, kEmuKC);
+    e.tiles_m = (nu2 + kEmuBM - 1) / kEmuBM;
     const int64_t rowsE = no * nu2, rowsF = no * no * d.NP;
-    if ((s = dalloc(&e.E8, e.slices * rowsE * e.KP8)) || (s = dalloc(&e.E8T, e.slices * rowsE * e.KP8)) ||
+    const int64_t bytesE = e.slices * no * e.tiles_m * kEmuBM * e.KP8;  // row tiles padded to 128 rows
+    if ((s = dalloc(&e.E8, bytesE)) || (s = dalloc(&e.E8T, bytesE)) ||
         (s = dalloc(&e.F8, e.slices * rowsF * e.KP8)) || (s = dalloc(&e.expE, rowsE)) ||
         (s = dalloc(&e.expET, rowsE)) || (s = dalloc(&e.expF, rowsF)) || (s = dalloc(&e.expRowF, rowsF)) ||
         (s = dalloc(&p->emu_jobs, p->tuples.size() * 3 * kNBuf)))
