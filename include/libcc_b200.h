@@ -81,6 +81,23 @@ int64_t ccT_num_tuples(int64_t no);
  * ets/etd/v1 sum linearly with the other shards. */
 int ccT_forward(ccT_plan *plan, int64_t begin, int64_t end, double *ets, double *etd, double *v1_out);
 
+/* Gradient of E(T) = ets + etd of the tuple range of the preceding ccT_forward
+ * (the saved context: same plan, same inputs, same [begin, end)) with respect
+ * to every input, written in the input layouts: d_eh (no), d_ep (nu), d_t1
+ * (no,nu), d_t2 (nu,nu,no,no), d_vm (no,nu,no,no), d_voe (nu,nu,no,no) and
+ * d_vvvo (the packed (nutr, nu*no) layout of ccT_set_inputs).  Together this
+ * is the (T) contribution to the CCSD(T) Lagrangian.  W is recomputed per
+ * tuple in FP64 whatever the plan's precision; nothing of size nu^3 is kept
+ * across tuples.  mem says whether the output pointers are host or device
+ * memory; any output pointer may be NULL to skip it.  No reference
+ * counterpart: the reference computes no gradient.  Returns CCT_ERR_STATE
+ * when no ccT_forward over [begin, end) precedes it. */
+int ccT_backward(ccT_plan *plan, int64_t begin, int64_t end, double *d_eh, double *d_ep, double *d_t1,
+                 double *d_t2, double *d_vm, double *d_voe, double *d_vvvo, int32_t mem);
+
+/* Milliseconds of device time the last ccT_backward spent (CUDA events). */
+double ccT_last_backward_ms(const ccT_plan *plan);
+
 /* Launch the plan's kernels on a caller-provided CUDA stream (a cudaStream_t
  * passed as void*); NULL restores the plan's own stream. */
 int ccT_set_stream(ccT_plan *plan, void *cuda_stream);

@@ -23,7 +23,7 @@ EXPORTS = [
     "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
     "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
     "ccT_last_error", "ccT_measure_fp64_peak", "ccT_measure_int8_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
-    "cc_triples_b200_", "ccT_reduce_w_noalloc",
+    "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms",
 ]
 
 
@@ -99,6 +99,10 @@ def load():
     lib.cc_triples_b200_.restype = None
     lib.ccT_reduce_w_noalloc.argtypes = [i64] * 5 + [vp] * 6 + [vp]
     lib.ccT_reduce_w_noalloc.restype = ctypes.c_int
+    lib.ccT_backward.argtypes = [vp, i64, i64] + [vp] * 7 + [i32]
+    lib.ccT_backward.restype = ctypes.c_int
+    lib.ccT_last_backward_ms.argtypes = [vp]
+    lib.ccT_last_backward_ms.restype = ctypes.c_double
     _lib = lib
     return lib
 

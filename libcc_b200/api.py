@@ -110,6 +110,21 @@ class TriplesPlan:
         N.check(N.load().ccT_forward(self._h, begin, end, ctypes.byref(ets), ctypes.byref(etd), vptr), "ccT_forward")
         return ets.value, etd.value, v1
 
+    def backward(self, begin: int = 0, end: int | None = None) -> dict:
+        """Gradient of E(T) = ets + etd of the last ``forward(begin, end)`` with
+        respect to every input, as host arrays in the input layouts: keys eh,
+        ep, t1, t2, vm, voe, vvvo (``ccT_backward``)."""
+        end = self.num_tuples if end is None else end
+        sizes = input_sizes(self.no, self.nu)
+        out = {k: np.zeros(sizes[k]) for k in ("eh", "ep", "t1", "t2", "vm", "voe", "vvvo")}
+        ptrs = [ctypes.c_void_p(out[k].ctypes.data) for k in ("eh", "ep", "t1", "t2", "vm", "voe", "vvvo")]
+        N.check(N.load().ccT_backward(self._h, begin, end, *ptrs, N.CCT_MEM_HOST), "ccT_backward")
+        return out
+
+    @property
+    def last_backward_ms(self) -> float:
+        return float(N.load().ccT_last_backward_ms(self._h))
+
     def set_stream(self, stream_handle: int | None):
         """Run on a caller's CUDA stream (an integer cudaStream_t, e.g.
         ``torch.cuda.current_stream().cuda_stream``); None restores the plan's own."""

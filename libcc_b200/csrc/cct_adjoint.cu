@@ -1,0 +1,902 @@
+// Adjoint of the (T) energy: dE(T)/d{eh, ep, T1, T2, VM, VOE, VVVO}.
+//
+// Per tuple (i,j,k) with weight w (1, or 1/2 for degenerate tuples) and
+// d = 1/D_abc, the forward computes (reduction of cct_reduce.cu, the full-sum
+// form of t1wt3.f90:46-95 and triples.F90:311-312)
+//   E_t = w sum_abc [ W (P W) + sum_m z_m S_m ] d,
+//   P W = 8 W_abc - 4 (W_acb + W_cba + W_bac) + 2 (W_bca + W_cab),
+//   S_m(a,b,c) = u_x(a) VOE(b,c,y,z),  u_x(a) = 2 T1(x,a),
+//   (m; x,y,z) = (1; i,j,k) (2; i,k,j) (3; j,i,k) (4; k,i,j) (5; j,k,i) (6; k,j,i),
+// with z_1..z_6 the combinations of t1wt3.f90:80-85.  Because D is symmetric in
+// (a,b,c), P is self-adjoint and a W at a permuted index can be moved onto S:
+//   dE/dW = w d (2 P W + H),   H = sum_m sum_pi c_pi S_m(pi^-1)     (adj_gw_kernel)
+//   dE/dVOE(b,c,y,z) = w sum_a z_m(a,b,c) u_x(a) d                   (adj_voe_kernel)
+//   dE/deh_x = -(multiplicity of x in ijk) sum_abc M,  dE/dep_p = sum over the
+//   three index positions of M restricted to p,  M = w W (P W + H) d^2  (adj_eps_*)
+//   dE/dT1(x,a) = 2 v1(a,x)                                          (adj_finish)
+// W is recomputed per tuple by the forward GEMMs (nothing of size nu^3 is kept
+// across tuples).  The W-build GEMM X_g(p,q,s) = sum_h sum_k E[x_h][perm_h(p,q)][k]
+// F[fyz_h][s][k] is bilinear, so with G_g = dE/dX_g:
+//   dE[x_h][perm_h(r)] += G_g(r,:) F[fyz_h]          (bwd_e_kernel, K = NP)
+//   dF[fyz_h]          += G_g^T E[x_h][perm_h(.)]     (bwd_f_kernel, K = nu^2, split-K)
+// and dE, dF are scattered back onto packed VVVO, T2 and VM (adj_scatter_*), the
+// adjoint of cct_layout.cu.  All sums run in a fixed order (no floating-point
+// atomics): gradients are bitwise reproducible.
+#include <algorithm>
+
+#include "cct_internal.cuh"
+
+namespace cct {
+namespace {
+
+__host__ __device__ constexpr int term_entry(int kind, int term, int f) {
+  // W(x0,x1,x2) += X_g(x_al0, x_al1, x_al2): {g, al0, al1, al2} (same table as cct_reduce.cu)
+  constexpr int tab[3][4][4] = {{{0, 0, 1, 2}, {1, 0, 2, 1}, {2, 1, 2, 0}, {0, 0, 0, 0}},
+                                {{0, 0, 1, 2}, {0, 0, 2, 1}, {1, 1, 2, 0}, {1, 2, 1, 0}},
+                                {{0, 0, 1, 2}, {0, 1, 0, 2}, {1, 0, 2, 1}, {1, 1, 2, 0}}};
+  return tab[kind][term][f];
+}
+__host__ __device__ constexpr int nterms(int kind) { return kind == kIJK ? 3 : 4; }
+
+struct AdjTuple {
+  const double *x[3];
+  int i, j, k;
+  double weight;
+};
+
+__device__ __forceinline__ int64_t widx(int nu, int a, int b, int c) { return ((int64_t)a * nu + b) * nu + c; }
+
+// ---------------------------------------------------------------------------- W assembly
+template <int KIND>
+__global__ void adj_wfull_kernel(int nu, int64_t NP, AdjTuple t, double *__restrict__ Wf) {
+  const int64_t n3 = (int64_t)nu * nu * nu;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e % nu);
+    const int64_t ab = e / nu;
+    const int b = (int)(ab % nu), a = (int)(ab / nu);
+    const int xs[3] = {a, b, c};
+    double w = 0.0;
+#pragma unroll
+    for (int term = 0; term < nterms(KIND); term++) {
+      const int g = term_entry(KIND, term, 0);
+      const int p = xs[term_entry(KIND, term, 1)], q = xs[term_entry(KIND, term, 2)],
+                s = xs[term_entry(KIND, term, 3)];
+      w += t.x[g][((int64_t)p * nu + q) * NP + s];
+    }
+    Wf[e] = (a == b && b == c) ? 0.0 : w;
+  }
+}
+
+// ---------------------------------------------------------------------------- dE/dW and M
+// S_m at the permuted triple (r0,r1,r2) of (a,b,c): u_x(r0) VOE(r1,r2,y,z).
+struct SmTable {
+  int x[6], y[6], z[6];
+};
+
+// H = sum_m sum_pi c_pi S_m(pi^-1) regrouped by which occupied role R (i, j, k)
+// feeds u and at which position p0 of (a,b,c) u is evaluated:
+//   H(a,b,c) = sum_R [ u_R(a) Q_R0(b,c) + u_R(b) Q_R1(a,c) + u_R(c) Q_R2(a,b) ],
+// each Q a signed sum of VOE planes, some transposed (built per tuple by adj_q_kernel).
+constexpr int kQTerms = 8;
+struct QTable {
+  int n[9];
+  int coef[9][kQTerms];
+  int64_t plane[9][kQTerms];  // offset of VOE(., ., y, z)
+  int trans[9][kQTerms];      // 1: the plane is read as V(s, r)
+};
+
+__global__ void adj_q_kernel(int nu, QTable q, const double *__restrict__ voe, double *__restrict__ Q) {
+  const int64_t nu2 = (int64_t)nu * nu;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 9 * nu2; e += (int64_t)gridDim.x * blockDim.x) {
+    const int g = (int)(e / nu2);
+    const int64_t rs = e - (int64_t)g * nu2;
+    const int r = (int)(rs / nu), sidx = (int)(rs - (int64_t)r * nu);
+    double v = 0.0;
+    for (int u = 0; u < q.n[g]; u++) {
+      const double *pl = voe + q.plane[g][u];
+      v += (double)q.coef[g][u] * (q.trans[g][u] ? pl[(int64_t)r * nu + sidx] : pl[(int64_t)sidx * nu + r]);
+    }
+    Q[e] = v;  // Q[g][r][s]
+  }
+}
+
+__global__ void adj_gw_kernel(int nu, int no, AdjTuple t, const double *__restrict__ Wf,
+                              const double *__restrict__ eh, const double *__restrict__ ep,
+                              const double *__restrict__ t1, const double *__restrict__ Q, double *__restrict__ GW,
+                              double *__restrict__ Mf) {
+  const int64_t n3 = (int64_t)nu * nu * nu, nu2 = (int64_t)nu * nu;
+  const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
+  const int xr[3] = {t.i, t.j, t.k};
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e % nu);
+    const int64_t ab = e / nu;
+    const int b = (int)(ab % nu), a = (int)(ab / nu);
+    const double wabc = Wf[e];
+    const double wacb = Wf[widx(nu, a, c, b)], wbac = Wf[widx(nu, b, a, c)], wbca = Wf[widx(nu, b, c, a)];
+    const double wcab = Wf[widx(nu, c, a, b)], wcba = Wf[widx(nu, c, b, a)];
+    const double pw = 8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab);
+    const double d = 1.0 / (dijk - (ep[a] + ep[b] + ep[c]));
+    double h = 0.0;
+#pragma unroll
+    for (int R = 0; R < 3; R++) {
+      const double *u = t1 + xr[R];  // T1(x_R, .) at stride no
+      const double *q = Q + (int64_t)(3 * R) * nu2;
+      h += 2.0 * u[(int64_t)a * no] * q[(int64_t)b * nu + c];
+      h += 2.0 * u[(int64_t)b * no] * q[nu2 + (int64_t)a * nu + c];
+      h += 2.0 * u[(int64_t)c * no] * q[2 * nu2 + (int64_t)a * nu + b];
+    }
+    const bool diag = (a == b && b == c);
+    GW[e] = diag ? 0.0 : t.weight * d * (2.0 * pw + h);
+    Mf[e] = diag ? 0.0 : t.weight * wabc * (pw + h) * d * d;
+  }
+}
+
+// ---------------------------------------------------------------------------- dVOE
+// Warp per (b,c) (b fastest over warps): lanes split the a-sum, then a fixed
+// shuffle tree; s_m = sum_a z_m(a,b,c) u_x(a) d and dVOE(b,c,y_m,z_m) += w s_m
+// for m = 1..6 in order.
+__global__ void adj_voe_kernel(int nu, int no, AdjTuple t, SmTable sm, const double *__restrict__ Wf,
+                               const double *__restrict__ eh, const double *__restrict__ ep,
+                               const double *__restrict__ t1, double *__restrict__ gvoe) {
+  const int64_t nu2 = (int64_t)nu * nu;
+  const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < nu2; e += wstride) {
+    const int b = (int)(e % nu), c = (int)(e / nu);
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    const double ebc = ep[b] + ep[c];
+    for (int a = lane; a < nu; a += 32) {
+      const double wabc = Wf[widx(nu, a, b, c)], wacb = Wf[widx(nu, a, c, b)], wbac = Wf[widx(nu, b, a, c)];
+      const double wbca = Wf[widx(nu, b, c, a)], wcab = Wf[widx(nu, c, a, b)], wcba = Wf[widx(nu, c, b, a)];
+      const double d = 1.0 / (dijk - (ep[a] + ebc));
+      const double z[6] = {(wabc - wbac) * 2.0 - wacb + wbca, (wacb - wbca) * 2.0 - wabc + wbac,
+                           (wbac - wabc) * 2.0 - wcab + wcba, (wbca - wacb) * 2.0 - wcba + wcab,
+                           (wcab - wcba) * 2.0 - wbac + wabc, (wcba - wcab) * 2.0 - wbca + wacb};
+#pragma unroll
+      for (int m = 0; m < 6; m++) s[m] = fma(z[m] * d, 2.0 * t1[sm.x[m] + (int64_t)no * a], s[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < 6; m++)
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) s[m] += __shfl_xor_sync(0xffffffffu, s[m], off);
+    if (lane == 0) {
+#pragma unroll
+      for (int m = 0; m < 6; m++) {
+        double *g = gvoe + ((int64_t)sm.z[m] * no + sm.y[m]) * nu2 + (int64_t)c * nu + b;
+        *g += t.weight * s[m];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------- dE/dX
+// G_g(y0,y1,y2) = sum over the terms of X_g of GW at x with x[al_r] = y_r;
+// columns y2 >= nu of the padded rows are zero.
+template <int KIND>
+__global__ void adj_gx_kernel(int nu, int64_t NP, const double *__restrict__ GW, double *G0, double *G1, double *G2) {
+  const int64_t n = (int64_t)nu * nu * NP;
+  double *G[3] = {G0, G1, G2};
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int y2 = (int)(e % NP);
+    const int64_t pq = e / NP;
+    const int y1 = (int)(pq % nu), y0 = (int)(pq / nu);
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (y2 < nu) {
+      const int ys[3] = {y0, y1, y2};
+#pragma unroll
+      for (int term = 0; term < nterms(KIND); term++) {
+        const int g = term_entry(KIND, term, 0);
+        int x[3];
+        x[term_entry(KIND, term, 1)] = ys[0];
+        x[term_entry(KIND, term, 2)] = ys[1];
+        x[term_entry(KIND, term, 3)] = ys[2];
+        acc[g] += GW[widx(nu, x[0], x[1], x[2])];
+      }
+    }
+    const int ng = KIND == kIJK ? 3 : 2;
+#pragma unroll
+    for (int g = 0; g < 3; g++)
+      if (g < ng) G[g][e] = acc[g];
+  }
+}
+
+// ---------------------------------------------------------------------------- eps
+// dE/dep_p = sum_bc M(p,b,c) + sum_ac M(a,p,c) + sum_ab M(a,b,p) and
+// dE/deh_x -= (multiplicity of x) sum_abc M, from two coalesced passes over M:
+//   rows:    Rw[a][b]      = sum_c M(a,b,c)                 (warp per row)
+//   columns: Cl[chunk][c]  = sum of M(row, c) over 64 rows   (thread per column)
+// then a warp per p sums Rw[p][:] + Rw[:][p] + Cl[:][p].  Every sum has a
+// fixed order.
+constexpr int kColChunk = 64;
+__global__ void adj_eps_rows_kernel(int nu, const double *__restrict__ Mf, double *__restrict__ Rw) {
+  const int64_t nrow = (int64_t)nu * nu;
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrow; r += wstride) {
+    double v = 0.0;
+    for (int c = lane; c < nu; c += 32) v += Mf[r * nu + c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) Rw[r] = v;
+  }
+}
+
+__global__ void adj_eps_cols_kernel(int nu, const double *__restrict__ Mf, double *__restrict__ Cl) {
+  const int64_t nrow = (int64_t)nu * nu;
+  const int64_t nchunk = (nrow + kColChunk - 1) / kColChunk;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nchunk * nu;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ch = e / nu;
+    const int c = (int)(e - ch * nu);
+    const int64_t r1 = min((ch + 1) * kColChunk, nrow);
+    double v = 0.0;
+    for (int64_t r = ch * kColChunk; r < r1; r++) v += Mf[r * nu + c];
+    Cl[e] = v;
+  }
+}
+
+__global__ void adj_eps_final_kernel(int nu, AdjTuple t, const double *__restrict__ Rw, const double *__restrict__ Cl,
+                                     double *__restrict__ gep, double *__restrict__ geh) {
+  const int64_t nchunk = ((int64_t)nu * nu + kColChunk - 1) / kColChunk;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const int p = blockIdx.x * wpb + (threadIdx.x >> 5);
+  if (p < nu) {
+    double v = 0.0;
+    for (int q = lane; q < nu; q += 32) v += Rw[(int64_t)p * nu + q] + Rw[(int64_t)q * nu + p];
+    for (int64_t ch = lane; ch < nchunk; ch += 32) v += Cl[ch * nu + p];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) gep[p] += v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 32) {  // sum_abc M = sum of all row sums, one warp
+    double tot = 0.0;
+    for (int64_t r = lane; r < (int64_t)nu * nu; r += 32) tot += Rw[r];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, off);
+    if (lane == 0) {
+      geh[t.i] -= tot;
+      geh[t.j] -= tot;
+      geh[t.k] -= tot;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------- backward GEMMs
+constexpr int BBM = 128, BBK = 16;  // N tile BN in {64, 48, 32}, chosen to fit KP
+constexpr int BWM = 32;                 // rows per warp
+constexpr int BNT = (BBM / BWM) * 32;   // 128 threads
+constexpr int BST = 3;                  // cp.async stages
+constexpr int LDA_MK = BBK + 4;         // A tile [m][k]
+constexpr int LDA_KM = BBM + 8;         // A tile [k][m]
+template <int BN>
+constexpr int ldb_kn() { return BN + 8; }  // B tile [k][n]; rows 16 banks apart (conflict-free)
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+__device__ __forceinline__ int64_t tperm(int64_t m, int nu, int perm) {
+  if (!perm) return m;
+  const int64_t p = m / nu, q = m - p * nu;
+  return q * nu + p;
+}
+
+constexpr int kMaxPairs = 6;  // (slot, half) pairs of one tuple: at most 3 x 2
+struct BwdPair {
+  const double *A;  // dE/dX_g (nu^2 x NP)
+  const double *B;  // bwd_e: F[fyz] (NP x KP); bwd_f: E[x] (nu^2 x KP)
+  int perm;         // 1: (p,q) <-> (q,p) row permutation of the half
+  int out;          // output index
+};
+struct BwdEArgs {
+  BwdPair pair[kMaxPairs];
+  double *out[3];
+  int first[4], npairs;  // pairs of output o are first[o] .. first[o+1]-1
+  int nu;
+  int64_t NP, KP;
+  int tiles_n;
+};
+
+// dE[x](r, n) += sum_pairs sum_s A[perm(r)][s] B[s][n]; M = nu^2, N = KP, K = NP per pair.
+template <int BN>
+__global__ void __launch_bounds__(BNT, 2) bwd_e_kernel(const BwdEArgs args) {
+  constexpr int BBN = BN, LDB_KN = ldb_kn<BN>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBM][LDA_MK]
+  double *Bs = As + BST * BBM * LDA_MK;                 // [BST][BBK][LDB_KN]
+  const int o = blockIdx.y;
+  const int tile_m = blockIdx.x / args.tiles_n, tile_n = blockIdx.x - tile_m * args.tiles_n;
+  const int nu = args.nu;
+  const int64_t M = (int64_t)nu * nu, NP = args.NP, KP = args.KP;
+  const int64_t m0 = (int64_t)tile_m * BBM;
+  const int n0 = tile_n * BBN;
+  const int tid = threadIdx.x;
+  const int p_begin = args.first[o], p_end = args.first[o + 1];
+  const int kt_per = (int)((NP + BBK - 1) / BBK);  // NP is a multiple of 8, not always of 16
+  const int ktiles = kt_per * (p_end - p_begin);
+
+  auto load_stage = [&](int stage, int kt) {
+    const int pi = p_begin + kt / kt_per;
+    const int64_t k0 = (int64_t)(kt % kt_per) * BBK;
+    const BwdPair &pr = args.pair[pi];
+    double *as = As + stage * BBM * LDA_MK;
+    double *bs = Bs + stage * BBK * LDB_KN;
+    const int chunk = tid & 7;  // 8 x 16 B per 16-double row
+    for (int rr = tid >> 3; rr < BBM; rr += BNT / 8) {
+      const int64_t m = m0 + rr;
+      const bool ok = m < M && k0 + chunk * 2 < NP;
+      const double *src = pr.A + (ok ? tperm(m, nu, pr.perm) * NP + k0 + chunk * 2 : 0);
+      cp_async16(as + rr * LDA_MK + chunk * 2, src, ok ? 16 : 0);
+    }
+    // B tile: 16 rows (s) x 64 columns (n): 32 chunks of 16 B per row
+    for (int c = tid; c < BBK * (BBN / 2); c += BNT) {
+      const int rr = c / (BBN / 2), cc = c - rr * (BBN / 2);
+      const int n = n0 + cc * 2;
+      const bool ok = n < KP && k0 + rr < NP;
+      const double *src = pr.B + (ok ? (k0 + rr) * KP + n : 0);
+      cp_async16(bs + rr * LDB_KN + cc * 2, src, ok ? 16 : 0);
+    }
+  };
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  constexpr int MF = BWM / 16, NF = BBN / 8;
+  double acc[MF][NF][4];
+#pragma unroll
+  for (int i = 0; i < MF; i++)
+#pragma unroll
+    for (int j = 0; j < NF; j++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < BST - 1; s++) {
+    if (s < ktiles) load_stage(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < ktiles; kt++) {
+    cp_async_wait<BST - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + BST - 1;
+      if (nk < ktiles) load_stage(nk % BST, nk);
+      cp_async_commit();
+    }
+    const double *as = As + (kt % BST) * BBM * LDA_MK + (warp * BWM) * LDA_MK;
+    const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
+#pragma unroll
+    for (int kk = 0; kk < BBK; kk += 4) {
+      double af[MF][2], bf[NF];
+#pragma unroll
+      for (int i = 0; i < MF; i++) {
+        af[i][0] = as[(i * 16 + g) * LDA_MK + kk + t];
+        af[i][1] = as[(i * 16 + g + 8) * LDA_MK + kk + t];
+      }
+#pragma unroll
+      for (int j = 0; j < NF; j++) bf[j] = bs[(kk + t) * LDB_KN + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < MF; i++)
+#pragma unroll
+        for (int j = 0; j < NF; j++) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+  if (ktiles == 0) return;
+  double *out = args.out[o];
+#pragma unroll
+  for (int i = 0; i < MF; i++) {
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      const int64_t m = m0 + warp * BWM + i * 16 + g + half * 8;
+      if (m >= M) continue;
+      double *orow = out + m * KP;
+#pragma unroll
+      for (int j = 0; j < NF; j++) {
+        const int n = n0 + j * 8 + 2 * t;
+        if (n < KP) {
+          double2 v = *reinterpret_cast<double2 *>(orow + n);
+          v.x += acc[i][j][2 * half];
+          v.y += acc[i][j][2 * half + 1];
+          *reinterpret_cast<double2 *>(orow + n) = v;
+        }
+      }
+    }
+  }
+}
+
+struct BwdFArgs {
+  BwdPair pair[6];
+  double *part;     // [pair][split][NP][KP]
+  int npairs, nsplit;
+  int64_t kchunk;   // rows of nu^2 per split (multiple of BBK)
+  int nu;
+  int64_t NP, KP;
+  int tiles_n;
+};
+
+// part[pair][split](s, n) = sum_{m in split} A[m][s] B[perm(m)][n]; M = NP, N = KP.
+template <int BN>
+__global__ void __launch_bounds__(BNT, 2) bwd_f_kernel(const BwdFArgs args) {
+  constexpr int BBN = BN, LDB_KN = ldb_kn<BN>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBK][LDA_KM]
+  double *Bs = As + BST * BBK * LDA_KM;                 // [BST][BBK][LDB_KN]
+  const int pi = blockIdx.y, split = blockIdx.z;
+  const BwdPair &pr = args.pair[pi];
+  const int tile_m = blockIdx.x / args.tiles_n, tile_n = blockIdx.x - tile_m * args.tiles_n;
+  const int nu = args.nu;
+  const int64_t Mtot = (int64_t)nu * nu, NP = args.NP, KP = args.KP;
+  const int64_t s0 = (int64_t)tile_m * BBM;
+  const int n0 = tile_n * BBN;
+  const int64_t kbeg = (int64_t)split * args.kchunk;
+  const int64_t kend = min(kbeg + args.kchunk, Mtot);
+  const int ktiles = kend > kbeg ? (int)((kend - kbeg + BBK - 1) / BBK) : 0;
+  const int tid = threadIdx.x;
+
+  auto load_stage = [&](int stage, int kt) {
+    const int64_t k0 = kbeg + (int64_t)kt * BBK;
+    double *as = As + stage * BBK * LDA_KM;
+    double *bs = Bs + stage * BBK * LDB_KN;
+    // A tile: 16 rows (m) x 128 columns (s): 64 chunks per row
+    for (int c = tid; c < BBK * (BBM / 2); c += BNT) {
+      const int rr = c / (BBM / 2), cc = c - rr * (BBM / 2);
+      const int64_t m = k0 + rr, s = s0 + cc * 2;
+      const bool ok = m < kend && s < NP;
+      const double *src = pr.A + (ok ? m * NP + s : 0);
+      cp_async16(as + rr * LDA_KM + cc * 2, src, ok ? 16 : 0);
+    }
+    for (int c = tid; c < BBK * (BBN / 2); c += BNT) {
+      const int rr = c / (BBN / 2), cc = c - rr * (BBN / 2);
+      const int64_t m = k0 + rr;
+      const int n = n0 + cc * 2;
+      const bool ok = m < kend && n < KP;
+      const double *src = pr.B + (ok ? tperm(m, nu, pr.perm) * KP + n : 0);
+      cp_async16(bs + rr * LDB_KN + cc * 2, src, ok ? 16 : 0);
+    }
+  };
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  constexpr int MF = BWM / 16, NF = BBN / 8;
+  double acc[MF][NF][4];
+#pragma unroll
+  for (int i = 0; i < MF; i++)
+#pragma unroll
+    for (int j = 0; j < NF; j++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < BST - 1; s++) {
+    if (s < ktiles) load_stage(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < ktiles; kt++) {
+    cp_async_wait<BST - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + BST - 1;
+      if (nk < ktiles) load_stage(nk % BST, nk);
+      cp_async_commit();
+    }
+    const double *as = As + (kt % BST) * BBK * LDA_KM + warp * BWM;
+    const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
+#pragma unroll
+    for (int kk = 0; kk < BBK; kk += 4) {
+      double af[MF][2], bf[NF];
+#pragma unroll
+      for (int i = 0; i < MF; i++) {
+        af[i][0] = as[(kk + t) * LDA_KM + i * 16 + g];
+        af[i][1] = as[(kk + t) * LDA_KM + i * 16 + g + 8];
+      }
+#pragma unroll
+      for (int j = 0; j < NF; j++) bf[j] = bs[(kk + t) * LDB_KN + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < MF; i++)
+#pragma unroll
+        for (int j = 0; j < NF; j++) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+  double *out = args.part + ((int64_t)pi * args.nsplit + split) * NP * KP;
+#pragma unroll
+  for (int i = 0; i < MF; i++) {
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      const int64_t s = s0 + warp * BWM + i * 16 + g + half * 8;
+      if (s >= NP) continue;
+#pragma unroll
+      for (int j = 0; j < NF; j++) {
+        const int n = n0 + j * 8 + 2 * t;
+        if (n < KP)
+          *reinterpret_cast<double2 *>(out + s * KP + n) =
+              make_double2(acc[i][j][2 * half], acc[i][j][2 * half + 1]);
+      }
+    }
+  }
+}
+
+// dF[out] += sum over the pairs writing it, then over splits, in order.
+struct BwdFReduceArgs {
+  double *dst[6];
+  int first[7];     // pairs of output o: first[o] .. first[o+1]-1 (pairs sorted by output)
+  int nout, nsplit;
+  int64_t n;        // NP * KP
+};
+__global__ void bwd_f_reduce_kernel(const BwdFReduceArgs a, const double *__restrict__ part) {
+  const int o = blockIdx.y;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < a.n; e += (int64_t)gridDim.x * blockDim.x) {
+    double s = a.dst[o][e];
+    for (int pi = a.first[o]; pi < a.first[o + 1]; pi++)
+      for (int sp = 0; sp < a.nsplit; sp++) s += part[((int64_t)pi * a.nsplit + sp) * a.n + e];
+    a.dst[o][e] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------- scatters
+// Packed VVVO: column x*nu + r1 holds (I >= J) of (I J | r1 x) at I(I+1)/2 + J, and
+// E[x][r1][r2][k] = col[tri(k, r2)] for k < nu; E[x][r1][r2][nu+l] = -T2(r1,r2,l,x).
+__global__ void adj_scatter_e_kernel(int nu, int no, int64_t KP, const double *__restrict__ dE,
+                                     double *__restrict__ gvvvo, double *__restrict__ gt2) {
+  const int64_t nutr = (int64_t)nu * (nu + 1) / 2;
+  const int64_t ncol = (int64_t)nu * no;
+  const int64_t nu2 = (int64_t)nu * nu;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ncol * nutr;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = e / nutr, tri = e - col * nutr;
+    const int x = (int)(col / nu), r1 = (int)(col - (int64_t)x * nu);
+    int I = (int)((sqrt(8.0 * (double)tri + 1.0) - 1.0) * 0.5);
+    while ((int64_t)I * (I + 1) / 2 > tri) I--;
+    while ((int64_t)(I + 1) * (I + 2) / 2 <= tri) I++;
+    const int J = (int)(tri - (int64_t)I * (I + 1) / 2);
+    const double *row = dE + ((int64_t)x * nu2 + (int64_t)r1 * nu) * KP;  // rows (r1, r2)
+    double v = row[(int64_t)J * KP + I];
+    if (I != J) v += row[(int64_t)I * KP + J];
+    gvvvo[e] += v;
+  }
+  // T2 part: thread per (x, r1, r2, l)
+  const int64_t nt2 = (int64_t)no * nu2 * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nt2; e += (int64_t)gridDim.x * blockDim.x) {
+    // e enumerates T2(r1, r2, l, x) in its Fortran order
+    const int r1 = (int)(e % nu);
+    const int64_t rest = e / nu;
+    const int r2 = (int)(rest % nu);
+    const int64_t lx = rest / nu;
+    const int l = (int)(lx % no), x = (int)(lx / no);
+    gt2[e] -= dE[((int64_t)x * nu2 + (int64_t)r1 * nu + r2) * KP + nu + l];
+  }
+}
+
+// F[y][z][s][k] = T2(s,k,y,z) for k < nu; F[y][z][s][nu+l] = VM(l,s,z,y).
+__global__ void adj_scatter_f_kernel(int nu, int no, int64_t NP, int64_t KP, const double *__restrict__ dF,
+                                     double *__restrict__ gt2, double *__restrict__ gvm) {
+  const int64_t nu2 = (int64_t)nu * nu;
+  const int64_t nt2 = nu2 * no * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nt2; e += (int64_t)gridDim.x * blockDim.x) {
+    // T2(s, k, y, z), Fortran order
+    const int s = (int)(e % nu);
+    const int64_t r = e / nu;
+    const int k = (int)(r % nu);
+    const int64_t yz = r / nu;
+    const int y = (int)(yz % no), z = (int)(yz / no);
+    gt2[e] += dF[(((int64_t)y * no + z) * NP + s) * KP + k];
+  }
+  const int64_t nvm = (int64_t)no * nu * no * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvm; e += (int64_t)gridDim.x * blockDim.x) {
+    // VM(l, s, z, y), Fortran order
+    const int l = (int)(e % no);
+    const int64_t r = e / no;
+    const int s = (int)(r % nu);
+    const int64_t zy = r / nu;
+    const int z = (int)(zy % no), y = (int)(zy / no);
+    gvm[e] += dF[(((int64_t)y * no + z) * NP + s) * KP + nu + l];
+  }
+}
+
+// dT1(x,a) = 2 v1(a,x)
+__global__ void adj_t1_kernel(int nu, int no, const double *__restrict__ v1, double *__restrict__ gt1) {
+  const int64_t n = (int64_t)nu * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(e % no), a = (int)(e / no);
+    gt1[e] = 2.0 * v1[(int64_t)x * nu + a];
+  }
+}
+
+int grid_for(int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+template <int BN>
+constexpr int smem_e() { return BST * (BBM * LDA_MK + BBK * ldb_kn<BN>()) * 8; }
+template <int BN>
+constexpr int smem_f() { return BST * (BBK * LDA_KM + BBK * ldb_kn<BN>()) * 8; }
+// N tile for an N extent of KP: least padding, ties to the wider tile
+inline int bwd_bn(int64_t KP) {
+  int best = 64;
+  for (int bn : {48, 32})
+    if (round_up(KP, bn) < round_up(KP, best)) best = bn;
+  return best;
+}
+template <int BN>
+int launch_bwd_e(const BwdEArgs &a, int tiles_m, int nx, cudaStream_t s) {
+  bwd_e_kernel<BN><<<dim3(tiles_m * a.tiles_n, nx), BNT, smem_e<BN>(), s>>>(a);
+  CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
+}
+template <int BN>
+int launch_bwd_f(const BwdFArgs &a, int tiles_m, cudaStream_t s) {
+  bwd_f_kernel<BN><<<dim3(tiles_m * a.tiles_n, a.npairs, a.nsplit), BNT, smem_f<BN>(), s>>>(a);
+  CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
+}
+constexpr int64_t kFChunk = 1024;  // nu^2 rows per split of the dF GEMM
+
+}  // namespace
+
+int adj_alloc(const Dims &d, AdjBuffers *b) {
+  const int64_t no = d.no, nu = d.nu, nu2 = nu * nu, nu3 = nu2 * nu;
+  auto al = [](double **p, int64_t n) -> int {
+    *p = nullptr;
+    CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(p), (size_t)(n < 1 ? 1 : n) * 8));
+    return CCT_OK;
+  };
+  b->nsplit = (nu2 + kFChunk - 1) / kFChunk;
+  CCT_TRY(al(&b->dE, no * nu2 * d.KP));
+  CCT_TRY(al(&b->dF, no * no * d.NP * d.KP));
+  CCT_TRY(al(&b->Wf, nu3));
+  CCT_TRY(al(&b->GW, nu3));
+  CCT_TRY(al(&b->Mf, nu3));
+  for (int g = 0; g < 3; g++) CCT_TRY(al(&b->GX[g], nu2 * d.NP));
+  CCT_TRY(al(&b->part, 6 * b->nsplit * d.NP * d.KP));
+  CCT_TRY(al(&b->Q, 9 * nu2));
+  CCT_TRY(al(&b->eps, nu2 + ((nu2 + kColChunk - 1) / kColChunk) * nu));
+  CCT_TRY(al(&b->v1, 5 + nu * no));
+  CCT_TRY(al(&b->g_eh, no));
+  CCT_TRY(al(&b->g_ep, nu));
+  CCT_TRY(al(&b->g_t1, no * nu));
+  CCT_TRY(al(&b->g_t2, nu2 * no * no));
+  CCT_TRY(al(&b->g_vm, no * nu * no * no));
+  CCT_TRY(al(&b->g_voe, nu2 * no * no));
+  CCT_TRY(al(&b->g_vvvo, nu * (nu + 1) / 2 * nu * no));
+  b->ready = true;
+  return CCT_OK;
+}
+
+void adj_free(AdjBuffers *b) {
+  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->Mf, b->GX[0], b->GX[1], b->GX[2], b->part, b->Q, b->eps, b->v1, b->g_eh,
+                    b->g_ep, b->g_t1, b->g_t2, b->g_vm, b->g_voe, b->g_vvvo})
+    if (q) cudaFree(q);
+  *b = AdjBuffers{};
+}
+
+int adj_zero(const Dims &d, AdjBuffers *b, cudaStream_t s) {
+  const int64_t no = d.no, nu = d.nu, nu2 = nu * nu;
+  CCT_CUDA(cudaMemsetAsync(b->dE, 0, (size_t)no * nu2 * d.KP * 8, s));
+  CCT_CUDA(cudaMemsetAsync(b->dF, 0, (size_t)no * no * d.NP * d.KP * 8, s));
+  CCT_CUDA(cudaMemsetAsync(b->g_eh, 0, (size_t)no * 8, s));
+  CCT_CUDA(cudaMemsetAsync(b->g_ep, 0, (size_t)nu * 8, s));
+  CCT_CUDA(cudaMemsetAsync(b->g_voe, 0, (size_t)nu2 * no * no * 8, s));
+  return CCT_OK;
+}
+
+// The jobs of one tuple as (x1, x2, x3, nhalves) per X slot, as cct_plan.cu's
+// build_jobs lays them out.
+static void tuple_slots(const Tuple &t, int slots[3][4], int *nslots) {
+  auto G = [&](int s, int x1, int x2, int x3) { slots[s][0] = x1, slots[s][1] = x2, slots[s][2] = x3, slots[s][3] = 2; };
+  auto H = [&](int s, int x1, int x2, int x3) { slots[s][0] = x1, slots[s][1] = x2, slots[s][2] = x3, slots[s][3] = 1; };
+  if (t.kind == kIJK) {
+    G(0, t.i, t.j, t.k);
+    G(1, t.i, t.k, t.j);
+    G(2, t.j, t.k, t.i);
+    *nslots = 3;
+  } else if (t.kind == kIJJ) {
+    G(0, t.i, t.j, t.j);
+    H(1, t.j, t.j, t.i);
+    *nslots = 2;
+  } else {
+    H(0, t.i, t.i, t.k);
+    G(1, t.i, t.k, t.i);
+    *nslots = 2;
+  }
+}
+
+int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E, const double *F,
+              const double *eh, const double *ep, const double *t1, const double *voe, AdjBuffers *b,
+              cudaStream_t s) {
+  const int no = d.no, nu = d.nu;
+  const int64_t nu2 = (int64_t)nu * nu, nu3 = nu2 * nu;
+  AdjTuple at;
+  at.x[0] = X[0];
+  at.x[1] = X[1];
+  at.x[2] = X[2];
+  at.i = t.i;
+  at.j = t.j;
+  at.k = t.k;
+  at.weight = t.kind == kIJK ? 1.0 : 0.5;
+  SmTable sm;
+  const int smx[6][3] = {{t.i, t.j, t.k}, {t.i, t.k, t.j}, {t.j, t.i, t.k},
+                         {t.k, t.i, t.j}, {t.j, t.k, t.i}, {t.k, t.j, t.i}};
+  for (int m = 0; m < 6; m++) sm.x[m] = smx[m][0], sm.y[m] = smx[m][1], sm.z[m] = smx[m][2];
+
+  switch (t.kind) {
+    case kIJK: adj_wfull_kernel<kIJK><<<grid_for(nu3), 256, 0, s>>>(nu, d.NP, at, b->Wf); break;
+    case kIJJ: adj_wfull_kernel<kIJJ><<<grid_for(nu3), 256, 0, s>>>(nu, d.NP, at, b->Wf); break;
+    default: adj_wfull_kernel<kIIJ><<<grid_for(nu3), 256, 0, s>>>(nu, d.NP, at, b->Wf); break;
+  }
+  CCT_CUDA(cudaGetLastError());
+  {
+    // H regrouped by (role of u, position of u): nine signed sums of VOE planes
+    constexpr int kAdj[6][4][4] = {{{2, 0, 1, 2}, {-2, 1, 0, 2}, {-1, 0, 2, 1}, {1, 2, 0, 1}},
+                                   {{2, 0, 2, 1}, {-2, 2, 0, 1}, {-1, 0, 1, 2}, {1, 1, 0, 2}},
+                                   {{2, 1, 0, 2}, {-2, 0, 1, 2}, {-1, 1, 2, 0}, {1, 2, 1, 0}},
+                                   {{2, 2, 0, 1}, {-2, 0, 2, 1}, {-1, 2, 1, 0}, {1, 1, 2, 0}},
+                                   {{2, 1, 2, 0}, {-2, 2, 1, 0}, {-1, 1, 0, 2}, {1, 0, 1, 2}},
+                                   {{2, 2, 1, 0}, {-2, 1, 2, 0}, {-1, 2, 0, 1}, {1, 0, 2, 1}}};
+    constexpr int kRole[6] = {0, 0, 1, 2, 1, 2};  // z_1..z_6 take u from i, i, j, k, j, k
+    QTable qt{};
+    for (int m = 0; m < 6; m++)
+      for (int r = 0; r < 4; r++) {
+        const int g = kRole[m] * 3 + kAdj[m][r][1];
+        if (qt.n[g] >= kQTerms) {
+          set_error("adjoint: Q table overflow");
+          return CCT_ERR_INVALID;
+        }
+        const int u = qt.n[g]++;
+        qt.coef[g][u] = kAdj[m][r][0];
+        qt.plane[g][u] = ((int64_t)sm.z[m] * no + sm.y[m]) * nu2;
+        qt.trans[g][u] = kAdj[m][r][2] > kAdj[m][r][3];
+      }
+    adj_q_kernel<<<grid_for(9 * nu2), 256, 0, s>>>(nu, qt, voe, b->Q);
+    CCT_CUDA(cudaGetLastError());
+  }
+  adj_gw_kernel<<<grid_for(nu3), 256, 0, s>>>(nu, no, at, b->Wf, eh, ep, t1, b->Q, b->GW, b->Mf);
+  CCT_CUDA(cudaGetLastError());
+  adj_voe_kernel<<<grid_for(nu2 * 32), 256, 0, s>>>(nu, no, at, sm, b->Wf, eh, ep, t1, b->g_voe);
+  CCT_CUDA(cudaGetLastError());
+  {
+    const int64_t nchunk = (nu2 + kColChunk - 1) / kColChunk;
+    double *Rw = b->eps, *Cl = b->eps + nu2;
+    adj_eps_rows_kernel<<<grid_for(nu2 * 32), 256, 0, s>>>(nu, b->Mf, Rw);
+    CCT_CUDA(cudaGetLastError());
+    adj_eps_cols_kernel<<<grid_for(nchunk * nu), 256, 0, s>>>(nu, b->Mf, Cl);
+    CCT_CUDA(cudaGetLastError());
+    adj_eps_final_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, at, Rw, Cl, b->g_ep, b->g_eh);
+  }
+  CCT_CUDA(cudaGetLastError());
+  const int64_t ngx = nu2 * d.NP;
+  switch (t.kind) {
+    case kIJK: adj_gx_kernel<kIJK><<<grid_for(ngx), 256, 0, s>>>(nu, d.NP, b->GW, b->GX[0], b->GX[1], b->GX[2]); break;
+    case kIJJ: adj_gx_kernel<kIJJ><<<grid_for(ngx), 256, 0, s>>>(nu, d.NP, b->GW, b->GX[0], b->GX[1], b->GX[2]); break;
+    default: adj_gx_kernel<kIIJ><<<grid_for(ngx), 256, 0, s>>>(nu, d.NP, b->GW, b->GX[0], b->GX[1], b->GX[2]); break;
+  }
+  CCT_CUDA(cudaGetLastError());
+
+  // (slot, half) pairs: half h reads E[x_h] with row permutation h and F[fyz_h]
+  int slots[3][4], ns = 0;
+  tuple_slots(t, slots, &ns);
+  struct P {
+    int g, h, x, fyz;
+  };
+  std::vector<P> pairs;
+  for (int g = 0; g < ns; g++)
+    for (int h = 0; h < slots[g][3]; h++) {
+      const int x = h == 0 ? slots[g][0] : slots[g][1];
+      const int fyz = (h == 0 ? slots[g][1] : slots[g][0]) * no + slots[g][2];
+      pairs.push_back({g, h, x, fyz});
+    }
+  auto Ex = [&](int x) { return E + (int64_t)x * nu2 * d.KP; };
+  auto Fyz = [&](int yz) { return F + (int64_t)yz * d.NP * d.KP; };
+
+  // dE: outputs grouped by x, pairs in a fixed order
+  {
+    BwdEArgs a{};
+    int xs[3], nx = 0;
+    for (const P &q : pairs) {
+      bool seen = false;
+      for (int u = 0; u < nx; u++) seen |= xs[u] == q.x;
+      if (!seen) xs[nx++] = q.x;
+    }
+    int np_ = 0;
+    for (int o = 0; o < nx; o++) {
+      a.first[o] = np_;
+      a.out[o] = b->dE + (int64_t)xs[o] * nu2 * d.KP;
+      for (const P &q : pairs)
+        if (q.x == xs[o]) {
+          if (np_ >= kMaxPairs) {
+            set_error("adjoint: too many GEMM pairs for one E slab");
+            return CCT_ERR_INVALID;
+          }
+          a.pair[np_++] = BwdPair{b->GX[q.g], Fyz(q.fyz), q.h, o};
+        }
+    }
+    a.first[nx] = np_;
+    a.npairs = np_;
+    a.nu = nu;
+    a.NP = d.NP;
+    a.KP = d.KP;
+    const int bn = bwd_bn(d.KP);
+    a.tiles_n = (int)((d.KP + bn - 1) / bn);
+    const int tiles_m = (int)((nu2 + BBM - 1) / BBM);
+    CCT_TRY(bn == 64 ? launch_bwd_e<64>(a, tiles_m, nx, s)
+                     : bn == 48 ? launch_bwd_e<48>(a, tiles_m, nx, s) : launch_bwd_e<32>(a, tiles_m, nx, s));
+  }
+  // dF: one partial per pair and split, then a fixed-order sum per output slab
+  {
+    BwdFArgs a{};
+    std::vector<P> sorted = pairs;
+    std::stable_sort(sorted.begin(), sorted.end(), [](const P &u, const P &v) { return u.fyz < v.fyz; });
+    BwdFReduceArgs r{};
+    int no_ = 0;
+    for (size_t q = 0; q < sorted.size(); q++) {
+      a.pair[q] = BwdPair{b->GX[sorted[q].g], Ex(sorted[q].x), sorted[q].h, 0};
+      if (q == 0 || sorted[q].fyz != sorted[q - 1].fyz) {
+        r.first[no_] = (int)q;
+        r.dst[no_] = b->dF + (int64_t)sorted[q].fyz * d.NP * d.KP;
+        no_++;
+      }
+    }
+    r.first[no_] = (int)sorted.size();
+    r.nout = no_;
+    r.nsplit = (int)b->nsplit;
+    r.n = d.NP * d.KP;
+    a.part = b->part;
+    a.npairs = (int)sorted.size();
+    a.nsplit = (int)b->nsplit;
+    a.kchunk = kFChunk;
+    a.nu = nu;
+    a.NP = d.NP;
+    a.KP = d.KP;
+    const int bn = bwd_bn(d.KP);
+    a.tiles_n = (int)((d.KP + bn - 1) / bn);
+    const int tiles_m = (int)((d.NP + BBM - 1) / BBM);
+    CCT_TRY(bn == 64 ? launch_bwd_f<64>(a, tiles_m, s)
+                     : bn == 48 ? launch_bwd_f<48>(a, tiles_m, s) : launch_bwd_f<32>(a, tiles_m, s));
+    bwd_f_reduce_kernel<<<dim3(grid_for(r.n) < 64 ? grid_for(r.n) : 64, r.nout), 256, 0, s>>>(r, b->part);
+    CCT_CUDA(cudaGetLastError());
+  }
+  return CCT_OK;
+}
+
+int adj_configure(int device) {
+  static int configured = -1;
+  if (configured == device) return CCT_OK;
+  CCT_CUDA(cudaFuncSetAttribute(bwd_e_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_e<64>()));
+  CCT_CUDA(cudaFuncSetAttribute(bwd_e_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_e<48>()));
+  CCT_CUDA(cudaFuncSetAttribute(bwd_e_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_e<32>()));
+  CCT_CUDA(cudaFuncSetAttribute(bwd_f_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_f<64>()));
+  CCT_CUDA(cudaFuncSetAttribute(bwd_f_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_f<48>()));
+  CCT_CUDA(cudaFuncSetAttribute(bwd_f_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_f<32>()));
+  configured = device;
+  return CCT_OK;
+}
+
+int adj_finish(const Dims &d, const double *v1, AdjBuffers *b, cudaStream_t s) {
+  const int64_t no = d.no, nu = d.nu, nu2 = nu * nu;
+  CCT_CUDA(cudaMemsetAsync(b->g_t2, 0, (size_t)nu2 * no * no * 8, s));
+  CCT_CUDA(cudaMemsetAsync(b->g_vm, 0, (size_t)no * nu * no * no * 8, s));
+  CCT_CUDA(cudaMemsetAsync(b->g_vvvo, 0, (size_t)(nu * (nu + 1) / 2) * nu * no * 8, s));
+  const int64_t ne = std::max<int64_t>((nu * (nu + 1) / 2) * nu * no, no * nu2 * no);
+  adj_scatter_e_kernel<<<grid_for(ne), 256, 0, s>>>(d.nu, d.no, d.KP, b->dE, b->g_vvvo, b->g_t2);
+  CCT_CUDA(cudaGetLastError());
+  adj_scatter_f_kernel<<<grid_for(nu2 * no * no), 256, 0, s>>>(d.nu, d.no, d.NP, d.KP, b->dF, b->g_t2, b->g_vm);
+  CCT_CUDA(cudaGetLastError());
+  adj_t1_kernel<<<grid_for(nu * no), 256, 0, s>>>(d.nu, d.no, v1, b->g_t1);
+  CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
+}
+
+}  // namespace cct

@@ -158,6 +158,29 @@ int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const
 int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const double *etd_acc, double *out3,
                cudaStream_t s);
 
+// adjoint.cu: device buffers of the backward pass (allocated at the first ccT_backward)
+struct AdjBuffers {
+  bool ready = false;
+  double *dE = nullptr, *dF = nullptr;                 // gradients of the GEMM operands E, F
+  double *Wf = nullptr, *GW = nullptr, *Mf = nullptr;  // dense nu^3: W, dE/dW, denominator terms
+  double *GX[3] = {};                                  // dE/dX_g, nu^2 x NP each
+  double *part = nullptr;                              // split-K partials of the dF GEMMs
+  int64_t nsplit = 0;
+  double *Q = nullptr;                                 // 9 nu^2 VOE combinations of dE/dW
+  double *eps = nullptr;                               // row sums and 64-row column sums of M
+  double *v1 = nullptr;                                // FP64 v1 of an emulated plan: 5 + nu*no
+  double *g_eh = nullptr, *g_ep = nullptr, *g_t1 = nullptr, *g_t2 = nullptr, *g_vm = nullptr, *g_voe = nullptr,
+         *g_vvvo = nullptr;                            // gradients in the input layouts
+};
+int adj_alloc(const Dims &d, AdjBuffers *b);
+void adj_free(AdjBuffers *b);
+int adj_configure(int device);
+int adj_zero(const Dims &d, AdjBuffers *b, cudaStream_t s);
+int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E, const double *F,
+              const double *eh, const double *ep, const double *t1, const double *voe, AdjBuffers *b,
+              cudaStream_t s);
+int adj_finish(const Dims &d, const double *v1, AdjBuffers *b, cudaStream_t s);
+
 // peak.cu
 double measure_fp64_peak(int device);
 double measure_int8_peak(int device);

@@ -81,6 +81,10 @@ struct ccT_plan {
   std::vector<int> prof_class;  // class of each recorded pair
   double kernel_ms[2] = {0.0, 0.0};
   int64_t kernel_launches[2] = {0, 0};
+  // backward: buffers and the saved context (range of the last successful forward)
+  AdjBuffers adj;
+  int64_t fwd_begin = -1, fwd_end = -1;
+  float last_bwd_ms = 0.f;
 };
 
 namespace {
@@ -436,6 +440,7 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   const int64_t nvvvo = nu * (nu + 1) / 2 * nu * no;
   const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   p->inputs_ready = false;
+  p->fwd_begin = p->fwd_end = -1;
   CCT_CUDA(cudaMemcpyAsync(p->eh, eh, no * 8, kind, p->stream));
   CCT_CUDA(cudaMemcpyAsync(p->ep, ep, nu * 8, kind, p->stream));
   CCT_CUDA(cudaMemcpyAsync(p->t1, t1, no * nu * 8, kind, p->stream));
@@ -517,6 +522,7 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   CCT_TRY(prof_collect(p));
   if (ets) *ets = out3[0];
   if (etd) *etd = out3[1];
+  p->fwd_begin = p->fwd_end = -1;
   if (werr) {
     set_error("an emulated W-build kernel ran out its bounded wait and unwound");
     return CCT_ERR_TIMEOUT;
@@ -525,8 +531,82 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
     set_error("E(T) is not finite");
     return CCT_ERR_NONFINITE;
   }
+  p->fwd_begin = begin;
+  p->fwd_end = end;
   return CCT_OK;
 }
+
+int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *d_ep, double *d_t1, double *d_t2,
+                 double *d_vm, double *d_voe, double *d_vvvo, int32_t mem) {
+  if (!p) {
+    set_error("plan is NULL");
+    return CCT_ERR_INVALID;
+  }
+  if (mem != CCT_MEM_HOST && mem != CCT_MEM_DEVICE) {
+    set_error("mem must be CCT_MEM_HOST or CCT_MEM_DEVICE");
+    return CCT_ERR_INVALID;
+  }
+  if (!p->inputs_ready || begin != p->fwd_begin || end != p->fwd_end) {
+    set_error("ccT_backward needs a successful ccT_forward over the same tuple range first");
+    return CCT_ERR_STATE;
+  }
+  DeviceGuard guard(p->device);
+  const Dims &d = p->d;
+  if (!p->adj.ready) {
+    const int s = adj_alloc(d, &p->adj);
+    if (s != CCT_OK) {
+      adj_free(&p->adj);
+      return s;
+    }
+  }
+  CCT_TRY(adj_configure(p->device));
+  const int64_t ntup = (int64_t)p->tuples.size();
+  CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
+  CCT_TRY(adj_zero(d, &p->adj, p->stream));
+  // dT1 = 2 v1: an emulated plan's v1 is rebuilt from the FP64 W of this pass
+  if (p->emulated) CCT_CUDA(cudaMemsetAsync(p->adj.v1, 0, (5 + (size_t)d.nu * d.no) * 8, p->stream));
+  for (int64_t t = begin; t < end; t++) {
+    const Tuple &tu = p->tuples[t];
+    // W recomputed in FP64 into X buffer set 0
+    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * (0 * ntup + t), tu.kind == kIJK ? 3 : 2, p->stream));
+    CCT_TRY(adj_tuple(d, tu, p->X[0], p->E, p->F, p->eh, p->ep, p->t1, p->voe, &p->adj, p->stream));
+    if (p->emulated) {
+      TupleDev td;
+      td.x[0] = p->X[0][0];
+      td.x[1] = p->X[0][1];
+      td.x[2] = p->X[0][2];
+      td.kind = tu.kind;
+      td.i = tu.i;
+      td.j = tu.j;
+      td.k = tu.k;
+      td.weight = tu.kind == kIJK ? 1.0 : 0.5;
+      CCT_TRY(launch_reduce(d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->stream));
+      CCT_TRY(launch_finalize(d, td, p->xpart, p->vpart, p->adj.v1, p->adj.v1 + 5, p->stream));
+    }
+  }
+  CCT_TRY(adj_finish(d, p->emulated ? p->adj.v1 + 5 : v1_acc(p), &p->adj, p->stream));
+  CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
+  const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const int64_t no = d.no, nu = d.nu, nu2 = nu * nu;
+  const struct {
+    double *dst;
+    const double *src;
+    int64_t n;
+  } outs[] = {{d_eh, p->adj.g_eh, no},
+              {d_ep, p->adj.g_ep, nu},
+              {d_t1, p->adj.g_t1, no * nu},
+              {d_t2, p->adj.g_t2, nu2 * no * no},
+              {d_vm, p->adj.g_vm, no * nu * no * no},
+              {d_voe, p->adj.g_voe, nu2 * no * no},
+              {d_vvvo, p->adj.g_vvvo, nu * (nu + 1) / 2 * nu * no}};
+  for (const auto &o : outs)
+    if (o.dst) CCT_CUDA(cudaMemcpyAsync(o.dst, o.src, (size_t)o.n * 8, kind, p->stream));
+  CCT_CUDA(cudaStreamSynchronize(p->stream));
+  CCT_CUDA(cudaEventElapsedTime(&p->last_bwd_ms, p->ev0, p->ev1));
+  return CCT_OK;
+}
+
+double ccT_last_backward_ms(const ccT_plan *p) { return p ? (double)p->last_bwd_ms : 0.0; }
 
 int ccT_set_stream(ccT_plan *p, void *cuda_stream) {
   if (!p) {
@@ -612,6 +692,7 @@ int ccT_plan_destroy(ccT_plan *p) {
   for (void *b : {(void *)p->emu.E8, (void *)p->emu.E8T, (void *)p->emu.F8, (void *)p->emu.expE,
                   (void *)p->emu.expET, (void *)p->emu.expF, (void *)p->emu.expRowF, (void *)p->emu_jobs})
     if (b) cudaFree(b);
+  adj_free(&p->adj);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   for (cudaEvent_t e : p->prof_events) cudaEventDestroy(e);

@@ -54,9 +54,12 @@ __device__ __forceinline__ T sel3(int m, T v0, T v1, T v2) {
   return m == 0 ? v0 : (m == 1 ? v1 : v2);
 }
 
-// VOE staging: three block pairs x six planes x 64: pair 0 (b,c), 1 (a,c), 2 (a,b);
-// planes 0..5 = (j,k) (k,j) (i,k) (k,i) (i,j) (j,i); plane ^ 1 swaps the pair's order.
-constexpr int VPAIR = 6 * 64;
+// VOE staging: three block pairs x two orientations x six planes x 64 entries:
+// pair 0 (b,c), 1 (a,c), 2 (a,b); orientation 0 holds VOE(lo, hi, y, z) of the
+// pair's lower and higher coordinates, orientation 1 VOE(hi, lo, y, z); planes
+// 0..5 = (y,z) = (j,k) (k,j) (i,k) (k,i) (i,j) (j,i).  Every element reads the
+// VOE entries t1wt3.f90:80-85 name, so no symmetry of VOE is assumed.
+constexpr int VPAIR = 2 * 6 * 64;
 __device__ __forceinline__ int nb_of(int nu) { return (nu + RB - 1) / RB; }
 constexpr int REDUCE_SMEM = (6 * SL + 3 * VPAIR) * 8;
 
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t N
   constexpr int NTERM = KIND == kIJK ? 3 : 4;
   extern __shared__ __align__(16) double dyn_smem[];
   double *Wsm = dyn_smem;             // [6][SL]
-  double *Vsm = Wsm + 6 * SL;         // [3][6][64]
+  double *Vsm = Wsm + 6 * SL;         // [3][2][6][64]
   __shared__ double red[RT / 32];
   __shared__ double warpA[RT / 32][RB][3], warpB[RT / 32][4][3], warpC[RT / 32][2][3];
 
@@ -140,9 +143,9 @@ __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t N
   {
     const int64_t nu2 = (int64_t)nu * nu;
     for (int q = tid; q < 3 * VPAIR; q += RT) {
-      const int pr = q / VPAIR, plane = (q / 64) % 6, r = q & 63;
-      const int B1 = pr == 0 ? S1 : S0, B2 = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
-      const int f = RB * B1 + (r & 7), s2 = RB * B2 + (r >> 3);
+      const int pr = q / VPAIR, orient = (q / 384) & 1, plane = (q / 64) % 6, r = q & 63;
+      const int Blo = pr == 0 ? S1 : S0, Bhi = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
+      const int f = RB * (orient ? Bhi : Blo) + (r & 7), s2 = RB * (orient ? Blo : Bhi) + (r >> 3);
       const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
       const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
       double v = 0.0;
@@ -173,13 +176,9 @@ __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t N
     for (int p = 0; p < 6; p++)
       w[p] = Wsm[slot[p] * SL + soff(lc[pm(p, 0)], lc[pm(p, 1)], lc[pm(p, 2)])];
     const double dinv = mult * __drcp_rn(dijk - (ep[a] + ep[b] + ep[c]));
-    // VOE values of the three index pairs, all six planes
-    double vo[3][6];
+    // VOE entry offsets of the three index pairs: (lo, hi) in orientation 0, (hi, lo) in 1
     const int rp[3] = {l1 + 8 * l2, l0 + 8 * l2, l0 + 8 * l1};
-#pragma unroll
-    for (int pr = 0; pr < 3; pr++)
-#pragma unroll
-      for (int pl = 0; pl < 6; pl++) vo[pr][pl] = Vsm[pr * VPAIR + pl * 64 + rp[pr]];
+    const int rpT[3] = {384 + l2 + 8 * l1, 384 + l2 + 8 * l0, 384 + l1 + 8 * l0};
 #pragma unroll
     for (int pi = 0; pi < 6; pi++) {
       // element pi(x); its role values: abc acb bac bca cab cba
@@ -196,11 +195,11 @@ __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t N
       // other two coordinates, in order (pm(pi,1), pm(pi,2))
       const int first = pm(pi, 0);
       const int pr = first;                         // pair index = the coordinate left out
-      const int flip = pm(pi, 1) > pm(pi, 2) ? 1 : 0;
-      const double *v = vo[pr];
-      const double ci = (z1 * v[0 ^ flip] + z2 * v[1 ^ flip]) * dinv;
-      const double cj = (z3 * v[2 ^ flip] + z5 * v[3 ^ flip]) * dinv;
-      const double ck = (z4 * v[4 ^ flip] + z6 * v[5 ^ flip]) * dinv;
+      const bool flip = pm(pi, 1) > pm(pi, 2);  // the element's (second, third) = (hi, lo)
+      const double *v = Vsm + pr * VPAIR + (flip ? rpT[pr] : rp[pr]);
+      const double ci = (z1 * v[0] + z2 * v[64]) * dinv;
+      const double cj = (z3 * v[128] + z5 * v[192]) * dinv;
+      const double ck = (z4 * v[256] + z6 * v[320]) * dinv;
       if (first == 0) {
         accA[0] += ci; accA[1] += cj; accA[2] += ck;
       } else if (first == 1) {

@@ -452,5 +452,129 @@ def closed_cc_triples(inp, tuples=None):
     return ets, etd, v1
 
 
+# --------------------------------------------------------------------------- adjoint (hand-derived)
+#
+# E(T) = sum_t w_t sum_abc [ W (P W) + sum_m z_m S_m ] / D           (closed_reduce, with
+#   P W = 8W_abc - 4(W_acb + W_cba + W_bac) + 2(W_bca + W_cab),      ets = 2 sum T1 v1
+#   S_m(a,b,c) = u_x(a) VOE(b,c,y,z),  u_x(a) = 2 T1(x,a)             written per tuple)
+# D is symmetric in (a,b,c), so  dE/dW = w (2 P W + H) / D  with H the adjoint of the
+# z_m combinations applied to S_m (each W at a permuted index moves to S at the
+# inverse permutation).  The W-build is bilinear: every closed-form term
+# W ±= A (x) B gives dA ±= dW (x) B and dB ±= A (x) dW.
+
+# (sign, einsum spec, operand A, operand B) of the twelve closed_w terms; operands
+# are ('T2', l-or-':' slice) etc. resolved per tuple.
+_W_TERMS = (
+    (-1, "abl,lc->abc", ("T2x", "i"), ("VM", "k", "j")),     # 0
+    (+1, "dba,cd->abc", ("veo", "i"), ("T2", "j", "k")),     # 11
+    (+1, "ad,dcb->abc", ("T2", "k", "i"), ("veo", "j")),     # 8
+    (-1, "la,bcl->abc", ("VM", "i", "k"), ("T2x", "j")),     # 3
+    (-1, "acl,lb->abc", ("T2x", "i"), ("VM", "j", "k")),     # 1
+    (+1, "dca,bd->abc", ("veo", "i"), ("T2", "k", "j")),     # 10
+    (+1, "ad,dbc->abc", ("T2", "j", "i"), ("veo", "k")),     # 6
+    (-1, "la,cbl->abc", ("VM", "i", "j"), ("T2x", "k")),     # 5
+    (-1, "bal,lc->abc", ("T2x", "j"), ("VM", "k", "i")),     # 2
+    (+1, "dab,cd->abc", ("veo", "j"), ("T2", "i", "k")),     # 9
+    (-1, "lb,cal->abc", ("VM", "j", "i"), ("T2x", "k")),     # 4
+    (+1, "bd,dac->abc", ("T2", "i", "j"), ("veo", "k")),     # 7
+)
+
+
+def _z_adjoint(s):
+    """H contributions of the six z_m: for z_m = sum_pi c_pi W(pi), sum_abc z_m S d =
+    sum_abc W (sum_pi c_pi S(pi^-1)) d.  Returns the six adjoint combinations in the
+    order z1..z6, each a list of (coefficient, spec) applied to that z's S."""
+    return {
+        1: ((2, "abc"), (-2, "bac"), (-1, "acb"), (1, "cab")),
+        2: ((2, "acb"), (-2, "cab"), (-1, "abc"), (1, "bac")),
+        3: ((2, "bac"), (-2, "abc"), (-1, "bca"), (1, "cba")),
+        4: ((2, "cab"), (-2, "acb"), (-1, "cba"), (1, "bca")),
+        5: ((2, "bca"), (-2, "cba"), (-1, "bac"), (1, "abc")),
+        6: ((2, "cba"), (-2, "bca"), (-1, "cab"), (1, "acb")),
+    }[s]
+
+
+def closed_grad(inp, tuples=None):
+    """Hand-derived FP64 gradient of E(T) = ets + etd with respect to every input,
+    in the input layouts: dict with eh (no), ep (nu), t1 (no*nu, file layout),
+    t2 (nu*nu*no*no), vm (no*nu*no*no), voe (nu*nu*no*no), vvvo (packed, like
+    the input), and e_t.  W is recomputed per tuple (nothing of size nu^3 is kept
+    across tuples)."""
+    V = _Views(inp)
+    no, nu = inp.no, inp.nu
+    tuples = tuples or all_tuples(no)
+    veo = {x: expand_vvvo(inp, x) for x in range(no)}
+    ets, etd, v1 = closed_cc_triples(inp, tuples)
+    gT2 = np.zeros((nu, nu, no, no), order="F")
+    gVM = np.zeros((no, nu, no, no), order="F")
+    gVOE = np.zeros((nu, nu, no, no), order="F")
+    gveo = {x: np.zeros((nu, nu, nu), order="F") for x in range(no)}
+    geh, gep = np.zeros(no), np.zeros(nu)
+    VOE4 = V.VOE.reshape((nu, nu, no, no), order="F")
+    u = 2.0 * V.t1  # u[x, a] = 2 T1(x, a)
+    r = np.arange(nu)
+    for kind, i, j, k in tuples:
+        weight = 1.0 if kind == 0 else 0.5
+        w = closed_w(V, i, j, k, veo)
+        d = _dinv(V, i, j, k)
+        P = lambda s, a=w: _perm(a, s)
+        pw = 8 * w - 4 * (P("acb") + P("cba") + P("bac")) + 2 * (P("bca") + P("cab"))
+        smap = {1: (i, j, k), 2: (i, k, j), 3: (j, i, k), 4: (k, i, j), 5: (j, k, i), 6: (k, j, i)}
+        H = np.zeros((nu, nu, nu))
+        for m, (x, y, z) in smap.items():
+            S = u[x][:, None, None] * VOE4[None, :, :, y, z]
+            for c, spec in _z_adjoint(m):
+                H += c * _perm(S, spec)
+        gw = weight * d * (2.0 * pw + H)
+        gw[r, r, r] = 0.0
+        # denominators: E_t = w sum N d with N ~ W (P W + H) on each permutation orbit
+        Mw = weight * w * (pw + H) * d * d
+        tot = float(Mw.sum())
+        for x in (i, j, k):
+            geh[x] -= tot
+        gep += Mw.sum(axis=(1, 2)) + Mw.sum(axis=(0, 2)) + Mw.sum(axis=(0, 1))
+        # VOE: dVOE(b,c,y,z) += w sum_a z_m(a,b,c) u_x(a) d(a,b,c)
+        zs = {1: (w - P("bac")) * 2 - P("acb") + P("bca"), 2: (P("acb") - P("bca")) * 2 - w + P("bac"),
+              3: (P("bac") - w) * 2 - P("cab") + P("cba"), 4: (P("bca") - P("acb")) * 2 - P("cba") + P("cab"),
+              5: (P("cab") - P("cba")) * 2 - P("bac") + w, 6: (P("cba") - P("cab")) * 2 - P("bca") + P("acb")}
+        for m, (x, y, z) in smap.items():
+            gVOE[:, :, y, z] += weight * np.einsum("abc,a->bc", zs[m] * d, u[x])
+        # the twelve W-build terms
+        idx = {"i": i, "j": j, "k": k}
+
+        def operand(spec):
+            kind_, *ix = spec
+            if kind_ == "T2x":
+                x = idx[ix[0]]
+                return V.T2f[:, :, :, x], gT2[:, :, :, x]
+            if kind_ == "T2":
+                return V.T2f[:, :, idx[ix[0]], idx[ix[1]]], gT2[:, :, idx[ix[0]], idx[ix[1]]]
+            if kind_ == "VM":
+                return V.VM[:, :, idx[ix[0]], idx[ix[1]]], gVM[:, :, idx[ix[0]], idx[ix[1]]]
+            x = idx[ix[0]]
+            return veo[x], gveo[x]
+
+        for sign, spec, sa, sb in _W_TERMS:
+            ins, out = spec.split("->")
+            sA, sB = ins.split(",")
+            A, gA = operand(sa)
+            B, gB = operand(sb)
+            gA += sign * np.einsum(f"{out},{sB}->{sA}", gw, B, optimize=True)
+            gB += sign * np.einsum(f"{sA},{out}->{sB}", A, gw, optimize=True)
+    # packed VVVO: column x*nu + c holds (I >= J) of (I J | c x), tril order
+    nutr = nu * (nu + 1) // 2
+    gvvvo = np.zeros((nu * no, nutr))
+    I, J = np.tril_indices(nu)
+    for x in range(no):
+        g = gveo[x]
+        for c in range(nu):
+            sq = g[:, :, c]
+            gvvvo[x * nu + c] = np.where(I == J, sq[I, J], sq[I, J] + sq[J, I])
+    gt1 = 2.0 * v1.T  # dE/dT1(x,a) = 2 v1(a,x)
+    return {"eh": geh, "ep": gep, "t1": np.asfortranarray(gt1).ravel(order="F"),
+            "t2": gT2.ravel(order="F"), "vm": gVM.ravel(order="F"), "voe": gVOE.ravel(order="F"),
+            "vvvo": gvvvo.ravel(), "e_t": ets + etd}
+
+
 def cpu_threads() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)

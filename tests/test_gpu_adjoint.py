@@ -1,0 +1,119 @@
+"""ccT_backward (hand-written adjoint kernels) against the hand-derived FP64 CPU
+gradient and central finite differences of the GPU forward."""
+import copy
+
+import numpy as np
+import pytest
+
+from libcc_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("eh", "ep", "t1", "t2", "vm", "voe", "vvvo")
+
+
+@pytest.fixture(scope="module")
+def api():
+    from libcc_b200 import api as A
+    return A
+
+
+def _close(got, ref, rel=1e-10):
+    scale = max(np.abs(ref).max(), 1e-300)
+    return np.abs(got - ref).max() <= rel * scale
+
+
+@pytest.mark.parametrize("no,nu,seed", [(4, 7, 0), (5, 16, 1), (3, 9, 2), (2, 12, 3), (6, 40, 4), (5, 33, 6)])
+def test_backward_matches_cpu_adjoint(api, no, nu, seed):
+    from oracle import oracle as O
+    inp = S.generate(no, nu, seed)
+    ref = O.closed_grad(inp)
+    with api.TriplesPlan(no, nu) as plan:
+        plan.set_system(inp)
+        plan.forward()
+        g = plan.backward()
+    for name in NAMES:
+        assert _close(g[name], ref[name]), (name, np.abs(g[name] - ref[name]).max(), np.abs(ref[name]).max())
+
+
+def test_backward_of_a_tuple_range(api):
+    from oracle import oracle as O
+    no, nu = 5, 20
+    inp = S.generate(no, nu, 11)
+    tuples = O.all_tuples(no)
+    for begin, end in [(0, 4), (7, 10), (10, len(tuples))]:
+        ref = O.closed_grad(inp, tuples[begin:end])
+        with api.TriplesPlan(no, nu) as plan:
+            plan.set_system(inp)
+            plan.forward(begin, end)
+            g = plan.backward(begin, end)
+        for name in NAMES:
+            assert _close(g[name], ref[name]), (begin, end, name)
+
+
+def test_backward_needs_matching_forward(api):
+    from libcc_b200 import _native as N
+    inp = S.generate(4, 10, 3)
+    with api.TriplesPlan(4, 10) as plan:
+        plan.set_system(inp)
+        with pytest.raises(N.CctError) as e:
+            plan.backward()
+        assert e.value.status == 6  # CCT_ERR_STATE
+        plan.forward(0, 3)
+        with pytest.raises(N.CctError):
+            plan.backward(0, 4)
+        plan.backward(0, 3)
+        plan.set_system(inp)  # new inputs drop the saved context
+        with pytest.raises(N.CctError):
+            plan.backward(0, 3)
+
+
+def test_backward_bitwise_reproducible(api):
+    inp = S.generate(5, 24, 8)
+    with api.TriplesPlan(5, 24) as plan:
+        plan.set_system(inp)
+        plan.forward()
+        a = plan.backward()
+        b = plan.backward()
+    for name in NAMES:
+        assert np.array_equal(a[name], b[name]), name
+
+
+def test_backward_after_emulated_forward(api):
+    """An emulated plan's backward recomputes W in FP64: same gradient as FP64."""
+    from oracle import oracle as O
+    inp = S.generate(4, 18, 9)
+    ref = O.closed_grad(inp)
+    with api.TriplesPlan(4, 18, precision="int8") as plan:
+        plan.set_system(inp)
+        plan.forward()
+        g = plan.backward()
+    for name in NAMES:
+        assert _close(g[name], ref[name]), name
+
+
+def test_backward_central_differences_of_gpu_forward(api):
+    """Central differences (h = 1e-5) of the GPU FP64 E(T) on random entries of
+    every input.  E(T) is at most quadratic in each single T2/VM/VVVO entry and
+    linear in T1/VOE, so the central difference is exact up to rounding there."""
+    no, nu = 6, 30
+    inp = S.generate(no, nu, 13)
+    with api.TriplesPlan(no, nu) as plan:
+        plan.set_system(inp)
+        plan.forward()
+        g = plan.backward()
+        rng = np.random.default_rng(2)
+        for name in NAMES:
+            arr = getattr(inp, name)
+            scale = np.abs(g[name]).max()
+            for idx in rng.choice(arr.size, size=min(6, arr.size), replace=False):
+                h = 1e-5 * max(1.0, abs(arr[idx]))
+                vals = []
+                for sgn in (1.0, -1.0):
+                    ip = copy.deepcopy(inp)
+                    getattr(ip, name)[idx] += sgn * h
+                    plan.set_system(ip)
+                    ets, etd, _ = plan.forward(want_v1=False)
+                    vals.append(ets + etd)
+                fd = (vals[0] - vals[1]) / (2 * h)
+                assert abs(fd - g[name][idx]) <= 1e-6 * scale + 1e-8 * abs(fd), (name, idx, fd, g[name][idx])
