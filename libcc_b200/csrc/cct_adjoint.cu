@@ -47,13 +47,12 @@ struct AdjTuple {
 __device__ __forceinline__ int64_t widx(int nu, int a, int b, int c) { return ((int64_t)a * nu + b) * nu + c; }
 
 // ---------------------------------------------------------------------------- W assembly
+// Grids of the dense nu^3 kernels: x = 128-wide blocks of c, y = b, z = a.
 template <int KIND>
 __global__ void adj_wfull_kernel(int nu, int64_t NP, AdjTuple t, double *__restrict__ Wf) {
-  const int64_t n3 = (int64_t)nu * nu * nu;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(e % nu);
-    const int64_t ab = e / nu;
-    const int b = (int)(ab % nu), a = (int)(ab / nu);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y, a = blockIdx.z;
+  if (c < nu) {
+    const int64_t e = widx(nu, a, b, c);
     const int xs[3] = {a, b, c};
     double w = 0.0;
 #pragma unroll
@@ -100,72 +99,74 @@ __global__ void adj_q_kernel(int nu, QTable q, const double *__restrict__ voe, d
   }
 }
 
+// Thread per (b, c) and chunk of kAChunk consecutive a (grid x: c blocks, y: b,
+// z: a chunks).  For each (a,b,c) of its chunk a thread forms dE/dW and M, and
+// accumulates s_m = sum_a z_m(a,b,c) u_x(a) d for the VOE gradient into
+// vpart[chunk][m][c][b]; adj_voe_sum_kernel adds the chunks in order.
+constexpr int kAChunk = 16;
 __global__ void adj_gw_kernel(int nu, int no, AdjTuple t, const double *__restrict__ Wf,
                               const double *__restrict__ eh, const double *__restrict__ ep,
                               const double *__restrict__ t1, const double *__restrict__ Q, double *__restrict__ GW,
-                              double *__restrict__ Mf) {
-  const int64_t n3 = (int64_t)nu * nu * nu, nu2 = (int64_t)nu * nu;
+                              double *__restrict__ Mf, double *__restrict__ vpart) {
+  const int64_t nu2 = (int64_t)nu * nu;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y, ach = blockIdx.z;
+  if (c >= nu) return;
   const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
   const int xr[3] = {t.i, t.j, t.k};
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(e % nu);
-    const int64_t ab = e / nu;
-    const int b = (int)(ab % nu), a = (int)(ab / nu);
+  double qb0[3], ub[3], uc[3];
+#pragma unroll
+  for (int R = 0; R < 3; R++) {
+    qb0[R] = Q[(int64_t)(3 * R) * nu2 + (int64_t)b * nu + c];  // Q_R0(b,c)
+    ub[R] = 2.0 * t1[xr[R] + (int64_t)no * b];
+    uc[R] = 2.0 * t1[xr[R] + (int64_t)no * c];
+  }
+  const double ebc = ep[b] + ep[c];
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  const int a1 = min(nu, (ach + 1) * kAChunk);
+  for (int a = ach * kAChunk; a < a1; a++) {
+    const int64_t e = widx(nu, a, b, c);
     const double wabc = Wf[e];
     const double wacb = Wf[widx(nu, a, c, b)], wbac = Wf[widx(nu, b, a, c)], wbca = Wf[widx(nu, b, c, a)];
     const double wcab = Wf[widx(nu, c, a, b)], wcba = Wf[widx(nu, c, b, a)];
     const double pw = 8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab);
-    const double d = 1.0 / (dijk - (ep[a] + ep[b] + ep[c]));
+    const double d = 1.0 / (dijk - (ep[a] + ebc));
     double h = 0.0;
+    double ua[3];
 #pragma unroll
     for (int R = 0; R < 3; R++) {
-      const double *u = t1 + xr[R];  // T1(x_R, .) at stride no
+      ua[R] = 2.0 * t1[xr[R] + (int64_t)no * a];
       const double *q = Q + (int64_t)(3 * R) * nu2;
-      h += 2.0 * u[(int64_t)a * no] * q[(int64_t)b * nu + c];
-      h += 2.0 * u[(int64_t)b * no] * q[nu2 + (int64_t)a * nu + c];
-      h += 2.0 * u[(int64_t)c * no] * q[2 * nu2 + (int64_t)a * nu + b];
+      h += ua[R] * qb0[R];
+      h += ub[R] * q[nu2 + (int64_t)a * nu + c];
+      h += uc[R] * q[2 * nu2 + (int64_t)a * nu + b];
     }
     const bool diag = (a == b && b == c);
     GW[e] = diag ? 0.0 : t.weight * d * (2.0 * pw + h);
     Mf[e] = diag ? 0.0 : t.weight * wabc * (pw + h) * d * d;
+    const double z[6] = {(wabc - wbac) * 2.0 - wacb + wbca, (wacb - wbca) * 2.0 - wabc + wbac,
+                         (wbac - wabc) * 2.0 - wcab + wcba, (wbca - wacb) * 2.0 - wcba + wcab,
+                         (wcab - wcba) * 2.0 - wbac + wabc, (wcba - wcab) * 2.0 - wbca + wacb};
+    // z_1..z_6 take u from the roles i, i, j, k, j, k
+    constexpr int role[6] = {0, 0, 1, 2, 1, 2};
+#pragma unroll
+    for (int m = 0; m < 6; m++) s[m] = fma(z[m] * d, ua[role[m]], s[m]);
   }
+#pragma unroll
+  for (int m = 0; m < 6; m++) vpart[((int64_t)ach * 6 + m) * nu2 + (int64_t)c * nu + b] = s[m];
 }
 
-// ---------------------------------------------------------------------------- dVOE
-// Warp per (b,c) (b fastest over warps): lanes split the a-sum, then a fixed
-// shuffle tree; s_m = sum_a z_m(a,b,c) u_x(a) d and dVOE(b,c,y_m,z_m) += w s_m
-// for m = 1..6 in order.
-__global__ void adj_voe_kernel(int nu, int no, AdjTuple t, SmTable sm, const double *__restrict__ Wf,
-                               const double *__restrict__ eh, const double *__restrict__ ep,
-                               const double *__restrict__ t1, double *__restrict__ gvoe) {
+// dVOE(b,c,y_m,z_m) += w sum_chunks vpart[chunk][m][c][b], m = 1..6 in order
+// (planes of a degenerate tuple may coincide, so one thread owns all six).
+__global__ void adj_voe_sum_kernel(int nu, int no, int nchunk, AdjTuple t, SmTable sm,
+                                   const double *__restrict__ vpart, double *__restrict__ gvoe) {
   const int64_t nu2 = (int64_t)nu * nu;
-  const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
-  const int lane = threadIdx.x & 31;
-  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < nu2; e += wstride) {
-    const int b = (int)(e % nu), c = (int)(e / nu);
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    const double ebc = ep[b] + ep[c];
-    for (int a = lane; a < nu; a += 32) {
-      const double wabc = Wf[widx(nu, a, b, c)], wacb = Wf[widx(nu, a, c, b)], wbac = Wf[widx(nu, b, a, c)];
-      const double wbca = Wf[widx(nu, b, c, a)], wcab = Wf[widx(nu, c, a, b)], wcba = Wf[widx(nu, c, b, a)];
-      const double d = 1.0 / (dijk - (ep[a] + ebc));
-      const double z[6] = {(wabc - wbac) * 2.0 - wacb + wbca, (wacb - wbca) * 2.0 - wabc + wbac,
-                           (wbac - wabc) * 2.0 - wcab + wcba, (wbca - wacb) * 2.0 - wcba + wcab,
-                           (wcab - wcba) * 2.0 - wbac + wabc, (wcba - wcab) * 2.0 - wbca + wacb};
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu2; e += (int64_t)gridDim.x * blockDim.x) {
+    // e = c*nu + b
 #pragma unroll
-      for (int m = 0; m < 6; m++) s[m] = fma(z[m] * d, 2.0 * t1[sm.x[m] + (int64_t)no * a], s[m]);
-    }
-#pragma unroll
-    for (int m = 0; m < 6; m++)
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) s[m] += __shfl_xor_sync(0xffffffffu, s[m], off);
-    if (lane == 0) {
-#pragma unroll
-      for (int m = 0; m < 6; m++) {
-        double *g = gvoe + ((int64_t)sm.z[m] * no + sm.y[m]) * nu2 + (int64_t)c * nu + b;
-        *g += t.weight * s[m];
-      }
+    for (int m = 0; m < 6; m++) {
+      double v = 0.0;
+      for (int ch = 0; ch < nchunk; ch++) v += vpart[((int64_t)ch * 6 + m) * nu2 + e];
+      gvoe[((int64_t)sm.z[m] * no + sm.y[m]) * nu2 + e] += t.weight * v;
     }
   }
 }
@@ -175,12 +176,10 @@ __global__ void adj_voe_kernel(int nu, int no, AdjTuple t, SmTable sm, const dou
 // columns y2 >= nu of the padded rows are zero.
 template <int KIND>
 __global__ void adj_gx_kernel(int nu, int64_t NP, const double *__restrict__ GW, double *G0, double *G1, double *G2) {
-  const int64_t n = (int64_t)nu * nu * NP;
   double *G[3] = {G0, G1, G2};
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int y2 = (int)(e % NP);
-    const int64_t pq = e / NP;
-    const int y1 = (int)(pq % nu), y0 = (int)(pq / nu);
+  const int y2 = blockIdx.x * blockDim.x + threadIdx.x, y1 = blockIdx.y, y0 = blockIdx.z;
+  if (y2 < NP) {
+    const int64_t e = ((int64_t)y0 * nu + y1) * NP + y2;
     double acc[3] = {0.0, 0.0, 0.0};
     if (y2 < nu) {
       const int ys[3] = {y0, y1, y2};
@@ -236,8 +235,8 @@ __global__ void adj_eps_cols_kernel(int nu, const double *__restrict__ Mf, doubl
   }
 }
 
-__global__ void adj_eps_final_kernel(int nu, AdjTuple t, const double *__restrict__ Rw, const double *__restrict__ Cl,
-                                     double *__restrict__ gep, double *__restrict__ geh) {
+__global__ void adj_eps_final_kernel(int nu, const double *__restrict__ Rw, const double *__restrict__ Cl,
+                                     double *__restrict__ gep) {
   const int64_t nchunk = ((int64_t)nu * nu + kColChunk - 1) / kColChunk;
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
@@ -250,16 +249,29 @@ __global__ void adj_eps_final_kernel(int nu, AdjTuple t, const double *__restric
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     if (lane == 0) gep[p] += v;
   }
-  if (blockIdx.x == 0 && threadIdx.x < 32) {  // sum_abc M = sum of all row sums, one warp
-    double tot = 0.0;
-    for (int64_t r = lane; r < (int64_t)nu * nu; r += 32) tot += Rw[r];
+}
+
+// R1[p] = sum_q Rw[p][q] (warp per p); then one warp: sum_abc M = sum_p R1[p].
+__global__ void adj_eps_planes_kernel(int nu, const double *__restrict__ Rw, double *__restrict__ R1) {
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (p >= nu) return;
+  double v = 0.0;
+  for (int q = lane; q < nu; q += 32) v += Rw[(int64_t)p * nu + q];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, off);
-    if (lane == 0) {
-      geh[t.i] -= tot;
-      geh[t.j] -= tot;
-      geh[t.k] -= tot;
-    }
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (lane == 0) R1[p] = v;
+}
+__global__ void adj_eps_total_kernel(int nu, AdjTuple t, const double *__restrict__ R1, double *__restrict__ geh) {
+  const int lane = threadIdx.x & 31;
+  double tot = 0.0;
+  for (int p = lane; p < nu; p += 32) tot += R1[p];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, off);
+  if (lane == 0) {
+    geh[t.i] -= tot;
+    geh[t.j] -= tot;
+    geh[t.k] -= tot;
   }
 }
 
@@ -269,9 +281,11 @@ constexpr int BWM = 32;                 // rows per warp
 constexpr int BNT = (BBM / BWM) * 32;   // 128 threads
 constexpr int BST = 3;                  // cp.async stages
 constexpr int LDA_MK = BBK + 4;         // A tile [m][k]
-constexpr int LDA_KM = BBM + 8;         // A tile [k][m]
+// Fragment loads are 64-bit, served per half-warp (lanes g = 0..3, t = 0..3):
+// a [k][.] tile is conflict-free when its row stride is 4 (mod 16) doubles.
+constexpr int LDA_KM = BBM + 4;         // A tile [k][m]
 template <int BN>
-constexpr int ldb_kn() { return BN + 8; }  // B tile [k][n]; rows 16 banks apart (conflict-free)
+constexpr int ldb_kn() { return BN + 4; }  // B tile [k][n]
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -288,10 +302,9 @@ __device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, dou
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
       : "d"(a0), "d"(a1), "d"(b0));
 }
-__device__ __forceinline__ int64_t tperm(int64_t m, int nu, int perm) {
-  if (!perm) return m;
-  const int64_t p = m / nu, q = m - p * nu;
-  return q * nu + p;
+// (p,q) <-> (q,p) row permutation through a table (no integer division per row)
+__device__ __forceinline__ int64_t tperm(int64_t m, const int *__restrict__ ptab, int perm) {
+  return perm ? (int64_t)ptab[m] : m;
 }
 
 constexpr int kMaxPairs = 6;  // (slot, half) pairs of one tuple: at most 3 x 2
@@ -305,6 +318,7 @@ struct BwdEArgs {
   BwdPair pair[kMaxPairs];
   double *out[3];
   int first[4], npairs;  // pairs of output o are first[o] .. first[o+1]-1
+  const int *ptab;       // ptab[p*nu+q] = q*nu+p
   int nu;
   int64_t NP, KP;
   int tiles_n;
@@ -338,7 +352,7 @@ __global__ void __launch_bounds__(BNT, 2) bwd_e_kernel(const BwdEArgs args) {
     for (int rr = tid >> 3; rr < BBM; rr += BNT / 8) {
       const int64_t m = m0 + rr;
       const bool ok = m < M && k0 + chunk * 2 < NP;
-      const double *src = pr.A + (ok ? tperm(m, nu, pr.perm) * NP + k0 + chunk * 2 : 0);
+      const double *src = pr.A + (ok ? tperm(m, args.ptab, pr.perm) * NP + k0 + chunk * 2 : 0);
       cp_async16(as + rr * LDA_MK + chunk * 2, src, ok ? 16 : 0);
     }
     // B tile: 16 rows (s) x 64 columns (n): 32 chunks of 16 B per row
@@ -422,6 +436,7 @@ struct BwdFArgs {
   double *part;     // [pair][split][NP][KP]
   int npairs, nsplit;
   int64_t kchunk;   // rows of nu^2 per split (multiple of BBK)
+  const int *ptab;
   int nu;
   int64_t NP, KP;
   int tiles_n;
@@ -463,7 +478,7 @@ __global__ void __launch_bounds__(BNT, 2) bwd_f_kernel(const BwdFArgs args) {
       const int64_t m = k0 + rr;
       const int n = n0 + cc * 2;
       const bool ok = m < kend && n < KP;
-      const double *src = pr.B + (ok ? tperm(m, nu, pr.perm) * KP + n : 0);
+      const double *src = pr.B + (ok ? tperm(m, args.ptab, pr.perm) * KP + n : 0);
       cp_async16(bs + rr * LDB_KN + cc * 2, src, ok ? 16 : 0);
     }
   };
@@ -660,10 +675,19 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
   CCT_TRY(al(&b->Wf, nu3));
   CCT_TRY(al(&b->GW, nu3));
   CCT_TRY(al(&b->Mf, nu3));
-  for (int g = 0; g < 3; g++) CCT_TRY(al(&b->GX[g], nu2 * d.NP));
+  for (int set = 0; set < 2; set++)
+    for (int g = 0; g < 3; g++) CCT_TRY(al(&b->GX[set][g], nu2 * d.NP));
   CCT_TRY(al(&b->part, 6 * b->nsplit * d.NP * d.KP));
   CCT_TRY(al(&b->Q, 9 * nu2));
-  CCT_TRY(al(&b->eps, nu2 + ((nu2 + kColChunk - 1) / kColChunk) * nu));
+  CCT_TRY(al(&b->vpart, ((nu + kAChunk - 1) / kAChunk) * 6 * nu2));
+  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&b->ptab), (size_t)nu2 * sizeof(int)));
+  {
+    std::vector<int> h(nu2);
+    for (int64_t p = 0; p < nu; p++)
+      for (int64_t q = 0; q < nu; q++) h[p * nu + q] = (int)(q * nu + p);
+    CCT_CUDA(cudaMemcpy(b->ptab, h.data(), (size_t)nu2 * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  CCT_TRY(al(&b->eps, nu2 + ((nu2 + kColChunk - 1) / kColChunk) * nu + nu));
   CCT_TRY(al(&b->v1, 5 + nu * no));
   CCT_TRY(al(&b->g_eh, no));
   CCT_TRY(al(&b->g_ep, nu));
@@ -677,7 +701,9 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
 }
 
 void adj_free(AdjBuffers *b) {
-  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->Mf, b->GX[0], b->GX[1], b->GX[2], b->part, b->Q, b->eps, b->v1, b->g_eh,
+  if (b->ptab) cudaFree(b->ptab);
+  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->Mf, b->GX[0][0], b->GX[0][1], b->GX[0][2], b->GX[1][0],
+                    b->GX[1][1], b->GX[1][2], b->part, b->Q, b->vpart, b->eps, b->v1, b->g_eh,
                     b->g_ep, b->g_t1, b->g_t2, b->g_vm, b->g_voe, b->g_vvvo})
     if (q) cudaFree(q);
   *b = AdjBuffers{};
@@ -714,9 +740,9 @@ static void tuple_slots(const Tuple &t, int slots[3][4], int *nslots) {
   }
 }
 
-int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E, const double *F,
-              const double *eh, const double *ep, const double *t1, const double *voe, AdjBuffers *b,
-              cudaStream_t s) {
+int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const double *eh, const double *ep,
+                        const double *t1, const double *voe, AdjBuffers *b, int set, cudaStream_t s) {
+  double *const *GX = b->GX[set];
   const int no = d.no, nu = d.nu;
   const int64_t nu2 = (int64_t)nu * nu, nu3 = nu2 * nu;
   AdjTuple at;
@@ -732,10 +758,11 @@ int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E
                          {t.k, t.i, t.j}, {t.j, t.k, t.i}, {t.k, t.j, t.i}};
   for (int m = 0; m < 6; m++) sm.x[m] = smx[m][0], sm.y[m] = smx[m][1], sm.z[m] = smx[m][2];
 
+  const dim3 g3((nu + 127) / 128, nu, nu);  // x: c blocks, y: b, z: a
   switch (t.kind) {
-    case kIJK: adj_wfull_kernel<kIJK><<<grid_for(nu3), 256, 0, s>>>(nu, d.NP, at, b->Wf); break;
-    case kIJJ: adj_wfull_kernel<kIJJ><<<grid_for(nu3), 256, 0, s>>>(nu, d.NP, at, b->Wf); break;
-    default: adj_wfull_kernel<kIIJ><<<grid_for(nu3), 256, 0, s>>>(nu, d.NP, at, b->Wf); break;
+    case kIJK: adj_wfull_kernel<kIJK><<<g3, 128, 0, s>>>(nu, d.NP, at, b->Wf); break;
+    case kIJJ: adj_wfull_kernel<kIJJ><<<g3, 128, 0, s>>>(nu, d.NP, at, b->Wf); break;
+    default: adj_wfull_kernel<kIIJ><<<g3, 128, 0, s>>>(nu, d.NP, at, b->Wf); break;
   }
   CCT_CUDA(cudaGetLastError());
   {
@@ -763,10 +790,14 @@ int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E
     adj_q_kernel<<<grid_for(9 * nu2), 256, 0, s>>>(nu, qt, voe, b->Q);
     CCT_CUDA(cudaGetLastError());
   }
-  adj_gw_kernel<<<grid_for(nu3), 256, 0, s>>>(nu, no, at, b->Wf, eh, ep, t1, b->Q, b->GW, b->Mf);
-  CCT_CUDA(cudaGetLastError());
-  adj_voe_kernel<<<grid_for(nu2 * 32), 256, 0, s>>>(nu, no, at, sm, b->Wf, eh, ep, t1, b->g_voe);
-  CCT_CUDA(cudaGetLastError());
+  {
+    const int nch = (nu + kAChunk - 1) / kAChunk;
+    adj_gw_kernel<<<dim3((nu + 127) / 128, nu, nch), 128, 0, s>>>(nu, no, at, b->Wf, eh, ep, t1, b->Q, b->GW, b->Mf,
+                                                                   b->vpart);
+    CCT_CUDA(cudaGetLastError());
+    adj_voe_sum_kernel<<<grid_for(nu2), 256, 0, s>>>(nu, no, nch, at, sm, b->vpart, b->g_voe);
+    CCT_CUDA(cudaGetLastError());
+  }
   {
     const int64_t nchunk = (nu2 + kColChunk - 1) / kColChunk;
     double *Rw = b->eps, *Cl = b->eps + nu2;
@@ -774,16 +805,29 @@ int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E
     CCT_CUDA(cudaGetLastError());
     adj_eps_cols_kernel<<<grid_for(nchunk * nu), 256, 0, s>>>(nu, b->Mf, Cl);
     CCT_CUDA(cudaGetLastError());
-    adj_eps_final_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, at, Rw, Cl, b->g_ep, b->g_eh);
+    adj_eps_final_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, Rw, Cl, b->g_ep);
+    CCT_CUDA(cudaGetLastError());
+    double *R1 = Cl + nchunk * nu;
+    adj_eps_planes_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, Rw, R1);
+    CCT_CUDA(cudaGetLastError());
+    adj_eps_total_kernel<<<1, 32, 0, s>>>(nu, at, R1, b->g_eh);
   }
   CCT_CUDA(cudaGetLastError());
-  const int64_t ngx = nu2 * d.NP;
+  const dim3 gx((unsigned)((d.NP + 127) / 128), nu, nu);
   switch (t.kind) {
-    case kIJK: adj_gx_kernel<kIJK><<<grid_for(ngx), 256, 0, s>>>(nu, d.NP, b->GW, b->GX[0], b->GX[1], b->GX[2]); break;
-    case kIJJ: adj_gx_kernel<kIJJ><<<grid_for(ngx), 256, 0, s>>>(nu, d.NP, b->GW, b->GX[0], b->GX[1], b->GX[2]); break;
-    default: adj_gx_kernel<kIIJ><<<grid_for(ngx), 256, 0, s>>>(nu, d.NP, b->GW, b->GX[0], b->GX[1], b->GX[2]); break;
+    case kIJK: adj_gx_kernel<kIJK><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]); break;
+    case kIJJ: adj_gx_kernel<kIJJ><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]); break;
+    default: adj_gx_kernel<kIIJ><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]); break;
   }
   CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
+}
+
+int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double *F, AdjBuffers *b, int set,
+                    cudaStream_t s, cudaStream_t sf) {
+  const int no = d.no, nu = d.nu;
+  const int64_t nu2 = (int64_t)nu * nu;
+  double *const *GX = b->GX[set];
 
   // (slot, half) pairs: half h reads E[x_h] with row permutation h and F[fyz_h]
   int slots[3][4], ns = 0;
@@ -820,11 +864,12 @@ int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E
             set_error("adjoint: too many GEMM pairs for one E slab");
             return CCT_ERR_INVALID;
           }
-          a.pair[np_++] = BwdPair{b->GX[q.g], Fyz(q.fyz), q.h, o};
+          a.pair[np_++] = BwdPair{GX[q.g], Fyz(q.fyz), q.h, o};
         }
     }
     a.first[nx] = np_;
     a.npairs = np_;
+    a.ptab = b->ptab;
     a.nu = nu;
     a.NP = d.NP;
     a.KP = d.KP;
@@ -842,7 +887,7 @@ int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E
     BwdFReduceArgs r{};
     int no_ = 0;
     for (size_t q = 0; q < sorted.size(); q++) {
-      a.pair[q] = BwdPair{b->GX[sorted[q].g], Ex(sorted[q].x), sorted[q].h, 0};
+      a.pair[q] = BwdPair{GX[sorted[q].g], Ex(sorted[q].x), sorted[q].h, 0};
       if (q == 0 || sorted[q].fyz != sorted[q - 1].fyz) {
         r.first[no_] = (int)q;
         r.dst[no_] = b->dF + (int64_t)sorted[q].fyz * d.NP * d.KP;
@@ -857,15 +902,16 @@ int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E
     a.npairs = (int)sorted.size();
     a.nsplit = (int)b->nsplit;
     a.kchunk = kFChunk;
+    a.ptab = b->ptab;
     a.nu = nu;
     a.NP = d.NP;
     a.KP = d.KP;
     const int bn = bwd_bn(d.KP);
     a.tiles_n = (int)((d.KP + bn - 1) / bn);
     const int tiles_m = (int)((d.NP + BBM - 1) / BBM);
-    CCT_TRY(bn == 64 ? launch_bwd_f<64>(a, tiles_m, s)
-                     : bn == 48 ? launch_bwd_f<48>(a, tiles_m, s) : launch_bwd_f<32>(a, tiles_m, s));
-    bwd_f_reduce_kernel<<<dim3(grid_for(r.n) < 64 ? grid_for(r.n) : 64, r.nout), 256, 0, s>>>(r, b->part);
+    CCT_TRY(bn == 64 ? launch_bwd_f<64>(a, tiles_m, sf)
+                     : bn == 48 ? launch_bwd_f<48>(a, tiles_m, sf) : launch_bwd_f<32>(a, tiles_m, sf));
+    bwd_f_reduce_kernel<<<dim3(grid_for(r.n) < 64 ? grid_for(r.n) : 64, r.nout), 256, 0, sf>>>(r, b->part);
     CCT_CUDA(cudaGetLastError());
   }
   return CCT_OK;

@@ -163,10 +163,12 @@ struct AdjBuffers {
   bool ready = false;
   double *dE = nullptr, *dF = nullptr;                 // gradients of the GEMM operands E, F
   double *Wf = nullptr, *GW = nullptr, *Mf = nullptr;  // dense nu^3: W, dE/dW, denominator terms
-  double *GX[3] = {};                                  // dE/dX_g, nu^2 x NP each
+  double *GX[2][3] = {};                               // dE/dX_g, nu^2 x NP each, two tuples in flight
   double *part = nullptr;                              // split-K partials of the dF GEMMs
   int64_t nsplit = 0;
   double *Q = nullptr;                                 // 9 nu^2 VOE combinations of dE/dW
+  double *vpart = nullptr;                             // per-a-chunk partial VOE gradients
+  int *ptab = nullptr;                                 // ptab[p*nu+q] = q*nu+p
   double *eps = nullptr;                               // row sums and 64-row column sums of M
   double *v1 = nullptr;                                // FP64 v1 of an emulated plan: 5 + nu*no
   double *g_eh = nullptr, *g_ep = nullptr, *g_t1 = nullptr, *g_t2 = nullptr, *g_vm = nullptr, *g_voe = nullptr,
@@ -176,9 +178,12 @@ int adj_alloc(const Dims &d, AdjBuffers *b);
 void adj_free(AdjBuffers *b);
 int adj_configure(int device);
 int adj_zero(const Dims &d, AdjBuffers *b, cudaStream_t s);
-int adj_tuple(const Dims &d, const Tuple &t, double *const X[3], const double *E, const double *F,
-              const double *eh, const double *ep, const double *t1, const double *voe, AdjBuffers *b,
-              cudaStream_t s);
+// Per tuple: the pointwise kernels (W assembly, dE/dW, dVOE, eps, dE/dX into GX
+// set `set`), then the backward GEMMs reading that GX set.
+int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const double *eh, const double *ep,
+                        const double *t1, const double *voe, AdjBuffers *b, int set, cudaStream_t s);
+int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double *F, AdjBuffers *b, int set,
+                    cudaStream_t s_e, cudaStream_t s_f);  // dE GEMM on s_e, dF GEMM + reduction on s_f
 int adj_finish(const Dims &d, const double *v1, AdjBuffers *b, cudaStream_t s);
 
 // peak.cu

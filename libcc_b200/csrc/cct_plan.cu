@@ -83,6 +83,8 @@ struct ccT_plan {
   int64_t kernel_launches[2] = {0, 0};
   // backward: buffers and the saved context (range of the last successful forward)
   AdjBuffers adj;
+  cudaStream_t bwd_stream = nullptr;   // the dF GEMMs of the backward
+  cudaEvent_t ev_bwdf[2] = {};
   int64_t fwd_begin = -1, fwd_end = -1;
   float last_bwd_ms = 0.f;
 };
@@ -550,6 +552,10 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     set_error("ccT_backward needs a successful ccT_forward over the same tuple range first");
     return CCT_ERR_STATE;
   }
+  if (p->d.nu > 4096) {
+    set_error("ccT_backward supports nu <= 4096");
+    return CCT_ERR_UNSUPPORTED;
+  }
   DeviceGuard guard(p->device);
   const Dims &d = p->d;
   if (!p->adj.ready) {
@@ -560,16 +566,32 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     }
   }
   CCT_TRY(adj_configure(p->device));
+  if (!p->bwd_stream) {
+    CCT_CUDA(cudaStreamCreateWithFlags(&p->bwd_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : p->ev_bwdf) CCT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
   const int64_t ntup = (int64_t)p->tuples.size();
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
   CCT_TRY(adj_zero(d, &p->adj, p->stream));
   // dT1 = 2 v1: an emulated plan's v1 is rebuilt from the FP64 W of this pass
   if (p->emulated) CCT_CUDA(cudaMemsetAsync(p->adj.v1, 0, (5 + (size_t)d.nu * d.no) * 8, p->stream));
+  // Three streams: the W recompute and the pointwise adjoint kernels of tuple t
+  // (red_stream) overlap the backward GEMMs of tuple t-1, the dE GEMM on
+  // gemm_stream and the dF GEMM on bwd_stream.  The GX buffer sets alternate;
+  // every accumulator is written by one stream only, in tuple order, so the
+  // results stay bitwise reproducible.
+  CCT_TRY(fork_streams(p));
+  cudaStream_t sP = p->red_stream, sG = p->gemm_stream, sF = p->bwd_stream;
+  CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_fork, 0));
   for (int64_t t = begin; t < end; t++) {
     const Tuple &tu = p->tuples[t];
-    // W recomputed in FP64 into X buffer set 0
-    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * (0 * ntup + t), tu.kind == kIJK ? 3 : 2, p->stream));
-    CCT_TRY(adj_tuple(d, tu, p->X[0], p->E, p->F, p->eh, p->ep, p->t1, p->voe, &p->adj, p->stream));
+    const int set = (int)((t - begin) & 1);
+    if (t - begin >= 2) {  // GX set read by the GEMMs of t-2
+      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gemm[set], 0));
+      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_bwdf[set], 0));
+    }
+    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * (0 * ntup + t), tu.kind == kIJK ? 3 : 2, sP));
+    CCT_TRY(adj_tuple_pointwise(d, tu, p->X[0], p->eh, p->ep, p->t1, p->voe, &p->adj, set, sP));
     if (p->emulated) {
       TupleDev td;
       td.x[0] = p->X[0][0];
@@ -580,10 +602,23 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
       td.j = tu.j;
       td.k = tu.k;
       td.weight = tu.kind == kIJK ? 1.0 : 0.5;
-      CCT_TRY(launch_reduce(d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->stream));
-      CCT_TRY(launch_finalize(d, td, p->xpart, p->vpart, p->adj.v1, p->adj.v1 + 5, p->stream));
+      CCT_TRY(launch_reduce(d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, sP));
+      CCT_TRY(launch_finalize(d, td, p->xpart, p->vpart, p->adj.v1, p->adj.v1 + 5, sP));
     }
+    CCT_CUDA(cudaEventRecord(p->ev_red[set], sP));
+    CCT_CUDA(cudaStreamWaitEvent(sG, p->ev_red[set], 0));
+    CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_red[set], 0));
+    CCT_TRY(adj_tuple_gemms(d, tu, p->E, p->F, &p->adj, set, sG, sF));
+    CCT_CUDA(cudaEventRecord(p->ev_gemm[set], sG));
+    CCT_CUDA(cudaEventRecord(p->ev_bwdf[set], sF));
   }
+  // p->stream after both streams
+  CCT_CUDA(cudaEventRecord(p->ev_join, sP));
+  CCT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_join, 0));
+  CCT_CUDA(cudaEventRecord(p->ev_fork, sG));
+  CCT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_fork, 0));
+  CCT_CUDA(cudaEventRecord(p->ev_bwdf[0], sF));
+  CCT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_bwdf[0], 0));
   CCT_TRY(adj_finish(d, p->emulated ? p->adj.v1 + 5 : v1_acc(p), &p->adj, p->stream));
   CCT_CUDA(cudaEventRecord(p->ev1, p->stream));
   const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
@@ -678,7 +713,7 @@ int64_t ccT_last_forward_launches(const ccT_plan *p) { return p ? p->last_launch
 int ccT_plan_destroy(ccT_plan *p) {
   if (!p) return CCT_OK;
   DeviceGuard guard(p->device);
-  for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream})
+  for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream, p->bwd_stream})
     if (st) cudaStreamSynchronize(st);
   double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->xpart, p->vpart, p->acc, p->stage};
   for (double *b : bufs)
@@ -703,6 +738,9 @@ int ccT_plan_destroy(ccT_plan *p) {
     if (p->ev_red[b]) cudaEventDestroy(p->ev_red[b]);
   }
   if (p->gemm_stream) cudaStreamDestroy(p->gemm_stream);
+  if (p->bwd_stream) cudaStreamDestroy(p->bwd_stream);
+  for (cudaEvent_t e : p->ev_bwdf)
+    if (e) cudaEventDestroy(e);
   if (p->red_stream) cudaStreamDestroy(p->red_stream);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
   delete p;
