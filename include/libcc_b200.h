@@ -98,6 +98,36 @@ int ccT_backward(ccT_plan *plan, int64_t begin, int64_t end, double *d_eh, doubl
 /* Milliseconds of device time the last ccT_backward spent (CUDA events). */
 double ccT_last_backward_ms(const ccT_plan *plan);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent systems of uneven (no, nu) evaluated together: every
+ * tuple of every system runs in one persistent kernel fed by a device-side
+ * work queue, captured in a CUDA graph.  FP64 form.  No reference counterpart
+ * (the reference runs one system per triples.x process); per system the
+ * results equal a single-system plan's bitwise. */
+typedef struct ccT_batch ccT_batch;
+
+int ccT_batch_create(ccT_batch **batch, int64_t nsys, const int64_t *no, const int64_t *nu,
+                     const ccT_options *opt);
+/* Inputs of system s, same layouts and meaning as ccT_set_inputs. */
+int ccT_batch_set_inputs(ccT_batch *batch, int64_t s, const double *eh, const double *ep, const double *t1,
+                         const double *t2, const double *vm, const double *voe, const double *vvvo_packed,
+                         int32_t mem);
+/* E(T) of every system: ets[s], etd[s] (arrays of nsys doubles, or NULL). */
+int ccT_batch_forward(ccT_batch *batch, double *ets, double *etd);
+/* v1(nu, no) of system s from the last ccT_batch_forward. */
+int ccT_batch_v1(ccT_batch *batch, int64_t s, double *v1_out);
+/* Fix the schedule: W-build N tile bn (32, 48 or 64), tuple order (0: by cost,
+ * largest first; 1: system by system) and scratch bytes per tuple group. */
+int ccT_batch_configure(ccT_batch *batch, int32_t bn, int32_t order, int64_t group_bytes);
+/* Autotune: time every (bn, order) candidate on the loaded inputs, keep the
+ * fastest and report it (outputs may be NULL). */
+int ccT_batch_tune(ccT_batch *batch, int32_t *best_bn, int32_t *best_order, double *best_ms);
+/* Device milliseconds of the last batch forward (CUDA events around the graph). */
+double ccT_batch_last_ms(const ccT_batch *batch);
+/* Work items (W-build tiles + reduction blocks) in the current schedule. */
+int64_t ccT_batch_work_items(const ccT_batch *batch);
+int ccT_batch_destroy(ccT_batch *batch);
+
 /* Launch the plan's kernels on a caller-provided CUDA stream (a cudaStream_t
  * passed as void*); NULL restores the plan's own stream. */
 int ccT_set_stream(ccT_plan *plan, void *cuda_stream);

@@ -24,6 +24,8 @@ EXPORTS = [
     "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
     "ccT_last_error", "ccT_measure_fp64_peak", "ccT_measure_int8_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
     "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms",
+    "ccT_batch_create", "ccT_batch_set_inputs", "ccT_batch_forward", "ccT_batch_v1", "ccT_batch_configure",
+    "ccT_batch_tune", "ccT_batch_last_ms", "ccT_batch_work_items", "ccT_batch_destroy",
 ]
 
 
@@ -103,6 +105,24 @@ def load():
     lib.ccT_backward.restype = ctypes.c_int
     lib.ccT_last_backward_ms.argtypes = [vp]
     lib.ccT_last_backward_ms.restype = ctypes.c_double
+    lib.ccT_batch_create.argtypes = [ctypes.POINTER(vp), i64, i64p, i64p, ctypes.POINTER(Options)]
+    lib.ccT_batch_create.restype = ctypes.c_int
+    lib.ccT_batch_set_inputs.argtypes = [vp, i64] + [vp] * 7 + [i32]
+    lib.ccT_batch_set_inputs.restype = ctypes.c_int
+    lib.ccT_batch_forward.argtypes = [vp, dp, dp]
+    lib.ccT_batch_forward.restype = ctypes.c_int
+    lib.ccT_batch_v1.argtypes = [vp, i64, dp]
+    lib.ccT_batch_v1.restype = ctypes.c_int
+    lib.ccT_batch_configure.argtypes = [vp, i32, i32, i64]
+    lib.ccT_batch_configure.restype = ctypes.c_int
+    lib.ccT_batch_tune.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), dp]
+    lib.ccT_batch_tune.restype = ctypes.c_int
+    lib.ccT_batch_last_ms.argtypes = [vp]
+    lib.ccT_batch_last_ms.restype = ctypes.c_double
+    lib.ccT_batch_work_items.argtypes = [vp]
+    lib.ccT_batch_work_items.restype = i64
+    lib.ccT_batch_destroy.argtypes = [vp]
+    lib.ccT_batch_destroy.restype = ctypes.c_int
     _lib = lib
     return lib
 

@@ -1,0 +1,102 @@
+"""Many independent (T) systems in one persistent kernel (``ccT_batch_*``).
+
+    from libcc_b200 import batch, synthetic
+    systems = synthetic.batch96()
+    with batch.TriplesBatch([(s.no, s.nu) for s in systems]) as b:
+        for k, s in enumerate(systems):
+            b.set_system(k, s)
+        b.tune()                      # optional: pick the N tile and tuple order
+        ets, etd = b.forward()        # arrays, one entry per system
+
+Every tuple of every system is a set of work items (W-build tiles, reduction
+blocks) taken from one device-side queue by a persistent kernel, replayed
+from a CUDA graph; per system the energies equal a single-system
+``TriplesPlan`` bitwise.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from .api import _host, input_sizes
+
+
+class TriplesBatch:
+    def __init__(self, shapes, device: int = 0):
+        lib = N.load()
+        self.shapes = [(int(no), int(nu)) for no, nu in shapes]
+        n = len(self.shapes)
+        no = (ctypes.c_int64 * n)(*[s[0] for s in self.shapes])
+        nu = (ctypes.c_int64 * n)(*[s[1] for s in self.shapes])
+        opt = N.Options()
+        lib.ccT_options_default(ctypes.byref(opt))
+        opt.device = device
+        h = ctypes.c_void_p()
+        N.check(lib.ccT_batch_create(ctypes.byref(h), n, no, nu, ctypes.byref(opt)), "ccT_batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.load().ccT_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.shapes)
+
+    def set_inputs(self, s: int, eh, ep, t1, t2, vm, voe, vvvo):
+        no, nu = self.shapes[s]
+        sizes = input_sizes(no, nu)
+        arrs = dict(eh=eh, ep=ep, t1=t1, t2=t2, vm=vm, voe=voe, vvvo=vvvo)
+        keep = [_host(a, sizes[k], k) for k, a in arrs.items()]
+        ptrs = [ctypes.c_void_p(a.ctypes.data) for a in keep]
+        N.check(N.load().ccT_batch_set_inputs(self._h, s, *ptrs, N.CCT_MEM_HOST), "ccT_batch_set_inputs")
+
+    def set_system(self, s: int, inp):
+        if (inp.no, inp.nu) != self.shapes[s]:
+            raise ValueError(f"system {s}: shape {(inp.no, inp.nu)} != {self.shapes[s]}")
+        self.set_inputs(s, *inp.arrays())
+
+    def forward(self):
+        """(ets, etd) arrays over the systems."""
+        n = len(self.shapes)
+        ets, etd = np.zeros(n), np.zeros(n)
+        dp = ctypes.POINTER(ctypes.c_double)
+        N.check(N.load().ccT_batch_forward(self._h, ets.ctypes.data_as(dp), etd.ctypes.data_as(dp)),
+                "ccT_batch_forward")
+        return ets, etd
+
+    def v1(self, s: int) -> np.ndarray:
+        no, nu = self.shapes[s]
+        out = np.zeros(no * nu)
+        N.check(N.load().ccT_batch_v1(self._h, s, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                "ccT_batch_v1")
+        return out
+
+    def configure(self, bn: int = 48, order: int = 0, group_bytes: int = 512 << 20):
+        N.check(N.load().ccT_batch_configure(self._h, bn, order, group_bytes), "ccT_batch_configure")
+
+    def tune(self):
+        """Time every (N tile, tuple order) candidate; keep the fastest.  Returns
+        (bn, order, ms)."""
+        bn, order, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        N.check(N.load().ccT_batch_tune(self._h, ctypes.byref(bn), ctypes.byref(order), ctypes.byref(ms)),
+                "ccT_batch_tune")
+        return bn.value, order.value, ms.value
+
+    @property
+    def last_ms(self) -> float:
+        return float(N.load().ccT_batch_last_ms(self._h))
+
+    @property
+    def work_items(self) -> int:
+        return int(N.load().ccT_batch_work_items(self._h))

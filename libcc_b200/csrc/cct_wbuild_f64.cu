@@ -17,154 +17,19 @@
 // 32 x BN; mma.sync.m16n8k4.f64; a 3-stage cp.async ring of 128x16 / BNx16
 // tiles with 16-byte-aligned rows padded to 20 doubles (conflict-free
 // fragment loads); two CTAs per SM.
-#include "cct_internal.cuh"
+#include "cct_wbuild_tile.cuh"
 
 namespace cct {
 namespace {
 
-constexpr int BM = 128, BK = kKB;
-constexpr int WM = 32;
-constexpr int NWARP = BM / WM;
-constexpr int NT = NWARP * 32;
-constexpr int STAGES = 3;
-constexpr int LDS = BK + 4;  // padded smem row (doubles)
-constexpr int MF = WM / 16;
-
-template <int BN>
-constexpr int smem_bytes() {
-  return STAGES * (BM + BN) * LDS * 8 + BM * 2 * 4;
-}
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-__device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, double b0) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
-      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a0), "d"(a1), "d"(b0));
-}
+using namespace wb;
 
 template <int BN>
 __global__ void __launch_bounds__(NT, 2) wbuild_f64_kernel(const GemmJob *__restrict__ jobs, int nu, int64_t KP,
                                                            int64_t NP, int tiles_n) {
-  constexpr int NF = BN / 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double *As = reinterpret_cast<double *>(smem_raw);
-  double *Bs = As + STAGES * BM * LDS;
-  int *rowoff = reinterpret_cast<int *>(Bs + STAGES * BN * LDS);  // [2][BM] row index into E (or -1)
-
-  const GemmJob job = jobs[blockIdx.y];
   const int tile_m = blockIdx.x / tiles_n, tile_n = blockIdx.x - tile_m * tiles_n;
-  const int64_t M = (int64_t)nu * nu;
-  const int64_t m0 = (int64_t)tile_m * BM;
-  const int n0 = tile_n * BN;
-  const int tid = threadIdx.x;
-
-  for (int r = tid; r < BM; r += NT) {
-    const int64_t m = m0 + r;
-    if (m < M) {
-      const int p = (int)(m / nu), q = (int)(m - (int64_t)(m / nu) * nu);
-      rowoff[r] = p * nu + q;
-      rowoff[BM + r] = q * nu + p;
-    } else {
-      rowoff[r] = -1;
-      rowoff[BM + r] = -1;
-    }
-  }
-  __syncthreads();
-
-  const int ktiles_half = (int)(KP / BK);
-  const int ktiles = ktiles_half * job.nhalves;
-
-  auto load_stage = [&](int stage, int kt) {
-    const int h = kt >= ktiles_half;
-    const int64_t k0 = (int64_t)(kt - h * ktiles_half) * BK;
-    const double *abase = h ? job.a1 : job.a0;
-    const double *bbase = h ? job.b1 : job.b0;
-    double *as = As + stage * BM * LDS;
-    double *bs = Bs + stage * BN * LDS;
-    const int chunk = tid & 7;  // 8 x 16 B per 16-double row
-#pragma unroll
-    for (int rr = tid >> 3; rr < BM; rr += NT / 8) {
-      const int ro = rowoff[h * BM + rr];
-      const double *src = abase + (ro < 0 ? 0 : (int64_t)ro * KP) + k0 + chunk * 2;
-      cp_async16(as + rr * LDS + chunk * 2, src, ro < 0 ? 0 : 16);
-    }
-#pragma unroll
-    for (int rr = tid >> 3; rr < BN; rr += NT / 8) {
-      const double *src = bbase + (int64_t)(n0 + rr) * KP + k0 + chunk * 2;
-      cp_async16(bs + rr * LDS + chunk * 2, src, 16);
-    }
-  };
-
-  const int warp = tid >> 5, lane = tid & 31;
-  const int g = lane >> 2, t = lane & 3;
-
-  double acc[MF][NF][4];
-#pragma unroll
-  for (int i = 0; i < MF; i++)
-#pragma unroll
-    for (int j = 0; j < NF; j++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0;
-
-#pragma unroll
-  for (int s = 0; s < STAGES - 1; s++) {
-    if (s < ktiles) load_stage(s, s);
-    cp_async_commit();
-  }
-
-  for (int kt = 0; kt < ktiles; kt++) {
-    cp_async_wait<STAGES - 2>();
-    __syncthreads();
-    {
-      const int nk = kt + STAGES - 1;
-      if (nk < ktiles) load_stage(nk % STAGES, nk);
-      cp_async_commit();
-    }
-    const double *as = As + (kt % STAGES) * BM * LDS + (warp * WM) * LDS;
-    const double *bs = Bs + (kt % STAGES) * BN * LDS;
-#pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double af[MF][2], bf[NF];
-#pragma unroll
-      for (int i = 0; i < MF; i++) {
-        af[i][0] = as[(i * 16 + g) * LDS + kk + t];
-        af[i][1] = as[(i * 16 + g + 8) * LDS + kk + t];
-      }
-#pragma unroll
-      for (int j = 0; j < NF; j++) bf[j] = bs[(j * 8 + g) * LDS + kk + t];
-#pragma unroll
-      for (int i = 0; i < MF; i++)
-#pragma unroll
-        for (int j = 0; j < NF; j++) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
-    }
-  }
-  cp_async_wait<0>();
-
-  // epilogue: X[(p*nu+q)*NP + s]
-#pragma unroll
-  for (int i = 0; i < MF; i++) {
-#pragma unroll
-    for (int half = 0; half < 2; half++) {
-      const int64_t m = m0 + warp * WM + i * 16 + g + half * 8;
-      if (m >= M) continue;
-      double *orow = job.out + m * NP + n0 + 2 * t;
-#pragma unroll
-      for (int j = 0; j < NF; j++) {
-        double2 v = make_double2(acc[i][j][2 * half], acc[i][j][2 * half + 1]);
-        *reinterpret_cast<double2 *>(orow + j * 8) = v;
-      }
-    }
-  }
+  wbuild_tile<BN>(jobs[blockIdx.y], nu, KP, NP, tile_m, tile_n, smem_raw);
 }
 
 template <int BN>
