@@ -99,11 +99,13 @@ int ccT_backward(ccT_plan *plan, int64_t begin, int64_t end, double *d_eh, doubl
 double ccT_last_backward_ms(const ccT_plan *plan);
 
 /* ---------------------------------------------------------------- batches
- * Many independent systems of uneven (no, nu) evaluated together: every
- * tuple of every system runs in one persistent kernel fed by a device-side
- * work queue, captured in a CUDA graph.  FP64 form.  No reference counterpart
- * (the reference runs one system per triples.x process); per system the
- * results equal a single-system plan's bitwise. */
+ * Many independent systems of uneven (no, nu) evaluated together.  Every tuple
+ * of every system is cut into work items (W-build tiles, reduction blocks) that
+ * run either in one persistent kernel fed by a device-side work queue (mode 0)
+ * or as grouped launches per tuple group on two streams (mode 1); either is
+ * captured in a CUDA graph, and ccT_batch_tune picks the faster.  FP64 form.
+ * No reference counterpart (the reference runs one system per triples.x
+ * process); per system the results equal a single-system plan's bitwise. */
 typedef struct ccT_batch ccT_batch;
 
 int ccT_batch_create(ccT_batch **batch, int64_t nsys, const int64_t *no, const int64_t *nu,
@@ -116,12 +118,17 @@ int ccT_batch_set_inputs(ccT_batch *batch, int64_t s, const double *eh, const do
 int ccT_batch_forward(ccT_batch *batch, double *ets, double *etd);
 /* v1(nu, no) of system s from the last ccT_batch_forward. */
 int ccT_batch_v1(ccT_batch *batch, int64_t s, double *v1_out);
-/* Fix the schedule: W-build N tile bn (32, 48 or 64), tuple order (0: by cost,
- * largest first; 1: system by system) and scratch bytes per tuple group. */
-int ccT_batch_configure(ccT_batch *batch, int32_t bn, int32_t order, int64_t group_bytes);
-/* Autotune: time every (bn, order) candidate on the loaded inputs, keep the
- * fastest and report it (outputs may be NULL). */
-int ccT_batch_tune(ccT_batch *batch, int32_t *best_bn, int32_t *best_order, double *best_ms);
+/* Fix the schedule: executor mode (0: one persistent kernel taking every work
+ * item from a device queue; 1: per tuple group, one launch of W-build tiles and
+ * one of reduction blocks on two streams), W-build N tile bn (32, 48 or 64, or
+ * 0 = the least-padding tile per system, mode 1 only),
+ * tuple order (0: by cost, largest first; 1: system by system) and X scratch
+ * bytes per tuple group. */
+int ccT_batch_configure(ccT_batch *batch, int32_t mode, int32_t bn, int32_t order, int64_t group_bytes);
+/* Autotune: time every (mode, bn, order) candidate on the loaded inputs, keep
+ * the fastest and report it (outputs may be NULL). */
+int ccT_batch_tune(ccT_batch *batch, int32_t *best_mode, int32_t *best_bn, int32_t *best_order,
+                   double *best_ms);
 /* Device milliseconds of the last batch forward (CUDA events around the graph). */
 double ccT_batch_last_ms(const ccT_batch *batch);
 /* Work items (W-build tiles + reduction blocks) in the current schedule. */

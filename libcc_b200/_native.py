@@ -113,9 +113,9 @@ def load():
     lib.ccT_batch_forward.restype = ctypes.c_int
     lib.ccT_batch_v1.argtypes = [vp, i64, dp]
     lib.ccT_batch_v1.restype = ctypes.c_int
-    lib.ccT_batch_configure.argtypes = [vp, i32, i32, i64]
+    lib.ccT_batch_configure.argtypes = [vp, i32, i32, i32, i64]
     lib.ccT_batch_configure.restype = ctypes.c_int
-    lib.ccT_batch_tune.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), dp]
+    lib.ccT_batch_tune.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), dp]
     lib.ccT_batch_tune.restype = ctypes.c_int
     lib.ccT_batch_last_ms.argtypes = [vp]
     lib.ccT_batch_last_ms.restype = ctypes.c_double

@@ -82,16 +82,19 @@ class TriplesBatch:
                 "ccT_batch_v1")
         return out
 
-    def configure(self, bn: int = 48, order: int = 0, group_bytes: int = 512 << 20):
-        N.check(N.load().ccT_batch_configure(self._h, bn, order, group_bytes), "ccT_batch_configure")
+    def configure(self, mode: int = 1, bn: int = 0, order: int = 0, group_bytes: int = 256 << 20):
+        """mode 0: one persistent kernel over a device work queue; mode 1: grouped
+        launches (W-build tiles / reduction blocks per tuple group, two streams).
+        bn: W-build N tile, 0 = per system (mode 1 only)."""
+        N.check(N.load().ccT_batch_configure(self._h, mode, bn, order, group_bytes), "ccT_batch_configure")
 
     def tune(self):
-        """Time every (N tile, tuple order) candidate; keep the fastest.  Returns
-        (bn, order, ms)."""
-        bn, order, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
-        N.check(N.load().ccT_batch_tune(self._h, ctypes.byref(bn), ctypes.byref(order), ctypes.byref(ms)),
-                "ccT_batch_tune")
-        return bn.value, order.value, ms.value
+        """Time every (mode, N tile, tuple order) candidate; keep the fastest.
+        Returns (mode, bn, order, ms)."""
+        mode, bn, order, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        N.check(N.load().ccT_batch_tune(self._h, ctypes.byref(mode), ctypes.byref(bn), ctypes.byref(order),
+                                        ctypes.byref(ms)), "ccT_batch_tune")
+        return mode.value, bn.value, order.value, ms.value
 
     @property
     def last_ms(self) -> float:

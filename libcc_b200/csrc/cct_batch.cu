@@ -19,17 +19,23 @@
 //     partials), and the last finalized tuple of a system sums the system
 //     (Neumaier etd in tuple order, v1, ets) -- the same arithmetic, in the
 //     same order, as a single-system plan, so results are bitwise equal;
-//   * the X scratch of group g lives in ring slot g % 3, so a W-build tile of
-//     group g waits until every tuple of group g-3 is finalized.
+//   * the X scratch of group g lives in ring slot g % R (R = 6), so a W-build
+//     tile of group g waits until every reduction block of group g-R is done
+//     (the reduction partials live outside the ring, one slab per tuple).
 // Every wait is on items dispensed earlier, which run on live CTAs and whose
 // own waits point further back, so the queue cannot deadlock; each wait is
 // also bounded (on timeout the error word is set and the item proceeds).
 // Data produced inside the kernel is read through L2 (ld.global.cg /
 // cp.async.cg), never through the incoherent L1.
 //
-// The forward (counter reset + the kernel) is captured once in a CUDA graph
-// and replayed.  The W-build N tile (BN) and the tuple order are chosen by
-// ccT_batch_tune, which times every candidate on the loaded batch.
+// A second executor (mode 1) runs the same items as grouped launches: per
+// tuple group, one launch of 128-row W-build tiles (two CTAs per SM) on one
+// stream, then one launch of its reduction blocks (two CTAs per SM, the last
+// block of a tuple finalizing it) on a second stream, the ring slots guarded
+// by stream events instead of counters.  Either forward (counter reset plus the
+// launches) is captured once in a CUDA graph and replayed.  The executor, the
+// W-build N tile (BN) and the tuple order are chosen by ccT_batch_tune, which
+// times every candidate on the loaded batch.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -46,9 +52,11 @@ namespace {
 
 constexpr int kBT = 256;   // threads per batch CTA (8 warps)
 constexpr int kBTM = 256;  // W-build tile rows: one 32-row slab per warp
-constexpr int kRing = 3;   // X scratch groups in flight
+constexpr int kRing = 6;   // X scratch groups in flight
 constexpr long kSpinLimit = 1L << 24;
-constexpr int kBatchBN[] = {32, 48, 64};
+// Batch-wide W-build N tiles; 0 = per system, the least-padding tile of
+// kBNChoices (grouped executor only: one W-build launch per tile width).
+constexpr int kBatchBN[] = {0, 32, 48, 64};
 
 struct SysDev {
   int no, nu, nb, tiles_m, tiles_n;
@@ -69,9 +77,9 @@ struct TupleRec {
 struct BatchArgs {
   const int4 *items;  // {kind 0 = W-build tile / 1 = reduction block, tuple, job slot | block, tile}
   int64_t nitems;
-  int *counters;      // [0] queue head, then wb_done[T], rd_done[T], group_final[G], sys_done[S]
+  int *counters;      // [0] queue head, then wb_done[T], rd_done[T], group_rd[G], sys_done[S]
   int ntuple, ngroup;
-  const int *group_ntuples;
+  const int *group_rd_items;  // reduction blocks per group
   const TupleRec *tuples;
   const GemmJob *jobs;  // [tuple][3]
   const SysDev *sys;
@@ -141,15 +149,19 @@ __device__ void system_sum(const SysDev &S, int s, const BatchArgs &A, double *r
     }
     red[kBT] = sum + comp;
   }
-  for (int a = tid; a < nu; a += kBT) {
-    for (int x = 0; x < no; x++) S.v1[a + (int64_t)nu * x] = 0.0;
+  // thread per v1 element (a, x): the contributions of the system's tuples in
+  // order, each tuple's columns i, j, k in that order (as finalize_kernel adds them)
+  for (int64_t e = tid; e < (int64_t)nu * no; e += kBT) {
+    const int x = (int)(e / nu), a = (int)(e - (int64_t)x * nu);
+    double v = 0.0;
     for (int64_t t = S.tuple_begin; t < S.tuple_begin + S.ntuples; t++) {
       const TupleRec &T = A.tuples[t];
       const double *tv = A.tuple_v1 + A.tuple_v1_off[t];
-      S.v1[a + (int64_t)nu * T.i] += __ldcg(tv + a);
-      S.v1[a + (int64_t)nu * T.j] += __ldcg(tv + nu + a);
-      S.v1[a + (int64_t)nu * T.k] += __ldcg(tv + 2 * nu + a);
+      if (T.i == x) v += __ldcg(tv + a);
+      if (T.j == x) v += __ldcg(tv + nu + a);
+      if (T.k == x) v += __ldcg(tv + 2 * nu + a);
     }
+    S.v1[e] = v;
   }
   __syncthreads();
   double sacc = 0.0;
@@ -185,8 +197,8 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
   __shared__ int s_flag;
   int *const wb_done = A.counters + 1;
   int *const rd_done = wb_done + A.ntuple;
-  int *const group_final = rd_done + A.ntuple;
-  int *const sys_done = group_final + A.ngroup;
+  int *const group_rd = rd_done + A.ntuple;
+  int *const sys_done = group_rd + A.ngroup;
   for (;;) {
     __syncthreads();  // the previous item is done with shared memory and s_item
     if (threadIdx.x == 0) s_item = atomicAdd(A.counters, 1);
@@ -199,7 +211,7 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
     const SysDev &S = A.sys[T.sys];
     if (it.x == 0) {  // ---- one W-build tile
       if (threadIdx.x == 0 && T.group >= kRing)
-        spin_until(group_final + (T.group - kRing), A.group_ntuples[T.group - kRing], A.err);
+        spin_until(group_rd + (T.group - kRing), A.group_rd_items[T.group - kRing], A.err);
       __syncthreads();
       const int tile_m = it.w / S.tiles_n, tile_n = it.w - tile_m * S.tiles_n;
       wb::wbuild_tile<BN, kBTM>(A.jobs[(int64_t)t * 3 + it.z], S.nu, S.KP, S.NP, tile_m, tile_n, smem);
@@ -230,17 +242,17 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
         red::reduce_block<kIIJ, true>(S.nu, S.no, S.NP, td, S.eh, S.ep, S.voe, S0, S1, S2, T.xpart + c, T.vpart, dsm);
       __threadfence();
       __syncthreads();
-      if (threadIdx.x == 0) s_flag = atomicAdd(rd_done + t, 1) == T.rd_items - 1;
+      if (threadIdx.x == 0) {
+        atomicAdd(group_rd + T.group, 1);  // this block no longer reads the group's X scratch
+        s_flag = atomicAdd(rd_done + t, 1) == T.rd_items - 1;
+      }
       __syncthreads();
       if (s_flag) {  // last block of the tuple: finalize it
         __threadfence();
         finalize_tuple(T, S, t, A, red);
         __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0) {
-          atomicAdd(group_final + T.group, 1);
-          s_flag = atomicAdd(sys_done + T.sys, 1) == S.ntuples - 1;
-        }
+        if (threadIdx.x == 0) s_flag = atomicAdd(sys_done + T.sys, 1) == S.ntuples - 1;
         __syncthreads();
         if (s_flag) {  // last tuple of the system: sum the system
           __threadfence();
@@ -250,6 +262,62 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
       }
     }
   }
+}
+
+// ---- grouped executor: per tuple group, one launch of W-build tiles (128-row
+// tiles, two CTAs per SM) and one launch of reduction blocks (several CTAs per
+// SM); ordering between the launches comes from the stream, so no item waits.
+template <int BN>
+__global__ void __launch_bounds__(wb::NT, 2) batch_wb_kernel(const BatchArgs A, int64_t item0) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int4 it = A.items[item0 + blockIdx.x];
+  const TupleRec &T = A.tuples[it.y];
+  const SysDev &S = A.sys[T.sys];
+  const int tile_m = it.w / S.tiles_n, tile_n = it.w - tile_m * S.tiles_n;
+  wb::wbuild_tile<BN, wb::BM>(A.jobs[(int64_t)it.y * 3 + it.z], S.nu, S.KP, S.NP, tile_m, tile_n, smem);
+}
+
+__global__ void __launch_bounds__(kBT, 2) batch_rd_kernel(const BatchArgs A, int64_t item0) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ double red[kBT + 1];
+  __shared__ int s_flag;
+  int *const rd_done = A.counters + 1 + A.ntuple;
+  int *const sys_done = rd_done + A.ntuple + A.ngroup;
+  const int4 it = A.items[item0 + blockIdx.x];
+  const int t = it.y;
+  const TupleRec &T = A.tuples[t];
+  const SysDev &S = A.sys[T.sys];
+  TupleDev td;
+  td.x[0] = T.x[0];
+  td.x[1] = T.x[1];
+  td.x[2] = T.x[2];
+  td.kind = T.kind;
+  td.i = T.i;
+  td.j = T.j;
+  td.k = T.k;
+  td.weight = T.kind == kIJK ? 1.0 : 0.5;
+  const int c = it.z;
+  const int S0 = S.cta_table[3 * c], S1 = S.cta_table[3 * c + 1], S2 = S.cta_table[3 * c + 2];
+  if (T.kind == kIJK)
+    red::reduce_block<kIJK>(S.nu, S.no, S.NP, td, S.eh, S.ep, S.voe, S0, S1, S2, T.xpart + c, T.vpart, dsm);
+  else if (T.kind == kIJJ)
+    red::reduce_block<kIJJ>(S.nu, S.no, S.NP, td, S.eh, S.ep, S.voe, S0, S1, S2, T.xpart + c, T.vpart, dsm);
+  else
+    red::reduce_block<kIIJ>(S.nu, S.no, S.NP, td, S.eh, S.ep, S.voe, S0, S1, S2, T.xpart + c, T.vpart, dsm);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_flag = atomicAdd(rd_done + t, 1) == T.rd_items - 1;
+  __syncthreads();
+  if (!s_flag) return;
+  __threadfence();
+  finalize_tuple(T, S, t, A, red);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_flag = atomicAdd(sys_done + T.sys, 1) == S.ntuples - 1;
+  __syncthreads();
+  if (!s_flag) return;
+  __threadfence();
+  system_sum(S, T.sys, A, red);
 }
 
 template <typename T>
@@ -278,9 +346,18 @@ struct ccT_batch {
   std::vector<BatchSystemHost> sys;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int bn = 48;
+  int bn = 0;                             // W-build N tile; 0 = per system
   int order = 0;                          // 0: tuples by cost, largest first; 1: system by system
-  int64_t group_budget = 512ll << 20;     // scratch bytes per tuple group
+  int mode = 1;                           // 0: one persistent kernel; 1: grouped launches per tuple group
+  cudaStream_t stream2 = nullptr;         // reduction launches of the grouped executor
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_wb[kRing] = {}, ev_ring[kRing] = {};
+  struct WbRange {
+    int64_t begin, count;
+    int bn;
+  };
+  std::vector<std::vector<WbRange>> grp_wb;  // per group: W-build item ranges, one per N tile width
+  std::vector<int64_t> grp_rd_begin, grp_rd_count;
+  int64_t group_budget = 256ll << 20;     // X scratch bytes per tuple group
   bool tuned = false;
   // schedule (device)
   bool scheduled = false;
@@ -289,7 +366,7 @@ struct ccT_batch {
   int4 *items = nullptr;
   int *counters = nullptr;
   int64_t ncounters = 0;
-  int *group_ntuples = nullptr;
+  int *group_rd_items = nullptr;
   TupleRec *tuples = nullptr;
   GemmJob *jobs = nullptr;
   SysDev *sysdev = nullptr;
@@ -305,13 +382,13 @@ namespace {
 void free_schedule(ccT_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
-  for (void *q : {(void *)b->items, (void *)b->counters, (void *)b->group_ntuples, (void *)b->tuples,
+  for (void *q : {(void *)b->items, (void *)b->counters, (void *)b->group_rd_items, (void *)b->tuples,
                   (void *)b->jobs, (void *)b->sysdev, (void *)b->tuple_etd, (void *)b->tuple_v1, (void *)b->sys_out,
                   (void *)b->scratch, (void *)b->tuple_v1_off, (void *)b->err})
     if (q) cudaFree(q);
   b->items = nullptr;
   b->counters = nullptr;
-  b->group_ntuples = nullptr;
+  b->group_rd_items = nullptr;
   b->tuples = nullptr;
   b->jobs = nullptr;
   b->sysdev = nullptr;
@@ -348,7 +425,7 @@ int build_schedule(ccT_batch *b) {
   // F depends on the N tile: rebuild every system's F for this bn
   for (int s = 0; s < nsys; s++) {
     BatchSystemHost &S = b->sys[s];
-    const Dims nd = batch_dims(S.no, S.nu, b->bn);
+    const Dims nd = batch_dims(S.no, S.nu, b->bn ? b->bn : choose_bn(S.nu));
     if (S.F && nd.NP != S.d.NP) {
       cudaFree(S.F);
       S.F = nullptr;
@@ -362,7 +439,8 @@ int build_schedule(ccT_batch *b) {
     const Dims &d = S.d;
     sys_begin[s] = (int64_t)th.size();
     const int64_t nu2 = (int64_t)S.nu * S.nu;
-    const int tiles_m = (int)((nu2 + kBTM - 1) / kBTM), tiles_n = (int)(d.NP / b->bn);
+    const int tm = b->mode == 0 ? kBTM : wb::BM;
+    const int tiles_m = (int)((nu2 + tm - 1) / tm), tiles_n = (int)(d.NP / d.BN);
     const int64_t npairs = (int64_t)d.nb * (d.nb + 1) / 2;
     for (const Tuple &t : tuple_list(S.no)) {
       TH h{};
@@ -375,7 +453,8 @@ int build_schedule(ccT_batch *b) {
       h.cost = (double)h.njobs * nu2 * d.NP * d.KP;
       // X, then the reduction partials; rounded to 256 B so every X buffer of
       // the next tuple stays 16-byte aligned (the W-build stores double2)
-      h.scratch = round_up((h.njobs * nu2 * d.NP + d.ncta + (int64_t)d.nb * kRB * 3 * npairs) * 8, 256);
+      h.scratch = round_up(h.njobs * nu2 * d.NP * 8, 256);  // rounded: X buffers stay 16-byte aligned
+      h.xpart_off = round_up(d.ncta + (int64_t)d.nb * kRB * 3 * npairs, 32);  // partial doubles (offset later)
       h.wb_items = h.njobs * tiles_m * tiles_n;
       h.rd_items = (int)d.ncta;
       th.push_back(h);
@@ -403,7 +482,14 @@ int build_schedule(ccT_batch *b) {
   }
   const int G = (int)groups.size();
   const int64_t slot_doubles = ring_slot / 8;
-  CCT_TRY(dmalloc(&b->scratch, (size_t)slot_doubles * kRing));
+  int64_t npart = 0;
+  for (int u = 0; u < T; u++) {
+    const int64_t n = th[u].xpart_off;
+    th[u].xpart_off = npart;
+    npart += n;
+  }
+  CCT_TRY(dmalloc(&b->scratch, (size_t)slot_doubles * kRing + (size_t)npart));
+  double *partials = b->scratch + slot_doubles * kRing;
   // device records
   std::vector<TupleRec> rec(T);
   std::vector<GemmJob> jobs((size_t)T * 3);
@@ -425,7 +511,7 @@ int build_schedule(ccT_batch *b) {
     r.wb_items = h.wb_items;
     r.rd_items = h.rd_items;
     for (int g = 0; g < 3; g++) r.x[g] = base + (int64_t)std::min(g, h.njobs - 1) * nu2 * d.NP;
-    r.xpart = base + h.njobs * nu2 * d.NP;
+    r.xpart = partials + h.xpart_off;
     r.vpart = r.xpart + d.ncta;
     rec[u] = r;
     v1off[u] = v1tot;
@@ -455,24 +541,40 @@ int build_schedule(ccT_batch *b) {
   }
   // items: WB(g0) WB(g1) RD(g0) WB(g2) RD(g1) ...
   std::vector<int4> items;
+  // (grouped executor: WB(g0) RD(g0) WB(g1) RD(g1) ..., one launch per range)
+  b->grp_wb.assign(G, {});
+  b->grp_rd_begin.assign(G, 0);
+  b->grp_rd_count.assign(G, 0);
   auto push_wb = [&](int g) {
-    for (int u : groups[g]) {
-      const BatchSystemHost &S = b->sys[th[u].sys];
-      const int ntiles = th[u].wb_items / th[u].njobs;
-      for (int slot = 0; slot < th[u].njobs; slot++)
-        for (int tile = 0; tile < ntiles; tile++) items.push_back(make_int4(0, u, slot, tile));
-      (void)S;
+    for (int bn : kBNChoices) {  // one range per N tile width (a single one unless bn is per system)
+      const int64_t begin = (int64_t)items.size();
+      for (int u : groups[g]) {
+        if (b->sys[th[u].sys].d.BN != bn) continue;
+        const int ntiles = th[u].wb_items / th[u].njobs;
+        for (int slot = 0; slot < th[u].njobs; slot++)
+          for (int tile = 0; tile < ntiles; tile++) items.push_back(make_int4(0, u, slot, tile));
+      }
+      if ((int64_t)items.size() > begin) b->grp_wb[g].push_back({begin, (int64_t)items.size() - begin, bn});
     }
   };
   auto push_rd = [&](int g) {
+    b->grp_rd_begin[g] = (int64_t)items.size();
     for (int u : groups[g])
       for (int c = 0; c < th[u].rd_items; c++) items.push_back(make_int4(1, u, c, 0));
+    b->grp_rd_count[g] = (int64_t)items.size() - b->grp_rd_begin[g];
   };
-  for (int g = 0; g < G; g++) {
-    push_wb(g);
-    if (g >= 1) push_rd(g - 1);
+  if (b->mode == 0) {
+    for (int g = 0; g < G; g++) {
+      push_wb(g);
+      if (g >= 1) push_rd(g - 1);
+    }
+    push_rd(G - 1);
+  } else {
+    for (int g = 0; g < G; g++) {
+      push_wb(g);
+      push_rd(g);
+    }
   }
-  push_rd(G - 1);
   // per-system device records; tuples of a system are consecutive in th
   std::vector<SysDev> sd(nsys);
   for (int s = 0; s < nsys; s++) {
@@ -481,8 +583,9 @@ int build_schedule(ccT_batch *b) {
     v.no = S.no;
     v.nu = S.nu;
     v.nb = S.d.nb;
-    v.tiles_m = (int)(((int64_t)S.nu * S.nu + kBTM - 1) / kBTM);
-    v.tiles_n = (int)(S.d.NP / b->bn);
+    const int tm = b->mode == 0 ? kBTM : wb::BM;
+    v.tiles_m = (int)(((int64_t)S.nu * S.nu + tm - 1) / tm);
+    v.tiles_n = (int)(S.d.NP / S.d.BN);
     v.KP = S.d.KP;
     v.NP = S.d.NP;
     v.ncta = S.d.ncta;
@@ -496,15 +599,16 @@ int build_schedule(ccT_batch *b) {
     v.v1 = S.v1;
     sd[s] = v;
   }
-  std::vector<int> gnt(G);
-  for (int g = 0; g < G; g++) gnt[g] = (int)groups[g].size();
+  std::vector<int> gnt(G, 0);
+  for (int g = 0; g < G; g++)
+    for (int u : groups[g]) gnt[g] += th[u].rd_items;
   b->ntuple = T;
   b->ngroup = G;
   b->nitems = (int64_t)items.size();
   b->ncounters = 1 + 2 * (int64_t)T + G + nsys;
   CCT_TRY(dmalloc(&b->items, items.size()));
   CCT_TRY(dmalloc(&b->counters, (size_t)b->ncounters));
-  CCT_TRY(dmalloc(&b->group_ntuples, (size_t)G));
+  CCT_TRY(dmalloc(&b->group_rd_items, (size_t)G));
   CCT_TRY(dmalloc(&b->tuples, (size_t)T));
   CCT_TRY(dmalloc(&b->jobs, (size_t)T * 3));
   CCT_TRY(dmalloc(&b->sysdev, (size_t)nsys));
@@ -514,7 +618,7 @@ int build_schedule(ccT_batch *b) {
   CCT_TRY(dmalloc(&b->sys_out, (size_t)3 * nsys));
   CCT_TRY(dmalloc(&b->err, 1));
   CCT_CUDA(cudaMemcpy(b->items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  CCT_CUDA(cudaMemcpy(b->group_ntuples, gnt.data(), G * sizeof(int), cudaMemcpyHostToDevice));
+  CCT_CUDA(cudaMemcpy(b->group_rd_items, gnt.data(), G * sizeof(int), cudaMemcpyHostToDevice));
   CCT_CUDA(cudaMemcpy(b->tuples, rec.data(), T * sizeof(TupleRec), cudaMemcpyHostToDevice));
   CCT_CUDA(cudaMemcpy(b->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
   CCT_CUDA(cudaMemcpy(b->sysdev, sd.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice));
@@ -524,19 +628,14 @@ int build_schedule(ccT_batch *b) {
   return CCT_OK;
 }
 
-// Kernel attributes are set once at batch creation (configure_all), outside any
-// stream capture.
-template <int BN>
-int launch_batch(ccT_batch *b) {
-  int nsm = 0;
-  CCT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device));
+BatchArgs batch_args(ccT_batch *b) {
   BatchArgs a;
   a.items = b->items;
   a.nitems = b->nitems;
   a.counters = b->counters;
   a.ntuple = b->ntuple;
   a.ngroup = b->ngroup;
-  a.group_ntuples = b->group_ntuples;
+  a.group_rd_items = b->group_rd_items;
   a.tuples = b->tuples;
   a.jobs = b->jobs;
   a.sys = b->sysdev;
@@ -545,6 +644,16 @@ int launch_batch(ccT_batch *b) {
   a.tuple_v1_off = b->tuple_v1_off;
   a.sys_out = b->sys_out;
   a.err = b->err;
+  return a;
+}
+
+// Kernel attributes are set once at batch creation (configure_all), outside any
+// stream capture.
+template <int BN>
+int launch_batch(ccT_batch *b) {
+  int nsm = 0;
+  CCT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device));
+  const BatchArgs a = batch_args(b);
   CCT_CUDA(cudaMemsetAsync(b->counters, 0, (size_t)b->ncounters * sizeof(int), b->stream));
   CCT_CUDA(cudaMemsetAsync(b->err, 0, sizeof(int), b->stream));
   batch_kernel<BN><<<nsm, kBT, batch_smem<BN>(), b->stream>>>(a);
@@ -552,15 +661,63 @@ int launch_batch(ccT_batch *b) {
   return CCT_OK;
 }
 
-int enqueue_forward(ccT_batch *b) {
-  switch (b->bn) {
-    case 32: return launch_batch<32>(b);
-    case 48: return launch_batch<48>(b);
-    case 64: return launch_batch<64>(b);
-    default:
-      set_error("unsupported batch N tile");
-      return CCT_ERR_INVALID;
+// Grouped executor: W-build launches on b->stream, reduction launches on
+// b->stream2; group g reuses the X ring slot of group g - kRing only after that
+// group's reduction launch.
+template <int BN>
+int launch_wb_range(const BatchArgs &a, int64_t begin, int64_t count, cudaStream_t s) {
+  batch_wb_kernel<BN><<<(unsigned)count, wb::NT, wb::smem_bytes<BN, wb::BM>(), s>>>(a, begin);
+  CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
+}
+
+int launch_grouped(ccT_batch *b) {
+  const BatchArgs a = batch_args(b);
+  CCT_CUDA(cudaMemsetAsync(b->counters, 0, (size_t)b->ncounters * sizeof(int), b->stream));
+  CCT_CUDA(cudaMemsetAsync(b->err, 0, sizeof(int), b->stream));
+  CCT_CUDA(cudaEventRecord(b->ev_fork, b->stream));
+  CCT_CUDA(cudaStreamWaitEvent(b->stream2, b->ev_fork, 0));
+  for (int g = 0; g < b->ngroup; g++) {
+    const int slot = g % kRing;
+    if (g >= kRing) CCT_CUDA(cudaStreamWaitEvent(b->stream, b->ev_ring[slot], 0));
+    for (const ccT_batch::WbRange &r : b->grp_wb[g]) {
+      switch (r.bn) {
+        case 64: CCT_TRY(launch_wb_range<64>(a, r.begin, r.count, b->stream)); break;
+        case 56: CCT_TRY(launch_wb_range<56>(a, r.begin, r.count, b->stream)); break;
+        case 48: CCT_TRY(launch_wb_range<48>(a, r.begin, r.count, b->stream)); break;
+        case 40: CCT_TRY(launch_wb_range<40>(a, r.begin, r.count, b->stream)); break;
+        case 32: CCT_TRY(launch_wb_range<32>(a, r.begin, r.count, b->stream)); break;
+        default:
+          set_error("unsupported W-build N tile in the batch");
+          return CCT_ERR_INVALID;
+      }
+    }
+    CCT_CUDA(cudaEventRecord(b->ev_wb[slot], b->stream));
+    CCT_CUDA(cudaStreamWaitEvent(b->stream2, b->ev_wb[slot], 0));
+    if (b->grp_rd_count[g] > 0) {
+      batch_rd_kernel<<<(unsigned)b->grp_rd_count[g], kBT, red::REDUCE_SMEM, b->stream2>>>(a, b->grp_rd_begin[g]);
+      CCT_CUDA(cudaGetLastError());
+    }
+    CCT_CUDA(cudaEventRecord(b->ev_ring[slot], b->stream2));
   }
+  CCT_CUDA(cudaEventRecord(b->ev_join, b->stream2));
+  CCT_CUDA(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+  return CCT_OK;
+}
+
+int enqueue_forward(ccT_batch *b) {
+  if (b->mode == 1) {
+    return launch_grouped(b);
+  } else {
+    switch (b->bn) {
+      case 32: return launch_batch<32>(b);
+      case 48: return launch_batch<48>(b);
+      case 64: return launch_batch<64>(b);
+      default: break;
+    }
+  }
+  set_error("unsupported batch N tile");
+  return CCT_ERR_INVALID;
 }
 
 // Capture counter reset + kernel once; replay afterwards.
@@ -600,6 +757,19 @@ int configure_all(ccT_batch *b) {
   CCT_CUDA(cudaFuncSetAttribute(batch_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem<32>()));
   CCT_CUDA(cudaFuncSetAttribute(batch_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem<48>()));
   CCT_CUDA(cudaFuncSetAttribute(batch_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem<64>()));
+  CCT_CUDA(cudaFuncSetAttribute(batch_wb_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                wb::smem_bytes<32, wb::BM>()));
+  CCT_CUDA(cudaFuncSetAttribute(batch_wb_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                wb::smem_bytes<48, wb::BM>()));
+  CCT_CUDA(cudaFuncSetAttribute(batch_wb_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                wb::smem_bytes<64, wb::BM>()));
+  CCT_CUDA(cudaFuncSetAttribute(batch_wb_kernel<56>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                wb::smem_bytes<56, wb::BM>()));
+  CCT_CUDA(cudaFuncSetAttribute(batch_wb_kernel<40>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                wb::smem_bytes<40, wb::BM>()));
+  CCT_CUDA(cudaFuncSetAttribute(batch_rd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, red::REDUCE_SMEM));
+  CCT_CUDA(cudaFuncSetAttribute(batch_rd_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared));
   (void)b;
   return CCT_OK;
 }
@@ -648,9 +818,16 @@ int ccT_batch_create(ccT_batch **out, int64_t nsys, const int64_t *no, const int
     ccT_batch_destroy(b);
     return st;
   };
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
-    set_error("cannot create the batch stream/events");
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreate(&b->ev0) == cudaSuccess && cudaEventCreate(&b->ev1) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess;
+  for (int r = 0; r < kRing && ok; r++)
+    ok = cudaEventCreateWithFlags(&b->ev_wb[r], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->ev_ring[r], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    set_error("cannot create the batch streams/events");
     return fail(CCT_ERR_CUDA);
   }
   int st = configure_all(b);
@@ -660,7 +837,7 @@ int ccT_batch_create(ccT_batch **out, int64_t nsys, const int64_t *no, const int
     BatchSystemHost &S = b->sys[s];
     S.no = (int)no[s];
     S.nu = (int)nu[s];
-    S.d = batch_dims(S.no, S.nu, b->bn);
+    S.d = batch_dims(S.no, S.nu, b->bn ? b->bn : choose_bn(S.nu));
     const int64_t n = S.no, v = S.nu, v2 = v * v;
     if ((st = dmalloc(&S.eh, n)) || (st = dmalloc(&S.ep, v)) || (st = dmalloc(&S.t1, n * v)) ||
         (st = dmalloc(&S.t2, v2 * n * n)) || (st = dmalloc(&S.vm, n * v * n * n)) ||
@@ -762,18 +939,21 @@ int ccT_batch_v1(ccT_batch *b, int64_t s, double *v1_out) {
   return CCT_OK;
 }
 
-int ccT_batch_configure(ccT_batch *b, int32_t bn, int32_t order, int64_t group_bytes) {
+int ccT_batch_configure(ccT_batch *b, int32_t mode, int32_t bn, int32_t order, int64_t group_bytes) {
   if (!b) {
     set_error("batch is NULL");
     return CCT_ERR_INVALID;
   }
   bool ok_bn = false;
   for (int c : kBatchBN) ok_bn |= c == bn;
-  if (!ok_bn || (order != 0 && order != 1) || group_bytes < (1 << 20)) {
-    set_error("bn must be 32, 48 or 64, order 0 or 1, group_bytes >= 1 MiB");
+  if (!ok_bn || (order != 0 && order != 1) || (mode != 0 && mode != 1) || group_bytes < (1 << 20) ||
+      (mode == 0 && bn == 0)) {
+    set_error("mode must be 0 or 1, bn 0 (per system, mode 1 only), 32, 48 or 64, order 0 or 1, "
+              "group_bytes >= 1 MiB");
     return CCT_ERR_INVALID;
   }
   Guard guard(b->device);
+  b->mode = mode;
   b->bn = bn;
   b->order = order;
   b->group_budget = group_bytes;
@@ -781,7 +961,7 @@ int ccT_batch_configure(ccT_batch *b, int32_t bn, int32_t order, int64_t group_b
   return CCT_OK;
 }
 
-int ccT_batch_tune(ccT_batch *b, int32_t *best_bn, int32_t *best_order, double *best_ms) {
+int ccT_batch_tune(ccT_batch *b, int32_t *best_mode, int32_t *best_bn, int32_t *best_order, double *best_ms) {
   if (!b) {
     set_error("batch is NULL");
     return CCT_ERR_INVALID;
@@ -789,9 +969,12 @@ int ccT_batch_tune(ccT_batch *b, int32_t *best_bn, int32_t *best_order, double *
   CCT_TRY(batch_inputs_ready(b));
   Guard guard(b->device);
   double best = INFINITY;
-  int bbn = b->bn, bord = b->order;
+  int bbn = b->bn, bord = b->order, bmode = b->mode;
+  for (int mode : {0, 1})
   for (int bn : kBatchBN)
     for (int order : {0, 1}) {
+      if (mode == 0 && bn == 0) continue;  // the persistent kernel has one N tile
+      b->mode = mode;
       b->bn = bn;
       b->order = order;
       CCT_TRY(build_schedule(b));
@@ -810,14 +993,17 @@ int ccT_batch_tune(ccT_batch *b, int32_t *best_bn, int32_t *best_order, double *
       }
       if (tot / 2 < best) {
         best = tot / 2;
+        bmode = mode;
         bbn = bn;
         bord = order;
       }
     }
+  b->mode = bmode;
   b->bn = bbn;
   b->order = bord;
   CCT_TRY(build_schedule(b));
   b->tuned = true;
+  if (best_mode) *best_mode = bmode;
   if (best_bn) *best_bn = bbn;
   if (best_order) *best_order = bord;
   if (best_ms) *best_ms = best;
@@ -832,13 +1018,19 @@ int ccT_batch_destroy(ccT_batch *b) {
   if (!b) return CCT_OK;
   Guard guard(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->stream2) cudaStreamSynchronize(b->stream2);
   free_schedule(b);
   for (BatchSystemHost &S : b->sys)
     for (void *q : {(void *)S.eh, (void *)S.ep, (void *)S.t1, (void *)S.t2, (void *)S.vm, (void *)S.voe,
                     (void *)S.vvvo, (void *)S.E, (void *)S.F, (void *)S.v1, (void *)S.cta_table})
       if (q) cudaFree(q);
-  if (b->ev0) cudaEventDestroy(b->ev0);
-  if (b->ev1) cudaEventDestroy(b->ev1);
+  for (cudaEvent_t e : {b->ev0, b->ev1, b->ev_fork, b->ev_join})
+    if (e) cudaEventDestroy(e);
+  for (int r = 0; r < kRing; r++) {
+    if (b->ev_wb[r]) cudaEventDestroy(b->ev_wb[r]);
+    if (b->ev_ring[r]) cudaEventDestroy(b->ev_ring[r]);
+  }
+  if (b->stream2) cudaStreamDestroy(b->stream2);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return CCT_OK;

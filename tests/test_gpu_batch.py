@@ -52,22 +52,25 @@ def test_batch_matches_oracle(systems):
         assert abs(ets[k] - ets_o) <= 1e-11 * abs(ets_o) + 1e-15, k
 
 
-@pytest.mark.parametrize("bn,order,group_mib", [(32, 0, 512), (64, 1, 512), (48, 0, 1), (32, 1, 1)])
-def test_schedules_agree(systems, single, bn, order, group_mib):
-    """Every N tile, tuple order and group size (1 MiB forces many groups, so the
-    X scratch ring is reused and the group waits are exercised) gives the same bits."""
+@pytest.mark.parametrize("mode,bn,order,group_mib", [
+    (0, 32, 0, 512), (0, 64, 1, 512), (0, 48, 0, 1), (0, 32, 1, 1),
+    (1, 0, 0, 512), (1, 0, 1, 1), (1, 64, 1, 512), (1, 48, 0, 1), (1, 32, 1, 1)])
+def test_schedules_agree(systems, single, mode, bn, order, group_mib):
+    """Both executors, every N tile, tuple order and group size (1 MiB forces many
+    groups, so the X scratch ring is reused and the group waits / stream events
+    are exercised) give the same bits."""
     with _batch(systems) as b:
-        b.configure(bn, order, group_mib << 20)
+        b.configure(mode, bn, order, group_mib << 20)
         for _ in range(2):  # second call replays the CUDA graph
             ets, etd = b.forward()
             for k in range(len(systems)):
-                assert ets[k] == single[k][0] and etd[k] == single[k][1], (bn, order, group_mib, k)
+                assert ets[k] == single[k][0] and etd[k] == single[k][1], (mode, bn, order, group_mib, k)
 
 
 def test_tune_picks_a_candidate(systems, single):
     with _batch(systems) as b:
-        bn, order, ms = b.tune()
-        assert bn in (32, 48, 64) and order in (0, 1) and ms > 0
+        mode, bn, order, ms = b.tune()
+        assert mode in (0, 1) and bn in (0, 32, 48, 64) and order in (0, 1) and ms > 0
         ets, etd = b.forward()
         assert b.last_ms > 0 and b.work_items > 0
         for k in range(len(systems)):
