@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the adjoint (no=12/nu=120) and batched-systems (96 uneven) measurements")
     ap.add_argument("--emu-slices", type=int, default=5, help="7-bit digits per operand of the emulated form (4..7)")
     return ap.parse_args()
 
@@ -181,6 +183,100 @@ def run_reference(args, rank, world):
             "note": "ms_per_step extrapolates the sampled tuples/s to all tuples of the workload"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def adjoint_extra(A, S, local):
+    """Forward + hand-written adjoint on the no=12/nu=120 system (seed 3): device
+    times, their ratio, and the gradient against the stored hand-derived FP64 CPU
+    gradient (200 seeded entries per input) and a few central differences."""
+    import copy
+    import numpy as np
+    g0 = json.loads((ROOT / "tests" / "golden" / "grad_no12-nu120.json").read_text())
+    inp = S.generate(g0["no"], g0["nu"], g0["seed"], g0["dist"])
+    with A.TriplesPlan(inp.no, inp.nu, device=local) as plan:
+        plan.set_system(inp)
+        fwd, bwd = [], []
+        for rep in range(4):
+            ets, etd, _ = plan.forward()
+            fwd.append(plan.last_forward_ms)
+            g = plan.backward()
+            bwd.append(plan.last_backward_ms)
+        f_ms, b_ms = statistics.median(fwd[1:]), statistics.median(bwd[1:])
+        rel = {}
+        for name, ref in g0["tensors"].items():
+            idx = np.array(ref["index"])
+            rel[name] = float(np.abs(g[name][idx] - np.array(ref["value"])).max() / ref["maxabs"])
+        rng = np.random.default_rng(5)
+        fd_rel = {}
+        for name in g0["tensors"]:
+            arr = getattr(inp, name)
+            worst = 0.0
+            for idx in rng.choice(arr.size, size=2, replace=False):
+                h = 1e-5 * max(1.0, abs(arr[idx]))
+                vals = []
+                for sgn in (1.0, -1.0):
+                    ip = copy.deepcopy(inp)
+                    getattr(ip, name)[idx] += sgn * h
+                    plan.set_system(ip)
+                    e1, e2, _ = plan.forward(want_v1=False)
+                    vals.append(e1 + e2)
+                fd = (vals[0] - vals[1]) / (2 * h)
+                worst = max(worst, abs(fd - g[name][idx]) / g0["tensors"][name]["maxabs"])
+            fd_rel[name] = worst
+    return {"workload": "no12-nu120 (seed 3, normal)", "forward_ms": f_ms, "backward_ms": b_ms,
+            "ratio_backward_over_forward": b_ms / f_ms, "e_t": ets + etd,
+            "max_rel_err_vs_cpu_gradient": rel, "central_difference_h": 1e-5,
+            "max_rel_err_vs_central_differences": fd_rel,
+            "note": "backward recomputes W per tuple in FP64; rel errors are relative to max|gradient| per input"}
+
+
+def batch_extra(A, S, local):
+    """The 96 uneven systems (no ~ U{3..12}, nu ~ U{24..140}, seed 100+s): the
+    batched executor (CUDA graph) against a per-system plan loop, and per-system
+    E(T) against the CPU oracle on the 8 smallest systems."""
+    import numpy as np
+    from libcc_b200 import batch as B
+    from oracle import oracle as O
+    systems = S.batch96()
+    plans = []
+    for inp in systems:
+        p = A.TriplesPlan(inp.no, inp.nu, device=local)
+        p.set_system(inp)
+        plans.append(p)
+    loop_ms, loop_res = [], None
+    for rep in range(3):
+        res, ms = [], 0.0
+        for p in plans:
+            res.append(p.forward(want_v1=False))
+            ms += p.last_forward_ms
+        loop_ms.append(ms)
+        loop_res = res
+    for p in plans:
+        p.close()
+    with B.TriplesBatch([(s.no, s.nu) for s in systems], device=local) as b:
+        for k, inp in enumerate(systems):
+            b.set_system(k, inp)
+        bms = []
+        for rep in range(3):
+            ets, etd = b.forward()
+            bms.append(b.last_ms)
+        items = b.work_items
+    same = all(ets[k] == loop_res[k][0] and etd[k] == loop_res[k][1] for k in range(len(systems)))
+    small = sorted(range(len(systems)), key=lambda k: S.flops(systems[k].no, systems[k].nu))[:8]
+    errs = []
+    for k in small:
+        e_o, d_o, _ = O.c_cc_triples(systems[k])
+        errs.append(abs((ets[k] + etd[k]) - (e_o + d_o)) / abs(e_o + d_o))
+    flops = sum(S.flops(s.no, s.nu) for s in systems)
+    lm, bm = statistics.median(loop_ms), statistics.median(bms)
+    return {"workload": "96 systems, no ~ U{3..12}, nu ~ U{24..140}, seed 100+s (normal)",
+            "tuples": int(sum(A.N.load().ccT_num_tuples(s.no) for s in systems)), "flops": flops,
+            "batched_ms": bm, "batched_tflops": flops / bm / 1e9, "per_system_loop_ms": lm,
+            "per_system_loop_tflops": flops / lm / 1e9, "speedup_batched_over_loop": lm / bm,
+            "work_items": items, "bitwise_equal_to_loop": bool(same),
+            "executor": "grouped launches per tuple group on two streams, per-system N tile, tuples by cost; "
+                        "CUDA graph replay",
+            "max_rel_err_vs_oracle_8_smallest": max(errs)}
 
 
 def make_plan(A, no, nu, device, form):
@@ -376,6 +472,9 @@ def main():
                                     "give |E(T)| ~ 7.7e9 Eh, where an absolute 1e-8 Eh is below FP64 resolution"},
                 "forms": forms,
                 "speedup_emulated_over_native": forms["fp64"]["ms_per_step"] / head["ms_per_step"]}
+        if world == 1 and not args.no_extras:
+            line["adjoint"] = adjoint_extra(A, S, local)
+            line["batch"] = batch_extra(A, S, local)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -117,3 +117,24 @@ def test_backward_central_differences_of_gpu_forward(api):
                     vals.append(ets + etd)
                 fd = (vals[0] - vals[1]) / (2 * h)
                 assert abs(fd - g[name][idx]) <= 1e-6 * scale + 1e-8 * abs(fd), (name, idx, fd, g[name][idx])
+
+
+def test_backward_matches_golden_gradient_no12_nu120(api):
+    """The no=12/nu=120 system (seed 3): GPU gradient against the hand-derived FP64
+    CPU gradient stored in tests/golden (200 seeded entries per input and
+    whole-tensor checksums)."""
+    import json
+    import pathlib
+    g0 = json.loads((pathlib.Path(__file__).parent / "golden" / "grad_no12-nu120.json").read_text())
+    inp = S.generate(g0["no"], g0["nu"], g0["seed"], g0["dist"])
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        ets, etd, _ = plan.forward()
+        g = plan.backward()
+    assert abs((ets + etd) - g0["e_t"]) <= 1e-12 * abs(g0["e_t"])
+    for name, ref in g0["tensors"].items():
+        got = g[name]
+        idx = np.array(ref["index"])
+        assert np.abs(got[idx] - np.array(ref["value"])).max() <= 1e-10 * ref["maxabs"], name
+        assert abs(got.sum() - ref["sum"]) <= 1e-10 * ref["maxabs"] * np.sqrt(got.size) + 1e-12 * abs(ref["sum"]), name
+        assert abs(np.dot(got, got) - ref["sumsq"]) <= 1e-9 * ref["sumsq"], name
