@@ -40,8 +40,8 @@
 namespace cct {
 namespace {
 
-constexpr int EBM = kEmuBM, EBN = kEmuBN;
-constexpr int A_BLK = kEmuABlk, B_BLK = kEmuBBlk;
+constexpr int EBM = kEmuBM;
+constexpr int A_BLK = kEmuABlk;
 // A stage holds KS consecutive K chunks (all S digit slices of each), so one
 // barrier round trip feeds KS S(S+1)/2 MMAs.  Ring depth: as many stages as
 // the shared-memory budget holds, between 2 and 8.
@@ -57,13 +57,13 @@ constexpr int A_BLK = kEmuABlk, B_BLK = kEmuBBlk;
 constexpr int KS = CCT_EMU_KS;
 constexpr int NDW = CCT_EMU_DRAIN_WARPS;  // drain warps: NDW/4 per TMEM lane quarter
 constexpr int EMU_THREADS = 64 + 32 * NDW;
-template <int S>
+template <int S, int EBN>
 constexpr int emu_stages() {
-  return CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + B_BLK)) > 8   ? 8
-         : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + B_BLK)) < 2 ? 2
-                                                                 : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + B_BLK));
+  return CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + EBN * kEmuKC)) > 8   ? 8
+         : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + EBN * kEmuKC)) < 2 ? 2
+                                                                        : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + EBN * kEmuKC));
 }
-template <int S>
+template <int S, int EBN>
 constexpr uint32_t emu_tmem_cols() { return S * EBN <= 256 ? 256u : 512u; }
 constexpr long kWaitLimit = 1L << 26;
 
@@ -119,6 +119,20 @@ __device__ __forceinline__ uint64_t desc_kmajor(const void *p) {
   return ((a & 0x3FFFF) >> 4) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46);
 }
 
+// tcgen05.ld of 16 / 8 consecutive 32-bit columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t *v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(addr));
+}
+
 struct EmuArgs {
   const EmuJob *jobs;
   const int8_t *E8, *E8T, *F8;
@@ -135,10 +149,12 @@ __device__ __forceinline__ double pow2(int e) {
   return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
 }
 
-template <int S>
+template <int S, int EBN>
 __global__ void __launch_bounds__(EMU_THREADS, 1) wbuild_emu_kernel(const EmuArgs args) {
-  constexpr uint32_t TCOLS = emu_tmem_cols<S>();
-  constexpr int ST = emu_stages<S>();
+  static_assert(S * EBN <= 512 && EBN % 16 == 0, "S diagonals of EBN columns must fit the tensor memory");
+  constexpr int B_BLK = EBN * kEmuKC;
+  constexpr uint32_t TCOLS = emu_tmem_cols<S, EBN>();
+  constexpr int ST = emu_stages<S, EBN>();
   constexpr int CA = S * A_BLK, CB = S * B_BLK;    // bytes of one K chunk per operand
   constexpr int SA = KS * CA, SB = KS * CB;        // bytes of one stage per operand
   extern __shared__ __align__(1024) uint8_t emu_smem[];
@@ -290,21 +306,22 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) wbuild_emu_kernel(const EmuArg
 #pragma unroll
       for (int c0 = 0; c0 < CW; c0 += 16) {
         constexpr int DB = S <= 5 ? S : 1;  // diagonals per tcgen05.wait::ld
+        const int w = CW - c0 >= 16 ? 16 : 8;  // the last chunk of a 40-column slice is 8 wide
 #pragma unroll
         for (int d0 = 0; d0 < S; d0 += DB) {
           uint32_t v[DB][16];
 #pragma unroll
-          for (int dd = 0; dd < DB; dd++)
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                "[%16];"
-                : "=r"(v[dd][0]), "=r"(v[dd][1]), "=r"(v[dd][2]), "=r"(v[dd][3]), "=r"(v[dd][4]), "=r"(v[dd][5]),
-                  "=r"(v[dd][6]), "=r"(v[dd][7]), "=r"(v[dd][8]), "=r"(v[dd][9]), "=r"(v[dd][10]), "=r"(v[dd][11]),
-                  "=r"(v[dd][12]), "=r"(v[dd][13]), "=r"(v[dd][14]), "=r"(v[dd][15])
-                : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((d0 + dd) * EBN + cbase + c0)));
+          for (int dd = 0; dd < DB; dd++) {
+            const uint32_t addr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((d0 + dd) * EBN + cbase + c0);
+            if (w == 16)
+              tmem_ld16(addr, v[dd]);
+            else
+              tmem_ld8(addr, v[dd]);
+          }
           asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
           for (int j = 0; j < 16; j++) {
+            if (j >= w) continue;
             double a = d0 == 0 ? 0.0 : acc[c0 + j];
 #pragma unroll
             for (int dd = 0; dd < DB; dd++) a = fma((double)(int32_t)v[dd][j], cd[d0 + dd], a);
@@ -432,9 +449,10 @@ __global__ void digits_e_kernel(const double *__restrict__ E, int no, int nu, in
 }
 
 __global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, int64_t NP, int64_t KP, int64_t KP8,
-                                int S, const int16_t *__restrict__ expF, int8_t *__restrict__ F8) {
+                                int S, int ebn, const int16_t *__restrict__ expF, int8_t *__restrict__ F8) {
   const int64_t rows = (int64_t)no * no * NP;
-  const int64_t KC = KP8 / kEmuKC, tiles_n = NP / kEmuBN;
+  const int64_t KC = KP8 / kEmuKC, tiles_n = NP / ebn;
+  const int64_t bblk = (int64_t)ebn * kEmuKC;
   const int lane = threadIdx.x & 31;
   int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -447,23 +465,23 @@ __global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, in
       digits4(F + row * KP, k, nu + no, e, S, w);
       const int64_t kc = k / kEmuKC;
       const int kb = (int)(k - kc * kEmuKC);
-      const int64_t b = ((yz * tiles_n + n / kEmuBN) * KC + kc) * S * kEmuBBlk + blk_off((int)(n % kEmuBN), kb);
-      for (int t = 0; t < S; t++) *reinterpret_cast<uint32_t *>(F8 + b + (int64_t)t * kEmuBBlk) = w[t];
+      const int64_t b = ((yz * tiles_n + n / ebn) * KC + kc) * S * bblk + blk_off((int)(n % ebn), kb);
+      for (int t = 0; t < S; t++) *reinterpret_cast<uint32_t *>(F8 + b + (int64_t)t * bblk) = w[t];
     }
   }
 }
 
 int g_num_sms[64] = {0};
 
-template <int S>
+template <int S, int EBN>
 int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err, cudaStream_t s) {
-  constexpr int smem = emu_stages<S>() * KS * S * (A_BLK + B_BLK) + 1024;
+  constexpr int smem = emu_stages<S, EBN>() * KS * S * (A_BLK + EBN * kEmuKC) + 1024;
   static int configured_device = -1;
   int dev = 0;
   CCT_CUDA(cudaGetDevice(&dev));
   if (configured_device != dev) {
-    CCT_CUDA(cudaFuncSetAttribute(wbuild_emu_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CCT_CUDA(cudaFuncSetAttribute(wbuild_emu_kernel<S>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    CCT_CUDA(cudaFuncSetAttribute(wbuild_emu_kernel<S, EBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CCT_CUDA(cudaFuncSetAttribute(wbuild_emu_kernel<S, EBN>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   cudaSharedmemCarveoutMaxShared));
     configured_device = dev;
   }
@@ -484,11 +502,15 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   a.kchunks = (int)(o.KP8 / kEmuKC);
   a.tiles_m = (int)o.tiles_m;
   a.tiles_n = (int)(d.NP / EBN);
+  if (d.EBN != EBN) {
+    set_error("emulated N tile mismatch");
+    return CCT_ERR_INVALID;
+  }
   a.NP = d.NP;
   a.err = err;
   const int64_t items = (int64_t)njobs * a.tiles_m * a.tiles_n;
   const int grid = (int)(items < g_num_sms[dev] ? items : g_num_sms[dev]);
-  wbuild_emu_kernel<S><<<grid, EMU_THREADS, smem, s>>>(a);
+  wbuild_emu_kernel<S, EBN><<<grid, EMU_THREADS, smem, s>>>(a);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
@@ -501,8 +523,8 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
               std::to_string(kEmuMaxSlices) + "]");
     return CCT_ERR_INVALID;
   }
-  if (d.NP % EBN != 0 || o->KP8 % kEmuKC != 0) {
-    set_error("emulated plan needs NP a multiple of 64 and KP8 a multiple of 32");
+  if (d.EBN <= 0 || d.NP % d.EBN != 0 || o->KP8 % kEmuKC != 0 || o->slices * d.EBN > 512) {
+    set_error("emulated plan needs NP a multiple of its N tile, KP8 a multiple of 32 and slices x N <= 512");
     return CCT_ERR_INVALID;
   }
   const int64_t rowsE = (int64_t)d.no * d.nu * d.nu, rowsF = (int64_t)d.no * d.no * d.NP;
@@ -530,20 +552,28 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
   digits_e_kernel<<<grid_rows(rowsE), 256, 0, s>>>(E, d.no, d.nu, d.KP, o->KP8, o->slices, o->tiles_m, o->expE,
                                                    o->E8, o->E8T);
   CCT_CUDA(cudaGetLastError());
-  digits_f_kernel<<<grid_rows(rowsF), 256, 0, s>>>(F, d.no, d.nu, d.NP, d.KP, o->KP8, o->slices, o->expF, o->F8);
+  digits_f_kernel<<<grid_rows(rowsF), 256, 0, s>>>(F, d.no, d.nu, d.NP, d.KP, o->KP8, o->slices, d.EBN, o->expF,
+                                                   o->F8);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
 
 int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
                       cudaStream_t s) {
-  switch (o.slices) {
-    case 4: return launch_emu_s<4>(o, d, jobs_dev, njobs, err, s);
-    case 5: return launch_emu_s<5>(o, d, jobs_dev, njobs, err, s);
-    case 6: return launch_emu_s<6>(o, d, jobs_dev, njobs, err, s);
-    case 7: return launch_emu_s<7>(o, d, jobs_dev, njobs, err, s);
+  // (slices, N tile) pairs with slices x N <= 512
+  const int key = o.slices * 1000 + d.EBN;
+  switch (key) {
+    case 4064: return launch_emu_s<4, 64>(o, d, jobs_dev, njobs, err, s);
+    case 4080: return launch_emu_s<4, 80>(o, d, jobs_dev, njobs, err, s);
+    case 4096: return launch_emu_s<4, 96>(o, d, jobs_dev, njobs, err, s);
+    case 5064: return launch_emu_s<5, 64>(o, d, jobs_dev, njobs, err, s);
+    case 5080: return launch_emu_s<5, 80>(o, d, jobs_dev, njobs, err, s);
+    case 5096: return launch_emu_s<5, 96>(o, d, jobs_dev, njobs, err, s);
+    case 6064: return launch_emu_s<6, 64>(o, d, jobs_dev, njobs, err, s);
+    case 6080: return launch_emu_s<6, 80>(o, d, jobs_dev, njobs, err, s);
+    case 7064: return launch_emu_s<7, 64>(o, d, jobs_dev, njobs, err, s);
     default:
-      set_error("unsupported slice count " + std::to_string(o.slices));
+      set_error("unsupported (slices, N tile) = (" + std::to_string(o.slices) + ", " + std::to_string(d.EBN) + ")");
       return CCT_ERR_INVALID;
   }
 }

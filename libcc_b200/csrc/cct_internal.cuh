@@ -81,7 +81,8 @@ struct Dims {
   int no, nu;
   int64_t KP;   // padded contraction length of one half: round_up(nu+no, kKB)
   int BN;       // N tile of the W-build GEMM (choose_bn)
-  int64_t NP;   // padded single-index length: round_up(nu, BN)
+  int64_t NP;   // padded single-index length: round_up(nu, BN) (emulated: round_up(nu, EBN))
+  int EBN;      // N tile of the emulated W-build (emulated plans), else 0
   int nb;       // reduction blocks per index: ceil(nu / kRB)
   int64_t ncta; // canonical block triples: nb(nb+1)(nb+2)/6
 };
@@ -97,7 +98,23 @@ struct TupleDev {
 // Digit count of the split-integer operands (7 bits each).  Measured on the
 // no=24/nu=320 workload: |dE|/|E| = 1.7e-7 (4 digits), 1.6e-9 (5), 1.4e-13 (7).
 constexpr int kEmuMinSlices = 4, kEmuMaxSlices = 7, kEmuDefaultSlices = 5;
-constexpr int kEmuBN = 64;  // N tile of the emulated W-build
+// N tile of the emulated W-build: the tensor memory holds S diagonal
+// accumulators of N int32 columns (S N <= 512), and an MMA instruction costs
+// about the same up to N ~ 80, so the widest N that pads nu least is used.
+constexpr int kEmuBNChoices[] = {96, 80, 64};
+inline int emu_choose_bn(int64_t nu, int slices) {
+  int best = 64;
+  int64_t best_np = (nu + 63) / 64 * 64;
+  for (int bn : kEmuBNChoices) {
+    if (slices * bn > 512) continue;
+    const int64_t np = (nu + bn - 1) / bn * bn;
+    if (np < best_np || (np == best_np && bn > best)) {
+      best = bn;
+      best_np = np;
+    }
+  }
+  return best;
+}
 
 // One emulated W-build GEMM: half h multiplies E-digit rows (half 0: E[x1] rows
 // (p,q); half 1: E^T[x2] rows (p,q) = E[x2] rows (q,p)) with F-digit rows of
@@ -118,13 +135,13 @@ struct EmuJob {
 constexpr int kEmuBM = 128;                      // rows per A tile
 constexpr int kEmuKC = 32;                       // K bytes per chunk (one kind::i8 MMA)
 constexpr int kEmuABlk = kEmuBM * kEmuKC;        // 4096 bytes
-constexpr int kEmuBBlk = kEmuBN * kEmuKC;        // 2048 bytes
+// B blocks hold EBN rows: EBN * kEmuKC bytes (2048, 2560 or 3072)
 struct EmuOperands {
   int slices = kEmuDefaultSlices;
   int64_t KP8 = 0;                           // digit row length: round_up(nu+no, 32)
   int64_t tiles_m = 0;                       // ceil(nu^2 / 128) row tiles per occupied index
   int8_t *E8 = nullptr, *E8T = nullptr;      // [x][tile_m][kchunk][slice][4096]; E8T rows (q,p)
-  int8_t *F8 = nullptr;                      // [y*no+z][tile_n][kchunk][slice][2048]
+  int8_t *F8 = nullptr;                      // [y*no+z][tile_n][kchunk][slice][EBN*32]
   // Digit scales shared by both halves of a GEMM, so one set of diagonal
   // accumulators serves the whole contraction: expE[p*nu+q] (symmetric) is the
   // largest row exponent of E[x][p][q] and E[x][q][p] over all x; expF[z*NP+n]

@@ -355,8 +355,23 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   d.nu = (int)nu;
   d.KP = round_up(nu + no, kKB);
   p->emulated = o.precision == CCT_PREC_INT8_EMU;
-  d.BN = p->emulated ? kEmuBN : choose_bn(nu);
-  d.NP = round_up(nu, d.BN);
+  if (p->emulated) {
+    // the emulated tile sets NP; the FP64 W-build (the backward's recompute)
+    // takes the widest of its tiles that divides NP (NP is a multiple of 64,
+    // 80 or 96, so 64, 40 or 48 always qualifies)
+    d.EBN = emu_choose_bn(nu, o.emu_slices ? o.emu_slices : kEmuDefaultSlices);
+    d.NP = round_up(nu, d.EBN);
+    d.BN = 0;
+    for (int bn : kBNChoices)
+      if (d.NP % bn == 0) {
+        d.BN = bn;
+        break;
+      }
+  } else {
+    d.EBN = 0;
+    d.BN = choose_bn(nu);
+    d.NP = round_up(nu, d.BN);
+  }
   d.nb = (int)((nu + kRB - 1) / kRB);
   d.ncta = (int64_t)d.nb * (d.nb + 1) * (d.nb + 2) / 6;
   p->tuples = tuple_list((int)no);

@@ -81,6 +81,19 @@ def test_emulated_tuple_kinds_and_shards(api):
             assert abs(etd - e_ref) <= 1e-11 * abs(e_ref), (kind, i, j, k)
 
 
+@pytest.mark.parametrize("no,nu,slices", [(4, 70, 5), (3, 90, 5), (5, 150, 6), (4, 75, 4)])
+def test_wide_n_tiles_meet_the_bar(api, no, nu, slices):
+    """nu chosen so the plan picks the 80- and 96-column emulated N tiles."""
+    from oracle import oracle as O
+    inp = S.generate(no, nu, 31 + nu, dist="log")
+    ets_o, etd_o, _ = O.literal_cc_triples(inp)
+    with _plan(api, inp, slices) as plan:
+        plan.set_system(inp)
+        ets, etd, _ = plan.forward()
+    bar = {4: 3e-6, 5: 3e-8, 6: 3e-10}[slices]
+    assert abs((ets + etd) - (ets_o + etd_o)) <= bar * abs(ets_o + etd_o), (ets + etd, ets_o + etd_o)
+
+
 def test_emulated_deterministic(api):
     inp = S.generate(4, 40, 12)
     with api.TriplesPlan(inp.no, inp.nu, precision="int8") as plan:
