@@ -51,6 +51,12 @@ constexpr int A_BLK = kEmuABlk;
 #ifndef CCT_EMU_DRAIN_WARPS
 #define CCT_EMU_DRAIN_WARPS 8
 #endif
+#ifndef CCT_EMU_MAXNREG
+#define CCT_EMU_MAXNREG 128
+#endif
+#ifndef CCT_EMU_DB
+#define CCT_EMU_DB 1
+#endif
 #ifndef CCT_EMU_SMEM_BUDGET
 #define CCT_EMU_SMEM_BUDGET (180 * 1024)
 #endif
@@ -150,7 +156,7 @@ __device__ __forceinline__ double pow2(int e) {
 }
 
 template <int S, int EBN>
-__global__ void __launch_bounds__(EMU_THREADS, 1) wbuild_emu_kernel(const EmuArgs args) {
+__global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs args) {
   static_assert(S * EBN <= 512 && EBN % 16 == 0, "S diagonals of EBN columns must fit the tensor memory");
   constexpr int B_BLK = EBN * kEmuKC;
   constexpr uint32_t TCOLS = emu_tmem_cols<S, EBN>();
@@ -305,7 +311,7 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) wbuild_emu_kernel(const EmuArg
       double acc[CW];
 #pragma unroll
       for (int c0 = 0; c0 < CW; c0 += 16) {
-        constexpr int DB = S <= 5 ? S : 1;  // diagonals per tcgen05.wait::ld
+        constexpr int DB = CCT_EMU_DB;  // diagonals per tcgen05.wait::ld
         const int w = CW - c0 >= 16 ? 16 : 8;  // the last chunk of a 40-column slice is 8 wide
 #pragma unroll
         for (int d0 = 0; d0 < S; d0 += DB) {
