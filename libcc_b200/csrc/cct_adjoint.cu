@@ -48,21 +48,66 @@ __device__ __forceinline__ int64_t widx(int nu, int a, int b, int c) { return ((
 
 // ---------------------------------------------------------------------------- W assembly
 // Grids of the dense nu^3 kernels: x = 128-wide blocks of c, y = b, z = a.
-template <int KIND>
-__global__ void adj_wfull_kernel(int nu, int64_t NP, AdjTuple t, double *__restrict__ Wf) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y, a = blockIdx.z;
-  if (c < nu) {
-    const int64_t e = widx(nu, a, b, c);
-    const int xs[3] = {a, b, c};
-    double w = 0.0;
+// W(a,b,c) = sum over the terms of X_g at a permutation of (a,b,c), for one
+// tile a in [a0, a0+8), b in [b0, b0+8), c in [c0, c0+32) per CTA (grid x: c
+// blocks, y: b blocks, z: a blocks).  Each term's X tile is staged in shared
+// memory by coalesced asynchronous copies in its own index order (innermost
+// extent and plane padded by one), then summed and written as 256-byte rows.
+constexpr int kWA = 8, kWB = 8, kWC = 32;
+constexpr int kWThreads = 256;
+constexpr int kWSlot = 2336;  // >= D0 * (D1 * (D2 + 1) + 1) for every order of (8, 8, 32)
+
+__host__ __device__ constexpr int wf_ext(int pos) { return pos == 2 ? kWC : (pos == 1 ? kWB : kWA); }
+
+template <int KIND, int TERM>
+__device__ __forceinline__ void wf_load_term(double *dst, const AdjTuple &t, int nu, int64_t NP, const int o[3]) {
+  constexpr int g = term_entry(KIND, TERM, 0);
+  constexpr int p0 = term_entry(KIND, TERM, 1), p1 = term_entry(KIND, TERM, 2), p2 = term_entry(KIND, TERM, 3);
+  constexpr int D0 = wf_ext(p0), D1 = wf_ext(p1), D2 = wf_ext(p2), PL = D1 * (D2 + 1) + 1;
+  const double *X = t.x[g];
 #pragma unroll
-    for (int term = 0; term < nterms(KIND); term++) {
-      const int g = term_entry(KIND, term, 0);
-      const int p = xs[term_entry(KIND, term, 1)], q = xs[term_entry(KIND, term, 2)],
-                s = xs[term_entry(KIND, term, 3)];
-      w += t.x[g][((int64_t)p * nu + q) * NP + s];
-    }
-    Wf[e] = (a == b && b == c) ? 0.0 : w;
+  for (int e = threadIdx.x; e < D0 * D1 * D2; e += kWThreads) {
+    const int k = e % D2, j = (e / D2) % D1, i = e / (D1 * D2);
+    const int x0 = o[p0] + i, x1 = o[p1] + j, x2 = o[p2] + k;
+    const bool ok = x0 < nu && x1 < nu && x2 < nu;
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + i * PL + j * (D2 + 1) + k);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa),
+                 "l"(X + (ok ? ((int64_t)x0 * nu + x1) * NP + x2 : 0)), "r"(ok ? 8 : 0));
+  }
+}
+
+template <int KIND, int TERM>
+__device__ __forceinline__ double wf_term(const double *src, const int l[3]) {
+  constexpr int p0 = term_entry(KIND, TERM, 1), p1 = term_entry(KIND, TERM, 2), p2 = term_entry(KIND, TERM, 3);
+  constexpr int D1 = wf_ext(p1), D2 = wf_ext(p2), PL = D1 * (D2 + 1) + 1;
+  return src[l[p0] * PL + l[p1] * (D2 + 1) + l[p2]];
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kWThreads) adj_wfull_kernel(int nu, int64_t NP, AdjTuple t,
+                                                              double *__restrict__ Wf) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *S = reinterpret_cast<double *>(smem_raw);
+  const int o[3] = {(int)blockIdx.z * kWA, (int)blockIdx.y * kWB, (int)blockIdx.x * kWC};
+  wf_load_term<KIND, 0>(S, t, nu, NP, o);
+  wf_load_term<KIND, 1>(S + kWSlot, t, nu, NP, o);
+  wf_load_term<KIND, 2>(S + 2 * kWSlot, t, nu, NP, o);
+  if (nterms(KIND) > 3) wf_load_term<KIND, (nterms(KIND) > 3 ? 3 : 0)>(S + 3 * kWSlot, t, nu, NP, o);
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  const int al = threadIdx.x >> 5, cl = threadIdx.x & 31;
+  const int a = o[0] + al, c = o[2] + cl;
+  if (a >= nu || c >= nu) return;
+#pragma unroll
+  for (int bl = 0; bl < kWB; bl++) {
+    const int b = o[1] + bl;
+    if (b >= nu) break;
+    const int l[3] = {al, bl, cl};
+    double w = wf_term<KIND, 0>(S, l) + wf_term<KIND, 1>(S + kWSlot, l);
+    w += wf_term<KIND, 2>(S + 2 * kWSlot, l);
+    if (nterms(KIND) > 3) w += wf_term<KIND, (nterms(KIND) > 3 ? 3 : 0)>(S + 3 * kWSlot, l);
+    Wf[widx(nu, a, b, c)] = (a == b && b == c) ? 0.0 : w;
   }
 }
 
@@ -99,35 +144,103 @@ __global__ void adj_q_kernel(int nu, QTable q, const double *__restrict__ voe, d
   }
 }
 
-// Thread per (b, c) and chunk of kAChunk consecutive a (grid x: c blocks, y: b,
-// z: a chunks).  For each (a,b,c) of its chunk a thread forms dE/dW and M, and
-// accumulates s_m = sum_a z_m(a,b,c) u_x(a) d for the VOE gradient into
-// vpart[chunk][m][c][b]; adj_voe_sum_kernel adds the chunks in order.
-constexpr int kAChunk = 16;
-__global__ void adj_gw_kernel(int nu, int no, AdjTuple t, const double *__restrict__ Wf,
-                              const double *__restrict__ eh, const double *__restrict__ ep,
-                              const double *__restrict__ t1, const double *__restrict__ Q, double *__restrict__ GW,
-                              double *__restrict__ Mf, double *__restrict__ vpart) {
+// One CTA of 256 threads per tile a in [a0, a0+32), b in [b0, b0+8), c in
+// [c0, c0+8) (grid x: c blocks, y: b blocks, z: a chunks).  The six index
+// permutations of W the tile needs are staged in shared memory by coalesced
+// loads (innermost extent padded by one against bank conflicts), so no W read
+// is strided.  Thread (ag, b, c) forms dE/dW and M for the eight a of its
+// group; then the CTA
+//   - writes dE/dW: for i>j>k tuples straight into the three dE/dX buffers,
+//     G0(a,b,c) = G1(a,c,b) = G2(b,c,a) = dE/dW(a,b,c), each as row segments
+//     (their padding columns stay zero from allocation); for degenerate
+//     tuples into GW, which adj_gx_kernel folds,
+//   - stores s_m(b,c) = sum_a z_m(a,b,c) u_x(a) d over its 32 a into
+//     vpart[chunk][m][c][b] (adj_voe_sum_kernel adds the chunks in order),
+//   - sums M over each pair of tile axes into the eps partials
+//     EA[bblk][cblk][a], EB[chunk][cblk][b], EC[chunk][bblk][c].
+// Every sum runs in a fixed order.
+constexpr int kTA = 32, kTB = 8;
+constexpr int kAChunk = kTA;
+constexpr int kGwThreads = 256;
+constexpr int kTabc = kTA * kTB * (kTB + 1);  // [32][8][8+1] tiles
+constexpr int kTbca = kTB * kTB * (kTA + 1);  // [8][8][32+1] tiles
+constexpr int kGwSmem = (4 * kTabc + 2 * kTbca) * 8;
+
+// Asynchronous 8-byte copies (zero fill outside the nu^3 box): all six tiles'
+// loads are in flight at once.
+template <int D0, int D1, int D2>
+__device__ __forceinline__ void gw_load_tile(double *dst, const double *__restrict__ W, int nu, int o0, int o1,
+                                             int o2) {
+#pragma unroll
+  for (int e = threadIdx.x; e < D0 * D1 * D2; e += kGwThreads) {
+    const int k = e % D2, j = (e / D2) % D1, i = e / (D1 * D2);
+    const int x0 = o0 + i, x1 = o1 + j, x2 = o2 + k;
+    const bool ok = x0 < nu && x1 < nu && x2 < nu;
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + (i * D1 + j) * (D2 + 1) + k);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa),
+                 "l"(W + (ok ? widx(nu, x0, x1, x2) : 0)), "r"(ok ? 8 : 0));
+  }
+}
+
+template <bool SCATTER>
+__global__ void __launch_bounds__(kGwThreads, 2)
+    adj_gw_kernel(int nu, int no, int64_t NP, AdjTuple t, const double *__restrict__ Wf,
+                  const double *__restrict__ eh, const double *__restrict__ ep, const double *__restrict__ t1,
+                  const double *__restrict__ Q, double *__restrict__ GW, double *__restrict__ G0,
+                  double *__restrict__ G1, double *__restrict__ G2, double *__restrict__ vpart,
+                  double *__restrict__ EA, double *__restrict__ EB, double *__restrict__ EC) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *T0 = reinterpret_cast<double *>(smem_raw);  // W(a,b,c) [a][b][c]
+  double *T1 = T0 + kTabc;                             // W(a,c,b) [a][c][b]
+  double *T2 = T1 + kTabc;                             // W(b,a,c) [b][a][c]
+  double *T4 = T2 + kTabc;                             // W(c,a,b) [c][a][b]
+  double *T3 = T4 + kTabc;                             // W(b,c,a) [b][c][a]
+  double *T5 = T3 + kTbca;                             // W(c,b,a) [c][b][a]
   const int64_t nu2 = (int64_t)nu * nu;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y, ach = blockIdx.z;
-  if (c >= nu) return;
+  const int nb = (nu + kTB - 1) / kTB;
+  const int cblk = blockIdx.x, bblk = blockIdx.y, ach = blockIdx.z;
+  const int c0 = cblk * kTB, b0 = bblk * kTB, a0 = ach * kTA;
+  const int tid = threadIdx.x;
+
+  gw_load_tile<kTA, kTB, kTB>(T0, Wf, nu, a0, b0, c0);
+  gw_load_tile<kTA, kTB, kTB>(T1, Wf, nu, a0, c0, b0);
+  gw_load_tile<kTB, kTA, kTB>(T2, Wf, nu, b0, a0, c0);
+  gw_load_tile<kTB, kTA, kTB>(T4, Wf, nu, c0, a0, b0);
+  gw_load_tile<kTB, kTB, kTA>(T3, Wf, nu, b0, c0, a0);
+  gw_load_tile<kTB, kTB, kTA>(T5, Wf, nu, c0, b0, a0);
+  asm volatile("cp.async.commit_group;\n" ::);
+
+  const int ag = tid >> 6, bl = (tid >> 3) & 7, cl = tid & 7;
+  const int b = b0 + bl, c = c0 + cl;
+  const bool bc_ok = b < nu && c < nu;
+  const int bs = bc_ok ? b : 0, cs = bc_ok ? c : 0;  // clamped for the per-thread loads
   const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
   const int xr[3] = {t.i, t.j, t.k};
   double qb0[3], ub[3], uc[3];
 #pragma unroll
   for (int R = 0; R < 3; R++) {
-    qb0[R] = Q[(int64_t)(3 * R) * nu2 + (int64_t)b * nu + c];  // Q_R0(b,c)
-    ub[R] = 2.0 * t1[xr[R] + (int64_t)no * b];
-    uc[R] = 2.0 * t1[xr[R] + (int64_t)no * c];
+    qb0[R] = Q[(int64_t)(3 * R) * nu2 + (int64_t)bs * nu + cs];  // Q_R0(b,c)
+    ub[R] = 2.0 * t1[xr[R] + (int64_t)no * bs];
+    uc[R] = 2.0 * t1[xr[R] + (int64_t)no * cs];
   }
-  const double ebc = ep[b] + ep[c];
+  const double ebc = ep[bs] + ep[cs];
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+
   double s[6] = {0, 0, 0, 0, 0, 0};
-  const int a1 = min(nu, (ach + 1) * kAChunk);
-  for (int a = ach * kAChunk; a < a1; a++) {
-    const int64_t e = widx(nu, a, b, c);
-    const double wabc = Wf[e];
-    const double wacb = Wf[widx(nu, a, c, b)], wbac = Wf[widx(nu, b, a, c)], wbca = Wf[widx(nu, b, c, a)];
-    const double wcab = Wf[widx(nu, c, a, b)], wcba = Wf[widx(nu, c, b, a)];
+  double gv[8], mv[8];
+#pragma unroll
+  for (int ia = 0; ia < 8; ia++) {
+    const int al = ag * 8 + ia, a = a0 + al;
+    gv[ia] = 0.0;
+    mv[ia] = 0.0;
+    if (!bc_ok || a >= nu) continue;
+    const double wabc = T0[(al * kTB + bl) * (kTB + 1) + cl];
+    const double wacb = T1[(al * kTB + cl) * (kTB + 1) + bl];
+    const double wbac = T2[(bl * kTA + al) * (kTB + 1) + cl];
+    const double wcab = T4[(cl * kTA + al) * (kTB + 1) + bl];
+    const double wbca = T3[(bl * kTB + cl) * (kTA + 1) + al];
+    const double wcba = T5[(cl * kTB + bl) * (kTA + 1) + al];
     const double pw = 8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab);
     const double d = 1.0 / (dijk - (ep[a] + ebc));
     double h = 0.0;
@@ -141,8 +254,8 @@ __global__ void adj_gw_kernel(int nu, int no, AdjTuple t, const double *__restri
       h += uc[R] * q[2 * nu2 + (int64_t)a * nu + b];
     }
     const bool diag = (a == b && b == c);
-    GW[e] = diag ? 0.0 : t.weight * d * (2.0 * pw + h);
-    Mf[e] = diag ? 0.0 : t.weight * wabc * (pw + h) * d * d;
+    gv[ia] = diag ? 0.0 : t.weight * d * (2.0 * pw + h);
+    mv[ia] = diag ? 0.0 : t.weight * wabc * (pw + h) * d * d;
     const double z[6] = {(wabc - wbac) * 2.0 - wacb + wbca, (wacb - wbca) * 2.0 - wabc + wbac,
                          (wbac - wabc) * 2.0 - wcab + wcba, (wbca - wacb) * 2.0 - wcba + wcab,
                          (wcab - wcba) * 2.0 - wbac + wabc, (wcba - wcab) * 2.0 - wbca + wacb};
@@ -151,8 +264,79 @@ __global__ void adj_gw_kernel(int nu, int no, AdjTuple t, const double *__restri
 #pragma unroll
     for (int m = 0; m < 6; m++) s[m] = fma(z[m] * d, ua[role[m]], s[m]);
   }
+  __syncthreads();  // the W tiles are dead from here on
+  double *Gs = T0, *Ms = T1, *Sv = T2, *Rab = T3, *Rac = T3 + kTA * kTB;
 #pragma unroll
-  for (int m = 0; m < 6; m++) vpart[((int64_t)ach * 6 + m) * nu2 + (int64_t)c * nu + b] = s[m];
+  for (int ia = 0; ia < 8; ia++) {
+    const int al = ag * 8 + ia;
+    Gs[(al * kTB + bl) * (kTB + 1) + cl] = gv[ia];
+    Ms[(al * kTB + bl) * (kTB + 1) + cl] = mv[ia];
+  }
+#pragma unroll
+  for (int m = 0; m < 6; m++) Sv[(ag * 6 + m) * 64 + bl * 8 + cl] = s[m];
+  __syncthreads();
+
+  // s_m over the chunk: the four a groups in order
+  for (int e = tid; e < 6 * 64; e += kGwThreads) {
+    const int m = e >> 6, r = e & 63, bj = r & 7, cj = r >> 3;
+    const double v = ((Sv[(0 * 6 + m) * 64 + bj * 8 + cj] + Sv[(1 * 6 + m) * 64 + bj * 8 + cj]) +
+                      Sv[(2 * 6 + m) * 64 + bj * 8 + cj]) +
+                     Sv[(3 * 6 + m) * 64 + bj * 8 + cj];
+    if (b0 + bj < nu && c0 + cj < nu) vpart[((int64_t)ach * 6 + m) * nu2 + (int64_t)(c0 + cj) * nu + b0 + bj] = v;
+  }
+  // M over pairs of tile axes
+  {
+    const int al = tid >> 3, x = tid & 7;
+    double rb = 0.0, rc = 0.0;
+#pragma unroll
+    for (int y = 0; y < kTB; y++) {
+      rb += Ms[(al * kTB + x) * (kTB + 1) + y];  // sum over c at b = x
+      rc += Ms[(al * kTB + y) * (kTB + 1) + x];  // sum over b at c = x
+    }
+    Rab[al * kTB + x] = rb;
+    Rac[al * kTB + x] = rc;
+  }
+  // dE/dX (or dE/dW) as row segments
+  for (int e = tid; e < kTA * kTB * kTB; e += kGwThreads) {
+    if (SCATTER) {
+      {  // G0(a,b,c): c fastest
+        const int cj = e & 7, bj = (e >> 3) & 7, aj = e >> 6;
+        const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
+        if (A < nu && B < nu && C < nu) G0[((int64_t)A * nu + B) * NP + C] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+      }
+      {  // G1(a,c,b): b fastest
+        const int bj = e & 7, cj = (e >> 3) & 7, aj = e >> 6;
+        const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
+        if (A < nu && B < nu && C < nu) G1[((int64_t)A * nu + C) * NP + B] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+      }
+      {  // G2(b,c,a): a fastest
+        const int aj = e & 31, cj = (e >> 5) & 7, bj = e >> 8;
+        const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
+        if (A < nu && B < nu && C < nu) G2[((int64_t)B * nu + C) * NP + A] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+      }
+    } else {
+      const int cj = e & 7, bj = (e >> 3) & 7, aj = e >> 6;
+      const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
+      if (A < nu && B < nu && C < nu) GW[widx(nu, A, B, C)] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+    }
+  }
+  __syncthreads();
+  if (tid < kTA) {  // EA: sum over (b, c) per a
+    double v = 0.0;
+#pragma unroll
+    for (int y = 0; y < kTB; y++) v += Rab[tid * kTB + y];
+    if (a0 + tid < nu) EA[((int64_t)bblk * nb + cblk) * nu + a0 + tid] = v;
+  } else if (tid >= 64 && tid < 64 + kTB) {  // EB: sum over (a, c) per b
+    const int x = tid - 64;
+    double v = 0.0;
+    for (int al = 0; al < kTA; al++) v += Rab[al * kTB + x];
+    if (b0 + x < nu) EB[((int64_t)ach * nb + cblk) * nu + b0 + x] = v;
+  } else if (tid >= 128 && tid < 128 + kTB) {  // EC: sum over (a, b) per c
+    const int x = tid - 128;
+    double v = 0.0;
+    for (int al = 0; al < kTA; al++) v += Rac[al * kTB + x];
+    if (c0 + x < nu) EC[((int64_t)ach * nb + bblk) * nu + c0 + x] = v;
+  }
 }
 
 // dVOE(b,c,y_m,z_m) += w sum_chunks vpart[chunk][m][c][b], m = 1..6 in order
@@ -202,66 +386,34 @@ __global__ void adj_gx_kernel(int nu, int64_t NP, const double *__restrict__ GW,
 
 // ---------------------------------------------------------------------------- eps
 // dE/dep_p = sum_bc M(p,b,c) + sum_ac M(a,p,c) + sum_ab M(a,b,p) and
-// dE/deh_x -= (multiplicity of x) sum_abc M, from two coalesced passes over M:
-//   rows:    Rw[a][b]      = sum_c M(a,b,c)                 (warp per row)
-//   columns: Cl[chunk][c]  = sum of M(row, c) over 64 rows   (thread per column)
-// then a warp per p sums Rw[p][:] + Rw[:][p] + Cl[:][p].  Every sum has a
-// fixed order.
-constexpr int kColChunk = 64;
-__global__ void adj_eps_rows_kernel(int nu, const double *__restrict__ Mf, double *__restrict__ Rw) {
-  const int64_t nrow = (int64_t)nu * nu;
-  const int lane = threadIdx.x & 31;
-  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrow; r += wstride) {
-    double v = 0.0;
-    for (int c = lane; c < nu; c += 32) v += Mf[r * nu + c];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0) Rw[r] = v;
-  }
-}
-
-__global__ void adj_eps_cols_kernel(int nu, const double *__restrict__ Mf, double *__restrict__ Cl) {
-  const int64_t nrow = (int64_t)nu * nu;
-  const int64_t nchunk = (nrow + kColChunk - 1) / kColChunk;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nchunk * nu;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t ch = e / nu;
-    const int c = (int)(e - ch * nu);
-    const int64_t r1 = min((ch + 1) * kColChunk, nrow);
-    double v = 0.0;
-    for (int64_t r = ch * kColChunk; r < r1; r++) v += Mf[r * nu + c];
-    Cl[e] = v;
-  }
-}
-
-__global__ void adj_eps_final_kernel(int nu, const double *__restrict__ Rw, const double *__restrict__ Cl,
-                                     double *__restrict__ gep) {
-  const int64_t nchunk = ((int64_t)nu * nu + kColChunk - 1) / kColChunk;
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
-  const int p = blockIdx.x * wpb + (threadIdx.x >> 5);
-  if (p < nu) {
-    double v = 0.0;
-    for (int q = lane; q < nu; q += 32) v += Rw[(int64_t)p * nu + q] + Rw[(int64_t)q * nu + p];
-    for (int64_t ch = lane; ch < nchunk; ch += 32) v += Cl[ch * nu + p];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0) gep[p] += v;
-  }
-}
-
-// R1[p] = sum_q Rw[p][q] (warp per p); then one warp: sum_abc M = sum_p R1[p].
-__global__ void adj_eps_planes_kernel(int nu, const double *__restrict__ Rw, double *__restrict__ R1) {
+// dE/deh_x -= (multiplicity of x) sum_abc M, from the per-tile partials of
+// adj_gw_kernel: a warp per p adds EA[.][.][p], EB[.][.][p], EC[.][.][p] (lanes
+// stride the partials, then a fixed shuffle tree), and Rp[p] = the EA part.
+__global__ void adj_eps_sum_kernel(int nu, int nb, int nch, const double *__restrict__ EA,
+                                   const double *__restrict__ EB, const double *__restrict__ EC,
+                                   double *__restrict__ gep, double *__restrict__ Rp) {
   const int lane = threadIdx.x & 31;
   const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (p >= nu) return;
-  double v = 0.0;
-  for (int q = lane; q < nu; q += 32) v += Rw[(int64_t)p * nu + q];
+  double va = 0.0, vb = 0.0, vc = 0.0;
+  for (int q = lane; q < nb * nb; q += 32) va += EA[(int64_t)q * nu + p];
+  for (int q = lane; q < nch * nb; q += 32) {
+    vb += EB[(int64_t)q * nu + p];
+    vc += EC[(int64_t)q * nu + p];
+  }
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  if (lane == 0) R1[p] = v;
+  for (int off = 16; off > 0; off >>= 1) {
+    va += __shfl_xor_sync(0xffffffffu, va, off);
+    vb += __shfl_xor_sync(0xffffffffu, vb, off);
+    vc += __shfl_xor_sync(0xffffffffu, vc, off);
+  }
+  if (lane == 0) {
+    gep[p] += (va + vb) + vc;
+    Rp[p] = va;
+  }
 }
+
+// One warp: sum_abc M = sum_p R1[p], subtracted from eh_i, eh_j, eh_k.
 __global__ void adj_eps_total_kernel(int nu, AdjTuple t, const double *__restrict__ R1, double *__restrict__ geh) {
   const int lane = threadIdx.x & 31;
   double tot = 0.0;
@@ -280,12 +432,15 @@ constexpr int BBM = 128, BBK = 16;  // N tile BN in {64, 48, 32}, chosen to fit 
 constexpr int BWM = 32;                 // rows per warp
 constexpr int BNT = (BBM / BWM) * 32;   // 128 threads
 constexpr int BST = 3;                  // cp.async stages
-constexpr int LDA_MK = BBK + 4;         // A tile [m][k]
-// Fragment loads are 64-bit, served per half-warp (lanes g = 0..3, t = 0..3):
-// a [k][.] tile is conflict-free when its row stride is 4 (mod 16) doubles.
-constexpr int LDA_KM = BBM + 4;         // A tile [k][m]
+// Fragment loads are 64-bit, served per half-warp (lanes g = 0..3, t = 0..3).
+// The dE A tile [m][k] is unpadded (16 doubles a row) with column c of row r
+// stored at c ^ 4 (r & 3): the four rows g of a half-warp then hit four
+// disjoint 32-byte bank groups.  [k][.] tiles are padded to a row stride of
+// 4 (mod 16) doubles instead.
+constexpr int LDA_KM = BBM + 4;         // dF A tile [k][m]
 template <int BN>
 constexpr int ldb_kn() { return BN + 4; }  // B tile [k][n]
+__device__ __forceinline__ int aswz(int r, int c) { return r * BBK + (c ^ ((r & 3) << 2)); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -302,9 +457,19 @@ __device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, dou
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
       : "d"(a0), "d"(a1), "d"(b0));
 }
-// (p,q) <-> (q,p) row permutation through a table (no integer division per row)
-__device__ __forceinline__ int64_t tperm(int64_t m, const int *__restrict__ ptab, int perm) {
-  return perm ? (int64_t)ptab[m] : m;
+// Row m = p*nu + q of a nu^2 x . operand and its (p,q) <-> (q,p) partner, for
+// m < 2^24 (nu <= 4096): the float quotient is within one of p, then corrected.
+__device__ __forceinline__ int swap_row(int m, int nu, float inv_nu) {
+  int p = __float2int_rz(__int2float_rn(m) * inv_nu);
+  int q = m - p * nu;
+  if (q < 0) {
+    p--;
+    q += nu;
+  } else if (q >= nu) {
+    p++;
+    q -= nu;
+  }
+  return q * nu + p;
 }
 
 constexpr int kMaxPairs = 6;  // (slot, half) pairs of one tuple: at most 3 x 2
@@ -318,7 +483,6 @@ struct BwdEArgs {
   BwdPair pair[kMaxPairs];
   double *out[3];
   int first[4], npairs;  // pairs of output o are first[o] .. first[o+1]-1
-  const int *ptab;       // ptab[p*nu+q] = q*nu+p
   int nu;
   int64_t NP, KP;
   int tiles_n;
@@ -326,11 +490,12 @@ struct BwdEArgs {
 
 // dE[x](r, n) += sum_pairs sum_s A[perm(r)][s] B[s][n]; M = nu^2, N = KP, K = NP per pair.
 template <int BN>
-__global__ void __launch_bounds__(BNT, 2) bwd_e_kernel(const BwdEArgs args) {
+__global__ void __launch_bounds__(BNT, 3) bwd_e_kernel(const BwdEArgs args) {
   constexpr int BBN = BN, LDB_KN = ldb_kn<BN>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBM][LDA_MK]
-  double *Bs = As + BST * BBM * LDA_MK;                 // [BST][BBK][LDB_KN]
+  double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBM][BBK], swizzled
+  double *Bs = As + BST * BBM * BBK;                    // [BST][BBK][LDB_KN]
+  int *rows = reinterpret_cast<int *>(Bs + BST * BBK * LDB_KN);  // [2][BBM]: row of A (or -1)
   const int o = blockIdx.y;
   const int tile_m = blockIdx.x / args.tiles_n, tile_n = blockIdx.x - tile_m * args.tiles_n;
   const int nu = args.nu;
@@ -342,20 +507,32 @@ __global__ void __launch_bounds__(BNT, 2) bwd_e_kernel(const BwdEArgs args) {
   const int kt_per = (int)((NP + BBK - 1) / BBK);  // NP is a multiple of 8, not always of 16
   const int ktiles = kt_per * (p_end - p_begin);
 
+  {
+    const float inv_nu = 1.0f / (float)nu;
+    for (int r = tid; r < BBM; r += BNT) {
+      const int64_t m = m0 + r;
+      rows[r] = m < M ? (int)m : -1;
+      rows[BBM + r] = m < M ? swap_row((int)m, nu, inv_nu) : -1;
+    }
+  }
+  __syncthreads();
+
   auto load_stage = [&](int stage, int kt) {
     const int pi = p_begin + kt / kt_per;
     const int64_t k0 = (int64_t)(kt % kt_per) * BBK;
     const BwdPair &pr = args.pair[pi];
-    double *as = As + stage * BBM * LDA_MK;
+    double *as = As + stage * BBM * BBK;
     double *bs = Bs + stage * BBK * LDB_KN;
+    const int *rw = rows + pr.perm * BBM;
     const int chunk = tid & 7;  // 8 x 16 B per 16-double row
+    const bool kok = k0 + chunk * 2 < NP;
     for (int rr = tid >> 3; rr < BBM; rr += BNT / 8) {
-      const int64_t m = m0 + rr;
-      const bool ok = m < M && k0 + chunk * 2 < NP;
-      const double *src = pr.A + (ok ? tperm(m, args.ptab, pr.perm) * NP + k0 + chunk * 2 : 0);
-      cp_async16(as + rr * LDA_MK + chunk * 2, src, ok ? 16 : 0);
+      const int row = rw[rr];
+      const bool ok = row >= 0 && kok;
+      const double *src = pr.A + (ok ? (int64_t)row * NP + k0 + chunk * 2 : 0);
+      cp_async16(as + aswz(rr, chunk * 2), src, ok ? 16 : 0);
     }
-    // B tile: 16 rows (s) x 64 columns (n): 32 chunks of 16 B per row
+    // B tile: 16 rows (s) x BN columns (n)
     for (int c = tid; c < BBK * (BBN / 2); c += BNT) {
       const int rr = c / (BBN / 2), cc = c - rr * (BBN / 2);
       const int n = n0 + cc * 2;
@@ -389,15 +566,19 @@ __global__ void __launch_bounds__(BNT, 2) bwd_e_kernel(const BwdEArgs args) {
       if (nk < ktiles) load_stage(nk % BST, nk);
       cp_async_commit();
     }
-    const double *as = As + (kt % BST) * BBM * LDA_MK + (warp * BWM) * LDA_MK;
+    const double *as = As + (kt % BST) * BBM * BBK;
     const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
+    // NP is a multiple of 8: the last k-tile of a pair may hold only 8 columns
+    const bool half_tile = NP - (int64_t)(kt % kt_per) * BBK <= BBK / 2;
 #pragma unroll
     for (int kk = 0; kk < BBK; kk += 4) {
+      if (kk >= BBK / 2 && half_tile) break;
       double af[MF][2], bf[NF];
 #pragma unroll
       for (int i = 0; i < MF; i++) {
-        af[i][0] = as[(i * 16 + g) * LDA_MK + kk + t];
-        af[i][1] = as[(i * 16 + g + 8) * LDA_MK + kk + t];
+        const int r = warp * BWM + i * 16 + g;
+        af[i][0] = as[aswz(r, kk + t)];
+        af[i][1] = as[aswz(r + 8, kk + t)];
       }
 #pragma unroll
       for (int j = 0; j < NF; j++) bf[j] = bs[(kk + t) * LDB_KN + j * 8 + g];
@@ -436,7 +617,6 @@ struct BwdFArgs {
   double *part;     // [pair][split][NP][KP]
   int npairs, nsplit;
   int64_t kchunk;   // rows of nu^2 per split (multiple of BBK)
-  const int *ptab;
   int nu;
   int64_t NP, KP;
   int tiles_n;
@@ -444,7 +624,7 @@ struct BwdFArgs {
 
 // part[pair][split](s, n) = sum_{m in split} A[m][s] B[perm(m)][n]; M = NP, N = KP.
 template <int BN>
-__global__ void __launch_bounds__(BNT, 2) bwd_f_kernel(const BwdFArgs args) {
+__global__ void __launch_bounds__(BNT, 3) bwd_f_kernel(const BwdFArgs args) {
   constexpr int BBN = BN, LDB_KN = ldb_kn<BN>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBK][LDA_KM]
@@ -453,6 +633,7 @@ __global__ void __launch_bounds__(BNT, 2) bwd_f_kernel(const BwdFArgs args) {
   const BwdPair &pr = args.pair[pi];
   const int tile_m = blockIdx.x / args.tiles_n, tile_n = blockIdx.x - tile_m * args.tiles_n;
   const int nu = args.nu;
+  const float inv_nu = 1.0f / (float)nu;
   const int64_t Mtot = (int64_t)nu * nu, NP = args.NP, KP = args.KP;
   const int64_t s0 = (int64_t)tile_m * BBM;
   const int n0 = tile_n * BBN;
@@ -478,7 +659,8 @@ __global__ void __launch_bounds__(BNT, 2) bwd_f_kernel(const BwdFArgs args) {
       const int64_t m = k0 + rr;
       const int n = n0 + cc * 2;
       const bool ok = m < kend && n < KP;
-      const double *src = pr.B + (ok ? tperm(m, args.ptab, pr.perm) * KP + n : 0);
+      const int64_t row = ok && pr.perm ? (int64_t)swap_row((int)m, nu, inv_nu) : m;
+      const double *src = pr.B + (ok ? row * KP + n : 0);
       cp_async16(bs + rr * LDB_KN + cc * 2, src, ok ? 16 : 0);
     }
   };
@@ -555,8 +737,18 @@ __global__ void bwd_f_reduce_kernel(const BwdFReduceArgs a, const double *__rest
   const int o = blockIdx.y;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < a.n; e += (int64_t)gridDim.x * blockDim.x) {
     double s = a.dst[o][e];
-    for (int pi = a.first[o]; pi < a.first[o + 1]; pi++)
-      for (int sp = 0; sp < a.nsplit; sp++) s += part[((int64_t)pi * a.nsplit + sp) * a.n + e];
+    for (int pi = a.first[o]; pi < a.first[o + 1]; pi++) {
+      const double *src = part + (int64_t)pi * a.nsplit * a.n + e;
+      int sp = 0;
+      for (; sp + 8 <= a.nsplit; sp += 8) {  // eight loads in flight, added in split order
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = src[(int64_t)(sp + u) * a.n];
+#pragma unroll
+        for (int u = 0; u < 8; u++) s += v[u];
+      }
+      for (; sp < a.nsplit; sp++) s += src[(int64_t)sp * a.n];
+    }
     a.dst[o][e] = s;
   }
 }
@@ -636,7 +828,7 @@ int grid_for(int64_t n, int threads = 256) {
 }
 
 template <int BN>
-constexpr int smem_e() { return BST * (BBM * LDA_MK + BBK * ldb_kn<BN>()) * 8; }
+constexpr int smem_e() { return BST * (BBM * BBK + BBK * ldb_kn<BN>()) * 8 + 2 * BBM * 4; }
 template <int BN>
 constexpr int smem_f() { return BST * (BBK * LDA_KM + BBK * ldb_kn<BN>()) * 8; }
 // N tile for an N extent of KP: least padding, ties to the wider tile
@@ -658,7 +850,6 @@ int launch_bwd_f(const BwdFArgs &a, int tiles_m, cudaStream_t s) {
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
-constexpr int64_t kFChunk = 1024;  // nu^2 rows per split of the dF GEMM
 
 }  // namespace
 
@@ -669,25 +860,35 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
     CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(p), (size_t)(n < 1 ? 1 : n) * 8));
     return CCT_OK;
   };
-  b->nsplit = (nu2 + kFChunk - 1) / kFChunk;
+  {
+    // dF GEMM split-K: about one wave of 3 CTAs per SM for the 6 pairs of an
+    // i>j>k tuple, rounded to whole k-tiles
+    int sms = 148, dev = 0;
+    CCT_CUDA(cudaGetDevice(&dev));
+    CCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int bn = bwd_bn(d.KP);
+    const int64_t tiles = ((d.NP + BBM - 1) / BBM) * ((d.KP + bn - 1) / bn) * 6;
+    int64_t ns = (3 * (int64_t)sms) / tiles;
+    ns = ns < 1 ? 1 : (ns > (nu2 + BBK - 1) / BBK ? (nu2 + BBK - 1) / BBK : ns);
+    b->kchunk = round_up((nu2 + ns - 1) / ns, BBK);
+    b->nsplit = (nu2 + b->kchunk - 1) / b->kchunk;
+  }
   CCT_TRY(al(&b->dE, no * nu2 * d.KP));
   CCT_TRY(al(&b->dF, no * no * d.NP * d.KP));
   CCT_TRY(al(&b->Wf, nu3));
   CCT_TRY(al(&b->GW, nu3));
-  CCT_TRY(al(&b->Mf, nu3));
   for (int set = 0; set < 2; set++)
-    for (int g = 0; g < 3; g++) CCT_TRY(al(&b->GX[set][g], nu2 * d.NP));
+    for (int g = 0; g < 3; g++) {
+      CCT_TRY(al(&b->GX[set][g], nu2 * d.NP));
+      CCT_CUDA(cudaMemset(b->GX[set][g], 0, (size_t)nu2 * d.NP * 8));  // padding columns stay zero
+    }
   CCT_TRY(al(&b->part, 6 * b->nsplit * d.NP * d.KP));
   CCT_TRY(al(&b->Q, 9 * nu2));
   CCT_TRY(al(&b->vpart, ((nu + kAChunk - 1) / kAChunk) * 6 * nu2));
-  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&b->ptab), (size_t)nu2 * sizeof(int)));
   {
-    std::vector<int> h(nu2);
-    for (int64_t p = 0; p < nu; p++)
-      for (int64_t q = 0; q < nu; q++) h[p * nu + q] = (int)(q * nu + p);
-    CCT_CUDA(cudaMemcpy(b->ptab, h.data(), (size_t)nu2 * sizeof(int), cudaMemcpyHostToDevice));
+    const int64_t nb = (nu + kTB - 1) / kTB, nch = (nu + kTA - 1) / kTA;
+    CCT_TRY(al(&b->eps, (nb * nb + 2 * nch * nb + 1) * nu));  // EA, EB, EC, Rp
   }
-  CCT_TRY(al(&b->eps, nu2 + ((nu2 + kColChunk - 1) / kColChunk) * nu + nu));
   CCT_TRY(al(&b->v1, 5 + nu * no));
   CCT_TRY(al(&b->g_eh, no));
   CCT_TRY(al(&b->g_ep, nu));
@@ -701,8 +902,7 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
 }
 
 void adj_free(AdjBuffers *b) {
-  if (b->ptab) cudaFree(b->ptab);
-  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->Mf, b->GX[0][0], b->GX[0][1], b->GX[0][2], b->GX[1][0],
+  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->GX[0][0], b->GX[0][1], b->GX[0][2], b->GX[1][0],
                     b->GX[1][1], b->GX[1][2], b->part, b->Q, b->vpart, b->eps, b->v1, b->g_eh,
                     b->g_ep, b->g_t1, b->g_t2, b->g_vm, b->g_voe, b->g_vvvo})
     if (q) cudaFree(q);
@@ -744,7 +944,7 @@ int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const
                         const double *t1, const double *voe, AdjBuffers *b, int set, cudaStream_t s) {
   double *const *GX = b->GX[set];
   const int no = d.no, nu = d.nu;
-  const int64_t nu2 = (int64_t)nu * nu, nu3 = nu2 * nu;
+  const int64_t nu2 = (int64_t)nu * nu;
   AdjTuple at;
   at.x[0] = X[0];
   at.x[1] = X[1];
@@ -758,11 +958,11 @@ int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const
                          {t.k, t.i, t.j}, {t.j, t.k, t.i}, {t.k, t.j, t.i}};
   for (int m = 0; m < 6; m++) sm.x[m] = smx[m][0], sm.y[m] = smx[m][1], sm.z[m] = smx[m][2];
 
-  const dim3 g3((nu + 127) / 128, nu, nu);  // x: c blocks, y: b, z: a
+  const dim3 g3((nu + kWC - 1) / kWC, (nu + kWB - 1) / kWB, (nu + kWA - 1) / kWA);
   switch (t.kind) {
-    case kIJK: adj_wfull_kernel<kIJK><<<g3, 128, 0, s>>>(nu, d.NP, at, b->Wf); break;
-    case kIJJ: adj_wfull_kernel<kIJJ><<<g3, 128, 0, s>>>(nu, d.NP, at, b->Wf); break;
-    default: adj_wfull_kernel<kIIJ><<<g3, 128, 0, s>>>(nu, d.NP, at, b->Wf); break;
+    case kIJK: adj_wfull_kernel<kIJK><<<g3, kWThreads, 3 * kWSlot * 8, s>>>(nu, d.NP, at, b->Wf); break;
+    case kIJJ: adj_wfull_kernel<kIJJ><<<g3, kWThreads, 4 * kWSlot * 8, s>>>(nu, d.NP, at, b->Wf); break;
+    default: adj_wfull_kernel<kIIJ><<<g3, kWThreads, 4 * kWSlot * 8, s>>>(nu, d.NP, at, b->Wf); break;
   }
   CCT_CUDA(cudaGetLastError());
   {
@@ -791,35 +991,32 @@ int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const
     CCT_CUDA(cudaGetLastError());
   }
   {
-    const int nch = (nu + kAChunk - 1) / kAChunk;
-    adj_gw_kernel<<<dim3((nu + 127) / 128, nu, nch), 128, 0, s>>>(nu, no, at, b->Wf, eh, ep, t1, b->Q, b->GW, b->Mf,
-                                                                   b->vpart);
+    const int nb = (nu + kTB - 1) / kTB, nch = (nu + kTA - 1) / kTA;
+    double *EA = b->eps, *EB = EA + (int64_t)nb * nb * nu, *EC = EB + (int64_t)nch * nb * nu,
+           *Rp = EC + (int64_t)nch * nb * nu;
+    const dim3 ggrid(nb, nb, nch);
+    if (t.kind == kIJK)
+      adj_gw_kernel<true><<<ggrid, kGwThreads, kGwSmem, s>>>(nu, no, d.NP, at, b->Wf, eh, ep, t1, b->Q, b->GW, GX[0],
+                                                              GX[1], GX[2], b->vpart, EA, EB, EC);
+    else
+      adj_gw_kernel<false><<<ggrid, kGwThreads, kGwSmem, s>>>(nu, no, d.NP, at, b->Wf, eh, ep, t1, b->Q, b->GW,
+                                                               GX[0], GX[1], GX[2], b->vpart, EA, EB, EC);
     CCT_CUDA(cudaGetLastError());
     adj_voe_sum_kernel<<<grid_for(nu2), 256, 0, s>>>(nu, no, nch, at, sm, b->vpart, b->g_voe);
     CCT_CUDA(cudaGetLastError());
-  }
-  {
-    const int64_t nchunk = (nu2 + kColChunk - 1) / kColChunk;
-    double *Rw = b->eps, *Cl = b->eps + nu2;
-    adj_eps_rows_kernel<<<grid_for(nu2 * 32), 256, 0, s>>>(nu, b->Mf, Rw);
+    adj_eps_sum_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, nb, nch, EA, EB, EC, b->g_ep, Rp);
     CCT_CUDA(cudaGetLastError());
-    adj_eps_cols_kernel<<<grid_for(nchunk * nu), 256, 0, s>>>(nu, b->Mf, Cl);
-    CCT_CUDA(cudaGetLastError());
-    adj_eps_final_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, Rw, Cl, b->g_ep);
-    CCT_CUDA(cudaGetLastError());
-    double *R1 = Cl + nchunk * nu;
-    adj_eps_planes_kernel<<<(nu + 7) / 8, 256, 0, s>>>(nu, Rw, R1);
-    CCT_CUDA(cudaGetLastError());
-    adj_eps_total_kernel<<<1, 32, 0, s>>>(nu, at, R1, b->g_eh);
+    adj_eps_total_kernel<<<1, 32, 0, s>>>(nu, at, Rp, b->g_eh);
   }
   CCT_CUDA(cudaGetLastError());
-  const dim3 gx((unsigned)((d.NP + 127) / 128), nu, nu);
-  switch (t.kind) {
-    case kIJK: adj_gx_kernel<kIJK><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]); break;
-    case kIJJ: adj_gx_kernel<kIJJ><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]); break;
-    default: adj_gx_kernel<kIIJ><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]); break;
+  if (t.kind != kIJK) {  // degenerate tuples: two dE/dW permutations feed each dE/dX element
+    const dim3 gx((unsigned)((d.NP + 127) / 128), nu, nu);
+    if (t.kind == kIJJ)
+      adj_gx_kernel<kIJJ><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]);
+    else
+      adj_gx_kernel<kIIJ><<<gx, 128, 0, s>>>(nu, d.NP, b->GW, GX[0], GX[1], GX[2]);
+    CCT_CUDA(cudaGetLastError());
   }
-  CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
 
@@ -869,7 +1066,6 @@ int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double
     }
     a.first[nx] = np_;
     a.npairs = np_;
-    a.ptab = b->ptab;
     a.nu = nu;
     a.NP = d.NP;
     a.KP = d.KP;
@@ -901,8 +1097,7 @@ int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double
     a.part = b->part;
     a.npairs = (int)sorted.size();
     a.nsplit = (int)b->nsplit;
-    a.kchunk = kFChunk;
-    a.ptab = b->ptab;
+    a.kchunk = b->kchunk;
     a.nu = nu;
     a.NP = d.NP;
     a.KP = d.KP;
@@ -920,6 +1115,11 @@ int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double
 int adj_configure(int device) {
   static int configured = -1;
   if (configured == device) return CCT_OK;
+  CCT_CUDA(cudaFuncSetAttribute(adj_wfull_kernel<kIJK>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * kWSlot * 8));
+  CCT_CUDA(cudaFuncSetAttribute(adj_wfull_kernel<kIJJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * kWSlot * 8));
+  CCT_CUDA(cudaFuncSetAttribute(adj_wfull_kernel<kIIJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * kWSlot * 8));
+  CCT_CUDA(cudaFuncSetAttribute(adj_gw_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGwSmem));
+  CCT_CUDA(cudaFuncSetAttribute(adj_gw_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGwSmem));
   CCT_CUDA(cudaFuncSetAttribute(bwd_e_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_e<64>()));
   CCT_CUDA(cudaFuncSetAttribute(bwd_e_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_e<48>()));
   CCT_CUDA(cudaFuncSetAttribute(bwd_e_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_e<32>()));

@@ -179,14 +179,13 @@ int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const doub
 struct AdjBuffers {
   bool ready = false;
   double *dE = nullptr, *dF = nullptr;                 // gradients of the GEMM operands E, F
-  double *Wf = nullptr, *GW = nullptr, *Mf = nullptr;  // dense nu^3: W, dE/dW, denominator terms
+  double *Wf = nullptr, *GW = nullptr;                 // dense nu^3: W, dE/dW (degenerate tuples)
   double *GX[2][3] = {};                               // dE/dX_g, nu^2 x NP each, two tuples in flight
   double *part = nullptr;                              // split-K partials of the dF GEMMs
-  int64_t nsplit = 0;
+  int64_t nsplit = 0, kchunk = 0;                      // splits of nu^2, rows per split
   double *Q = nullptr;                                 // 9 nu^2 VOE combinations of dE/dW
   double *vpart = nullptr;                             // per-a-chunk partial VOE gradients
-  int *ptab = nullptr;                                 // ptab[p*nu+q] = q*nu+p
-  double *eps = nullptr;                               // row sums and 64-row column sums of M
+  double *eps = nullptr;                               // per-tile sums of M over pairs of axes
   double *v1 = nullptr;                                // FP64 v1 of an emulated plan: 5 + nu*no
   double *g_eh = nullptr, *g_ep = nullptr, *g_t1 = nullptr, *g_t2 = nullptr, *g_vm = nullptr, *g_voe = nullptr,
          *g_vvvo = nullptr;                            // gradients in the input layouts
