@@ -144,30 +144,48 @@ __global__ void adj_q_kernel(int nu, QTable q, const double *__restrict__ voe, d
   }
 }
 
-// One CTA of 256 threads per tile a in [a0, a0+32), b in [b0, b0+8), c in
+// One CTA of 256 threads per tile a in [a0, a0+16), b in [b0, b0+8), c in
 // [c0, c0+8) (grid x: c blocks, y: b blocks, z: a chunks).  The six index
-// permutations of W the tile needs are staged in shared memory by coalesced
-// loads (innermost extent padded by one against bank conflicts), so no W read
-// is strided.  Thread (ag, b, c) forms dE/dW and M for the eight a of its
-// group; then the CTA
+// permutations of W the tile needs, u_R(a), ep(a) and the Q_R1(a,c), Q_R2(a,b)
+// blocks are staged in shared memory by coalesced asynchronous copies, so no
+// W read is strided and the inner loop reads no global memory.  A tile of
+// extents (D0, D1, D2) keeps element (i,j,k) at i*(D1*(D2+1)+1) + j*(D2+1) + k:
+// both pads are odd, so the strided tile reads of a half-warp spread over the
+// banks.  61 KB of shared memory: three CTAs per SM.  Thread (ag, b, c) forms
+// dE/dW and M for the four a of its group; then the CTA
 //   - writes dE/dW: for i>j>k tuples straight into the three dE/dX buffers,
 //     G0(a,b,c) = G1(a,c,b) = G2(b,c,a) = dE/dW(a,b,c), each as row segments
 //     (their padding columns stay zero from allocation); for degenerate
 //     tuples into GW, which adj_gx_kernel folds,
-//   - stores s_m(b,c) = sum_a z_m(a,b,c) u_x(a) d over its 32 a into
+//   - stores s_m(b,c) = sum_a z_m(a,b,c) u_x(a) d over its 16 a into
 //     vpart[chunk][m][c][b] (adj_voe_sum_kernel adds the chunks in order),
 //   - sums M over each pair of tile axes into the eps partials
 //     EA[bblk][cblk][a], EB[chunk][cblk][b], EC[chunk][bblk][c].
 // Every sum runs in a fixed order.
-constexpr int kTA = 32, kTB = 8;
+constexpr int kTA = 16, kTB = 8;
 constexpr int kAChunk = kTA;
 constexpr int kGwThreads = 256;
-constexpr int kTabc = kTA * kTB * (kTB + 1);  // [32][8][8+1] tiles
-constexpr int kTbca = kTB * kTB * (kTA + 1);  // [8][8][32+1] tiles
-constexpr int kGwSmem = (4 * kTabc + 2 * kTbca) * 8;
+constexpr int kGwPer = kTA * kTB * kTB / kGwThreads;  // a per thread
+template <int D1, int D2>
+__device__ __forceinline__ int tix(int i, int j, int k) {
+  return i * (D1 * (D2 + 1) + 1) + j * (D2 + 1) + k;
+}
+template <int D0, int D1, int D2>
+constexpr int tsize() { return D0 * (D1 * (D2 + 1) + 1); }
+constexpr int kTabc = tsize<kTA, kTB, kTB>();  // W(a,b,c), W(a,c,b)
+constexpr int kTbac = tsize<kTB, kTA, kTB>();  // W(b,a,c), W(c,a,b)
+constexpr int kTbca = tsize<kTB, kTB, kTA>();  // W(b,c,a), W(c,b,a)
+constexpr int kGwSmem = (2 * (kTabc + kTbac + kTbca) + 4 * kTA + 6 * kTA * kTB) * 8;
+static_assert(2 * kTbac >= 4 * 6 * 64, "s_m staging fits the W(b,a,c), W(c,a,b) tiles");
+static_assert(kTbca >= 2 * kTA * kTB, "M pair sums fit the W(b,c,a) tile");
 
-// Asynchronous 8-byte copies (zero fill outside the nu^3 box): all six tiles'
-// loads are in flight at once.
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool ok) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(ok ? 8 : 0));
+}
+
+// Asynchronous 8-byte copies (zero fill outside the nu^3 box): all tiles' loads
+// are in flight at once.
 template <int D0, int D1, int D2>
 __device__ __forceinline__ void gw_load_tile(double *dst, const double *__restrict__ W, int nu, int o0, int o1,
                                              int o2) {
@@ -176,14 +194,12 @@ __device__ __forceinline__ void gw_load_tile(double *dst, const double *__restri
     const int k = e % D2, j = (e / D2) % D1, i = e / (D1 * D2);
     const int x0 = o0 + i, x1 = o1 + j, x2 = o2 + k;
     const bool ok = x0 < nu && x1 < nu && x2 < nu;
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + (i * D1 + j) * (D2 + 1) + k);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa),
-                 "l"(W + (ok ? widx(nu, x0, x1, x2) : 0)), "r"(ok ? 8 : 0));
+    cp_async8(dst + tix<D1, D2>(i, j, k), W + (ok ? widx(nu, x0, x1, x2) : 0), ok);
   }
 }
 
 template <bool SCATTER>
-__global__ void __launch_bounds__(kGwThreads, 2)
+__global__ void __launch_bounds__(kGwThreads, 3)
     adj_gw_kernel(int nu, int no, int64_t NP, AdjTuple t, const double *__restrict__ Wf,
                   const double *__restrict__ eh, const double *__restrict__ ep, const double *__restrict__ t1,
                   const double *__restrict__ Q, double *__restrict__ GW, double *__restrict__ G0,
@@ -193,14 +209,18 @@ __global__ void __launch_bounds__(kGwThreads, 2)
   double *T0 = reinterpret_cast<double *>(smem_raw);  // W(a,b,c) [a][b][c]
   double *T1 = T0 + kTabc;                             // W(a,c,b) [a][c][b]
   double *T2 = T1 + kTabc;                             // W(b,a,c) [b][a][c]
-  double *T4 = T2 + kTabc;                             // W(c,a,b) [c][a][b]
-  double *T3 = T4 + kTabc;                             // W(b,c,a) [b][c][a]
+  double *T4 = T2 + kTbac;                             // W(c,a,b) [c][a][b]
+  double *T3 = T4 + kTbac;                             // W(b,c,a) [b][c][a]
   double *T5 = T3 + kTbca;                             // W(c,b,a) [c][b][a]
+  double *Ua = T5 + kTbca;                             // [3][kTA] u_R(a), then [kTA] ep(a)
+  double *Q1s = Ua + 4 * kTA;                          // [3][kTA][8] Q_R1(a, c)
+  double *Q2s = Q1s + 3 * kTA * kTB;                   // [3][kTA][8] Q_R2(a, b)
   const int64_t nu2 = (int64_t)nu * nu;
   const int nb = (nu + kTB - 1) / kTB;
   const int cblk = blockIdx.x, bblk = blockIdx.y, ach = blockIdx.z;
   const int c0 = cblk * kTB, b0 = bblk * kTB, a0 = ach * kTA;
   const int tid = threadIdx.x;
+  const int xr[3] = {t.i, t.j, t.k};
 
   gw_load_tile<kTA, kTB, kTB>(T0, Wf, nu, a0, b0, c0);
   gw_load_tile<kTA, kTB, kTB>(T1, Wf, nu, a0, c0, b0);
@@ -208,14 +228,26 @@ __global__ void __launch_bounds__(kGwThreads, 2)
   gw_load_tile<kTB, kTA, kTB>(T4, Wf, nu, c0, a0, b0);
   gw_load_tile<kTB, kTB, kTA>(T3, Wf, nu, b0, c0, a0);
   gw_load_tile<kTB, kTB, kTA>(T5, Wf, nu, c0, b0, a0);
+  for (int e = tid; e < 6 * kTA * kTB; e += kGwThreads) {  // Q_R1(a, c0+x), Q_R2(a, b0+x)
+    const int x = e % kTB, al = (e / kTB) % kTA, RR = e / (kTA * kTB);  // RR = 0..5
+    const int R = RR % 3, which = RR / 3;
+    const int a = a0 + al, y = (which ? b0 : c0) + x;
+    const bool ok = a < nu && y < nu;
+    cp_async8(Q1s + e, Q + (ok ? (int64_t)(3 * R + 1 + which) * nu2 + (int64_t)a * nu + y : 0), ok);
+  }
   asm volatile("cp.async.commit_group;\n" ::);
+  if (tid < kTA) {
+    const int a = a0 + tid < nu ? a0 + tid : 0;
+#pragma unroll
+    for (int R = 0; R < 3; R++) Ua[R * kTA + tid] = 2.0 * t1[xr[R] + (int64_t)no * a];
+    Ua[3 * kTA + tid] = ep[a];
+  }
 
   const int ag = tid >> 6, bl = (tid >> 3) & 7, cl = tid & 7;
   const int b = b0 + bl, c = c0 + cl;
   const bool bc_ok = b < nu && c < nu;
   const int bs = bc_ok ? b : 0, cs = bc_ok ? c : 0;  // clamped for the per-thread loads
   const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
-  const int xr[3] = {t.i, t.j, t.k};
   double qb0[3], ub[3], uc[3];
 #pragma unroll
   for (int R = 0; R < 3; R++) {
@@ -228,30 +260,29 @@ __global__ void __launch_bounds__(kGwThreads, 2)
   __syncthreads();
 
   double s[6] = {0, 0, 0, 0, 0, 0};
-  double gv[8], mv[8];
+  double gv[kGwPer], mv[kGwPer];
 #pragma unroll
-  for (int ia = 0; ia < 8; ia++) {
-    const int al = ag * 8 + ia, a = a0 + al;
+  for (int ia = 0; ia < kGwPer; ia++) {
+    const int al = ag * kGwPer + ia, a = a0 + al;
     gv[ia] = 0.0;
     mv[ia] = 0.0;
     if (!bc_ok || a >= nu) continue;
-    const double wabc = T0[(al * kTB + bl) * (kTB + 1) + cl];
-    const double wacb = T1[(al * kTB + cl) * (kTB + 1) + bl];
-    const double wbac = T2[(bl * kTA + al) * (kTB + 1) + cl];
-    const double wcab = T4[(cl * kTA + al) * (kTB + 1) + bl];
-    const double wbca = T3[(bl * kTB + cl) * (kTA + 1) + al];
-    const double wcba = T5[(cl * kTB + bl) * (kTA + 1) + al];
+    const double wabc = T0[tix<kTB, kTB>(al, bl, cl)];
+    const double wacb = T1[tix<kTB, kTB>(al, cl, bl)];
+    const double wbac = T2[tix<kTA, kTB>(bl, al, cl)];
+    const double wcab = T4[tix<kTA, kTB>(cl, al, bl)];
+    const double wbca = T3[tix<kTB, kTA>(bl, cl, al)];
+    const double wcba = T5[tix<kTB, kTA>(cl, bl, al)];
     const double pw = 8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab);
-    const double d = 1.0 / (dijk - (ep[a] + ebc));
+    const double d = 1.0 / (dijk - (Ua[3 * kTA + al] + ebc));
     double h = 0.0;
     double ua[3];
 #pragma unroll
     for (int R = 0; R < 3; R++) {
-      ua[R] = 2.0 * t1[xr[R] + (int64_t)no * a];
-      const double *q = Q + (int64_t)(3 * R) * nu2;
+      ua[R] = Ua[R * kTA + al];
       h += ua[R] * qb0[R];
-      h += ub[R] * q[nu2 + (int64_t)a * nu + c];
-      h += uc[R] * q[2 * nu2 + (int64_t)a * nu + b];
+      h += ub[R] * Q1s[(R * kTA + al) * kTB + cl];
+      h += uc[R] * Q2s[(R * kTA + al) * kTB + bl];
     }
     const bool diag = (a == b && b == c);
     gv[ia] = diag ? 0.0 : t.weight * d * (2.0 * pw + h);
@@ -267,10 +298,10 @@ __global__ void __launch_bounds__(kGwThreads, 2)
   __syncthreads();  // the W tiles are dead from here on
   double *Gs = T0, *Ms = T1, *Sv = T2, *Rab = T3, *Rac = T3 + kTA * kTB;
 #pragma unroll
-  for (int ia = 0; ia < 8; ia++) {
-    const int al = ag * 8 + ia;
-    Gs[(al * kTB + bl) * (kTB + 1) + cl] = gv[ia];
-    Ms[(al * kTB + bl) * (kTB + 1) + cl] = mv[ia];
+  for (int ia = 0; ia < kGwPer; ia++) {
+    const int al = ag * kGwPer + ia;
+    Gs[tix<kTB, kTB>(al, bl, cl)] = gv[ia];
+    Ms[tix<kTB, kTB>(al, bl, cl)] = mv[ia];
   }
 #pragma unroll
   for (int m = 0; m < 6; m++) Sv[(ag * 6 + m) * 64 + bl * 8 + cl] = s[m];
@@ -285,13 +316,13 @@ __global__ void __launch_bounds__(kGwThreads, 2)
     if (b0 + bj < nu && c0 + cj < nu) vpart[((int64_t)ach * 6 + m) * nu2 + (int64_t)(c0 + cj) * nu + b0 + bj] = v;
   }
   // M over pairs of tile axes
-  {
+  if (tid < kTA * kTB) {
     const int al = tid >> 3, x = tid & 7;
     double rb = 0.0, rc = 0.0;
 #pragma unroll
     for (int y = 0; y < kTB; y++) {
-      rb += Ms[(al * kTB + x) * (kTB + 1) + y];  // sum over c at b = x
-      rc += Ms[(al * kTB + y) * (kTB + 1) + x];  // sum over b at c = x
+      rb += Ms[tix<kTB, kTB>(al, x, y)];  // sum over c at b = x
+      rc += Ms[tix<kTB, kTB>(al, y, x)];  // sum over b at c = x
     }
     Rab[al * kTB + x] = rb;
     Rac[al * kTB + x] = rc;
@@ -302,22 +333,22 @@ __global__ void __launch_bounds__(kGwThreads, 2)
       {  // G0(a,b,c): c fastest
         const int cj = e & 7, bj = (e >> 3) & 7, aj = e >> 6;
         const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
-        if (A < nu && B < nu && C < nu) G0[((int64_t)A * nu + B) * NP + C] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+        if (A < nu && B < nu && C < nu) G0[((int64_t)A * nu + B) * NP + C] = Gs[tix<kTB, kTB>(aj, bj, cj)];
       }
       {  // G1(a,c,b): b fastest
         const int bj = e & 7, cj = (e >> 3) & 7, aj = e >> 6;
         const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
-        if (A < nu && B < nu && C < nu) G1[((int64_t)A * nu + C) * NP + B] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+        if (A < nu && B < nu && C < nu) G1[((int64_t)A * nu + C) * NP + B] = Gs[tix<kTB, kTB>(aj, bj, cj)];
       }
       {  // G2(b,c,a): a fastest
-        const int aj = e & 31, cj = (e >> 5) & 7, bj = e >> 8;
+        const int aj = e % kTA, cj = (e / kTA) & 7, bj = e / (kTA * kTB);
         const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
-        if (A < nu && B < nu && C < nu) G2[((int64_t)B * nu + C) * NP + A] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+        if (A < nu && B < nu && C < nu) G2[((int64_t)B * nu + C) * NP + A] = Gs[tix<kTB, kTB>(aj, bj, cj)];
       }
     } else {
       const int cj = e & 7, bj = (e >> 3) & 7, aj = e >> 6;
       const int A = a0 + aj, B = b0 + bj, C = c0 + cj;
-      if (A < nu && B < nu && C < nu) GW[widx(nu, A, B, C)] = Gs[(aj * kTB + bj) * (kTB + 1) + cj];
+      if (A < nu && B < nu && C < nu) GW[widx(nu, A, B, C)] = Gs[tix<kTB, kTB>(aj, bj, cj)];
     }
   }
   __syncthreads();
@@ -451,11 +482,14 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
-__device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, double b0) {
+// D(16x8) += A(16x8) B(8x8).  Lane (g = lane/4, t = lane%4) holds
+// a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]}, b = {B[t][g], B[t+4][g]} and
+// d = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}.
+__device__ __forceinline__ void dmma_16x8x8(double *d, const double *a, const double *b) {
   asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a0), "d"(a1), "d"(b0));
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 // Row m = p*nu + q of a nu^2 x . operand and its (p,q) <-> (q,p) partner, for
 // m < 2^24 (nu <= 4096): the float quotient is within one of p, then corrected.
@@ -489,8 +523,9 @@ struct BwdEArgs {
 };
 
 // dE[x](r, n) += sum_pairs sum_s A[perm(r)][s] B[s][n]; M = nu^2, N = KP, K = NP per pair.
+// 3 CTAs per SM (2 for BN = 64, whose shared memory does not fit three)
 template <int BN>
-__global__ void __launch_bounds__(BNT, 3) bwd_e_kernel(const BwdEArgs args) {
+__global__ void __launch_bounds__(BNT, BN == 64 ? 2 : 3) bwd_e_kernel(const BwdEArgs args) {
   constexpr int BBN = BN, LDB_KN = ldb_kn<BN>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBM][BBK], swizzled
@@ -545,13 +580,25 @@ __global__ void __launch_bounds__(BNT, 3) bwd_e_kernel(const BwdEArgs args) {
   const int warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
   constexpr int MF = BWM / 16, NF = BBN / 8;
+  // The accumulators start from the current dE tile (all loads in flight at
+  // once, before the main loop), so the epilogue only stores.
+  if (ktiles == 0) return;
+  double *out = args.out[o];
   double acc[MF][NF][4];
 #pragma unroll
   for (int i = 0; i < MF; i++)
 #pragma unroll
-    for (int j = 0; j < NF; j++)
+    for (int half = 0; half < 2; half++) {
+      const int64_t m = m0 + warp * BWM + i * 16 + g + half * 8;
 #pragma unroll
-      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0;
+      for (int j = 0; j < NF; j++) {
+        const int n = n0 + j * 8 + 2 * t;
+        double2 v = make_double2(0.0, 0.0);
+        if (m < M && n < KP) v = *reinterpret_cast<const double2 *>(out + m * KP + n);
+        acc[i][j][2 * half] = v.x;
+        acc[i][j][2 * half + 1] = v.y;
+      }
+    }
 
 #pragma unroll
   for (int s = 0; s < BST - 1; s++) {
@@ -571,26 +618,29 @@ __global__ void __launch_bounds__(BNT, 3) bwd_e_kernel(const BwdEArgs args) {
     // NP is a multiple of 8: the last k-tile of a pair may hold only 8 columns
     const bool half_tile = NP - (int64_t)(kt % kt_per) * BBK <= BBK / 2;
 #pragma unroll
-    for (int kk = 0; kk < BBK; kk += 4) {
+    for (int kk = 0; kk < BBK; kk += 8) {
       if (kk >= BBK / 2 && half_tile) break;
-      double af[MF][2], bf[NF];
+      double af[MF][4], bf[NF][2];
 #pragma unroll
       for (int i = 0; i < MF; i++) {
         const int r = warp * BWM + i * 16 + g;
         af[i][0] = as[aswz(r, kk + t)];
         af[i][1] = as[aswz(r + 8, kk + t)];
+        af[i][2] = as[aswz(r, kk + 4 + t)];
+        af[i][3] = as[aswz(r + 8, kk + 4 + t)];
       }
 #pragma unroll
-      for (int j = 0; j < NF; j++) bf[j] = bs[(kk + t) * LDB_KN + j * 8 + g];
+      for (int j = 0; j < NF; j++) {
+        bf[j][0] = bs[(kk + t) * LDB_KN + j * 8 + g];
+        bf[j][1] = bs[(kk + 4 + t) * LDB_KN + j * 8 + g];
+      }
 #pragma unroll
       for (int i = 0; i < MF; i++)
 #pragma unroll
-        for (int j = 0; j < NF; j++) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
+        for (int j = 0; j < NF; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
     }
   }
   cp_async_wait<0>();
-  if (ktiles == 0) return;
-  double *out = args.out[o];
 #pragma unroll
   for (int i = 0; i < MF; i++) {
 #pragma unroll
@@ -601,12 +651,8 @@ __global__ void __launch_bounds__(BNT, 3) bwd_e_kernel(const BwdEArgs args) {
 #pragma unroll
       for (int j = 0; j < NF; j++) {
         const int n = n0 + j * 8 + 2 * t;
-        if (n < KP) {
-          double2 v = *reinterpret_cast<double2 *>(orow + n);
-          v.x += acc[i][j][2 * half];
-          v.y += acc[i][j][2 * half + 1];
-          *reinterpret_cast<double2 *>(orow + n) = v;
-        }
+        if (n < KP)
+          *reinterpret_cast<double2 *>(orow + n) = make_double2(acc[i][j][2 * half], acc[i][j][2 * half + 1]);
       }
     }
   }
@@ -624,7 +670,7 @@ struct BwdFArgs {
 
 // part[pair][split](s, n) = sum_{m in split} A[m][s] B[perm(m)][n]; M = NP, N = KP.
 template <int BN>
-__global__ void __launch_bounds__(BNT, 3) bwd_f_kernel(const BwdFArgs args) {
+__global__ void __launch_bounds__(BNT, BN == 64 ? 2 : 3) bwd_f_kernel(const BwdFArgs args) {
   constexpr int BBN = BN, LDB_KN = ldb_kn<BN>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);  // [BST][BBK][LDA_KM]
@@ -692,19 +738,24 @@ __global__ void __launch_bounds__(BNT, 3) bwd_f_kernel(const BwdFArgs args) {
     const double *as = As + (kt % BST) * BBK * LDA_KM + warp * BWM;
     const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
 #pragma unroll
-    for (int kk = 0; kk < BBK; kk += 4) {
-      double af[MF][2], bf[NF];
+    for (int kk = 0; kk < BBK; kk += 8) {
+      double af[MF][4], bf[NF][2];
 #pragma unroll
       for (int i = 0; i < MF; i++) {
         af[i][0] = as[(kk + t) * LDA_KM + i * 16 + g];
         af[i][1] = as[(kk + t) * LDA_KM + i * 16 + g + 8];
+        af[i][2] = as[(kk + 4 + t) * LDA_KM + i * 16 + g];
+        af[i][3] = as[(kk + 4 + t) * LDA_KM + i * 16 + g + 8];
       }
 #pragma unroll
-      for (int j = 0; j < NF; j++) bf[j] = bs[(kk + t) * LDB_KN + j * 8 + g];
+      for (int j = 0; j < NF; j++) {
+        bf[j][0] = bs[(kk + t) * LDB_KN + j * 8 + g];
+        bf[j][1] = bs[(kk + 4 + t) * LDB_KN + j * 8 + g];
+      }
 #pragma unroll
       for (int i = 0; i < MF; i++)
 #pragma unroll
-        for (int j = 0; j < NF; j++) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
+        for (int j = 0; j < NF; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
     }
   }
   cp_async_wait<0>();

@@ -84,7 +84,9 @@ struct ccT_plan {
   // backward: buffers and the saved context (range of the last successful forward)
   AdjBuffers adj;
   cudaStream_t bwd_stream = nullptr;   // the dF GEMMs of the backward
+  cudaStream_t rec_stream = nullptr;   // the W recompute of the backward
   cudaEvent_t ev_bwdf[2] = {};
+  cudaEvent_t ev_rec[kNBuf] = {}, ev_pw[kNBuf] = {};  // X buffer b: W rebuilt / read by the pointwise pass
   int64_t fwd_begin = -1, fwd_end = -1;
   float last_bwd_ms = 0.f;
 };
@@ -583,35 +585,47 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   CCT_TRY(adj_configure(p->device));
   if (!p->bwd_stream) {
     CCT_CUDA(cudaStreamCreateWithFlags(&p->bwd_stream, cudaStreamNonBlocking));
+    CCT_CUDA(cudaStreamCreateWithFlags(&p->rec_stream, cudaStreamNonBlocking));
     for (cudaEvent_t &e : p->ev_bwdf) CCT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (int b = 0; b < kNBuf; b++) {
+      CCT_CUDA(cudaEventCreateWithFlags(&p->ev_rec[b], cudaEventDisableTiming));
+      CCT_CUDA(cudaEventCreateWithFlags(&p->ev_pw[b], cudaEventDisableTiming));
+    }
   }
   const int64_t ntup = (int64_t)p->tuples.size();
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
   CCT_TRY(adj_zero(d, &p->adj, p->stream));
   // dT1 = 2 v1: an emulated plan's v1 is rebuilt from the FP64 W of this pass
   if (p->emulated) CCT_CUDA(cudaMemsetAsync(p->adj.v1, 0, (5 + (size_t)d.nu * d.no) * 8, p->stream));
-  // Three streams: the W recompute and the pointwise adjoint kernels of tuple t
-  // (red_stream) overlap the backward GEMMs of tuple t-1, the dE GEMM on
-  // gemm_stream and the dF GEMM on bwd_stream.  The GX buffer sets alternate;
-  // every accumulator is written by one stream only, in tuple order, so the
-  // results stay bitwise reproducible.
+  // Four streams.  rec_stream rebuilds W of tuple t into X buffer t mod 3,
+  // ahead of red_stream, which runs the pointwise adjoint kernels of tuple t
+  // (dE/dW, dVOE, deps and dE/dX into GX set t mod 2); then gemm_stream runs
+  // the dE GEMM and bwd_stream the dF GEMM of tuple t.  So the latency-bound
+  // pointwise chain of tuple t overlaps the GEMMs of t-1 and the recompute of
+  // t+1.  Every accumulator is written by one stream only, in tuple order, so
+  // the results stay bitwise reproducible.
   CCT_TRY(fork_streams(p));
-  cudaStream_t sP = p->red_stream, sG = p->gemm_stream, sF = p->bwd_stream;
+  cudaStream_t sW = p->rec_stream, sP = p->red_stream, sG = p->gemm_stream, sF = p->bwd_stream;
   CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_fork, 0));
+  CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_fork, 0));
   for (int64_t t = begin; t < end; t++) {
     const Tuple &tu = p->tuples[t];
     const int set = (int)((t - begin) & 1);
+    const int xb = (int)((t - begin) % kNBuf);
+    if (t - begin >= kNBuf) CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_pw[xb], 0));  // X buffer read by t-3
+    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2, sW));
+    CCT_CUDA(cudaEventRecord(p->ev_rec[xb], sW));
+    CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_rec[xb], 0));
     if (t - begin >= 2) {  // GX set read by the GEMMs of t-2
       CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gemm[set], 0));
       CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_bwdf[set], 0));
     }
-    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * (0 * ntup + t), tu.kind == kIJK ? 3 : 2, sP));
-    CCT_TRY(adj_tuple_pointwise(d, tu, p->X[0], p->eh, p->ep, p->t1, p->voe, &p->adj, set, sP));
+    CCT_TRY(adj_tuple_pointwise(d, tu, p->X[xb], p->eh, p->ep, p->t1, p->voe, &p->adj, set, sP));
     if (p->emulated) {
       TupleDev td;
-      td.x[0] = p->X[0][0];
-      td.x[1] = p->X[0][1];
-      td.x[2] = p->X[0][2];
+      td.x[0] = p->X[xb][0];
+      td.x[1] = p->X[xb][1];
+      td.x[2] = p->X[xb][2];
       td.kind = tu.kind;
       td.i = tu.i;
       td.j = tu.j;
@@ -620,6 +634,7 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
       CCT_TRY(launch_reduce(d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, sP));
       CCT_TRY(launch_finalize(d, td, p->xpart, p->vpart, p->adj.v1, p->adj.v1 + 5, sP));
     }
+    CCT_CUDA(cudaEventRecord(p->ev_pw[xb], sP));
     CCT_CUDA(cudaEventRecord(p->ev_red[set], sP));
     CCT_CUDA(cudaStreamWaitEvent(sG, p->ev_red[set], 0));
     CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_red[set], 0));
@@ -627,7 +642,7 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     CCT_CUDA(cudaEventRecord(p->ev_gemm[set], sG));
     CCT_CUDA(cudaEventRecord(p->ev_bwdf[set], sF));
   }
-  // p->stream after both streams
+  // p->stream after every stream (red_stream already waited for rec_stream)
   CCT_CUDA(cudaEventRecord(p->ev_join, sP));
   CCT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_join, 0));
   CCT_CUDA(cudaEventRecord(p->ev_fork, sG));
@@ -728,7 +743,7 @@ int64_t ccT_last_forward_launches(const ccT_plan *p) { return p ? p->last_launch
 int ccT_plan_destroy(ccT_plan *p) {
   if (!p) return CCT_OK;
   DeviceGuard guard(p->device);
-  for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream, p->bwd_stream})
+  for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream, p->bwd_stream, p->rec_stream})
     if (st) cudaStreamSynchronize(st);
   double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->xpart, p->vpart, p->acc, p->stage};
   for (double *b : bufs)
@@ -754,8 +769,13 @@ int ccT_plan_destroy(ccT_plan *p) {
   }
   if (p->gemm_stream) cudaStreamDestroy(p->gemm_stream);
   if (p->bwd_stream) cudaStreamDestroy(p->bwd_stream);
+  if (p->rec_stream) cudaStreamDestroy(p->rec_stream);
   for (cudaEvent_t e : p->ev_bwdf)
     if (e) cudaEventDestroy(e);
+  for (int b = 0; b < kNBuf; b++) {
+    if (p->ev_rec[b]) cudaEventDestroy(p->ev_rec[b]);
+    if (p->ev_pw[b]) cudaEventDestroy(p->ev_pw[b]);
+  }
   if (p->red_stream) cudaStreamDestroy(p->red_stream);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
   delete p;
