@@ -7,6 +7,7 @@ triples.F90:316) with the device time.
     python -m libcc_b200.run --workload no16-nu200 --form fp64
     python -m libcc_b200.run --restart triples.restart --form int8:5
     python -m libcc_b200.run --workload no24-nu320 --tuples 4      # first 4 tuples only
+    python -m libcc_b200.run --workload no12-nu120 --backward      # then the adjoint pass
 """
 from __future__ import annotations
 
@@ -47,6 +48,8 @@ def main(argv=None) -> int:
     ap.add_argument("--form", default="fp64", help="fp64 or int8[:digits] (default fp64)")
     ap.add_argument("--tuples", type=int, default=0, help="run only the first N tuples (default all)")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--backward", action="store_true",
+                    help="after the forward, run the adjoint (ccT_backward) over the same tuples")
     args = ap.parse_args(argv)
 
     from . import restart, synthetic
@@ -62,6 +65,10 @@ def main(argv=None) -> int:
         print(format_energies(ets, etd))
         print(f" device ms={plan.last_forward_ms:.3f} set_inputs s={t1 - t0:.3f} "
               f"launches={plan.last_forward_launches}")
+        if args.backward:
+            plan.backward(0, end)
+            print(f" backward device ms={plan.last_backward_ms:.3f} "
+                  f"ratio={plan.last_backward_ms / plan.last_forward_ms:.2f}")
     return 0
 
 
