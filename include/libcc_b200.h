@@ -49,7 +49,8 @@ typedef struct {
     int32_t precision;       /* ccT_precision                                    */
     int32_t device;          /* CUDA device ordinal                              */
     int32_t check_inputs;    /* 1: reject NaN/Inf inputs and D >= 0 (default 1)  */
-    int32_t emu_slices;      /* INT8 emulation: 0 = choose per tile, else fixed  */
+    int32_t emu_slices;      /* INT8 emulation: 0 = per tile, at most 5 (default);
+                                4..7 = that many digits on every tile          */
     int32_t reserved[4];
 } ccT_options;
 
@@ -97,6 +98,15 @@ int ccT_backward(ccT_plan *plan, int64_t begin, int64_t end, double *d_eh, doubl
 
 /* Milliseconds of device time the last ccT_backward spent (CUDA events). */
 double ccT_last_backward_ms(const ccT_plan *plan);
+
+/* Emulated plans: hist[s] = work items (128-row x N-column W tiles) the last
+ * ccT_forward ran with s digits per operand, s = 0..n-1.  With emu_slices = 0
+ * the default count is the maximum and every tile takes the digits its
+ * exponents need (a tile whose largest row scales sum g bits below the
+ * system's top runs max(1, S - floor(g/7)) digits), so the bound on the
+ * error of any W entry is the top tile's.  FP64 plans: all zero.  No
+ * reference counterpart (the reference has no emulation). */
+int ccT_emu_slice_histogram(ccT_plan *plan, int64_t *hist, int32_t n);
 
 /* ---------------------------------------------------------------- batches
  * Many independent systems of uneven (no, nu) evaluated together.  Every tuple

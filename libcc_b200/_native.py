@@ -23,7 +23,7 @@ EXPORTS = [
     "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
     "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
     "ccT_last_error", "ccT_measure_fp64_peak", "ccT_measure_int8_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
-    "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms",
+    "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms", "ccT_emu_slice_histogram",
     "ccT_batch_create", "ccT_batch_set_inputs", "ccT_batch_forward", "ccT_batch_v1", "ccT_batch_configure",
     "ccT_batch_tune", "ccT_batch_last_ms", "ccT_batch_work_items", "ccT_batch_destroy",
 ]
@@ -105,6 +105,8 @@ def load():
     lib.ccT_backward.restype = ctypes.c_int
     lib.ccT_last_backward_ms.argtypes = [vp]
     lib.ccT_last_backward_ms.restype = ctypes.c_double
+    lib.ccT_emu_slice_histogram.argtypes = [vp, i64p, i32]
+    lib.ccT_emu_slice_histogram.restype = i32
     lib.ccT_batch_create.argtypes = [ctypes.POINTER(vp), i64, i64p, i64p, ctypes.POINTER(Options)]
     lib.ccT_batch_create.restype = ctypes.c_int
     lib.ccT_batch_set_inputs.argtypes = [vp, i64] + [vp] * 7 + [i32]

@@ -125,6 +125,14 @@ class TriplesPlan:
     def last_backward_ms(self) -> float:
         return float(N.load().ccT_last_backward_ms(self._h))
 
+    def emu_slice_histogram(self) -> list:
+        """Emulated plans: work items of the last forward per digit count
+        (index s = digits per operand, 0..7); all zero for FP64 plans."""
+        import ctypes
+        h = (ctypes.c_int64 * 8)()
+        N.check(N.load().ccT_emu_slice_histogram(self._h, h, 8), "ccT_emu_slice_histogram")
+        return [int(v) for v in h]
+
     def set_stream(self, stream_handle: int | None):
         """Run on a caller's CUDA stream (an integer cudaStream_t, e.g.
         ``torch.cuda.current_stream().cuda_stream``); None restores the plan's own."""

@@ -13,25 +13,31 @@
 // 2^(-7(S+1)) of |A||B| per term).  Each D_d is an exact int32 accumulation
 // (|D_d| <= 2 S K 127^2 < 2^31 for K <= 4096); FP64 enters only when the
 // diagonals are scaled and summed in the epilogue.  Digit count S (4..7) is a
-// plan option: about 7S - 2 bits of each operand row survive.
+// plan option: about 7S - 2 bits of each operand row survive.  An adaptive
+// plan takes S as the maximum and gives each work item (row tile, column
+// tile) its own count s <= S from the tile's exponents (EmuOperands::tileExp):
+// a tile whose largest row scales sum `gap` bits below the plan's top runs
+// s = S - floor(gap / 7) digits, s(s+1)/2 MMAs per K chunk instead of
+// S(S+1)/2, and its dropped products stay below the top tile's.
 //
 // Operands are pre-tiled (EmuOperands): the digits of one 32-byte K chunk of
 // a 128-row A tile, all S slices, are one contiguous S x 4 KB run already in
-// the tensor core's K-major no-swizzle layout, and likewise S x 2 KB for a
-// 64-row B tile.  A pipeline stage is therefore two bulk copies
+// the tensor core's K-major no-swizzle layout, and likewise S x N x 32 B for
+// an N-row B tile.  A pipeline stage is therefore two bulk copies
 // (cp.async.bulk) of large contiguous runs instead of 2S narrow tensor boxes.
 //
-// Persistent kernel, one 192-thread CTA per SM, work items (job, row tile,
-// column tile) taken round-robin with the column tile fastest, so the CTAs
-// in flight share A tiles through L2:
-//   warp 0      producer: per K chunk, one bulk copy of the A digits and one
-//               of the B digits into a ring of stages; it runs ahead across
-//               work items, so the ring never drains between tiles
-//   warp 1      TMEM owner + MMA issuer (one thread): S(S+1)/2 MMAs per chunk
-//               into S diagonal accumulators (64 int32 columns each)
-//   warps 2..5  drain: tcgen05.ld every diagonal, scale, sum in FP64, store X,
-//               then hand the tensor memory back to the issuer (the ring keeps
-//               filling meanwhile, so the next item's MMAs start at once)
+// Persistent kernel, one CTA of 64 + 32 NDW threads per SM, work items (job,
+// row tile, column tile) taken round-robin with the column tile fastest, so
+// the CTAs in flight share A tiles through L2:
+//   warp 0      producer: per stage, one bulk copy of the A digits and one
+//               of the B digits (KS K chunks) into a ring of stages; it runs
+//               ahead across work items, so the ring never drains between tiles
+//   warp 1      TMEM owner + MMA issuer (one thread): s(s+1)/2 MMAs per chunk
+//               into s diagonal accumulators (N int32 columns each)
+//   warps 2..   drain (NDW warps): tcgen05.ld one diagonal at a time, sum in
+//               FP64, hand the tensor memory back to the issuer, then scale
+//               and store X (the ring keeps filling meanwhile, so the next
+//               item's MMAs start at once)
 // Every mbarrier wait is bounded and also ends when another role aborted; a
 // timeout sets the error word, the producer waits for its copies in flight,
 // the issuer for its MMAs, and the CTA frees its tensor memory and returns.
@@ -143,12 +149,25 @@ struct EmuArgs {
   const EmuJob *jobs;
   const int8_t *E8, *E8T, *F8;
   const int16_t *expE, *expF;
-  int nu, njobs, kchunks, tiles_m, tiles_n;
+  const int *tileExp;  // adaptive plans: see EmuOperands::tileExp; nullptr: every item runs S digits
+  unsigned long long *slice_hist;
+  int nu, no, njobs, kchunks, tiles_m, tiles_n;
   int64_t NP;
   int *err;
 };
 
 constexpr int kNoRowExp = -30000;  // exponent of an all-zero row: never the maximum
+
+// Digits of work item (row tile tm, column tile tn of job z = x3).
+template <int S>
+__device__ __forceinline__ int item_slices(const EmuArgs &a, int tm, int tn, int z) {
+  if (!a.tileExp) return S;
+  const int ea = a.tileExp[tm], eb = a.tileExp[a.tiles_m + z * a.tiles_n + tn];
+  const int top = a.tileExp[a.tiles_m + a.no * a.tiles_n] + a.tileExp[a.tiles_m + a.no * a.tiles_n + 1];
+  if (ea <= kNoRowExp || eb <= kNoRowExp) return 1;  // all-zero rows or columns: X is zero
+  const int s = S - (top - (ea + eb)) / 7;
+  return s < 1 ? 1 : (s > S ? S : s);
+}
 
 __device__ __forceinline__ double pow2(int e) {
   // exact 2^e for normal exponents; ldexp covers the subnormal range
@@ -210,6 +229,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
         const int rem = (int)(it - (int64_t)jb * per_job);
         const int tm = rem / args.tiles_n, tn = rem - tm * args.tiles_n;
         const EmuJob job = args.jobs[jb];
+        const int sl = item_slices<S>(args, tm, tn, job.x3);
         for (int h = 0; h < job.nhalves && ok; h++) {
           const int8_t *A = (h == 0 ? args.E8 + job.x1 * aslab : args.E8T + job.x2 * aslab) + (int64_t)tm * KC * CA;
           const int8_t *B = args.F8 + job.fyz[h] * bslab + (int64_t)tn * KC * CB;
@@ -220,9 +240,17 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
               ok = false;
               break;
             }
-            mbar_expect_tx(&full[st], nch * (CA + CB));
-            bulk_load(sA + st * SA, A + (int64_t)kc * CA, nch * CA, &full[st]);
-            bulk_load(sB + st * SB, B + (int64_t)kc * CB, nch * CB, &full[st]);
+            if (sl == S) {  // all digits: the stage's chunks are one contiguous run per operand
+              mbar_expect_tx(&full[st], nch * (CA + CB));
+              bulk_load(sA + st * SA, A + (int64_t)kc * CA, nch * CA, &full[st]);
+              bulk_load(sB + st * SB, B + (int64_t)kc * CB, nch * CB, &full[st]);
+            } else {  // the leading sl digit slices of each chunk
+              mbar_expect_tx(&full[st], nch * (uint32_t)sl * (A_BLK + B_BLK));
+              for (uint32_t c = 0; c < nch; c++) {
+                bulk_load(sA + st * SA + c * CA, A + (int64_t)(kc + c) * CA, (uint32_t)sl * A_BLK, &full[st]);
+                bulk_load(sB + st * SB + c * CB, B + (int64_t)(kc + c) * CB, (uint32_t)sl * B_BLK, &full[st]);
+              }
+            }
           }
         }
       }
@@ -231,7 +259,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
     }
   } else if (warp == 1) {
     if (lane == 0) {  // ---------------- MMA issuer
-      // kind::i8, D s32, A/B s8, K-major, M = 128, N = 64
+      // kind::i8, D s32, A/B s8, K-major, M = 128, N = EBN
       const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(EBN >> 3) << 17) | (8u << 24);
       const uint64_t dA0 = desc_kmajor(sA), dB0 = desc_kmajor(sB);
       uint32_t g = 0, n = 0;
@@ -243,7 +271,13 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const int nh = args.jobs[it / per_job].nhalves;
+        const int jb = (int)(it / per_job);
+        const int rem = (int)(it - (int64_t)jb * per_job);
+        const int tm = rem / args.tiles_n, tn = rem - tm * args.tiles_n;
+        const EmuJob job = args.jobs[jb];
+        const int nh = job.nhalves;
+        const int sl = item_slices<S>(args, tm, tn, job.x3);
+        if (args.slice_hist) atomicAdd(args.slice_hist + sl, 1ull);
         for (int h = 0; h < nh && ok; h++) {
           for (int kc = 0; kc < KC; kc += KS, g++) {
             const int st = (int)(g % ST);
@@ -262,8 +296,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
               const uint32_t first = (h == 0 && kc == 0 && c == 0) ? 0u : 1u;  // accumulate flag of the t = 0 row
 #pragma unroll
               for (int t = 0; t < S; t++) {
+                if (t >= sl) break;
 #pragma unroll
                 for (int u = 0; u < S - t; u++) {
+                  if (u >= sl - t) break;
                   asm volatile(
                       "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; "
                       "}" ::"r"(tmem + (uint32_t)((t + u) * EBN)),
@@ -305,6 +341,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       const bool live = m < M;
       const int eA = live ? args.expE[m] : 0;
       const int n0 = tn * EBN + cbase;
+      const int sl = item_slices<S>(args, tm, tn, job.x3);
       // warp-uniform decision: the tcgen05.ld below are .sync.aligned
       if (!__all_sync(0xffffffffu, mbar_wait(&acc_full, n & 1, args.err, abort_flag))) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
@@ -315,6 +352,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
         const int w = CW - c0 >= 16 ? 16 : 8;  // the last chunk of a 40-column slice is 8 wide
 #pragma unroll
         for (int d0 = 0; d0 < S; d0 += DB) {
+          if (d0 >= sl) break;  // diagonals past the item's digit count were not written
           uint32_t v[DB][16];
 #pragma unroll
           for (int dd = 0; dd < DB; dd++) {
@@ -330,7 +368,8 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
             if (j >= w) continue;
             double a = d0 == 0 ? 0.0 : acc[c0 + j];
 #pragma unroll
-            for (int dd = 0; dd < DB; dd++) a = fma((double)(int32_t)v[dd][j], cd[d0 + dd], a);
+            for (int dd = 0; dd < DB; dd++)
+              if (d0 + dd < sl) a = fma((double)(int32_t)v[dd][j], cd[d0 + dd], a);
             acc[c0 + j] = a;
           }
         }
@@ -396,6 +435,59 @@ __global__ void shared_exp_f_kernel(const int16_t *__restrict__ rowexp, int no, 
     int e = kNoRowExp;
     for (int y = 0; y < no; y++) e = max(e, (int)rowexp[((int64_t)y * no + z) * NP + n]);
     expF[zn] = (int16_t)(e == kNoRowExp ? 0 : e);
+  }
+}
+
+// Pass 2c (adaptive plans): the largest nonzero row exponent of every A row
+// tile (over x and both halves' row orders) and of every B column tile of each
+// z (over y): one block per tile.  tile_exp_top_kernel then appends the two
+// maxima.
+__global__ void tile_exp_kernel(const int16_t *__restrict__ rowexpE, const int16_t *__restrict__ rowexpF, int no,
+                                int nu, int64_t NP, int ebn, int tiles_m, int tiles_n, int *__restrict__ tileExp) {
+  const int64_t nu2 = (int64_t)nu * nu;
+  const int tile = blockIdx.x;
+  int e = kNoRowExp;
+  if (tile < tiles_m) {
+    for (int r = threadIdx.x; r < kEmuBM; r += blockDim.x) {
+      const int64_t m = (int64_t)tile * kEmuBM + r;
+      if (m >= nu2) break;
+      const int64_t p = m / nu, q = m - p * nu, mt = q * nu + p;
+      for (int x = 0; x < no; x++) e = max(e, max((int)rowexpE[x * nu2 + m], (int)rowexpE[x * nu2 + mt]));
+    }
+  } else {
+    const int zt = tile - tiles_m, z = zt / tiles_n, tn = zt - z * tiles_n;
+    for (int r = threadIdx.x; r < ebn; r += blockDim.x) {
+      const int64_t n = (int64_t)tn * ebn + r;
+      for (int y = 0; y < no; y++) e = max(e, (int)rowexpF[((int64_t)y * no + z) * NP + n]);
+    }
+  }
+  __shared__ int red[256];
+  red[threadIdx.x] = e;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) tileExp[tile] = red[0];
+}
+__global__ void tile_exp_top_kernel(int tiles_m, int nbt, int *__restrict__ tileExp) {
+  __shared__ int red[2][256];
+  int ea = kNoRowExp, eb = kNoRowExp;
+  for (int t = threadIdx.x; t < tiles_m; t += blockDim.x) ea = max(ea, tileExp[t]);
+  for (int t = threadIdx.x; t < nbt; t += blockDim.x) eb = max(eb, tileExp[tiles_m + t]);
+  red[0][threadIdx.x] = ea;
+  red[1][threadIdx.x] = eb;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      red[0][threadIdx.x] = max(red[0][threadIdx.x], red[0][threadIdx.x + w]);
+      red[1][threadIdx.x] = max(red[1][threadIdx.x], red[1][threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    tileExp[tiles_m + nbt] = red[0][0];
+    tileExp[tiles_m + nbt + 1] = red[1][0];
   }
 }
 
@@ -503,7 +595,10 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   a.F8 = o.F8;
   a.expE = o.expE;
   a.expF = o.expF;
+  a.tileExp = o.adaptive ? o.tileExp : nullptr;
+  a.slice_hist = o.slice_hist;
   a.nu = d.nu;
+  a.no = d.no;
   a.njobs = njobs;
   a.kchunks = (int)(o.KP8 / kEmuKC);
   a.tiles_m = (int)o.tiles_m;
@@ -561,6 +656,14 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
   digits_f_kernel<<<grid_rows(rowsF), 256, 0, s>>>(F, d.no, d.nu, d.NP, d.KP, o->KP8, o->slices, d.EBN, o->expF,
                                                    o->F8);
   CCT_CUDA(cudaGetLastError());
+  if (o->adaptive) {
+    const int tiles_n = (int)(d.NP / d.EBN), nbt = d.no * tiles_n;
+    tile_exp_kernel<<<(int)o->tiles_m + nbt, 256, 0, s>>>(o->expET, o->expRowF, d.no, d.nu, d.NP, d.EBN,
+                                                          (int)o->tiles_m, tiles_n, o->tileExp);
+    CCT_CUDA(cudaGetLastError());
+    tile_exp_top_kernel<<<1, 256, 0, s>>>((int)o->tiles_m, nbt, o->tileExp);
+    CCT_CUDA(cudaGetLastError());
+  }
   return CCT_OK;
 }
 

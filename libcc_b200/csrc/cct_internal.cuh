@@ -148,6 +148,15 @@ struct EmuOperands {
   // the largest of F[y][z][n] over all y.  expET and expRowF hold the per-row
   // exponents they are reduced from.
   int16_t *expE = nullptr, *expET = nullptr, *expF = nullptr, *expRowF = nullptr;
+  // Per-tile digit counts (adaptive plans): tileExp holds the largest nonzero
+  // row exponent of every A row tile [tiles_m], of every B column tile
+  // [no][tiles_n] (z = x3 of the job), then the maxima of both sets.  A work
+  // item (row tile, column tile) whose exponents sum `gap` below the top runs
+  // S - floor(gap / 7) digits (at least 1): its dropped digit products stay
+  // below the top tile's, so the bound on |X error| is the same everywhere.
+  bool adaptive = false;
+  int *tileExp = nullptr;
+  unsigned long long *slice_hist = nullptr;  // [kEmuMaxSlices + 1] work items per digit count
 };
 
 int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOperands *o, cudaStream_t s);

@@ -411,6 +411,7 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   if (p->emulated) {
     EmuOperands &e = p->emu;
     e.slices = o.emu_slices ? o.emu_slices : kEmuDefaultSlices;
+    e.adaptive = o.emu_slices == 0;  // 0: the default count is the maximum, each tile takes what it needs
     e.KP8 = round_up(nu + no, kEmuKC);
     e.tiles_m = (nu2 + kEmuBM - 1) / kEmuBM;
     const int64_t rowsE = no * nu2, rowsF = no * no * d.NP;
@@ -418,7 +419,9 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     if ((s = dalloc(&e.E8, bytesE)) || (s = dalloc(&e.E8T, bytesE)) ||
         (s = dalloc(&e.F8, e.slices * rowsF * e.KP8)) || (s = dalloc(&e.expE, rowsE)) ||
         (s = dalloc(&e.expET, rowsE)) || (s = dalloc(&e.expF, rowsF)) || (s = dalloc(&e.expRowF, rowsF)) ||
-        (s = dalloc(&p->emu_jobs, p->tuples.size() * 3 * kNBuf)))
+        (s = dalloc(&p->emu_jobs, p->tuples.size() * 3 * kNBuf)) ||
+        (s = dalloc(&e.tileExp, e.tiles_m + no * (d.NP / d.EBN) + 2)) ||
+        (s = dalloc(&e.slice_hist, kEmuMaxSlices + 1)))
       return fail(s);
   }
   std::vector<int16_t> table(d.ncta * 3);
@@ -523,6 +526,8 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   p->last_launches = 0;
   CCT_CUDA(cudaMemsetAsync(p->acc, 0, (5 + (int64_t)d.nu * d.no) * 8, p->stream));
   CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
+  if (p->emulated)
+    CCT_CUDA(cudaMemsetAsync(p->emu.slice_hist, 0, (kEmuMaxSlices + 1) * sizeof(unsigned long long), p->stream));
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
   CCT_TRY(fork_streams(p));
   for (int64_t t = begin; t < end; t++) CCT_TRY(run_tuple(p, t));
@@ -673,6 +678,21 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
 
 double ccT_last_backward_ms(const ccT_plan *p) { return p ? (double)p->last_bwd_ms : 0.0; }
 
+int ccT_emu_slice_histogram(ccT_plan *p, int64_t *hist, int32_t n) {
+  if (!p || !hist || n < 1) {
+    set_error("need a plan, an output array and n >= 1");
+    return CCT_ERR_INVALID;
+  }
+  for (int32_t s = 0; s < n; s++) hist[s] = 0;
+  if (!p->emulated) return CCT_OK;
+  DeviceGuard guard(p->device);
+  unsigned long long h[kEmuMaxSlices + 1];
+  CCT_CUDA(cudaStreamSynchronize(p->stream));
+  CCT_CUDA(cudaMemcpy(h, p->emu.slice_hist, sizeof(h), cudaMemcpyDeviceToHost));
+  for (int32_t s = 0; s < n && s <= kEmuMaxSlices; s++) hist[s] = (int64_t)h[s];
+  return CCT_OK;
+}
+
 int ccT_set_stream(ccT_plan *p, void *cuda_stream) {
   if (!p) {
     set_error("plan is NULL");
@@ -755,7 +775,8 @@ int ccT_plan_destroy(ccT_plan *p) {
   if (p->jobs) cudaFree(p->jobs);
   if (p->flags) cudaFree(p->flags);
   for (void *b : {(void *)p->emu.E8, (void *)p->emu.E8T, (void *)p->emu.F8, (void *)p->emu.expE,
-                  (void *)p->emu.expET, (void *)p->emu.expF, (void *)p->emu.expRowF, (void *)p->emu_jobs})
+                  (void *)p->emu.expET, (void *)p->emu.expF, (void *)p->emu.expRowF, (void *)p->emu_jobs,
+                  (void *)p->emu.tileExp, (void *)p->emu.slice_hist})
     if (b) cudaFree(b);
   adj_free(&p->adj);
   if (p->ev0) cudaEventDestroy(p->ev0);

@@ -124,6 +124,30 @@ def generate(no: int, nu: int, seed: int, dist: str = "normal", name: str = "") 
                          vvvo=vvvo.ravel(), name=name or f"no{no}-nu{nu}-s{seed}", seed=seed)
 
 
+def with_decay(inp: TriplesInputs, bits_per_index: float) -> TriplesInputs:
+    """A copy of ``inp`` whose magnitudes fall by 2^-bits_per_index per virtual
+    index, like integrals over localised orbitals ordered by distance: every
+    entry is scaled by g(a) = 2^(-bits_per_index * a) for each virtual index a
+    it carries (T1, T2, VM, VOE, VVVO).  Energies stay finite; W tiles then
+    span many binary orders of magnitude, which the per-tile digit count of the
+    emulated form exploits."""
+    no, nu = inp.no, inp.nu
+    g = 2.0 ** (-bits_per_index * np.arange(nu))
+    t1 = (inp.t1.reshape(nu, no) * g[:, None]).ravel()
+    t2 = (inp.t2.reshape(no, no, nu, nu) * g[None, None, :, None] * g[None, None, None, :]).ravel()
+    vm = (inp.vm.reshape(no, no, nu, no) * g[None, None, :, None]).ravel()
+    voe = (inp.voe.reshape(no, no, nu, nu) * g[None, None, :, None] * g[None, None, None, :]).ravel()
+    ii = np.arange(nu)
+    I, J = np.meshgrid(ii, ii, indexing="ij")
+    low = I >= J
+    gp = np.zeros(nu * (nu + 1) // 2)
+    gp[(I * (I + 1) // 2 + J)[low]] = (g[:, None] * g[None, :])[low]      # packed (I >= J)
+    col = np.tile(g, no)                                                  # column x*nu + r1 -> g(r1)
+    vvvo = (inp.vvvo.reshape(nu * no, -1) * col[:, None] * gp[None, :]).ravel()
+    return TriplesInputs(no=no, nu=nu, eh=inp.eh.copy(), ep=inp.ep.copy(), t1=t1, t2=t2, vm=vm, voe=voe,
+                         vvvo=vvvo, name=f"{inp.name}-decay{bits_per_index:g}", seed=inp.seed)
+
+
 def workload(name: str) -> TriplesInputs:
     """One of the named single-system workloads."""
     cfg = WORKLOADS[name]

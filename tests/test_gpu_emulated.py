@@ -101,3 +101,42 @@ def test_emulated_deterministic(api):
         a = plan.forward()
         b = plan.forward()
     assert a[1] == b[1] and np.array_equal(a[2], b[2])
+
+
+def test_per_tile_digits_follow_exponent_spread(api):
+    """emu_slices = 0: each 128 x N tile runs max(1, 5 - floor(gap/7)) digits, gap
+    = bits its largest row scales sum below the system's top.  On a system whose
+    magnitudes fall by half a bit per virtual index the tiles spread over 1..5
+    digits; the energy keeps the 5-digit bar and stays close to fixed 5 digits."""
+    from oracle import oracle as O
+    inp = S.with_decay(S.generate(4, 64, 21, dist="normal"), 0.5)
+    ets_o, etd_o, _ = O.c_cc_triples(inp)
+    e_ref = ets_o + etd_o
+    with _plan(api, inp, 0) as plan:
+        plan.set_system(inp)
+        ets_a, etd_a, v1_a = plan.forward()
+        hist = plan.emu_slice_histogram()
+    with _plan(api, inp, 5) as plan:
+        plan.set_system(inp)
+        ets_f, etd_f, _ = plan.forward()
+        hist_f = plan.emu_slice_histogram()
+    assert sum(hist[1:5]) > 0 and hist[5] > 0 and sum(hist[6:]) == 0, hist
+    assert hist_f[5] == sum(hist) and sum(hist_f) == hist_f[5], hist_f
+    err_a, err_f = abs((ets_a + etd_a) - e_ref), abs((ets_f + etd_f) - e_ref)
+    assert err_a <= 3e-8 * abs(e_ref), (err_a, e_ref)
+    assert err_a <= 10.0 * err_f + 1e-14 * abs(e_ref), (err_a, err_f)
+
+
+def test_per_tile_digits_uniform_system_equals_fixed(api):
+    """Without an exponent spread every tile takes the maximum: bitwise the
+    fixed 5-digit result."""
+    inp = S.generate(4, 40, 12, dist="log")
+    with _plan(api, inp, 0) as plan:
+        plan.set_system(inp)
+        a = plan.forward()
+        hist = plan.emu_slice_histogram()
+    with _plan(api, inp, 5) as plan:
+        plan.set_system(inp)
+        b = plan.forward()
+    assert hist[5] == sum(hist) > 0, hist
+    assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
