@@ -230,6 +230,35 @@ def adjoint_extra(A, S, local):
             "note": "backward recomputes W per tuple in FP64; rel errors are relative to max|gradient| per input"}
 
 
+def adaptive_extra(A, S, local):
+    """Per-tile digit counts of the emulated form (emu_slices = 0, at most 5) against
+    fixed 5 digits and native FP64 on the no=16/nu=200 system with magnitudes
+    falling 2^-0.25 per virtual index (synthetic.with_decay): device time of a
+    whole (T) step, the digit histogram over W tiles and the error vs FP64."""
+    inp = S.with_decay(S.workload("no16-nu200"), 0.25)
+    res = {}
+    for form in ("fp64", "int8:5", "int8"):
+        with make_plan(A, inp.no, inp.nu, local, form) as plan:
+            plan.set_system(inp)
+            times = []
+            for _ in range(3):
+                ets, etd, _ = plan.forward()
+                times.append(plan.last_forward_ms)
+            res[form] = {"ms": statistics.median(times[1:]), "e_t": ets + etd,
+                         "digit_histogram": plan.emu_slice_histogram() if form != "fp64" else None}
+    ref = res["fp64"]["e_t"]
+    for form in ("int8:5", "int8"):
+        res[form]["rel_err_vs_fp64"] = abs(res[form]["e_t"] - ref) / abs(ref)
+    return {"workload": "no16-nu200 (seed 1, normal) with magnitudes x 2^(-0.25 a) per virtual index a",
+            "fp64_ms": res["fp64"]["ms"], "fixed5_ms": res["int8:5"]["ms"], "per_tile_ms": res["int8"]["ms"],
+            "speedup_per_tile_over_fixed5": res["int8:5"]["ms"] / res["int8"]["ms"],
+            "fixed5_rel_err_vs_fp64": res["int8:5"]["rel_err_vs_fp64"],
+            "per_tile_rel_err_vs_fp64": res["int8"]["rel_err_vs_fp64"],
+            "per_tile_digit_histogram": res["int8"]["digit_histogram"],
+            "note": "histogram index = 7-bit digits per operand of a 128 x N W tile; the bench headline runs "
+                    "fixed 5 digits, where the per-tile rule also picks 5 on every tile of its workload"}
+
+
 def batch_extra(A, S, local):
     """The 96 uneven systems (no ~ U{3..12}, nu ~ U{24..140}, seed 100+s): the
     batched executor (CUDA graph) against a per-system plan loop, and per-system
@@ -280,7 +309,8 @@ def batch_extra(A, S, local):
 
 
 def make_plan(A, no, nu, device, form):
-    """Plan for one form: 'fp64' (native mma.sync f64) or 'int8:S' (S-digit emulation)."""
+    """Plan for one form: 'fp64' (native mma.sync f64), 'int8:S' (S-digit emulation)
+    or 'int8' (per-tile digit counts, at most 5)."""
     if form == "fp64":
         return A.TriplesPlan(no, nu, device=device)
     import ctypes
@@ -290,7 +320,7 @@ def make_plan(A, no, nu, device, form):
     lib.ccT_options_default(ctypes.byref(opt))
     opt.precision = N.CCT_PREC_INT8_EMU
     opt.device = device
-    opt.emu_slices = int(form.split(":")[1])
+    opt.emu_slices = int(form.split(":")[1]) if ":" in form else 0
     h = ctypes.c_void_p()
     N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
     plan = A.TriplesPlan.__new__(A.TriplesPlan)
@@ -475,6 +505,7 @@ def main():
         if world == 1 and not args.no_extras:
             line["adjoint"] = adjoint_extra(A, S, local)
             line["batch"] = batch_extra(A, S, local)
+            line["per_tile_digits"] = adaptive_extra(A, S, local)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
