@@ -33,7 +33,8 @@
 //               of the B digits (KS K chunks) into a ring of stages; it runs
 //               ahead across work items, so the ring never drains between tiles
 //   warp 1      TMEM owner + MMA issuer (one thread): s(s+1)/2 MMAs per chunk
-//               into s diagonal accumulators (N int32 columns each)
+//               into s diagonal accumulators (N int32 columns each), at 5 or
+//               more digits diagonal by diagonal within the chunk
 //   warps 2..   drain (NDW warps): tcgen05.ld one diagonal at a time, sum in
 //               FP64, hand the tensor memory back to the issuer, then scale
 //               and store X (the ring keeps filling meanwhile, so the next
@@ -294,17 +295,32 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
               const uint64_t dA = dA0 + (uint64_t)((st * SA + c * CA) >> 4);
               const uint64_t dB = dB0 + (uint64_t)((st * SB + c * CB) >> 4);
               const uint32_t first = (h == 0 && kc == 0 && c == 0) ? 0u : 1u;  // accumulate flag of the t = 0 row
+              auto mma = [&](int t, int u) {
+                asm volatile(
+                    "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; "
+                    "}" ::"r"(tmem + (uint32_t)((t + u) * EBN)),
+                    "l"(dA + (uint64_t)(t * (A_BLK >> 4))), "l"(dB + (uint64_t)(u * (B_BLK >> 4))), "r"(idesc),
+                    "r"(t > 0 ? 1u : first));
+              };
+              if constexpr (S >= 5) {
+                // diagonal by diagonal: runs of MMAs into one accumulator
+                // (measured 19-20% faster than row order at 5 and 6 digits,
+                // 3% slower at 4)
 #pragma unroll
-              for (int t = 0; t < S; t++) {
-                if (t >= sl) break;
+                for (int d = 0; d < S; d++) {
+                  if (d >= sl) break;
 #pragma unroll
-                for (int u = 0; u < S - t; u++) {
-                  if (u >= sl - t) break;
-                  asm volatile(
-                      "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; "
-                      "}" ::"r"(tmem + (uint32_t)((t + u) * EBN)),
-                      "l"(dA + (uint64_t)(t * (A_BLK >> 4))), "l"(dB + (uint64_t)(u * (B_BLK >> 4))), "r"(idesc),
-                      "r"(t > 0 ? 1u : first));
+                  for (int t = 0; t <= d; t++) mma(t, d - t);
+                }
+              } else {
+#pragma unroll
+                for (int t = 0; t < S; t++) {
+                  if (t >= sl) break;
+#pragma unroll
+                  for (int u = 0; u < S - t; u++) {
+                    if (u >= sl - t) break;
+                    mma(t, u);
+                  }
                 }
               }
             }
