@@ -10,9 +10,10 @@
 // with z_1..z_6 the combinations of t1wt3.f90:80-85.  Because D is symmetric in
 // (a,b,c), P is self-adjoint and a W at a permuted index can be moved onto S:
 //   dE/dW = w d (2 P W + H),   H = sum_m sum_pi c_pi S_m(pi^-1)     (adj_gw_kernel)
-//   dE/dVOE(b,c,y,z) = w sum_a z_m(a,b,c) u_x(a) d                   (adj_voe_kernel)
+//   dE/dVOE(b,c,y,z) = w sum_a z_m(a,b,c) u_x(a) d      (adj_gw_kernel + adj_voe_sum_kernel)
 //   dE/deh_x = -(multiplicity of x in ijk) sum_abc M,  dE/dep_p = sum over the
-//   three index positions of M restricted to p,  M = w W (P W + H) d^2  (adj_eps_*)
+//   three index positions of M restricted to p,  M = w W (P W + H) d^2
+//   (partial sums in adj_gw_kernel, adj_eps_sum_kernel, adj_eps_total_kernel)
 //   dE/dT1(x,a) = 2 v1(a,x)                                          (adj_finish)
 // W is recomputed per tuple by the forward GEMMs (nothing of size nu^3 is kept
 // across tuples).  The W-build GEMM X_g(p,q,s) = sum_h sum_k E[x_h][perm_h(p,q)][k]
