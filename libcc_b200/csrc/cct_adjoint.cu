@@ -507,7 +507,7 @@ __device__ __forceinline__ int swap_row(int m, int nu, float inv_nu) {
   return q * nu + p;
 }
 
-constexpr int kMaxPairs = 6;  // (slot, half) pairs of one tuple: at most 3 x 2
+constexpr int kMaxPairs = 12;  // (slot, half) pairs of up to two tuples: at most 2 x 3 x 2
 struct BwdPair {
   const double *A;  // dE/dX_g (nu^2 x NP)
   const double *B;  // bwd_e: F[fyz] (NP x KP); bwd_f: E[x] (nu^2 x KP)
@@ -516,8 +516,8 @@ struct BwdPair {
 };
 struct BwdEArgs {
   BwdPair pair[kMaxPairs];
-  double *out[3];
-  int first[4], npairs;  // pairs of output o are first[o] .. first[o+1]-1
+  double *out[6];
+  int first[7], npairs;  // pairs of output o are first[o] .. first[o+1]-1
   int nu;
   int64_t NP, KP;
   int tiles_n;
@@ -929,7 +929,7 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
   CCT_TRY(al(&b->dF, no * no * d.NP * d.KP));
   CCT_TRY(al(&b->Wf, nu3));
   CCT_TRY(al(&b->GW, nu3));
-  for (int set = 0; set < 2; set++)
+  for (int set = 0; set < kGXSets; set++)
     for (int g = 0; g < 3; g++) {
       CCT_TRY(al(&b->GX[set][g], nu2 * d.NP));
       CCT_CUDA(cudaMemset(b->GX[set][g], 0, (size_t)nu2 * d.NP * 8));  // padding columns stay zero
@@ -954,8 +954,10 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
 }
 
 void adj_free(AdjBuffers *b) {
-  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->GX[0][0], b->GX[0][1], b->GX[0][2], b->GX[1][0],
-                    b->GX[1][1], b->GX[1][2], b->part, b->Q, b->vpart, b->eps, b->v1, b->g_eh,
+  for (int set = 0; set < kGXSets; set++)
+    for (int g = 0; g < 3; g++)
+      if (b->GX[set][g]) cudaFree(b->GX[set][g]);
+  for (double *q : {b->dE, b->dF, b->Wf, b->GW, b->part, b->Q, b->vpart, b->eps, b->v1, b->g_eh,
                     b->g_ep, b->g_t1, b->g_t2, b->g_vm, b->g_voe, b->g_vvvo})
     if (q) cudaFree(q);
   *b = AdjBuffers{};
@@ -1072,95 +1074,107 @@ int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const
   return CCT_OK;
 }
 
-int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double *F, AdjBuffers *b, int set,
-                    cudaStream_t s, cudaStream_t sf) {
-  const int no = d.no, nu = d.nu;
-  const int64_t nu2 = (int64_t)nu * nu;
-  double *const *GX = b->GX[set];
-
-  // (slot, half) pairs: half h reads E[x_h] with row permutation h and F[fyz_h]
+namespace {
+// (slot, half) pairs of one tuple: half h of slot g reads E[x] with row
+// permutation h and F[fyz]
+struct GemmPair {
+  int g, h, x, fyz;
+};
+std::vector<GemmPair> tuple_pairs(const Tuple &t, int no) {
   int slots[3][4], ns = 0;
   tuple_slots(t, slots, &ns);
-  struct P {
-    int g, h, x, fyz;
-  };
-  std::vector<P> pairs;
+  std::vector<GemmPair> pairs;
   for (int g = 0; g < ns; g++)
     for (int h = 0; h < slots[g][3]; h++) {
       const int x = h == 0 ? slots[g][0] : slots[g][1];
       const int fyz = (h == 0 ? slots[g][1] : slots[g][0]) * no + slots[g][2];
       pairs.push_back({g, h, x, fyz});
     }
-  auto Ex = [&](int x) { return E + (int64_t)x * nu2 * d.KP; };
-  auto Fyz = [&](int yz) { return F + (int64_t)yz * d.NP * d.KP; };
+  return pairs;
+}
+}  // namespace
 
-  // dE: outputs grouped by x, pairs in a fixed order
-  {
-    BwdEArgs a{};
-    int xs[3], nx = 0;
-    for (const P &q : pairs) {
+int adj_tuple_gemm_e(const Dims &d, const Tuple *tu, const int *sets, int ntup, const double *F, AdjBuffers *b,
+                     cudaStream_t s) {
+  const int nu = d.nu;
+  const int64_t nu2 = (int64_t)nu * nu;
+  auto Fyz = [&](int yz) { return F + (int64_t)yz * d.NP * d.KP; };
+  // dE: outputs in order of first appearance; per output the pairs of the
+  // first tuple, then of the second, each in slot order (a fixed order)
+  std::vector<GemmPair> pairs[2];
+  for (int u = 0; u < ntup; u++) pairs[u] = tuple_pairs(tu[u], d.no);
+  BwdEArgs a{};
+  int xs[6], nx = 0;
+  for (int u = 0; u < ntup; u++)
+    for (const GemmPair &q : pairs[u]) {
       bool seen = false;
-      for (int u = 0; u < nx; u++) seen |= xs[u] == q.x;
+      for (int v = 0; v < nx; v++) seen |= xs[v] == q.x;
       if (!seen) xs[nx++] = q.x;
     }
-    int np_ = 0;
-    for (int o = 0; o < nx; o++) {
-      a.first[o] = np_;
-      a.out[o] = b->dE + (int64_t)xs[o] * nu2 * d.KP;
-      for (const P &q : pairs)
+  int np_ = 0;
+  for (int o = 0; o < nx; o++) {
+    a.first[o] = np_;
+    a.out[o] = b->dE + (int64_t)xs[o] * nu2 * d.KP;
+    for (int u = 0; u < ntup; u++)
+      for (const GemmPair &q : pairs[u])
         if (q.x == xs[o]) {
           if (np_ >= kMaxPairs) {
-            set_error("adjoint: too many GEMM pairs for one E slab");
+            set_error("adjoint: too many GEMM pairs for one dE launch");
             return CCT_ERR_INVALID;
           }
-          a.pair[np_++] = BwdPair{GX[q.g], Fyz(q.fyz), q.h, o};
+          a.pair[np_++] = BwdPair{b->GX[sets[u]][q.g], Fyz(q.fyz), q.h, o};
         }
-    }
-    a.first[nx] = np_;
-    a.npairs = np_;
-    a.nu = nu;
-    a.NP = d.NP;
-    a.KP = d.KP;
-    const int bn = bwd_bn(d.KP);
-    a.tiles_n = (int)((d.KP + bn - 1) / bn);
-    const int tiles_m = (int)((nu2 + BBM - 1) / BBM);
-    CCT_TRY(bn == 64 ? launch_bwd_e<64>(a, tiles_m, nx, s)
-                     : bn == 48 ? launch_bwd_e<48>(a, tiles_m, nx, s) : launch_bwd_e<32>(a, tiles_m, nx, s));
   }
+  a.first[nx] = np_;
+  a.npairs = np_;
+  a.nu = nu;
+  a.NP = d.NP;
+  a.KP = d.KP;
+  const int bn = bwd_bn(d.KP);
+  a.tiles_n = (int)((d.KP + bn - 1) / bn);
+  const int tiles_m = (int)((nu2 + BBM - 1) / BBM);
+  return bn == 64 ? launch_bwd_e<64>(a, tiles_m, nx, s)
+                  : bn == 48 ? launch_bwd_e<48>(a, tiles_m, nx, s) : launch_bwd_e<32>(a, tiles_m, nx, s);
+}
+
+int adj_tuple_gemm_f(const Dims &d, const Tuple &t, const double *E, AdjBuffers *b, int set, cudaStream_t sf) {
+  const int nu = d.nu;
+  const int64_t nu2 = (int64_t)nu * nu;
+  double *const *GX = b->GX[set];
+  auto Ex = [&](int x) { return E + (int64_t)x * nu2 * d.KP; };
   // dF: one partial per pair and split, then a fixed-order sum per output slab
-  {
-    BwdFArgs a{};
-    std::vector<P> sorted = pairs;
-    std::stable_sort(sorted.begin(), sorted.end(), [](const P &u, const P &v) { return u.fyz < v.fyz; });
-    BwdFReduceArgs r{};
-    int no_ = 0;
-    for (size_t q = 0; q < sorted.size(); q++) {
-      a.pair[q] = BwdPair{GX[sorted[q].g], Ex(sorted[q].x), sorted[q].h, 0};
-      if (q == 0 || sorted[q].fyz != sorted[q - 1].fyz) {
-        r.first[no_] = (int)q;
-        r.dst[no_] = b->dF + (int64_t)sorted[q].fyz * d.NP * d.KP;
-        no_++;
-      }
+  BwdFArgs a{};
+  std::vector<GemmPair> sorted = tuple_pairs(t, d.no);
+  std::stable_sort(sorted.begin(), sorted.end(),
+                   [](const GemmPair &u, const GemmPair &v) { return u.fyz < v.fyz; });
+  BwdFReduceArgs r{};
+  int no_ = 0;
+  for (size_t q = 0; q < sorted.size(); q++) {
+    a.pair[q] = BwdPair{GX[sorted[q].g], Ex(sorted[q].x), sorted[q].h, 0};
+    if (q == 0 || sorted[q].fyz != sorted[q - 1].fyz) {
+      r.first[no_] = (int)q;
+      r.dst[no_] = b->dF + (int64_t)sorted[q].fyz * d.NP * d.KP;
+      no_++;
     }
-    r.first[no_] = (int)sorted.size();
-    r.nout = no_;
-    r.nsplit = (int)b->nsplit;
-    r.n = d.NP * d.KP;
-    a.part = b->part;
-    a.npairs = (int)sorted.size();
-    a.nsplit = (int)b->nsplit;
-    a.kchunk = b->kchunk;
-    a.nu = nu;
-    a.NP = d.NP;
-    a.KP = d.KP;
-    const int bn = bwd_bn(d.KP);
-    a.tiles_n = (int)((d.KP + bn - 1) / bn);
-    const int tiles_m = (int)((d.NP + BBM - 1) / BBM);
-    CCT_TRY(bn == 64 ? launch_bwd_f<64>(a, tiles_m, sf)
-                     : bn == 48 ? launch_bwd_f<48>(a, tiles_m, sf) : launch_bwd_f<32>(a, tiles_m, sf));
-    bwd_f_reduce_kernel<<<dim3(grid_for(r.n) < 64 ? grid_for(r.n) : 64, r.nout), 256, 0, sf>>>(r, b->part);
-    CCT_CUDA(cudaGetLastError());
   }
+  r.first[no_] = (int)sorted.size();
+  r.nout = no_;
+  r.nsplit = (int)b->nsplit;
+  r.n = d.NP * d.KP;
+  a.part = b->part;
+  a.npairs = (int)sorted.size();
+  a.nsplit = (int)b->nsplit;
+  a.kchunk = b->kchunk;
+  a.nu = nu;
+  a.NP = d.NP;
+  a.KP = d.KP;
+  const int bn = bwd_bn(d.KP);
+  a.tiles_n = (int)((d.KP + bn - 1) / bn);
+  const int tiles_m = (int)((d.NP + BBM - 1) / BBM);
+  CCT_TRY(bn == 64 ? launch_bwd_f<64>(a, tiles_m, sf)
+                   : bn == 48 ? launch_bwd_f<48>(a, tiles_m, sf) : launch_bwd_f<32>(a, tiles_m, sf));
+  bwd_f_reduce_kernel<<<dim3(grid_for(r.n) < 64 ? grid_for(r.n) : 64, r.nout), 256, 0, sf>>>(r, b->part);
+  CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
 

@@ -185,11 +185,12 @@ int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const doub
                cudaStream_t s);
 
 // adjoint.cu: device buffers of the backward pass (allocated at the first ccT_backward)
+constexpr int kGXSets = 4;  // backward: GX sets, two dE-GEMM tuple pairs in flight
 struct AdjBuffers {
   bool ready = false;
   double *dE = nullptr, *dF = nullptr;                 // gradients of the GEMM operands E, F
   double *Wf = nullptr, *GW = nullptr;                 // dense nu^3: W, dE/dW (degenerate tuples)
-  double *GX[2][3] = {};                               // dE/dX_g, nu^2 x NP each, two tuples in flight
+  double *GX[kGXSets][3] = {};                         // dE/dX_g, nu^2 x NP each, kGXSets tuples in flight
   double *part = nullptr;                              // split-K partials of the dF GEMMs
   int64_t nsplit = 0, kchunk = 0;                      // splits of nu^2, rows per split
   double *Q = nullptr;                                 // 9 nu^2 VOE combinations of dE/dW
@@ -207,8 +208,11 @@ int adj_zero(const Dims &d, AdjBuffers *b, cudaStream_t s);
 // set `set`), then the backward GEMMs reading that GX set.
 int adj_tuple_pointwise(const Dims &d, const Tuple &t, double *const X[3], const double *eh, const double *ep,
                         const double *t1, const double *voe, AdjBuffers *b, int set, cudaStream_t s);
-int adj_tuple_gemms(const Dims &d, const Tuple &t, const double *E, const double *F, AdjBuffers *b, int set,
-                    cudaStream_t s_e, cudaStream_t s_f);  // dE GEMM on s_e, dF GEMM + reduction on s_f
+// dE GEMM of one tuple or of two consecutive tuples (GX sets sets[0..ntup-1])
+// in one launch, on s; dF GEMM + its split-K sum of one tuple, on s.
+int adj_tuple_gemm_e(const Dims &d, const Tuple *t, const int *sets, int ntup, const double *F, AdjBuffers *b,
+                     cudaStream_t s);
+int adj_tuple_gemm_f(const Dims &d, const Tuple &t, const double *E, AdjBuffers *b, int set, cudaStream_t s);
 int adj_finish(const Dims &d, const double *v1, AdjBuffers *b, cudaStream_t s);
 
 // peak.cu

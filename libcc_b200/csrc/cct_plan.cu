@@ -86,6 +86,8 @@ struct ccT_plan {
   cudaStream_t bwd_stream = nullptr;   // the dF GEMMs of the backward
   cudaStream_t rec_stream = nullptr;   // the W recompute of the backward
   cudaEvent_t ev_bwdf[2] = {};
+  // backward, per GX set: pointwise pass done / dE GEMM done / dF GEMM done reading it
+  cudaEvent_t ev_gx_pw[kGXSets] = {}, ev_gx_e[kGXSets] = {}, ev_gx_f[kGXSets] = {};
   cudaEvent_t ev_rec[kNBuf] = {}, ev_pw[kNBuf] = {};  // X buffer b: W rebuilt / read by the pointwise pass
   int64_t fwd_begin = -1, fwd_end = -1;
   float last_bwd_ms = 0.f;
@@ -592,6 +594,9 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     CCT_CUDA(cudaStreamCreateWithFlags(&p->bwd_stream, cudaStreamNonBlocking));
     CCT_CUDA(cudaStreamCreateWithFlags(&p->rec_stream, cudaStreamNonBlocking));
     for (cudaEvent_t &e : p->ev_bwdf) CCT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (int g = 0; g < kGXSets; g++)
+      for (cudaEvent_t *e : {&p->ev_gx_pw[g], &p->ev_gx_e[g], &p->ev_gx_f[g]})
+        CCT_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     for (int b = 0; b < kNBuf; b++) {
       CCT_CUDA(cudaEventCreateWithFlags(&p->ev_rec[b], cudaEventDisableTiming));
       CCT_CUDA(cudaEventCreateWithFlags(&p->ev_pw[b], cudaEventDisableTiming));
@@ -604,26 +609,28 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   if (p->emulated) CCT_CUDA(cudaMemsetAsync(p->adj.v1, 0, (5 + (size_t)d.nu * d.no) * 8, p->stream));
   // Four streams.  rec_stream rebuilds W of tuple t into X buffer t mod 3,
   // ahead of red_stream, which runs the pointwise adjoint kernels of tuple t
-  // (dE/dW, dVOE, deps and dE/dX into GX set t mod 2); then gemm_stream runs
-  // the dE GEMM and bwd_stream the dF GEMM of tuple t.  So the latency-bound
-  // pointwise chain of tuple t overlaps the GEMMs of t-1 and the recompute of
-  // t+1.  Every accumulator is written by one stream only, in tuple order, so
-  // the results stay bitwise reproducible.
+  // (dE/dW, dVOE, deps and dE/dX into GX set t mod 4); bwd_stream then runs
+  // the dF GEMM of tuple t, and gemm_stream one dE GEMM for each pair of
+  // consecutive tuples (twice the K per output slab, one read-modify-write of
+  // dE per pair).  So the latency-bound pointwise chain overlaps the GEMMs of
+  // earlier tuples and the recompute of later ones.  Every accumulator is
+  // written by one stream only, in tuple order, so the results stay bitwise
+  // reproducible.
   CCT_TRY(fork_streams(p));
   cudaStream_t sW = p->rec_stream, sP = p->red_stream, sG = p->gemm_stream, sF = p->bwd_stream;
   CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_fork, 0));
   CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_fork, 0));
   for (int64_t t = begin; t < end; t++) {
     const Tuple &tu = p->tuples[t];
-    const int set = (int)((t - begin) & 1);
+    const int set = (int)((t - begin) % kGXSets);
     const int xb = (int)((t - begin) % kNBuf);
     if (t - begin >= kNBuf) CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_pw[xb], 0));  // X buffer read by t-3
     CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2, sW));
     CCT_CUDA(cudaEventRecord(p->ev_rec[xb], sW));
     CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_rec[xb], 0));
-    if (t - begin >= 2) {  // GX set read by the GEMMs of t-2
-      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gemm[set], 0));
-      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_bwdf[set], 0));
+    if (t - begin >= kGXSets) {  // GX set read by the GEMMs of t-4
+      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gx_e[set], 0));
+      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gx_f[set], 0));
     }
     CCT_TRY(adj_tuple_pointwise(d, tu, p->X[xb], p->eh, p->ep, p->t1, p->voe, &p->adj, set, sP));
     if (p->emulated) {
@@ -640,12 +647,21 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
       CCT_TRY(launch_finalize(d, td, p->xpart, p->vpart, p->adj.v1, p->adj.v1 + 5, sP));
     }
     CCT_CUDA(cudaEventRecord(p->ev_pw[xb], sP));
-    CCT_CUDA(cudaEventRecord(p->ev_red[set], sP));
-    CCT_CUDA(cudaStreamWaitEvent(sG, p->ev_red[set], 0));
-    CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_red[set], 0));
-    CCT_TRY(adj_tuple_gemms(d, tu, p->E, p->F, &p->adj, set, sG, sF));
-    CCT_CUDA(cudaEventRecord(p->ev_gemm[set], sG));
-    CCT_CUDA(cudaEventRecord(p->ev_bwdf[set], sF));
+    CCT_CUDA(cudaEventRecord(p->ev_gx_pw[set], sP));
+    CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_gx_pw[set], 0));
+    CCT_TRY(adj_tuple_gemm_f(d, tu, p->E, &p->adj, set, sF));
+    CCT_CUDA(cudaEventRecord(p->ev_gx_f[set], sF));
+    const bool second = ((t - begin) & 1) == 1;
+    if (second || t == end - 1) {  // the dE GEMM of the pair (t-1, t), or of a last lone tuple
+      CCT_CUDA(cudaStreamWaitEvent(sG, p->ev_gx_pw[set], 0));  // also covers t-1: same stream, earlier
+      const int prev = (set + kGXSets - 1) % kGXSets;
+      const Tuple pair[2] = {second ? p->tuples[t - 1] : tu, tu};
+      const int sets[2] = {second ? prev : set, set};
+      CCT_TRY(second ? adj_tuple_gemm_e(d, pair, sets, 2, p->F, &p->adj, sG)
+                     : adj_tuple_gemm_e(d, &tu, &set, 1, p->F, &p->adj, sG));
+      CCT_CUDA(cudaEventRecord(p->ev_gx_e[set], sG));
+      if (second) CCT_CUDA(cudaEventRecord(p->ev_gx_e[prev], sG));
+    }
   }
   // p->stream after every stream (red_stream already waited for rec_stream)
   CCT_CUDA(cudaEventRecord(p->ev_join, sP));
@@ -797,6 +813,9 @@ int ccT_plan_destroy(ccT_plan *p) {
     if (p->ev_rec[b]) cudaEventDestroy(p->ev_rec[b]);
     if (p->ev_pw[b]) cudaEventDestroy(p->ev_pw[b]);
   }
+  for (int g = 0; g < kGXSets; g++)
+    for (cudaEvent_t e : {p->ev_gx_pw[g], p->ev_gx_e[g], p->ev_gx_f[g]})
+      if (e) cudaEventDestroy(e);
   if (p->red_stream) cudaStreamDestroy(p->red_stream);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
   delete p;
