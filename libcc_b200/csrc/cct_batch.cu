@@ -29,7 +29,7 @@
 // cp.async.cg), never through the incoherent L1.
 //
 // A second executor (mode 1) runs the same items as grouped launches: per
-// tuple group, one launch of 128-row W-build tiles (two CTAs per SM) on one
+// tuple group, one launch of 128-row W-build tiles (three CTAs per SM) on one
 // stream, then one launch of its reduction blocks (two CTAs per SM, the last
 // block of a tuple finalizing it) on a second stream, the ring slots guarded
 // by stream events instead of counters.  Either forward (counter reset plus the
@@ -265,10 +265,10 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
 }
 
 // ---- grouped executor: per tuple group, one launch of W-build tiles (128-row
-// tiles, two CTAs per SM) and one launch of reduction blocks (several CTAs per
+// tiles, three CTAs per SM) and one launch of reduction blocks (several CTAs per
 // SM); ordering between the launches comes from the stream, so no item waits.
 template <int BN>
-__global__ void __launch_bounds__(wb::NT, 2) batch_wb_kernel(const BatchArgs A, int64_t item0) {
+__global__ void __launch_bounds__(wb::NT, 3) batch_wb_kernel(const BatchArgs A, int64_t item0) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int4 it = A.items[item0 + blockIdx.x];
   const TupleRec &T = A.tuples[it.y];

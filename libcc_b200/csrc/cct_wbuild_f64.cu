@@ -15,8 +15,8 @@
 // Kernel: one CTA per 128 x BN output tile of one job (BN in {32..64}, chosen
 // per system so nu needs little padding); 4 warps stacked along M, each
 // 32 x BN; mma.sync.m16n8k4.f64; a 3-stage cp.async ring of 128x16 / BNx16
-// tiles with 16-byte-aligned rows padded to 20 doubles (conflict-free
-// fragment loads); two CTAs per SM.
+// tiles in unpadded, XOR-swizzled rows (conflict-free fragment loads); three
+// CTAs per SM.
 #include "cct_wbuild_tile.cuh"
 
 namespace cct {
@@ -25,7 +25,7 @@ namespace {
 using namespace wb;
 
 template <int BN>
-__global__ void __launch_bounds__(NT, 2) wbuild_f64_kernel(const GemmJob *__restrict__ jobs, int nu, int64_t KP,
+__global__ void __launch_bounds__(NT, 3) wbuild_f64_kernel(const GemmJob *__restrict__ jobs, int nu, int64_t KP,
                                                            int64_t NP, int tiles_n) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tile_m = blockIdx.x / tiles_n, tile_n = blockIdx.x - tile_m * tiles_n;

@@ -12,7 +12,12 @@ constexpr int WM = 32;
 constexpr int NWARP = BM / WM;
 constexpr int NT = NWARP * 32;
 constexpr int STAGES = 3;
-constexpr int LDS = BK + 4;  // padded smem row (doubles)
+// Shared tiles are unpadded (16 doubles a row) with column c of row r stored
+// at c ^ 4 (r & 3): the 64-bit fragment loads of a half-warp (rows g = 0..3,
+// columns t = 0..3) then hit four disjoint 32-byte bank groups, and a CTA
+// needs 64-75 KB, so three fit on an SM.
+constexpr int LDS = BK;
+__device__ __forceinline__ int swz(int r, int c) { return r * LDS + (c ^ ((r & 3) << 2)); }
 constexpr int MF = WM / 16;
 
 template <int BN, int TM = BM>
@@ -84,12 +89,12 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
     for (int rr = tid >> 3; rr < BM; rr += NT / 8) {
       const int ro = rowoff[h * BM + rr];
       const double *src = abase + (ro < 0 ? 0 : (int64_t)ro * KP) + k0 + chunk * 2;
-      cp_async16(as + rr * LDS + chunk * 2, src, ro < 0 ? 0 : 16);
+      cp_async16(as + swz(rr, chunk * 2), src, ro < 0 ? 0 : 16);
     }
 #pragma unroll
     for (int rr = tid >> 3; rr < BN; rr += NT / 8) {
       const double *src = bbase + (int64_t)(n0 + rr) * KP + k0 + chunk * 2;
-      cp_async16(bs + rr * LDS + chunk * 2, src, 16);
+      cp_async16(bs + swz(rr, chunk * 2), src, 16);
     }
   };
 
@@ -125,11 +130,11 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
       double af[MF][2], bf[NF];
 #pragma unroll
       for (int i = 0; i < MF; i++) {
-        af[i][0] = as[(i * 16 + g) * LDS + kk + t];
-        af[i][1] = as[(i * 16 + g + 8) * LDS + kk + t];
+        af[i][0] = as[swz(i * 16 + g, kk + t)];
+        af[i][1] = as[swz(i * 16 + g + 8, kk + t)];
       }
 #pragma unroll
-      for (int j = 0; j < NF; j++) bf[j] = bs[(j * 8 + g) * LDS + kk + t];
+      for (int j = 0; j < NF; j++) bf[j] = bs[swz(j * 8 + g, kk + t)];
 #pragma unroll
       for (int i = 0; i < MF; i++)
 #pragma unroll
