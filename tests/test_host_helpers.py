@@ -1,0 +1,43 @@
+"""Host-side helpers that need no GPU: the decaying-magnitude synthetic systems
+and the traffic figures bench.py reads from the committed ncu summaries."""
+import importlib.util
+import pathlib
+
+import numpy as np
+
+from libcc_b200 import synthetic as S
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def test_with_decay_scales_each_virtual_index():
+    no, nu, f = 3, 10, 0.75
+    inp = S.generate(no, nu, 1)
+    d = S.with_decay(inp, f)
+    g = 2.0 ** (-f * np.arange(nu))
+    # T2(a,b,i,j) at a + nu*(b + nu*(i + no*j)); VM(l,c,x,y) at l + no*(c + nu*(x + no*y))
+    for a, b, i, j in [(0, 0, 0, 0), (3, 5, 1, 2), (9, 2, 2, 0)]:
+        idx = a + nu * (b + nu * (i + no * j))
+        assert np.isclose(d.t2[idx], inp.t2[idx] * g[a] * g[b], rtol=1e-15, atol=0)
+        assert np.isclose(d.voe[idx], inp.voe[idx] * g[a] * g[b], rtol=1e-15, atol=0)
+    for l, c, x, y in [(0, 4, 1, 2), (2, 9, 0, 0)]:
+        idx = l + no * (c + nu * (x + no * y))
+        assert np.isclose(d.vm[idx], inp.vm[idx] * g[c], rtol=1e-15, atol=0)
+    ntr = nu * (nu + 1) // 2
+    for x, r1, I, J in [(2, 4, 7, 3), (0, 0, 0, 0), (1, 9, 9, 9)]:
+        k = (x * nu + r1) * ntr + I * (I + 1) // 2 + J
+        assert np.isclose(d.vvvo[k], inp.vvvo[k] * g[r1] * g[I] * g[J], rtol=1e-15, atol=0)
+    assert np.array_equal(d.eh, inp.eh) and np.array_equal(d.ep, inp.ep)
+    z = S.with_decay(inp, 0.0)
+    for name in ("t1", "t2", "vm", "voe", "vvvo"):
+        assert np.array_equal(getattr(z, name), getattr(inp, name)), name
+
+
+def test_bench_reads_traffic_from_the_committed_summaries():
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for kind in ("f64", "emu"):
+        t = bench.read_traffic("no24-nu320", kind)
+        assert t is not None and 1e9 < t < 5e9, (kind, t)
+    assert bench.read_traffic("no-such-workload", "f64") is None
