@@ -51,6 +51,14 @@ constexpr int VPAIR = 2 * 6 * 64;
 __device__ __forceinline__ int nb_of(int nu) { return (nu + RB - 1) / RB; }
 constexpr int REDUCE_SMEM = (6 * SL + 3 * VPAIR) * 8;
 
+// 8-byte global->shared copy that does not wait; ok == false stores 0.0.
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool ok) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(ok ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // One CTA per unordered block triple {A<=B<=C}.  Phase A assembles W on every
 // distinct ordered block of the orbit in shared memory (term by term, fixed
 // order).  Phase B: each thread evaluates orbits -- the six index permutations
@@ -85,17 +93,51 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
         slot[p] = q;
   }
 
-  // ---- phase A: W on the orbit blocks, one X term at a time
+  // ---- VOE staging: asynchronous copies, in flight during phase A's X loads
+  {
+    const int64_t nu2 = (int64_t)nu * nu;
+#pragma unroll
+    for (int it = 0; it < 3 * VPAIR / RT; it++) {
+      const int q = tid + RT * it;
+      const int pr = q / VPAIR, orient = (q / 384) & 1, plane = (q / 64) % 6, r = q & 63;
+      const int Blo = pr == 0 ? S1 : S0, Bhi = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
+      const int f = RB * (orient ? Bhi : Blo) + (r & 7), s2 = RB * (orient ? Blo : Bhi) + (r >> 3);
+      const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
+      const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
+      const bool ok = f < nu && s2 < nu;
+      cp_async8(Vsm + q, voe + (ok ? ((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2 : 0), ok);
+    }
+    cp_async_commit();
+  }
+
+  // ---- phase A: W on the orbit blocks, one X term at a time.  Term 0 (the
+  // identity placement X0(a,b,c) for every kind) is copied straight into W
+  // asynchronously, unless X is being written by other CTAs of this kernel.
 #pragma unroll
   for (int term = 0; term < NTERM; term++) {
-    constexpr int dummy = 0;
-    (void)dummy;
     const int g = term_entry(KIND, term, 0);
     const int al0 = term_entry(KIND, term, 1), al1 = term_entry(KIND, term, 2), al2 = term_entry(KIND, term, 3);
     const double *X = t.x[0];
     if (g == 1) X = t.x[1];
     if (g == 2) X = t.x[2];
-    double xv[6][2];
+    if (!COHERENT && term == 0) {
+#pragma unroll
+      for (int p = 0; p < 6; p++) {
+        if (slot[p] != p) continue;
+        const int O0 = Sm(pm(p, 0)), O1 = Sm(pm(p, 1)), O2 = Sm(pm(p, 2));
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int idx = tid + RT * e;
+          const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
+          const int xp = RB * O0 + u0, xq = RB * O1 + u1, xs = RB * O2 + u2;
+          const bool ok = xp < nu && xq < nu && xs < nu;
+          cp_async8(Wsm + p * SL + soff(u0, u1, u2), X + (ok ? ((int64_t)xp * nu + xq) * NP + xs : 0), ok);
+        }
+      }
+      cp_async_commit();
+      continue;
+    }
+    double xv[12];  // [6 blocks][2 elements], flat: the compiler kept a 2-D array in local memory
 #pragma unroll
     for (int p = 0; p < 6; p++) {
       const bool live = slot[p] == p;
@@ -111,8 +153,12 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
           const double *src = X + ((int64_t)xp * nu + xq) * NP + xs;
           v = COHERENT ? __ldcg(src) : __ldg(src);
         }
-        xv[p][e] = v;
+        xv[2 * p + e] = v;
       }
+    }
+    if (!COHERENT && term == 1) {
+      cp_async_wait_all();  // term 0 is in W
+      __syncthreads();
     }
 #pragma unroll
     for (int p = 0; p < 6; p++) {
@@ -124,26 +170,14 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
         const int so = u0 * kstride(al0) + u1 * kstride(al1) + u2 * kstride(al2);
         double *w = Wsm + p * SL + so;
         if (term == 0)
-          *w = xv[p][e];
+          *w = xv[2 * p + e];
         else
-          *w += xv[p][e];
+          *w += xv[2 * p + e];
       }
     }
     __syncthreads();
   }
-  {
-    const int64_t nu2 = (int64_t)nu * nu;
-    for (int q = tid; q < 3 * VPAIR; q += RT) {
-      const int pr = q / VPAIR, orient = (q / 384) & 1, plane = (q / 64) % 6, r = q & 63;
-      const int Blo = pr == 0 ? S1 : S0, Bhi = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
-      const int f = RB * (orient ? Bhi : Blo) + (r & 7), s2 = RB * (orient ? Blo : Bhi) + (r >> 3);
-      const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
-      const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
-      double v = 0.0;
-      if (f < nu && s2 < nu) v = voe[((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2];
-      Vsm[q] = v;
-    }
-  }
+  cp_async_wait_all();  // VOE staging (and term 0 when it went asynchronously)
   if (S0 == S1 && S1 == S2 && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;  // W_aaa = 0 (ZEROT3)
   __syncthreads();
 
