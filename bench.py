@@ -462,19 +462,21 @@ def main():
         # three whole runs (plan, uploads, operand build, all tuples, teardown);
         # the median is reported: the host side (large allocations, pinned
         # copies) varies by a few tenths of a second from run to run
-        runs = []
+        runs, dev_runs = [], []
         for _ in range(3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             with make_plan(A, no, nu, local, emu_form) as p2:
                 p2.set_inputs(*pinned)
                 r = shard.sharded_cc_triples(p2)
+                dev_runs.append(p2.last_forward_ms * 1e-3)
             e2e_e = r[0] + r[1]
             torch.cuda.synchronize()
             runs.append(allreduce([time.perf_counter() - t0], op="max")[0])
         e2e_s = statistics.median(runs)
         e2e = {"value": flop_step / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "seconds_per_run": runs, "steps": 1,
+               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "seconds_per_run": runs,
+               "forward_device_seconds_per_run": dev_runs, "steps": 1,
                "form": emu_form,
                "path": "ccT_plan_create/ccT_set_inputs(host)/ccT_forward/ccT_plan_destroy (C ABI), pinned inputs"
                        + (" + NCCL all-reduce of the shard energies" if world > 1 else ""),

@@ -24,6 +24,7 @@
 // adjoint of cct_layout.cu.  All sums run in a fixed order (no floating-point
 // atomics): gradients are bitwise reproducible.
 #include <algorithm>
+#include <type_traits>
 
 #include "cct_internal.cuh"
 
@@ -520,6 +521,7 @@ struct BwdEArgs {
   int first[7], npairs;  // pairs of output o are first[o] .. first[o+1]-1
   int nu;
   int64_t NP, KP;
+  int64_t KV;  // columns that are not padding: nu + no
   int tiles_n;
 };
 
@@ -538,6 +540,7 @@ __global__ void __launch_bounds__(BNT, BN == 64 ? 2 : 3) bwd_e_kernel(const BwdE
   const int64_t M = (int64_t)nu * nu, NP = args.NP, KP = args.KP;
   const int64_t m0 = (int64_t)tile_m * BBM;
   const int n0 = tile_n * BBN;
+  const bool full = n0 + BBN - 8 < args.KV;
   const int tid = threadIdx.x;
   const int p_begin = args.first[o], p_end = args.first[o + 1];
   const int kt_per = (int)((NP + BBK - 1) / BBK);  // NP is a multiple of 8, not always of 16
@@ -606,41 +609,50 @@ __global__ void __launch_bounds__(BNT, BN == 64 ? 2 : 3) bwd_e_kernel(const BwdE
     if (s < ktiles) load_stage(s, s);
     cp_async_commit();
   }
-  for (int kt = 0; kt < ktiles; kt++) {
-    cp_async_wait<BST - 2>();
-    __syncthreads();
-    {
-      const int nk = kt + BST - 1;
-      if (nk < ktiles) load_stage(nk % BST, nk);
-      cp_async_commit();
-    }
-    const double *as = As + (kt % BST) * BBM * BBK;
-    const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
-    // NP is a multiple of 8: the last k-tile of a pair may hold only 8 columns
-    const bool half_tile = NP - (int64_t)(kt % kt_per) * BBK <= BBK / 2;
-#pragma unroll
-    for (int kk = 0; kk < BBK; kk += 8) {
-      if (kk >= BBK / 2 && half_tile) break;
-      double af[MF][4], bf[NF][2];
-#pragma unroll
-      for (int i = 0; i < MF; i++) {
-        const int r = warp * BWM + i * 16 + g;
-        af[i][0] = as[aswz(r, kk + t)];
-        af[i][1] = as[aswz(r + 8, kk + t)];
-        af[i][2] = as[aswz(r, kk + 4 + t)];
-        af[i][3] = as[aswz(r + 8, kk + 4 + t)];
+  // NFR: n8 fragments computed; the tile's last one is skipped when all its
+  // columns are padding (>= nu + no)
+  auto mainloop = [&](auto nfr_c) {
+    constexpr int NFR = decltype(nfr_c)::value;
+    for (int kt = 0; kt < ktiles; kt++) {
+      cp_async_wait<BST - 2>();
+      __syncthreads();
+      {
+        const int nk = kt + BST - 1;
+        if (nk < ktiles) load_stage(nk % BST, nk);
+        cp_async_commit();
       }
+      const double *as = As + (kt % BST) * BBM * BBK;
+      const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
+      // NP is a multiple of 8: the last k-tile of a pair may hold only 8 columns
+      const bool half_tile = NP - (int64_t)(kt % kt_per) * BBK <= BBK / 2;
 #pragma unroll
-      for (int j = 0; j < NF; j++) {
-        bf[j][0] = bs[(kk + t) * LDB_KN + j * 8 + g];
-        bf[j][1] = bs[(kk + 4 + t) * LDB_KN + j * 8 + g];
+      for (int kk = 0; kk < BBK; kk += 8) {
+        if (kk >= BBK / 2 && half_tile) break;
+        double af[MF][4], bf[NF][2];
+#pragma unroll
+        for (int i = 0; i < MF; i++) {
+          const int r = warp * BWM + i * 16 + g;
+          af[i][0] = as[aswz(r, kk + t)];
+          af[i][1] = as[aswz(r + 8, kk + t)];
+          af[i][2] = as[aswz(r, kk + 4 + t)];
+          af[i][3] = as[aswz(r + 8, kk + 4 + t)];
+        }
+#pragma unroll
+        for (int j = 0; j < NFR; j++) {
+          bf[j][0] = bs[(kk + t) * LDB_KN + j * 8 + g];
+          bf[j][1] = bs[(kk + 4 + t) * LDB_KN + j * 8 + g];
+        }
+#pragma unroll
+        for (int i = 0; i < MF; i++)
+#pragma unroll
+          for (int j = 0; j < NFR; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
       }
-#pragma unroll
-      for (int i = 0; i < MF; i++)
-#pragma unroll
-        for (int j = 0; j < NF; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
     }
-  }
+  };
+  if (full)
+    mainloop(std::integral_constant<int, NF>{});
+  else
+    mainloop(std::integral_constant<int, NF - 1>{});
   cp_async_wait<0>();
 #pragma unroll
   for (int i = 0; i < MF; i++) {
@@ -666,6 +678,7 @@ struct BwdFArgs {
   int64_t kchunk;   // rows of nu^2 per split (multiple of BBK)
   int nu;
   int64_t NP, KP;
+  int64_t KV;       // columns that are not padding: nu + no
   int tiles_n;
 };
 
@@ -684,6 +697,7 @@ __global__ void __launch_bounds__(BNT, BN == 64 ? 2 : 3) bwd_f_kernel(const BwdF
   const int64_t Mtot = (int64_t)nu * nu, NP = args.NP, KP = args.KP;
   const int64_t s0 = (int64_t)tile_m * BBM;
   const int n0 = tile_n * BBN;
+  const bool full = n0 + BBN - 8 < args.KV;  // else the last n8 fragment is all padding
   const int64_t kbeg = (int64_t)split * args.kchunk;
   const int64_t kend = min(kbeg + args.kchunk, Mtot);
   const int ktiles = kend > kbeg ? (int)((kend - kbeg + BBK - 1) / BBK) : 0;
@@ -728,37 +742,44 @@ __global__ void __launch_bounds__(BNT, BN == 64 ? 2 : 3) bwd_f_kernel(const BwdF
     if (s < ktiles) load_stage(s, s);
     cp_async_commit();
   }
-  for (int kt = 0; kt < ktiles; kt++) {
-    cp_async_wait<BST - 2>();
-    __syncthreads();
-    {
-      const int nk = kt + BST - 1;
-      if (nk < ktiles) load_stage(nk % BST, nk);
-      cp_async_commit();
-    }
-    const double *as = As + (kt % BST) * BBK * LDA_KM + warp * BWM;
-    const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
-#pragma unroll
-    for (int kk = 0; kk < BBK; kk += 8) {
-      double af[MF][4], bf[NF][2];
-#pragma unroll
-      for (int i = 0; i < MF; i++) {
-        af[i][0] = as[(kk + t) * LDA_KM + i * 16 + g];
-        af[i][1] = as[(kk + t) * LDA_KM + i * 16 + g + 8];
-        af[i][2] = as[(kk + 4 + t) * LDA_KM + i * 16 + g];
-        af[i][3] = as[(kk + 4 + t) * LDA_KM + i * 16 + g + 8];
+  auto mainloop = [&](auto nfr_c) {  // NFR n8 fragments, as in bwd_e_kernel
+    constexpr int NFR = decltype(nfr_c)::value;
+    for (int kt = 0; kt < ktiles; kt++) {
+      cp_async_wait<BST - 2>();
+      __syncthreads();
+      {
+        const int nk = kt + BST - 1;
+        if (nk < ktiles) load_stage(nk % BST, nk);
+        cp_async_commit();
       }
+      const double *as = As + (kt % BST) * BBK * LDA_KM + warp * BWM;
+      const double *bs = Bs + (kt % BST) * BBK * LDB_KN;
 #pragma unroll
-      for (int j = 0; j < NF; j++) {
-        bf[j][0] = bs[(kk + t) * LDB_KN + j * 8 + g];
-        bf[j][1] = bs[(kk + 4 + t) * LDB_KN + j * 8 + g];
+      for (int kk = 0; kk < BBK; kk += 8) {
+        double af[MF][4], bf[NF][2];
+#pragma unroll
+        for (int i = 0; i < MF; i++) {
+          af[i][0] = as[(kk + t) * LDA_KM + i * 16 + g];
+          af[i][1] = as[(kk + t) * LDA_KM + i * 16 + g + 8];
+          af[i][2] = as[(kk + 4 + t) * LDA_KM + i * 16 + g];
+          af[i][3] = as[(kk + 4 + t) * LDA_KM + i * 16 + g + 8];
+        }
+#pragma unroll
+        for (int j = 0; j < NFR; j++) {
+          bf[j][0] = bs[(kk + t) * LDB_KN + j * 8 + g];
+          bf[j][1] = bs[(kk + 4 + t) * LDB_KN + j * 8 + g];
+        }
+#pragma unroll
+        for (int i = 0; i < MF; i++)
+#pragma unroll
+          for (int j = 0; j < NFR; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
       }
-#pragma unroll
-      for (int i = 0; i < MF; i++)
-#pragma unroll
-        for (int j = 0; j < NF; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
     }
-  }
+  };
+  if (full)
+    mainloop(std::integral_constant<int, NF>{});
+  else
+    mainloop(std::integral_constant<int, NF - 1>{});
   cp_async_wait<0>();
   double *out = args.part + ((int64_t)pi * args.nsplit + split) * NP * KP;
 #pragma unroll
@@ -1130,6 +1151,7 @@ int adj_tuple_gemm_e(const Dims &d, const Tuple *tu, const int *sets, int ntup, 
   a.nu = nu;
   a.NP = d.NP;
   a.KP = d.KP;
+  a.KV = d.nu + d.no;
   const int bn = bwd_bn(d.KP);
   a.tiles_n = (int)((d.KP + bn - 1) / bn);
   const int tiles_m = (int)((nu2 + BBM - 1) / BBM);
@@ -1168,6 +1190,7 @@ int adj_tuple_gemm_f(const Dims &d, const Tuple &t, const double *E, AdjBuffers 
   a.nu = nu;
   a.NP = d.NP;
   a.KP = d.KP;
+  a.KV = d.nu + d.no;
   const int bn = bwd_bn(d.KP);
   a.tiles_n = (int)((d.KP + bn - 1) / bn);
   const int tiles_m = (int)((d.NP + BBM - 1) / BBM);

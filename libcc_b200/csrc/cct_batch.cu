@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
         spin_until(group_rd + (T.group - kRing), A.group_rd_items[T.group - kRing], A.err);
       __syncthreads();
       const int tile_m = it.w / S.tiles_n, tile_n = it.w - tile_m * S.tiles_n;
-      wb::wbuild_tile<BN, kBTM>(A.jobs[(int64_t)t * 3 + it.z], S.nu, S.KP, S.NP, tile_m, tile_n, smem);
+      wb::wbuild_tile<BN, kBTM>(A.jobs[(int64_t)t * 3 + it.z], S.nu, S.KP, S.nu + S.no, S.NP, tile_m, tile_n, smem);
       __threadfence();
       __syncthreads();
       if (threadIdx.x == 0) atomicAdd(wb_done + t, 1);
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(wb::NT, 3) batch_wb_kernel(const BatchArgs A, 
   const TupleRec &T = A.tuples[it.y];
   const SysDev &S = A.sys[T.sys];
   const int tile_m = it.w / S.tiles_n, tile_n = it.w - tile_m * S.tiles_n;
-  wb::wbuild_tile<BN, wb::BM>(A.jobs[(int64_t)it.y * 3 + it.z], S.nu, S.KP, S.NP, tile_m, tile_n, smem);
+  wb::wbuild_tile<BN, wb::BM>(A.jobs[(int64_t)it.y * 3 + it.z], S.nu, S.KP, S.nu + S.no, S.NP, tile_m, tile_n, smem);
 }
 
 __global__ void __launch_bounds__(kBT, 2) batch_rd_kernel(const BatchArgs A, int64_t item0) {

@@ -26,10 +26,10 @@ using namespace wb;
 
 template <int BN>
 __global__ void __launch_bounds__(NT, 3) wbuild_f64_kernel(const GemmJob *__restrict__ jobs, int nu, int64_t KP,
-                                                           int64_t NP, int tiles_n) {
+                                                           int64_t KV, int64_t NP, int tiles_n) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tile_m = blockIdx.x / tiles_n, tile_n = blockIdx.x - tile_m * tiles_n;
-  wbuild_tile<BN>(jobs[blockIdx.y], nu, KP, NP, tile_m, tile_n, smem_raw);
+  wbuild_tile<BN>(jobs[blockIdx.y], nu, KP, KV, NP, tile_m, tile_n, smem_raw);
 }
 
 template <int BN>
@@ -46,7 +46,7 @@ int launch_bn(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStream_t s)
   const int tiles_m = (int)((M + BM - 1) / BM);
   const int tiles_n = (int)(d.NP / BN);
   dim3 grid(tiles_m * tiles_n, njobs);
-  wbuild_f64_kernel<BN><<<grid, NT, smem, s>>>(jobs_dev, d.nu, d.KP, d.NP, tiles_n);
+  wbuild_f64_kernel<BN><<<grid, NT, smem, s>>>(jobs_dev, d.nu, d.KP, d.nu + d.no, d.NP, tiles_n);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }

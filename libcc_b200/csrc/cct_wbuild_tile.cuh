@@ -43,12 +43,14 @@ __device__ __forceinline__ void dmma_16x8x4(double *d, double a0, double a1, dou
 }
 
 // One TM x BN output tile (tile_m, tile_n) of one W-build GEMM job, TM/32
-// warps of 32 rows each; every thread of the TM-thread CTA calls it.  smem_raw
-// holds smem_bytes<BN, TM>().  It starts with a barrier, so a persistent CTA
-// can call it for consecutive tiles on the same shared memory.
+// warps of 32 rows each; every thread of the TM-thread CTA calls it.  Each
+// KP-long half of the contraction holds KV = nu + no columns and zero
+// padding, whose k4 steps are skipped.  smem_raw holds smem_bytes<BN, TM>().
+// It starts with a barrier, so a persistent CTA can call it for consecutive
+// tiles on the same shared memory.
 template <int BN, int TM = BM>
-__device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t KP, int64_t NP, int tile_m,
-                                            int tile_n, unsigned char *smem_raw) {
+__device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t KP, int64_t KV, int64_t NP,
+                                            int tile_m, int tile_n, unsigned char *smem_raw) {
   constexpr int BM = TM, NT = TM;
   constexpr int NF = BN / 8;
   double *As = reinterpret_cast<double *>(smem_raw);
@@ -125,8 +127,11 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
     }
     const double *as = As + (kt % STAGES) * BM * LDS + (warp * WM) * LDS;
     const double *bs = Bs + (kt % STAGES) * BN * LDS;
+    // columns of this k-tile below nu + no; the k4 steps past them multiply zero padding
+    const int64_t kv = KV - (int64_t)(kt < ktiles_half ? kt : kt - ktiles_half) * BK;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
+      if (kk >= kv) break;
       double af[MF][2], bf[NF];
 #pragma unroll
       for (int i = 0; i < MF; i++) {
