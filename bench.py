@@ -462,21 +462,27 @@ def main():
         # three whole runs (plan, uploads, operand build, all tuples, teardown);
         # the median is reported: the host side (large allocations, pinned
         # copies) varies by a few tenths of a second from run to run
-        runs, dev_runs = [], []
+        runs, dev_runs, phases = [], [], []
         for _ in range(3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             with make_plan(A, no, nu, local, emu_form) as p2:
+                t1 = time.perf_counter()
                 p2.set_inputs(*pinned)
+                t2 = time.perf_counter()
                 r = shard.sharded_cc_triples(p2)
+                t3 = time.perf_counter()
                 dev_runs.append(p2.last_forward_ms * 1e-3)
             e2e_e = r[0] + r[1]
             torch.cuda.synchronize()
-            runs.append(allreduce([time.perf_counter() - t0], op="max")[0])
+            t4 = time.perf_counter()
+            phases.append({"plan_create": t1 - t0, "set_inputs": t2 - t1, "forward": t3 - t2,
+                           "plan_destroy": t4 - t3})
+            runs.append(allreduce([t4 - t0], op="max")[0])
         e2e_s = statistics.median(runs)
         e2e = {"value": flop_step / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "seconds": e2e_s, "seconds_per_run": runs,
-               "forward_device_seconds_per_run": dev_runs, "steps": 1,
+               "forward_device_seconds_per_run": dev_runs, "host_seconds_per_phase": phases, "steps": 1,
                "form": emu_form,
                "path": "ccT_plan_create/ccT_set_inputs(host)/ccT_forward/ccT_plan_destroy (C ABI), pinned inputs"
                        + (" + NCCL all-reduce of the shard energies" if world > 1 else ""),

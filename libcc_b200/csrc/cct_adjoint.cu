@@ -374,17 +374,32 @@ __global__ void __launch_bounds__(kGwThreads, 3)
 
 // dVOE(b,c,y_m,z_m) += w sum_chunks vpart[chunk][m][c][b], m = 1..6 in order
 // (planes of a degenerate tuple may coincide, so one thread owns all six).
+// The chunks are summed in order; 24 loads (four chunks of all six m) are in
+// flight at a time.
 __global__ void adj_voe_sum_kernel(int nu, int no, int nchunk, AdjTuple t, SmTable sm,
                                    const double *__restrict__ vpart, double *__restrict__ gvoe) {
+  constexpr int U = 4;
   const int64_t nu2 = (int64_t)nu * nu;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu2; e += (int64_t)gridDim.x * blockDim.x) {
     // e = c*nu + b
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int ch = 0;
+    for (; ch + U <= nchunk; ch += U) {
+      double x[6 * U];  // flat: [m][u]
 #pragma unroll
-    for (int m = 0; m < 6; m++) {
-      double v = 0.0;
-      for (int ch = 0; ch < nchunk; ch++) v += vpart[((int64_t)ch * 6 + m) * nu2 + e];
-      gvoe[((int64_t)sm.z[m] * no + sm.y[m]) * nu2 + e] += t.weight * v;
+      for (int m = 0; m < 6; m++)
+#pragma unroll
+        for (int u = 0; u < U; u++) x[m * U + u] = vpart[((int64_t)(ch + u) * 6 + m) * nu2 + e];
+#pragma unroll
+      for (int m = 0; m < 6; m++)
+#pragma unroll
+        for (int u = 0; u < U; u++) v[m] += x[m * U + u];
     }
+    for (; ch < nchunk; ch++)
+#pragma unroll
+      for (int m = 0; m < 6; m++) v[m] += vpart[((int64_t)ch * 6 + m) * nu2 + e];
+#pragma unroll
+    for (int m = 0; m < 6; m++) gvoe[((int64_t)sm.z[m] * no + sm.y[m]) * nu2 + e] += t.weight * v[m];
   }
 }
 
