@@ -26,6 +26,7 @@ import pathlib
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = pathlib.Path(__file__).resolve().parent
@@ -57,7 +58,8 @@ def workload_desc(inp, dist):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples every 200 ms while running."""
+    """nvidia-smi clock/throttle samples every 200 ms while running, into a CSV
+    under $CCT_CLOCKS_DIR (default: the system temporary directory)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -66,7 +68,8 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_bench_{os.getpid()}.csv"
+        out = os.environ.get("CCT_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = pathlib.Path(out) / f"clocks_bench_{os.getpid()}.csv"
 
     def __enter__(self):
         try:
