@@ -1,5 +1,6 @@
 """Host-side helpers that need no GPU: the decaying-magnitude synthetic systems
-and the traffic figures bench.py reads from the committed ncu summaries."""
+the traffic figures bench.py reads from the committed ncu summaries, and its
+clock-sample summary."""
 import importlib.util
 import pathlib
 
@@ -41,3 +42,26 @@ def test_bench_reads_traffic_from_the_committed_summaries():
         t = bench.read_traffic("no24-nu320", kind)
         assert t is not None and 1e9 < t < 5e9, (kind, t)
     assert bench.read_traffic("no-such-workload", "f64") is None
+
+
+def test_clock_summary_reads_loaded_samples_and_reasons(tmp_path, monkeypatch):
+    """The bench's clock evidence: median SM clock over the samples under load
+    (power at least half the maximum), and every throttle reason seen active."""
+    monkeypatch.setenv("CCT_CLOCKS_DIR", str(tmp_path))
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    cs = bench.ClockSampler(0)
+    assert cs.path.parent == tmp_path
+    rows = ["0, 1965, 1965, 150.0, 0x0, Not Active, Not Active, Not Active, Not Active",   # idle: ignored
+            "0, 1750, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1730, 1965, 1001.0, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1760, 1965, 995.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "garbage line"]
+    cs.path.write_text("\n".join(rows) + "\n")
+    cs.proc = object()  # a sampler that ran
+    s = cs.summary()
+    assert s["sm_mhz"] == 1750.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["samples"] == 3 and s["power_w_max"] == 1001.0
+    cs.path.write_text("0, 1500, 1965, 900.0, 0x8, Not Active, Active, Not Active, Not Active\n")
+    assert cs.summary()["reasons"] == ["hw_thermal_slowdown"]
