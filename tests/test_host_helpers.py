@@ -1,4 +1,4 @@
-"""Host-side helpers that need no GPU: the decaying-magnitude synthetic systems
+"""Host-side helpers that need no GPU: the decaying-magnitude synthetic systems,
 the traffic figures bench.py reads from the committed ncu summaries, and its
 clock-sample summary."""
 import importlib.util
