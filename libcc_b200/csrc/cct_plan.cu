@@ -474,8 +474,10 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   const double *vvvo_dev = vvvo;
   double *staged = nullptr;
   if (mem == CCT_MEM_HOST) {
-    // the packed VVVO is only needed to build E; stage it in a transient buffer
-    CCT_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&staged), nvvvo * 8, p->stream));
+    // the packed VVVO is only needed to build E; stage it in a transient
+    // buffer.  Plain cudaMalloc/cudaFree: with the stream-ordered pool this
+    // call took 0.12-0.21 s at no=24/nu=320 (3.2 GB staged), 0.08-0.10 s so.
+    CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&staged), nvvvo * 8));
     CCT_CUDA(cudaMemcpyAsync(staged, vvvo, nvvvo * 8, cudaMemcpyHostToDevice, p->stream));
     vvvo_dev = staged;
   }
@@ -487,7 +489,10 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   if (s == CCT_OK) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
   if (s == CCT_OK && p->emulated) s = emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
-  if (staged) cudaFreeAsync(staged, p->stream);
+  if (staged) {
+    cudaStreamSynchronize(p->stream);  // E is built before the staging buffer goes
+    cudaFree(staged);
+  }
   if (s != CCT_OK) return s;
   p->host_eh.resize(no);
   p->host_ep.resize(nu);
