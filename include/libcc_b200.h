@@ -64,7 +64,10 @@ void ccT_options_default(ccT_options *opt);
 int ccT_plan_create(ccT_plan **plan, int64_t no, int64_t nu, const ccT_options *opt);
 
 /* Load the inputs (reference layouts).  mem = CCT_MEM_HOST copies from host
- * memory, CCT_MEM_DEVICE reads device pointers already in HBM.  Replaces
+ * memory (pinned memory copies fastest), CCT_MEM_DEVICE reads device pointers
+ * already in HBM.  From host memory the packed VVVO passes through a transient
+ * device buffer of its own size, allocated and freed inside the call.  The
+ * call returns once the GEMM operands are built.  Replaces
  * program.F90:195-223 (restart read) plus the DDI put/bcast of T2/VM/VOE/VVVO. */
 int ccT_set_inputs(ccT_plan *plan, const double *eh, const double *ep, const double *t1,
                    const double *t2, const double *vm, const double *voe,
