@@ -103,3 +103,39 @@ class TriplesBatch:
     @property
     def work_items(self) -> int:
         return int(N.load().ccT_batch_work_items(self._h))
+
+
+def main(argv=None) -> int:
+    """``python -m libcc_b200.batch``: the first N systems of the 96-system
+    batched workload through one executor configuration (or the tuner), one
+    untimed and one timed forward; prints the device time and the energies."""
+    import argparse
+    from . import synthetic
+    ap = argparse.ArgumentParser(prog="python -m libcc_b200.batch", description=main.__doc__)
+    ap.add_argument("--systems", type=int, default=96, help="first N systems of the workload (default 96)")
+    ap.add_argument("--mode", type=int, default=1, help="0: one persistent kernel; 1: grouped launches")
+    ap.add_argument("--bn", type=int, default=0, help="W-build N tile, 0 = per system")
+    ap.add_argument("--order", type=int, default=0, help="0: tuples by cost; 1: system by system")
+    ap.add_argument("--group-mib", type=int, default=256, help="X scratch per tuple group, MiB")
+    ap.add_argument("--tune", action="store_true", help="let the tuner pick mode, N tile and order")
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+    systems = synthetic.batch96(args.systems)
+    with TriplesBatch([(s.no, s.nu) for s in systems], device=args.device) as b:
+        for k, s in enumerate(systems):
+            b.set_system(k, s)
+        if args.tune:
+            mode, bn, order, ms = b.tune()
+            print(f"tuned: mode {mode} bn {bn} order {order} ({ms:.2f} ms)")
+        else:
+            b.configure(args.mode, args.bn, args.order, args.group_mib << 20)
+        b.forward()
+        ets, etd = b.forward()
+        print(f"{len(systems)} systems, {b.work_items} work items, {b.last_ms:.2f} ms")
+        for k, s in enumerate(systems):
+            print(f"  {s.name} no={s.no} nu={s.nu} ets={ets[k]:.10f} etd={etd[k]:.10f}")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

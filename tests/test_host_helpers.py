@@ -1,10 +1,11 @@
 """Host-side helpers that need no GPU: the decaying-magnitude synthetic systems,
-the traffic figures bench.py reads from the committed ncu summaries, and its
-clock-sample summary."""
+the traffic figures bench.py reads from the committed ncu summaries, its
+clock-sample summary, and the batch command line's argument parsing."""
 import importlib.util
 import pathlib
 
 import numpy as np
+import pytest
 
 from libcc_b200 import synthetic as S
 
@@ -65,3 +66,11 @@ def test_clock_summary_reads_loaded_samples_and_reasons(tmp_path, monkeypatch):
     assert s["reasons"] == ["sw_power_cap"] and s["samples"] == 3 and s["power_w_max"] == 1001.0
     cs.path.write_text("0, 1500, 1965, 900.0, 0x8, Not Active, Active, Not Active, Not Active\n")
     assert cs.summary()["reasons"] == ["hw_thermal_slowdown"]
+
+
+def test_batch_command_line_parses_without_a_gpu(capsys):
+    from libcc_b200 import batch
+    with pytest.raises(SystemExit) as e:
+        batch.main(["--help"])
+    assert e.value.code == 0
+    assert "--systems" in capsys.readouterr().out
