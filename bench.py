@@ -312,24 +312,10 @@ def batch_extra(A, S, local):
 
 
 def make_plan(A, no, nu, device, form):
-    """Plan for one form: 'fp64' (native mma.sync f64), 'int8:S' (S-digit emulation)
-    or 'int8' (per-tile digit counts, at most 5)."""
-    if form == "fp64":
-        return A.TriplesPlan(no, nu, device=device)
-    import ctypes
-    N = A.N
-    lib = N.load()
-    opt = N.Options()
-    lib.ccT_options_default(ctypes.byref(opt))
-    opt.precision = N.CCT_PREC_INT8_EMU
-    opt.device = device
-    opt.emu_slices = int(form.split(":")[1]) if ":" in form else 0
-    h = ctypes.c_void_p()
-    N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
-    plan = A.TriplesPlan.__new__(A.TriplesPlan)
-    plan._h, plan.no, plan.nu, plan.precision, plan.device = h, no, nu, form, device
-    plan.num_tuples = int(lib.ccT_num_tuples(no))
-    return plan
+    """Plan for one form: 'fp64' (native mma.sync f64), 'int8:S' (S-digit
+    emulation), 'int8' (automatic digits, 1e-8 Eh target) or 'int8@R'
+    (automatic digits, relative target R)."""
+    return A.TriplesPlan.for_form(no, nu, form, device=device)
 
 
 def main():

@@ -49,14 +49,23 @@ typedef struct {
     int32_t precision;       /* ccT_precision                                    */
     int32_t device;          /* CUDA device ordinal                              */
     int32_t check_inputs;    /* 1: reject NaN/Inf inputs and D >= 0 (default 1)  */
-    int32_t emu_slices;      /* INT8 emulation: 0 = per tile, at most 5 (default);
-                                4..7 = that many digits on every tile          */
-    int32_t reserved[4];
+    int32_t emu_slices;      /* INT8 emulation: 0 = automatic (default): the plan
+                                stores 7 digits and ccT_set_inputs picks the
+                                smallest count, 3..7, whose calibrated |dE(T)|
+                                meets the target below, each tile then taking
+                                at most that many; 3..7 = that many digits on
+                                every tile                                      */
+    double emu_tol;          /* automatic digits: target |dE(T)| in Eh against the
+                                FP64 form (0 = default 1e-8)                    */
+    double emu_tol_rel;      /* automatic digits: relative floor; the target is
+                                max(emu_tol, emu_tol_rel |E(T)|) (0 = default
+                                2e-14, the FP64 evaluation-order round-off)     */
 } ccT_options;
 
 typedef struct ccT_plan ccT_plan;
 
-/* Fill *opt with defaults (FP64, device 0, input checks on). */
+/* Fill *opt with defaults (FP64, device 0, input checks on, automatic digits
+ * with a 1e-8 Eh target). */
 void ccT_options_default(ccT_options *opt);
 
 /* Plan for one system of no occupied and nu virtual orbitals.  Allocates the
@@ -65,10 +74,16 @@ int ccT_plan_create(ccT_plan **plan, int64_t no, int64_t nu, const ccT_options *
 
 /* Load the inputs (reference layouts).  mem = CCT_MEM_HOST copies from host
  * memory (pinned memory copies fastest), CCT_MEM_DEVICE reads device pointers
- * already in HBM.  From host memory the packed VVVO passes through a transient
- * device buffer of its own size, allocated and freed inside the call.  The
- * call returns once the GEMM operands are built.  Replaces
- * program.F90:195-223 (restart read) plus the DDI put/bcast of T2/VM/VOE/VVVO. */
+ * already in HBM.  Ordering of device inputs: on the plan's own stream the call
+ * first waits for all work on the device (cudaDeviceSynchronize), so inputs
+ * written by any stream are complete; after ccT_set_stream(plan, s) the reads
+ * are ordered after the work already queued on s, and inputs written on other
+ * streams must be complete or ordered before s by the caller.  From host
+ * memory the packed VVVO passes through a transient device buffer of its own
+ * size, allocated and freed inside the call.  The call returns once the GEMM
+ * operands are built; for an automatic emulated plan it also calibrates the
+ * digit count (ccT_emu_digits).  Replaces program.F90:195-223 (restart read)
+ * plus the DDI put/bcast of T2/VM/VOE/VVVO. */
 int ccT_set_inputs(ccT_plan *plan, const double *eh, const double *ep, const double *t1,
                    const double *t2, const double *vm, const double *voe,
                    const double *vvvo_packed, int32_t mem);
@@ -104,12 +119,34 @@ double ccT_last_backward_ms(const ccT_plan *plan);
 
 /* Emulated plans: hist[s] = work items (128-row x N-column W tiles) the last
  * ccT_forward ran with s digits per operand, s = 0..n-1.  With emu_slices = 0
- * the default count is the maximum and every tile takes the digits its
+ * the calibrated count S is the maximum and every tile takes the digits its
  * exponents need (a tile whose largest row scales sum g bits below the
  * system's top runs max(1, S - floor(g/7)) digits), so the bound on the
  * error of any W entry is the top tile's.  FP64 plans: all zero.  No
  * reference counterpart (the reference has no emulation). */
 int ccT_emu_slice_histogram(ccT_plan *plan, int64_t *hist, int32_t n);
+
+/* Emulated plans: the digit count the W build runs (*digits), the calibrated
+ * bound on |dE(T)| against the FP64 form at that count (*est_err, Eh) and the
+ * target it was picked for (*target, Eh).  Calibration (automatic plans, in
+ * ccT_set_inputs): up to five tuples spread over the tuple list are evaluated
+ * with the FP64 W build and with every digit count 3..7; the estimate for a
+ * count is 2 x (largest per-tuple |dE| / tuple weight) x (sum of the weights of
+ * all tuples), i.e. every tuple's error at the worst sampled size and with
+ * the same sign.  Fixed-count plans report their count and zeros.  FP64 plans:
+ * CCT_ERR_STATE.  No reference counterpart. */
+int ccT_emu_digits(const ccT_plan *plan, int32_t *digits, double *est_err, double *target);
+
+/* W_abc of one tuple of the global list as this plan's W build forms it (FP64,
+ * or the emulated digits at the plan's count), after the degenerate tuples'
+ * symmetrisation and with W_aaa = 0: the V3 array of ijk_tuple_formv3 /
+ * ijj_tuple_formv3+SYMT311 / iij_tuple_formv3+SYMT311 followed by ZEROT3
+ * (src/triples-abc/ijk_tuple.f90:1-53, ijj_tuple.f90, iij_tuple.f90,
+ * ddcc_aux.f:84-94, 217-253), in the reference's layout w(a,b,c) at
+ * a + nu*(b + nu*c).  w holds nu^3 doubles; mem says host or device.  A
+ * diagnostic (it allocates a transient nu^3 buffer) for checking W against
+ * the reference element by element. */
+int ccT_tuple_w(ccT_plan *plan, int64_t tuple, double *w, int32_t mem);
 
 /* ---------------------------------------------------------------- batches
  * Many independent systems of uneven (no, nu) evaluated together.  Every tuple
@@ -142,6 +179,15 @@ int ccT_batch_configure(ccT_batch *batch, int32_t mode, int32_t bn, int32_t orde
  * the fastest and report it (outputs may be NULL). */
 int ccT_batch_tune(ccT_batch *batch, int32_t *best_mode, int32_t *best_bn, int32_t *best_order,
                    double *best_ms);
+/* Testing hook of the persistent executor (mode 0): from the next forward on,
+ * the reduction blocks of the tuple at position `tuple` of the queue order
+ * wait for one W-build tile more than that tuple has, so their bounded
+ * counter wait runs out after spin_limit polls (0 = the default limit); the
+ * kernel then finishes its queue and the forward returns CCT_ERR_TIMEOUT with
+ * the context intact.  tuple < 0 removes the stall.  No reference
+ * counterpart (the reference's only failure handling is stop,
+ * program.F90:221-222). */
+int ccT_batch_debug_stall(ccT_batch *batch, int64_t tuple, int64_t spin_limit);
 /* Device milliseconds of the last batch forward (CUDA events around the graph). */
 double ccT_batch_last_ms(const ccT_batch *batch);
 /* Work items (W-build tiles + reduction blocks) in the current schedule. */
@@ -209,9 +255,12 @@ double ccT_measure_int8_peak(int32_t device);
  * held by every GPU that loads the library until the process exits).  Larger
  * nu is rejected with CCT_ERR_INVALID.  The first call on a device looks up
  * that array's device address (cudaGetSymbolAddress) with the device current,
- * so make the first call before any stream capture.  All calls share the
- * array: calls whose kernels overlap on the GPU (different streams with no
- * ordering between them) race; calls ordered on one stream are safe. */
+ * so make the first call before any stream capture.  The looked-up address
+ * is kept for the life of the process: do not call the entry point again on
+ * a device after cudaDeviceReset (or any teardown of its primary context).
+ * All calls share the array: calls whose kernels overlap on the GPU (different
+ * streams with no ordering between them) race; calls ordered on one stream
+ * are safe. */
 #define CCT_NOALLOC_MAX_NU 320
 int ccT_reduce_w_noalloc(int64_t no, int64_t nu, int64_t i, int64_t j, int64_t k, const double *w,
                          const double *eh, const double *ep, const double *voe, double *etd_acc,

@@ -25,7 +25,8 @@ EXPORTS = [
     "ccT_last_error", "ccT_measure_fp64_peak", "ccT_measure_int8_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
     "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms", "ccT_emu_slice_histogram",
     "ccT_batch_create", "ccT_batch_set_inputs", "ccT_batch_forward", "ccT_batch_v1", "ccT_batch_configure",
-    "ccT_batch_tune", "ccT_batch_last_ms", "ccT_batch_work_items", "ccT_batch_destroy",
+    "ccT_batch_tune", "ccT_batch_last_ms", "ccT_batch_work_items", "ccT_batch_destroy", "ccT_emu_digits",
+    "ccT_tuple_w", "ccT_batch_debug_stall",
 ]
 
 
@@ -41,7 +42,7 @@ class CctError(RuntimeError):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("check_inputs", ctypes.c_int32),
-                ("emu_slices", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+                ("emu_slices", ctypes.c_int32), ("emu_tol", ctypes.c_double), ("emu_tol_rel", ctypes.c_double)]
 
 
 _lib = None
@@ -125,6 +126,12 @@ def load():
     lib.ccT_batch_work_items.restype = i64
     lib.ccT_batch_destroy.argtypes = [vp]
     lib.ccT_batch_destroy.restype = ctypes.c_int
+    lib.ccT_emu_digits.argtypes = [vp, ctypes.POINTER(i32), dp, dp]
+    lib.ccT_emu_digits.restype = ctypes.c_int
+    lib.ccT_tuple_w.argtypes = [vp, i64, vp, i32]
+    lib.ccT_tuple_w.restype = ctypes.c_int
+    lib.ccT_batch_debug_stall.argtypes = [vp, i64, i64]
+    lib.ccT_batch_debug_stall.restype = ctypes.c_int
     _lib = lib
     return lib
 

@@ -46,16 +46,44 @@ def input_sizes(no: int, nu: int):
                 voe=nu * nu * no * no, vvvo=nutr * nu * no)
 
 
-class TriplesPlan:
-    """Device plan for one system: owns the HBM buffers that replace the DDI arrays."""
+def parse_form(form: str) -> dict:
+    """Plan keyword arguments of a form name: 'fp64' (native FP64), 'int8'
+    (emulated, automatic digit count), 'int8:S' (emulated, S digits on every
+    tile) or 'int8@R' (emulated, automatic digits with relative target R)."""
+    if form == "fp64":
+        return dict(precision="fp64")
+    if form == "int8":
+        return dict(precision="int8")
+    if form.startswith("int8:"):
+        return dict(precision="int8", emu_slices=int(form[5:]))
+    if form.startswith("int8@"):
+        return dict(precision="int8", emu_tol_rel=float(form[5:]))
+    raise ValueError(f"unknown form {form!r}")
 
-    def __init__(self, no: int, nu: int, precision: str = "fp64", device: int = 0, check_inputs: bool = True):
+
+class TriplesPlan:
+    """Device plan for one system: owns the HBM buffers that replace the DDI arrays.
+
+    ``precision`` is "fp64" (native FP64 tensor-core W build) or "int8"
+    (split-integer emulation).  Emulated plans take ``emu_slices`` (0: the
+    digit count is calibrated in ``set_inputs`` against the target
+    max(emu_tol, emu_tol_rel |E(T)|); 3..7: that many digits on every tile);
+    ``emu_tol`` / ``emu_tol_rel`` of 0 keep the library defaults (1e-8 Eh,
+    2e-14)."""
+
+    def __init__(self, no: int, nu: int, precision: str = "fp64", device: int = 0, check_inputs: bool = True,
+                 emu_slices: int = 0, emu_tol: float = 0.0, emu_tol_rel: float = 0.0):
         lib = N.load()
         opt = N.Options()
         lib.ccT_options_default(ctypes.byref(opt))
         opt.precision = {"fp64": N.CCT_PREC_FP64, "int8": N.CCT_PREC_INT8_EMU}[precision]
         opt.device = device
         opt.check_inputs = 1 if check_inputs else 0
+        opt.emu_slices = emu_slices
+        if emu_tol:
+            opt.emu_tol = emu_tol
+        if emu_tol_rel:
+            opt.emu_tol_rel = emu_tol_rel
         h = ctypes.c_void_p()
         N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
         self._h = h
@@ -75,8 +103,16 @@ class TriplesPlan:
     def __exit__(self, *exc):
         self.close()
 
+    @classmethod
+    def for_form(cls, no: int, nu: int, form: str, device: int = 0, **kw):
+        """Plan for a form name (``parse_form``)."""
+        return cls(no, nu, device=device, **parse_form(form), **kw)
+
     def set_inputs(self, eh, ep, t1, t2, vm, voe, vvvo):
-        """Load the seven input arrays (all host numpy arrays, or all CUDA tensors)."""
+        """Load the seven input arrays (all host numpy arrays, or all CUDA tensors).
+        Device tensors are read after all work on the device has finished (the
+        plan's own stream), or in order on the caller's stream after
+        ``set_stream``."""
         arrs = dict(eh=eh, ep=ep, t1=t1, t2=t2, vm=vm, voe=voe, vvvo=vvvo)
         sizes = input_sizes(self.no, self.nu)
         dev = [_is_device(a) for a in arrs.values()]
@@ -121,6 +157,22 @@ class TriplesPlan:
         N.check(N.load().ccT_backward(self._h, begin, end, *ptrs, N.CCT_MEM_HOST), "ccT_backward")
         return out
 
+    def emu_digits(self) -> dict:
+        """Emulated plans: the digit count the W build runs, the calibrated bound
+        on |dE(T)| against the FP64 form and its target (``ccT_emu_digits``)."""
+        dg, err, tgt = ctypes.c_int32(), ctypes.c_double(), ctypes.c_double()
+        N.check(N.load().ccT_emu_digits(self._h, ctypes.byref(dg), ctypes.byref(err), ctypes.byref(tgt)),
+                "ccT_emu_digits")
+        return {"digits": dg.value, "est_err": err.value, "target": tgt.value}
+
+    def tuple_w(self, tuple_index: int) -> np.ndarray:
+        """W_abc of one tuple as this plan's W build forms it, flat in the
+        reference's layout (a fastest), nu^3 doubles (``ccT_tuple_w``)."""
+        w = np.empty(self.nu ** 3)
+        N.check(N.load().ccT_tuple_w(self._h, tuple_index, ctypes.c_void_p(w.ctypes.data), N.CCT_MEM_HOST),
+                "ccT_tuple_w")
+        return w
+
     @property
     def last_backward_ms(self) -> float:
         return float(N.load().ccT_last_backward_ms(self._h))
@@ -128,7 +180,6 @@ class TriplesPlan:
     def emu_slice_histogram(self) -> list:
         """Emulated plans: work items of the last forward per digit count
         (index s = digits per operand, 0..7); all zero for FP64 plans."""
-        import ctypes
         h = (ctypes.c_int64 * 8)()
         N.check(N.load().ccT_emu_slice_histogram(self._h, h, 8), "ccT_emu_slice_histogram")
         return [int(v) for v in h]

@@ -88,6 +88,11 @@ class TriplesBatch:
         bn: W-build N tile, 0 = per system (mode 1 only)."""
         N.check(N.load().ccT_batch_configure(self._h, mode, bn, order, group_bytes), "ccT_batch_configure")
 
+    def debug_stall(self, tuple_pos: int = 0, spin_limit: int = 0):
+        """Testing hook (``ccT_batch_debug_stall``): make the persistent
+        executor's counter wait of one tuple run out; ``tuple_pos`` < 0 clears it."""
+        N.check(N.load().ccT_batch_debug_stall(self._h, tuple_pos, spin_limit), "ccT_batch_debug_stall")
+
     def tune(self):
         """Time every (mode, N tile, tuple order) candidate; keep the fastest.
         Returns (mode, bn, order, ms)."""

@@ -113,6 +113,22 @@ __global__ void __launch_bounds__(kWThreads) adj_wfull_kernel(int nu, int64_t NP
   }
 }
 
+// W in the reference's layout: wf[(c nu + b) nu + a] = wc[(a nu + b) nu + c],
+// one 32 x 32 (a, c) tile of one b per block.
+__global__ void w_fortran_kernel(int nu, const double *__restrict__ wc, double *__restrict__ wf) {
+  __shared__ double tile[32][33];
+  const int b = blockIdx.z, a0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, c = c0 + threadIdx.x;
+    tile[r][threadIdx.x] = (a < nu && c < nu) ? wc[widx(nu, a, b, c)] : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int c = c0 + r, a = a0 + threadIdx.x;
+    if (a < nu && c < nu) wf[((int64_t)c * nu + b) * nu + a] = tile[threadIdx.x][r];
+  }
+}
+
 // ---------------------------------------------------------------------------- dE/dW and M
 // S_m at the permuted triple (r0,r1,r2) of (a,b,c): u_x(r0) VOE(r1,r2,y,z).
 struct SmTable {
@@ -997,6 +1013,29 @@ void adj_free(AdjBuffers *b) {
                     b->g_ep, b->g_t1, b->g_t2, b->g_vm, b->g_voe, b->g_vvvo})
     if (q) cudaFree(q);
   *b = AdjBuffers{};
+}
+
+int assemble_w_fortran(const Dims &d, const Tuple &t, double *const X[3], double *wc, double *wf, cudaStream_t s) {
+  const int nu = d.nu;
+  AdjTuple at;
+  at.x[0] = X[0];
+  at.x[1] = X[1];
+  at.x[2] = X[2];
+  at.i = t.i;
+  at.j = t.j;
+  at.k = t.k;
+  at.weight = t.kind == kIJK ? 1.0 : 0.5;
+  const dim3 g3((nu + kWC - 1) / kWC, (nu + kWB - 1) / kWB, (nu + kWA - 1) / kWA);
+  switch (t.kind) {
+    case kIJK: adj_wfull_kernel<kIJK><<<g3, kWThreads, 3 * kWSlot * 8, s>>>(nu, d.NP, at, wc); break;
+    case kIJJ: adj_wfull_kernel<kIJJ><<<g3, kWThreads, 4 * kWSlot * 8, s>>>(nu, d.NP, at, wc); break;
+    default: adj_wfull_kernel<kIIJ><<<g3, kWThreads, 4 * kWSlot * 8, s>>>(nu, d.NP, at, wc); break;
+  }
+  CCT_CUDA(cudaGetLastError());
+  const dim3 gt((nu + 31) / 32, (nu + 31) / 32, nu);
+  w_fortran_kernel<<<gt, dim3(32, 8), 0, s>>>(nu, wc, wf);
+  CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
 }
 
 int adj_zero(const Dims &d, AdjBuffers *b, cudaStream_t s) {

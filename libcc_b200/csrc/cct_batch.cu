@@ -87,6 +87,7 @@ struct BatchArgs {
   const int64_t *tuple_v1_off;
   double *sys_out;               // [sys][3] = ets, etd, ets+etd
   int *err;
+  long spin_limit;               // iterations of a bounded counter wait
 };
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
@@ -96,8 +97,8 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
 }
 // Bounded wait for *p >= target.  Once any wait has timed out (*err set) every
 // later wait returns at once, so a failure cannot cascade into a long stall.
-__device__ void spin_until(const int *p, int target, int *err) {
-  for (long it = 0; it < kSpinLimit; it++) {
+__device__ void spin_until(const int *p, int target, int *err, long limit) {
+  for (long it = 0; it < limit; it++) {
     if (ld_acquire(p) >= target) return;
     if (*(volatile int *)err) return;
     __nanosleep(64);
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
     const SysDev &S = A.sys[T.sys];
     if (it.x == 0) {  // ---- one W-build tile
       if (threadIdx.x == 0 && T.group >= kRing)
-        spin_until(group_rd + (T.group - kRing), A.group_rd_items[T.group - kRing], A.err);
+        spin_until(group_rd + (T.group - kRing), A.group_rd_items[T.group - kRing], A.err, A.spin_limit);
       __syncthreads();
       const int tile_m = it.w / S.tiles_n, tile_n = it.w - tile_m * S.tiles_n;
       wb::wbuild_tile<BN, kBTM>(A.jobs[(int64_t)t * 3 + it.z], S.nu, S.KP, S.nu + S.no, S.NP, tile_m, tile_n, smem);
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(kBT, 1) batch_kernel(const BatchArgs A) {
       __syncthreads();
       if (threadIdx.x == 0) atomicAdd(wb_done + t, 1);
     } else {  // ---- one reduction block
-      if (threadIdx.x == 0) spin_until(wb_done + t, T.wb_items, A.err);
+      if (threadIdx.x == 0) spin_until(wb_done + t, T.wb_items, A.err, A.spin_limit);
       __syncthreads();
       __threadfence();
       TupleDev td;
@@ -358,6 +359,10 @@ struct ccT_batch {
   std::vector<std::vector<WbRange>> grp_wb;  // per group: W-build item ranges, one per N tile width
   std::vector<int64_t> grp_rd_begin, grp_rd_count;
   int64_t group_budget = 256ll << 20;     // X scratch bytes per tuple group
+  // testing hook (ccT_batch_debug_stall): the reduction blocks of this tuple
+  // (position in queue order) wait for one W-build tile more than it has
+  int64_t stall_tuple = -1;
+  long spin_limit = kSpinLimit;
   bool tuned = false;
   // schedule (device)
   bool scheduled = false;
@@ -508,7 +513,7 @@ int build_schedule(ccT_batch *b) {
     r.j = h.j;
     r.k = h.k;
     r.group = h.group;
-    r.wb_items = h.wb_items;
+    r.wb_items = h.wb_items + (u == b->stall_tuple ? 1 : 0);
     r.rd_items = h.rd_items;
     for (int g = 0; g < 3; g++) r.x[g] = base + (int64_t)std::min(g, h.njobs - 1) * nu2 * d.NP;
     r.xpart = partials + h.xpart_off;
@@ -644,6 +649,7 @@ BatchArgs batch_args(ccT_batch *b) {
   a.tuple_v1_off = b->tuple_v1_off;
   a.sys_out = b->sys_out;
   a.err = b->err;
+  a.spin_limit = b->spin_limit;
   return a;
 }
 
@@ -883,6 +889,8 @@ int ccT_batch_set_inputs(ccT_batch *b, int64_t s, const double *eh, const double
   BatchSystemHost &S = b->sys[s];
   const int64_t n = S.no, v = S.nu, v2 = v * v;
   const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  // device inputs may still be being written on any stream (as ccT_set_inputs)
+  if (mem == CCT_MEM_DEVICE) CCT_CUDA(cudaDeviceSynchronize());
   CCT_CUDA(cudaMemcpyAsync(S.eh, eh, n * 8, kind, b->stream));
   CCT_CUDA(cudaMemcpyAsync(S.ep, ep, v * 8, kind, b->stream));
   CCT_CUDA(cudaMemcpyAsync(S.t1, t1, n * v * 8, kind, b->stream));
@@ -1011,6 +1019,21 @@ int ccT_batch_tune(ccT_batch *b, int32_t *best_mode, int32_t *best_bn, int32_t *
 }
 
 double ccT_batch_last_ms(const ccT_batch *b) { return b ? (double)b->last_ms : 0.0; }
+
+int ccT_batch_debug_stall(ccT_batch *b, int64_t tuple, int64_t spin_limit) {
+  if (!b) {
+    set_error("batch is NULL");
+    return CCT_ERR_INVALID;
+  }
+  if (spin_limit < 0) {
+    set_error("spin_limit must be >= 0 (0 = the default)");
+    return CCT_ERR_INVALID;
+  }
+  b->stall_tuple = tuple < 0 ? -1 : tuple;
+  b->spin_limit = spin_limit > 0 ? (long)spin_limit : kSpinLimit;
+  free_schedule(b);  // the next forward rebuilds the schedule and its graph
+  return CCT_OK;
+}
 
 int64_t ccT_batch_work_items(const ccT_batch *b) { return b ? b->nitems : 0; }
 

@@ -3,28 +3,48 @@
 //
 // Same three grouped GEMMs per tuple as cct_wbuild_f64.cu,
 //   X_g(p,q,s) = sum_k E[x1][p][q][k] F[x2][x3][s][k] + sum_k E[x2][q][p][k] F[x1][x3][s][k].
-// Every operand row is written as 2^e * sum_{t=1..S} a_t 2^(-7t), a_t int8 in
-// [-127,127] (truncated digits).  The scale e is shared by the two halves: for
-// an A row (p,q) it is the largest row exponent of E[x][p][q] and E[x][q][p]
-// over all x; for a B row (z,n) the largest over y of F[y][z][n].  Then
-//   X(m,n) = 2^(eA(m)+eB(n)) sum_{d=2..S+1} 2^(-7d) D_d,
+// Every operand row is written as 2^(e+1) * sum_{t=1..S} a_t 2^(-7t) with
+// round-to-nearest digits a_t in [-64, 64]: |v 2^-(e+1)| < 1/2, each digit is
+// rint(128 y) of the running remainder y, which stays in [-1/2, 1/2].  The
+// scale e is shared by the two halves: for an A row (p,q) it is the largest
+// row exponent of E[x][p][q] and E[x][q][p] over all x; for a B row (z,n) the
+// largest over y of F[y][z][n].  Then
+//   X(m,n) = 2^(eA(m)+eB(n)+2) sum_{d=2..S+1} 2^(-7d) D_d,
 //   D_d = sum_{halves} sum_{t+u=d} sum_k a_t b_u,
 // keeping digit products with t+u <= S+1 (the dropped tail is below
 // 2^(-7(S+1)) of |A||B| per term).  Each D_d is an exact int32 accumulation
-// (|D_d| <= 2 S K 127^2 < 2^31 for K <= 4096); FP64 enters only when the
-// diagonals are scaled and summed in the epilogue.  Digit count S (4..7) is a
-// plan option: about 7S - 2 bits of each operand row survive.  An adaptive
-// plan takes S as the maximum and gives each work item (row tile, column
-// tile) its own count s <= S from the tile's exponents (EmuOperands::tileExp):
-// a tile whose largest row scales sum `gap` bits below the plan's top runs
-// s = S - floor(gap / 7) digits, s(s+1)/2 MMAs per K chunk instead of
-// S(S+1)/2, and its dropped products stay below the top tile's.
+// (|D_d| <= 2 S K 64^2 < 2^31 for K <= 4096); FP64 enters only when the
+// diagonals are scaled and summed in the epilogue.  Rounded digits leave an
+// unbiased remainder: truncated digits (remainder of the value's own sign)
+// shrink every product the same way, and that bias adds up over the K sum,
+// the a,b,c sum and the tuples into the energy.  On seeded systems the
+// rounded digits give E(T) errors 300-700x smaller at the same digit count.
+// Digit count S (3..7) is a plan option, or picked per system from an energy
+// error target (cct_plan.cu).  An adaptive plan takes S as the maximum and
+// gives each work item (row tile, column tile) its own count s <= S from the
+// tile's exponents (EmuOperands::tileExp): a tile whose largest row scales sum
+// `gap` bits below the plan's top runs s = S - floor(gap / 7) digits,
+// s(s+1)/2 digit products per K chunk instead of S(S+1)/2, and its dropped
+// products stay below the top tile's.
 //
 // Operands are pre-tiled (EmuOperands): the digits of one 32-byte K chunk of
-// a 128-row A tile, all S slices, are one contiguous S x 4 KB run already in
-// the tensor core's K-major no-swizzle layout, and likewise S x N x 32 B for
-// an N-row B tile.  A pipeline stage is therefore two bulk copies
-// (cp.async.bulk) of large contiguous runs instead of 2S narrow tensor boxes.
+// a 128-row A tile, all slices of the operand, are one contiguous run already
+// in the tensor core's K-major no-swizzle layout, and likewise for an N-row B
+// tile.  A pipeline stage is therefore two bulk copies (cp.async.bulk) of
+// large contiguous runs instead of 2S narrow tensor boxes.  The operand may
+// hold more slices than a launch runs (an automatic plan builds 7 and runs
+// the count its error target needs); the producer then copies the leading
+// slices of each chunk.
+//
+// Merged digit products.  B's slices of one chunk sit back to back in shared
+// memory (slice u at u N rows, 8-row core-matrix groups 256 B apart), so the
+// slices u0..u0+c-1 form one B operand of c N rows, and the accumulator
+// columns of diagonal d sit at d N.  One MMA of A slice t against that operand
+// therefore adds A_t B_u into diagonal t+u for all c slices at once: a chunk
+// needs, per t, ceil((S-t) N / 256) MMAs of up to 256 columns instead of S-t
+// MMAs of N columns (7 instead of 15 at S = 5, N = 80).  An N = 80 MMA is
+// bound by its shared-memory operand reads (A 4 KB + B 2.5 KB); a wide one
+// reads A once for up to three B slices.
 //
 // Persistent kernel, one CTA of 64 + 32 NDW threads per SM, work items (job,
 // row tile, column tile) taken round-robin with the column tile fastest, so
@@ -32,9 +52,9 @@
 //   warp 0      producer: per stage, one bulk copy of the A digits and one
 //               of the B digits (KS K chunks) into a ring of stages; it runs
 //               ahead across work items, so the ring never drains between tiles
-//   warp 1      TMEM owner + MMA issuer (one thread): s(s+1)/2 MMAs per chunk
-//               into s diagonal accumulators (N int32 columns each), at 5 or
-//               more digits diagonal by diagonal within the chunk
+//   warp 1      TMEM owner + MMA issuer (one thread): per chunk and A slice t,
+//               merged MMAs over the B slices 0..s-1-t into the s diagonal
+//               accumulators (N int32 columns each)
 //   warps 2..   drain (NDW warps): tcgen05.ld one diagonal at a time, sum in
 //               FP64, hand the tensor memory back to the issuer, then scale
 //               and store X (the ring keeps filling meanwhile, so the next
@@ -153,6 +173,7 @@ struct EmuArgs {
   const int *tileExp;  // adaptive plans: see EmuOperands::tileExp; nullptr: every item runs S digits
   unsigned long long *slice_hist;
   int nu, no, njobs, kchunks, tiles_m, tiles_n;
+  int sop;  // digit slices stored per K chunk in the operands (>= the S of the launch)
   int64_t NP;
   int *err;
 };
@@ -181,8 +202,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
   constexpr int B_BLK = EBN * kEmuKC;
   constexpr uint32_t TCOLS = emu_tmem_cols<S, EBN>();
   constexpr int ST = emu_stages<S, EBN>();
-  constexpr int CA = S * A_BLK, CB = S * B_BLK;    // bytes of one K chunk per operand
+  constexpr int CA = S * A_BLK, CB = S * B_BLK;    // bytes of one K chunk per operand in shared memory
   constexpr int SA = KS * CA, SB = KS * CB;        // bytes of one stage per operand
+  constexpr int MPS = 256 / EBN;                   // B slices per merged MMA (N <= 256)
+  static_assert(MPS >= 1, "N tile above 256 columns");
   extern __shared__ __align__(1024) uint8_t emu_smem[];
   uint8_t *base = (uint8_t *)(((uintptr_t)emu_smem + 1023) & ~(uintptr_t)1023);
   uint8_t *sA = base;            // [stage][chunk][slice][4096]
@@ -197,8 +220,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
   const int per_job = args.tiles_m * args.tiles_n;
   const int64_t nitems = (int64_t)args.njobs * per_job;
   const int KC = args.kchunks;
-  const int64_t aslab = (int64_t)args.tiles_m * KC * CA;  // bytes per occupied index
-  const int64_t bslab = (int64_t)args.tiles_n * KC * CB;  // bytes per (y,z)
+  const int64_t GA = (int64_t)args.sop * A_BLK, GB = (int64_t)args.sop * B_BLK;  // bytes of one K chunk in HBM
+  const int64_t aslab = (int64_t)args.tiles_m * KC * GA;  // bytes per occupied index
+  const int64_t bslab = (int64_t)args.tiles_n * KC * GB;  // bytes per (y,z)
+  const bool whole = args.sop == S;  // operand chunks hold exactly the launch's slices
 
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base)),
@@ -232,8 +257,8 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
         const EmuJob job = args.jobs[jb];
         const int sl = item_slices<S>(args, tm, tn, job.x3);
         for (int h = 0; h < job.nhalves && ok; h++) {
-          const int8_t *A = (h == 0 ? args.E8 + job.x1 * aslab : args.E8T + job.x2 * aslab) + (int64_t)tm * KC * CA;
-          const int8_t *B = args.F8 + job.fyz[h] * bslab + (int64_t)tn * KC * CB;
+          const int8_t *A = (h == 0 ? args.E8 + job.x1 * aslab : args.E8T + job.x2 * aslab) + (int64_t)tm * KC * GA;
+          const int8_t *B = args.F8 + job.fyz[h] * bslab + (int64_t)tn * KC * GB;
           for (int kc = 0; kc < KC; kc += KS, g++) {
             const int st = (int)(g % ST);
             const uint32_t nch = KC - kc < KS ? (uint32_t)(KC - kc) : (uint32_t)KS;  // the last stage may be short
@@ -241,15 +266,15 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
               ok = false;
               break;
             }
-            if (sl == S) {  // all digits: the stage's chunks are one contiguous run per operand
+            if (sl == S && whole) {  // all digits: the stage's chunks are one contiguous run per operand
               mbar_expect_tx(&full[st], nch * (CA + CB));
-              bulk_load(sA + st * SA, A + (int64_t)kc * CA, nch * CA, &full[st]);
-              bulk_load(sB + st * SB, B + (int64_t)kc * CB, nch * CB, &full[st]);
+              bulk_load(sA + st * SA, A + (int64_t)kc * GA, nch * CA, &full[st]);
+              bulk_load(sB + st * SB, B + (int64_t)kc * GB, nch * CB, &full[st]);
             } else {  // the leading sl digit slices of each chunk
               mbar_expect_tx(&full[st], nch * (uint32_t)sl * (A_BLK + B_BLK));
               for (uint32_t c = 0; c < nch; c++) {
-                bulk_load(sA + st * SA + c * CA, A + (int64_t)(kc + c) * CA, (uint32_t)sl * A_BLK, &full[st]);
-                bulk_load(sB + st * SB + c * CB, B + (int64_t)(kc + c) * CB, (uint32_t)sl * B_BLK, &full[st]);
+                bulk_load(sA + st * SA + c * CA, A + (int64_t)(kc + c) * GA, (uint32_t)sl * A_BLK, &full[st]);
+                bulk_load(sB + st * SB + c * CB, B + (int64_t)(kc + c) * GB, (uint32_t)sl * B_BLK, &full[st]);
               }
             }
           }
@@ -260,8 +285,8 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
     }
   } else if (warp == 1) {
     if (lane == 0) {  // ---------------- MMA issuer
-      // kind::i8, D s32, A/B s8, K-major, M = 128, N = EBN
-      const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(EBN >> 3) << 17) | (8u << 24);
+      // kind::i8, D s32, A/B s8, K-major, M = 128; N (bits 17-22, N >> 3) per MMA
+      const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | (8u << 24);
       const uint64_t dA0 = desc_kmajor(sA), dB0 = desc_kmajor(sB);
       uint32_t g = 0, n = 0;
       bool ok = true;
@@ -295,32 +320,29 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
               const uint64_t dA = dA0 + (uint64_t)((st * SA + c * CA) >> 4);
               const uint64_t dB = dB0 + (uint64_t)((st * SB + c * CB) >> 4);
               const uint32_t first = (h == 0 && kc == 0 && c == 0) ? 0u : 1u;  // accumulate flag of the t = 0 row
-              auto mma = [&](int t, int u) {
+              // A slice t against B slices u0 .. u0+cnt-1 (one operand of cnt
+              // EBN rows) into diagonals t+u0 .. t+u0+cnt-1
+              auto mma = [&](int t, int u0, int cnt) {
+                const uint32_t idesc = idesc0 | ((uint32_t)((cnt * EBN) >> 3) << 17);
                 asm volatile(
                     "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; "
-                    "}" ::"r"(tmem + (uint32_t)((t + u) * EBN)),
-                    "l"(dA + (uint64_t)(t * (A_BLK >> 4))), "l"(dB + (uint64_t)(u * (B_BLK >> 4))), "r"(idesc),
+                    "}" ::"r"(tmem + (uint32_t)((t + u0) * EBN)),
+                    "l"(dA + (uint64_t)(t * (A_BLK >> 4))), "l"(dB + (uint64_t)(u0 * (B_BLK >> 4))), "r"(idesc),
                     "r"(t > 0 ? 1u : first));
               };
-              if constexpr (S >= 5) {
-                // diagonal by diagonal: runs of MMAs into one accumulator
-                // (measured 19-20% faster than row order at 5 and 6 digits,
-                // 3% slower at 4)
+              // t = 0 first: with the accumulate flag clear it initialises
+              // every diagonal of the item; later rows add into them
 #pragma unroll
-                for (int d = 0; d < S; d++) {
-                  if (d >= sl) break;
-#pragma unroll
-                  for (int t = 0; t <= d; t++) mma(t, d - t);
-                }
-              } else {
-#pragma unroll
-                for (int t = 0; t < S; t++) {
-                  if (t >= sl) break;
-#pragma unroll
-                  for (int u = 0; u < S - t; u++) {
-                    if (u >= sl - t) break;
-                    mma(t, u);
-                  }
+              for (int t = 0; t < S; t++) {
+                if (t >= sl) break;
+                const int n = sl - t;                       // B slices this A slice meets
+                const int parts = (n + MPS - 1) / MPS;      // MMAs of at most MPS slices, sizes within one
+                const int base = n / parts, extra = n - base * parts;
+                int u0 = 0;
+                for (int q = 0; q < parts; q++) {
+                  const int cnt = base + (q < extra ? 1 : 0);
+                  mma(t, u0, cnt);
+                  u0 += cnt;
                 }
               }
             }
@@ -342,10 +364,11 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
     const int q = warp & 3;
     const int row = q * 32 + lane;
     const int cbase = ((warp - 2) / 4) * CW;
-    // diagonal d = t + u (0-based digits) carries 2^(-7(d+2))
+    // diagonal d = t + u (0-based digits) carries 2^(-7(d+2)), times 2^2 for
+    // the two operand scales 2^(e+1)
     double cd[S];
 #pragma unroll
-    for (int d = 0; d < S; d++) cd[d] = pow2(-7 * (d + 2));
+    for (int d = 0; d < S; d++) cd[d] = pow2(2 - 7 * (d + 2));
     uint32_t n = 0;
     for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x, n++) {
       // everything that does not depend on the MMAs is fetched before the wait
@@ -511,21 +534,23 @@ __global__ void tile_exp_top_kernel(int tiles_m, int nbt, int *__restrict__ tile
 // core matrices, K halves 128 B apart, 8-row groups 256 B apart.
 __host__ __device__ constexpr int blk_off(int r, int kb) { return (r >> 3) * 256 + (kb >> 4) * 128 + (r & 7) * 16 + (kb & 15); }
 
-// Pass 3: S truncated 7-bit digits of value * 2^-e, |value * 2^-e| < 1.  A
-// lane takes four consecutive K bytes, so each slice gets one 32-bit store;
-// the four bytes are adjacent in the tiled layout (kb % 4 == 0).
+// Pass 3: S rounded 7-bit digits of y = value * 2^-(e+1), |y| < 1/2: each
+// digit is rint(128 y) of the running remainder (|digit| <= 64, the remainder
+// stays in [-1/2, 1/2]; every step is exact).  A lane takes four consecutive
+// K bytes, so each slice gets one 32-bit store; the four bytes are adjacent in
+// the tiled layout (kb % 4 == 0).
 __device__ __forceinline__ void digits4(const double *__restrict__ src, int64_t k, int64_t kvalid, int e, int S,
                                         uint32_t *w) {
   double y[4];
 #pragma unroll
-  for (int i = 0; i < 4; i++) y[i] = (k + i) < kvalid ? ldexp(src[k + i], -e) : 0.0;
+  for (int i = 0; i < 4; i++) y[i] = (k + i) < kvalid ? ldexp(src[k + i], -(e + 1)) : 0.0;
   for (int t = 0; t < S; t++) {
     uint32_t word = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       y[i] *= 128.0;
-      const double a = trunc(y[i]);  // |a| <= 127
-      y[i] -= a;                     // exact
+      const double a = rint(y[i]);  // |a| <= 64
+      y[i] -= a;                    // exact, in [-1/2, 1/2]
       word |= (uint32_t)(uint8_t)(int8_t)a << (8 * i);
     }
     w[t] = word;
@@ -617,10 +642,11 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   a.no = d.no;
   a.njobs = njobs;
   a.kchunks = (int)(o.KP8 / kEmuKC);
+  a.sop = o.slices;
   a.tiles_m = (int)o.tiles_m;
   a.tiles_n = (int)(d.NP / EBN);
-  if (d.EBN != EBN) {
-    set_error("emulated N tile mismatch");
+  if (d.EBN != EBN || o.slices < S) {
+    set_error("emulated N tile mismatch, or fewer operand digits than the launch runs");
     return CCT_ERR_INVALID;
   }
   a.NP = d.NP;
@@ -685,9 +711,12 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
 
 int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
                       cudaStream_t s) {
-  // (slices, N tile) pairs with slices x N <= 512
-  const int key = o.slices * 1000 + d.EBN;
+  // (digits run, N tile) pairs with digits x N <= 512 tensor-memory columns
+  const int key = o.run_slices * 1000 + d.EBN;
   switch (key) {
+    case 3064: return launch_emu_s<3, 64>(o, d, jobs_dev, njobs, err, s);
+    case 3080: return launch_emu_s<3, 80>(o, d, jobs_dev, njobs, err, s);
+    case 3096: return launch_emu_s<3, 96>(o, d, jobs_dev, njobs, err, s);
     case 4064: return launch_emu_s<4, 64>(o, d, jobs_dev, njobs, err, s);
     case 4080: return launch_emu_s<4, 80>(o, d, jobs_dev, njobs, err, s);
     case 4096: return launch_emu_s<4, 96>(o, d, jobs_dev, njobs, err, s);
@@ -698,7 +727,8 @@ int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_de
     case 6080: return launch_emu_s<6, 80>(o, d, jobs_dev, njobs, err, s);
     case 7064: return launch_emu_s<7, 64>(o, d, jobs_dev, njobs, err, s);
     default:
-      set_error("unsupported (slices, N tile) = (" + std::to_string(o.slices) + ", " + std::to_string(d.EBN) + ")");
+      set_error("unsupported (digits, N tile) = (" + std::to_string(o.run_slices) + ", " + std::to_string(d.EBN) +
+                ")");
       return CCT_ERR_INVALID;
   }
 }

@@ -95,9 +95,10 @@ struct TupleDev {
 };
 
 // ----------------------------------------------------------------------------- INT8 emulation
-// Digit count of the split-integer operands (7 bits each).  Measured on the
-// no=24/nu=320 workload: |dE|/|E| = 1.7e-7 (4 digits), 1.6e-9 (5), 1.4e-13 (7).
-constexpr int kEmuMinSlices = 4, kEmuMaxSlices = 7, kEmuDefaultSlices = 5;
+// Digit count of the split-integer operands (7 bits each).  An automatic plan
+// (emu_slices = 0) builds kEmuMaxSlices digits and runs the smallest count in
+// [kEmuMinSlices, kEmuMaxSlices] whose calibrated E(T) error meets its target.
+constexpr int kEmuMinSlices = 3, kEmuMaxSlices = 7;
 // N tile of the emulated W-build: the tensor memory holds S diagonal
 // accumulators of N int32 columns (S N <= 512), and an MMA instruction costs
 // about the same up to N ~ 80, so the widest N that pads nu least is used.
@@ -137,7 +138,8 @@ constexpr int kEmuKC = 32;                       // K bytes per chunk (one kind:
 constexpr int kEmuABlk = kEmuBM * kEmuKC;        // 4096 bytes
 // B blocks hold EBN rows: EBN * kEmuKC bytes (2048, 2560 or 3072)
 struct EmuOperands {
-  int slices = kEmuDefaultSlices;
+  int slices = kEmuMaxSlices;                // digit slices stored per K chunk
+  int run_slices = kEmuMaxSlices;            // digits the W build runs (<= slices; the calibrated count)
   int64_t KP8 = 0;                           // digit row length: round_up(nu+no, 32)
   int64_t tiles_m = 0;                       // ceil(nu^2 / 128) row tiles per occupied index
   int8_t *E8 = nullptr, *E8T = nullptr;      // [x][tile_m][kchunk][slice][4096]; E8T rows (q,p)
@@ -214,6 +216,9 @@ int adj_tuple_gemm_e(const Dims &d, const Tuple *t, const int *sets, int ntup, c
                      cudaStream_t s);
 int adj_tuple_gemm_f(const Dims &d, const Tuple &t, const double *E, AdjBuffers *b, int set, cudaStream_t s);
 int adj_finish(const Dims &d, const double *v1, AdjBuffers *b, cudaStream_t s);
+// W(a,b,c) of tuple t from its X buffers: into wc in C order (a slowest), then
+// into wf in the reference's layout (a fastest).  Needs adj_configure.
+int assemble_w_fortran(const Dims &d, const Tuple &t, double *const X[3], double *wc, double *wf, cudaStream_t s);
 
 // peak.cu
 double measure_fp64_peak(int device);

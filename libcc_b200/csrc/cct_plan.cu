@@ -65,6 +65,8 @@ struct ccT_plan {
   double *acc = nullptr;  // [etd_sum, etd_comp, out3[3], v1(nu*no)]
   GemmJob *jobs = nullptr;  // [buffer][tuple][3]
   bool emulated = false;    // INT8 split-integer W-build
+  bool emu_auto = false;    // digit count picked by calibration in ccT_set_inputs
+  double emu_est_err = 0.0, emu_target = 0.0;  // calibrated |dE(T)| bound and its target (Eh)
   EmuOperands emu;
   EmuJob *emu_jobs = nullptr;  // [buffer][tuple][3]
   int *flags = nullptr;
@@ -239,22 +241,28 @@ int join_streams(ccT_plan *p) {
   return CCT_OK;
 }
 
+// The W-build GEMMs of tuple tix into X buffer b on stream st: the plan's
+// own form, or the FP64 kernel when fp64 is set (emulated plans keep the FP64
+// jobs for the backward's recompute and the digit calibration).
+int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st) {
+  const Tuple &t = p->tuples[tix];
+  const int njobs = t.kind == kIJK ? 3 : 2;
+  const int64_t ntup = (int64_t)p->tuples.size();
+  if (p->emulated && !fp64)
+    return launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1, st);
+  return launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, st);
+}
+
 // W-build of tuple tix into X buffer b on the GEMM stream, then its reduction on
 // the reduction stream.  The GEMM waits until the reduction that last read
 // buffer b (two tuples earlier) is done; the reduction waits for its GEMM.
-int run_tuple(ccT_plan *p, int64_t tix) {
+int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
   const Tuple &t = p->tuples[tix];
-  const int njobs = t.kind == kIJK ? 3 : 2;
   const int b = (int)(p->tick % kNBuf);
   p->tick++;
-  const int64_t ntup = (int64_t)p->tuples.size();
   CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[b], 0));
   CCT_TRY(prof_mark(p, CCT_KERNEL_WBUILD, p->gemm_stream));
-  if (p->emulated)
-    CCT_TRY(launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1,
-                              p->gemm_stream));
-  else
-    CCT_TRY(launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, p->gemm_stream));
+  CCT_TRY(wbuild_tuple(p, tix, b, fp64, p->gemm_stream));
   CCT_TRY(prof_mark(p, -1, p->gemm_stream));
   CCT_CUDA(cudaEventRecord(p->ev_gemm[b], p->gemm_stream));
   CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_gemm[b], 0));
@@ -276,6 +284,90 @@ int run_tuple(ccT_plan *p, int64_t tix) {
   return CCT_OK;
 }
 
+// E(T) contribution (etd + ets) of one tuple alone, with the plan's W build or
+// the FP64 one.  Leaves the plan's accumulators holding that tuple only.
+int tuple_energy(ccT_plan *p, int64_t tix, bool fp64, double *e) {
+  const Dims &d = p->d;
+  CCT_CUDA(cudaMemsetAsync(p->acc, 0, (5 + (int64_t)d.nu * d.no) * 8, p->stream));
+  CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
+  CCT_TRY(fork_streams(p));
+  CCT_TRY(run_tuple(p, tix, fp64));
+  CCT_TRY(join_streams(p));
+  CCT_TRY(launch_ets(d, p->t1, v1_acc(p), p->acc, p->acc + 2, p->stream));
+  double out3[3];
+  int werr = 0;
+  CCT_CUDA(cudaMemcpyAsync(&werr, p->flags + 1, 4, cudaMemcpyDeviceToHost, p->stream));
+  CCT_CUDA(cudaMemcpyAsync(out3, p->acc + 2, 3 * 8, cudaMemcpyDeviceToHost, p->stream));
+  CCT_CUDA(cudaStreamSynchronize(p->stream));
+  if (werr) {
+    set_error("an emulated W-build kernel ran out its bounded wait and unwound");
+    return CCT_ERR_TIMEOUT;
+  }
+  *e = out3[0] + out3[1];
+  return CCT_OK;
+}
+
+// Automatic digit count of an emulated plan.  Up to kCalSamples tuples spread
+// evenly over the tuple list run once with the FP64 W build and once per digit
+// count, kEmuMinSlices upward.  The error bound for a count assumes every
+// tuple errs by the largest sampled |dE| per unit of tuple weight, all with
+// the same sign (the weight of an i>j>k tuple is 1, of a degenerate one 1/2),
+// times kCalSafety.  The first count whose bound meets
+// max(emu_tol, emu_tol_rel |E(T)|), with E(T) extrapolated the same way from
+// the FP64 samples, is kept; failing that, the largest count.
+constexpr int kCalSamples = 5;
+constexpr double kCalSafety = 2.0;
+constexpr double kDefaultTol = 1e-8, kDefaultTolRel = 2e-14;
+
+int calibrate_digits(ccT_plan *p) {
+  const int64_t n = (int64_t)p->tuples.size();
+  std::vector<int64_t> idx;
+  for (int q = 0; q < kCalSamples; q++) {
+    const int64_t t = n <= 1 ? 0 : (int64_t)q * (n - 1) / (kCalSamples - 1);
+    if (idx.empty() || idx.back() != t) idx.push_back(t);
+  }
+  auto weight = [&](int64_t t) { return p->tuples[t].kind == kIJK ? 1.0 : 0.5; };
+  double wsum_all = 0.0;
+  for (const Tuple &t : p->tuples) wsum_all += t.kind == kIJK ? 1.0 : 0.5;
+  const bool prof = p->profiling;
+  p->profiling = false;
+  std::vector<double> e64(idx.size());
+  double esum = 0.0, wsum = 0.0;
+  int s = CCT_OK;
+  for (size_t q = 0; q < idx.size() && s == CCT_OK; q++) {
+    s = tuple_energy(p, idx[q], true, &e64[q]);
+    esum += e64[q];
+    wsum += weight(idx[q]);
+  }
+  const double e_est = wsum > 0.0 ? esum / wsum * wsum_all : 0.0;
+  const double tol = p->opt.emu_tol > 0.0 ? p->opt.emu_tol : kDefaultTol;
+  const double rel = p->opt.emu_tol_rel > 0.0 ? p->opt.emu_tol_rel : kDefaultTolRel;
+  const double target = std::fmax(tol, rel * std::fabs(e_est));
+  int chosen = p->emu.slices;
+  double chosen_err = INFINITY;
+  for (int sl = kEmuMinSlices; sl <= p->emu.slices && s == CCT_OK; sl++) {
+    p->emu.run_slices = sl;
+    double worst = 0.0;
+    for (size_t q = 0; q < idx.size() && s == CCT_OK; q++) {
+      double e = 0.0;
+      s = tuple_energy(p, idx[q], false, &e);
+      const double err = std::fabs(e - e64[q]) / weight(idx[q]);
+      worst = std::isfinite(err) ? std::fmax(worst, err) : INFINITY;
+    }
+    const double est = kCalSafety * worst * wsum_all;
+    if (s == CCT_OK && (est <= target || sl == p->emu.slices)) {
+      chosen = sl;
+      chosen_err = est;
+      break;
+    }
+  }
+  p->profiling = prof;
+  p->emu.run_slices = chosen;
+  p->emu_est_err = chosen_err;
+  p->emu_target = target;
+  return s;
+}
+
 [[noreturn]] void legacy_stop(const char *where, int status) {
   std::fprintf(stderr, "libcc_b200: %s failed: %s (%s)\n", where, ccT_status_string(status), last_error());
   std::fflush(stderr);
@@ -293,6 +385,8 @@ void ccT_options_default(ccT_options *opt) {
   opt->device = 0;
   opt->check_inputs = 1;
   opt->emu_slices = 0;
+  opt->emu_tol = kDefaultTol;
+  opt->emu_tol_rel = kDefaultTolRel;
 }
 
 const char *ccT_status_string(int status) {
@@ -340,8 +434,12 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   }
   if (o.precision == CCT_PREC_INT8_EMU &&
       o.emu_slices != 0 && (o.emu_slices < kEmuMinSlices || o.emu_slices > kEmuMaxSlices)) {
-    set_error("emu_slices must be 0 (default) or in [" + std::to_string(kEmuMinSlices) + ", " +
+    set_error("emu_slices must be 0 (automatic, the default) or in [" + std::to_string(kEmuMinSlices) + ", " +
               std::to_string(kEmuMaxSlices) + "]");
+    return CCT_ERR_INVALID;
+  }
+  if (!(o.emu_tol >= 0.0) || !(o.emu_tol_rel >= 0.0)) {
+    set_error("emu_tol and emu_tol_rel must be >= 0 (0 = default)");
     return CCT_ERR_INVALID;
   }
   int ndev = 0;
@@ -363,7 +461,7 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     // the emulated tile sets NP; the FP64 W-build (the backward's recompute)
     // takes the widest of its tiles that divides NP (NP is a multiple of 64,
     // 80 or 96, so 64, 40 or 48 always qualifies)
-    d.EBN = emu_choose_bn(nu, o.emu_slices ? o.emu_slices : kEmuDefaultSlices);
+    d.EBN = emu_choose_bn(nu, o.emu_slices ? o.emu_slices : kEmuMaxSlices);
     d.NP = round_up(nu, d.EBN);
     d.BN = 0;
     for (int bn : kBNChoices)
@@ -412,8 +510,10 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
       if ((s = dalloc(&p->X[b][g], nu2 * d.NP))) return fail(s);
   if (p->emulated) {
     EmuOperands &e = p->emu;
-    e.slices = o.emu_slices ? o.emu_slices : kEmuDefaultSlices;
-    e.adaptive = o.emu_slices == 0;  // 0: the default count is the maximum, each tile takes what it needs
+    e.slices = o.emu_slices ? o.emu_slices : kEmuMaxSlices;
+    e.run_slices = e.slices;         // an automatic plan lowers it at calibration
+    e.adaptive = o.emu_slices == 0;  // automatic: the calibrated count is the maximum, each tile takes what it needs
+    p->emu_auto = o.emu_slices == 0;
     e.KP8 = round_up(nu + no, kEmuKC);
     e.tiles_m = (nu2 + kEmuBM - 1) / kEmuBM;
     const int64_t rowsE = no * nu2, rowsF = no * no * d.NP;
@@ -465,32 +565,45 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   p->inputs_ready = false;
   p->fwd_begin = p->fwd_end = -1;
-  CCT_CUDA(cudaMemcpyAsync(p->eh, eh, no * 8, kind, p->stream));
-  CCT_CUDA(cudaMemcpyAsync(p->ep, ep, nu * 8, kind, p->stream));
-  CCT_CUDA(cudaMemcpyAsync(p->t1, t1, no * nu * 8, kind, p->stream));
-  CCT_CUDA(cudaMemcpyAsync(p->t2, t2, nu2 * no * no * 8, kind, p->stream));
-  CCT_CUDA(cudaMemcpyAsync(p->vm, vm, no * nu * no * no * 8, kind, p->stream));
-  CCT_CUDA(cudaMemcpyAsync(p->voe, voe, nu2 * no * no * 8, kind, p->stream));
+  // Device inputs on the plan's own (non-blocking) stream: the caller may
+  // still be writing them on any stream, so wait for the whole device.  On a
+  // caller stream (ccT_set_stream) the copies are ordered after its work.
+  if (mem == CCT_MEM_DEVICE && p->stream == p->own_stream) CCT_CUDA(cudaDeviceSynchronize());
+  // From here on a failure is recorded in s and the transient staging buffer
+  // is still freed.
+  int s = CCT_OK;
+  auto cuda = [&](cudaError_t e, const char *what) {
+    if (s == CCT_OK && e != cudaSuccess) {
+      set_error(std::string(what) + ": " + cudaGetErrorString(e));
+      s = e == cudaErrorMemoryAllocation ? CCT_ERR_NOMEM : CCT_ERR_CUDA;
+    }
+  };
+  cuda(cudaMemcpyAsync(p->eh, eh, no * 8, kind, p->stream), "copy eh");
+  cuda(cudaMemcpyAsync(p->ep, ep, nu * 8, kind, p->stream), "copy ep");
+  cuda(cudaMemcpyAsync(p->t1, t1, no * nu * 8, kind, p->stream), "copy t1");
+  cuda(cudaMemcpyAsync(p->t2, t2, nu2 * no * no * 8, kind, p->stream), "copy t2");
+  cuda(cudaMemcpyAsync(p->vm, vm, no * nu * no * no * 8, kind, p->stream), "copy vm");
+  cuda(cudaMemcpyAsync(p->voe, voe, nu2 * no * no * 8, kind, p->stream), "copy voe");
   const double *vvvo_dev = vvvo;
   double *staged = nullptr;
-  if (mem == CCT_MEM_HOST) {
+  if (s == CCT_OK && mem == CCT_MEM_HOST) {
     // the packed VVVO is only needed to build E; stage it in a transient
     // buffer.  Plain cudaMalloc/cudaFree: with the stream-ordered pool this
     // call took 0.12-0.21 s at no=24/nu=320 (3.2 GB staged), 0.08-0.10 s so.
-    CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&staged), nvvvo * 8));
-    CCT_CUDA(cudaMemcpyAsync(staged, vvvo, nvvvo * 8, cudaMemcpyHostToDevice, p->stream));
+    cuda(cudaMalloc(reinterpret_cast<void **>(&staged), nvvvo * 8), "stage vvvo");
+    if (s == CCT_OK) cuda(cudaMemcpyAsync(staged, vvvo, nvvvo * 8, cudaMemcpyHostToDevice, p->stream), "copy vvvo");
     vvvo_dev = staged;
   }
-  int s = CCT_OK;
-  if (p->opt.check_inputs) {
-    CCT_CUDA(cudaMemsetAsync(p->flags, 0, 16, p->stream));
-    s = launch_check_inputs(d, p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, vvvo_dev, p->flags, p->stream);
+  if (s == CCT_OK && p->opt.check_inputs) {
+    cuda(cudaMemsetAsync(p->flags, 0, 16, p->stream), "clear flags");
+    if (s == CCT_OK)
+      s = launch_check_inputs(d, p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, vvvo_dev, p->flags, p->stream);
   }
   if (s == CCT_OK) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
   if (s == CCT_OK && p->emulated) s = emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
   if (staged) {
-    cudaStreamSynchronize(p->stream);  // E is built before the staging buffer goes
+    cudaStreamSynchronize(p->stream);  // E is built (or the stream failed) before the staging buffer goes
     cudaFree(staged);
   }
   if (s != CCT_OK) return s;
@@ -509,6 +622,10 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
     CCT_TRY(check_denominators(p));
   }
   std::fill(p->e_built.begin(), p->e_built.end(), 1);
+  if (p->emu_auto) {
+    const int c = calibrate_digits(p);
+    if (c != CCT_OK) return c;
+  }
   p->inputs_ready = true;
   return CCT_OK;
 }
@@ -712,6 +829,76 @@ int ccT_emu_slice_histogram(ccT_plan *p, int64_t *hist, int32_t n) {
   CCT_CUDA(cudaMemcpy(h, p->emu.slice_hist, sizeof(h), cudaMemcpyDeviceToHost));
   for (int32_t s = 0; s < n && s <= kEmuMaxSlices; s++) hist[s] = (int64_t)h[s];
   return CCT_OK;
+}
+
+int ccT_emu_digits(const ccT_plan *p, int32_t *digits, double *est_err, double *target) {
+  if (!p) {
+    set_error("plan is NULL");
+    return CCT_ERR_INVALID;
+  }
+  if (!p->emulated) {
+    set_error("ccT_emu_digits: an FP64 plan has no digit count");
+    return CCT_ERR_STATE;
+  }
+  if (digits) *digits = p->emu.run_slices;
+  if (est_err) *est_err = p->emu_auto ? p->emu_est_err : 0.0;
+  if (target) *target = p->emu_auto ? p->emu_target : 0.0;
+  return CCT_OK;
+}
+
+int ccT_tuple_w(ccT_plan *p, int64_t tuple, double *w, int32_t mem) {
+  if (!p || !w) {
+    set_error("need a plan and an output pointer");
+    return CCT_ERR_INVALID;
+  }
+  if (mem != CCT_MEM_HOST && mem != CCT_MEM_DEVICE) {
+    set_error("mem must be CCT_MEM_HOST or CCT_MEM_DEVICE");
+    return CCT_ERR_INVALID;
+  }
+  if (!p->inputs_ready) {
+    set_error("ccT_tuple_w before ccT_set_inputs");
+    return CCT_ERR_STATE;
+  }
+  if (tuple < 0 || tuple >= (int64_t)p->tuples.size()) {
+    set_error("tuple index out of range");
+    return CCT_ERR_INVALID;
+  }
+  DeviceGuard guard(p->device);
+  CCT_TRY(adj_configure(p->device));
+  const int64_t n3 = (int64_t)p->d.nu * p->d.nu * p->d.nu;
+  // X buffer set 0 and the plan's stream, after everything already issued
+  CCT_CUDA(cudaStreamSynchronize(p->gemm_stream));
+  CCT_CUDA(cudaStreamSynchronize(p->red_stream));
+  double *wc = nullptr, *wf = nullptr;
+  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&wc), n3 * 8));
+  int s = CCT_OK;
+  if (mem == CCT_MEM_HOST) {
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&wf), n3 * 8);
+    if (e != cudaSuccess) {
+      set_error(std::string("ccT_tuple_w: ") + cudaGetErrorString(e));
+      s = CCT_ERR_NOMEM;
+    }
+  } else {
+    wf = w;
+  }
+  if (s == CCT_OK) CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
+  if (s == CCT_OK) s = wbuild_tuple(p, tuple, 0, false, p->stream);
+  if (s == CCT_OK) s = assemble_w_fortran(p->d, p->tuples[tuple], p->X[0], wc, wf, p->stream);
+  int werr = 0;
+  if (s == CCT_OK && cudaMemcpyAsync(&werr, p->flags + 1, 4, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess)
+    s = CCT_ERR_CUDA;
+  if (s == CCT_OK && mem == CCT_MEM_HOST &&
+      cudaMemcpyAsync(w, wf, n3 * 8, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess)
+    s = CCT_ERR_CUDA;
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess && s == CCT_OK) s = CCT_ERR_CUDA;
+  if (s == CCT_ERR_CUDA) set_error("ccT_tuple_w: a CUDA call failed");
+  cudaFree(wc);
+  if (mem == CCT_MEM_HOST && wf) cudaFree(wf);
+  if (s == CCT_OK && werr) {
+    set_error("an emulated W-build kernel ran out its bounded wait and unwound");
+    s = CCT_ERR_TIMEOUT;
+  }
+  return s;
 }
 
 int ccT_set_stream(ccT_plan *p, void *cuda_stream) {

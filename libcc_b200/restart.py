@@ -12,7 +12,11 @@ file that ``program.F90:42-49,195-223`` reads back:
 
 Every record is framed by a length marker before and after it.  The reference
 runs used 4-byte markers (the recorded file sizes only fit that, see
-``restart_file_size``); ``read`` detects 4- or 8-byte markers.
+``restart_file_size``); ``read`` detects 4- or 8-byte markers.  With 4-byte
+markers gfortran splits a record longer than 2,147,483,639 bytes into
+subrecords: a negative leading marker means another subrecord follows, a
+negative trailing marker that one came before (large T2/VOE records, e.g.
+no=40, nu=500, take this form).
 """
 from __future__ import annotations
 
@@ -24,35 +28,57 @@ import numpy as np
 from .synthetic import TriplesInputs
 
 
-def restart_file_size(no: int, nu: int, marker: int = 4, int_bytes: int = 8) -> int:
+# longest subrecord gfortran writes with 4-byte markers
+MAX_SUBRECORD = 2_147_483_639
+
+
+def _subrecords(nbytes: int, marker: int, max_sub: int) -> int:
+    return 1 if marker == 8 or nbytes <= max_sub else -(-nbytes // max_sub)
+
+
+def restart_file_size(no: int, nu: int, marker: int = 4, int_bytes: int = 8, max_sub: int = MAX_SUBRECORD) -> int:
     """Size in bytes of a triples.restart for (no, nu)."""
     nutr = nu * (nu + 1) // 2
-    doubles = no + nu + no * nu + 2 * nu * nu * no * no + no ** 3 * nu + no * nu * nutr
-    records = 8 + no * nu
-    return doubles * 8 + 2 * int_bytes + records * 2 * marker
+    payloads = [int_bytes, int_bytes] + [8 * n for n in (no, nu, no * nu, nu * nu * no * no, no ** 3 * nu,
+                                                         nu * nu * no * no)]
+    payloads += [8 * nutr] * (no * nu)
+    return sum(p + 2 * marker * _subrecords(p, marker, max_sub) for p in payloads)
 
 
-def _write_record(fh, payload: bytes, marker: int):
+def _write_record(fh, payload: bytes, marker: int, max_sub: int = MAX_SUBRECORD):
+    """One record; with 4-byte markers split into gfortran subrecords of at most
+    max_sub bytes (leading marker negative while more follow, trailing marker
+    negative on every subrecord after the first)."""
     fmt = "<i" if marker == 4 else "<q"
-    n = struct.pack(fmt, len(payload))
-    fh.write(n)
-    fh.write(payload)
-    fh.write(n)
+    if marker == 8 or len(payload) <= max_sub:
+        n = struct.pack(fmt, len(payload))
+        fh.write(n)
+        fh.write(payload)
+        fh.write(n)
+        return
+    view = memoryview(payload)
+    nsub = _subrecords(len(payload), marker, max_sub)
+    for q in range(nsub):
+        part = view[q * max_sub:(q + 1) * max_sub]
+        fh.write(struct.pack(fmt, -len(part) if q < nsub - 1 else len(part)))
+        fh.write(part)
+        fh.write(struct.pack(fmt, -len(part) if q > 0 else len(part)))
 
 
-def write(path, inp: TriplesInputs, marker: int = 4) -> int:
-    """Write ``inp`` as a triples.restart; returns the file size."""
+def write(path, inp: TriplesInputs, marker: int = 4, max_sub: int = MAX_SUBRECORD) -> int:
+    """Write ``inp`` as a triples.restart; returns the file size.  ``max_sub``
+    is the subrecord limit of 4-byte markers (gfortran's by default)."""
     path = pathlib.Path(path)
     no, nu = inp.no, inp.nu
     nutr = nu * (nu + 1) // 2
     with open(path, "wb") as fh:
-        _write_record(fh, struct.pack("<q", no), marker)
-        _write_record(fh, struct.pack("<q", nu), marker)
+        _write_record(fh, struct.pack("<q", no), marker, max_sub)
+        _write_record(fh, struct.pack("<q", nu), marker, max_sub)
         for a in (inp.eh, inp.ep, inp.t1, inp.t2, inp.vm, inp.voe):
-            _write_record(fh, np.ascontiguousarray(a, dtype="<f8").tobytes(), marker)
+            _write_record(fh, np.ascontiguousarray(a, dtype="<f8").tobytes(), marker, max_sub)
         cols = inp.vvvo.reshape(no * nu, nutr)
         for j in range(no * nu):
-            _write_record(fh, np.ascontiguousarray(cols[j], dtype="<f8").tobytes(), marker)
+            _write_record(fh, np.ascontiguousarray(cols[j], dtype="<f8").tobytes(), marker, max_sub)
     return path.stat().st_size
 
 
@@ -79,19 +105,33 @@ def read(path) -> TriplesInputs:
     fmt = "<i" if marker == 4 else "<q"
     pos = 0
 
-    def record(expect_bytes: int) -> memoryview:
+    def record(expect_bytes: int):
         nonlocal pos
-        if pos + marker > len(buf):
-            raise RestartFormatError("error reading restart file: truncated")
-        (n,) = struct.unpack_from(fmt, buf, pos)
-        if n != expect_bytes:
-            raise RestartFormatError(f"error reading restart file: record of {n} bytes, expected {expect_bytes}")
-        start = pos + marker
-        end = start + n
-        if end + marker > len(buf) or struct.unpack_from(fmt, buf, end)[0] != n:
-            raise RestartFormatError("error reading restart file: bad record trailer")
-        pos = end + marker
-        return memoryview(buf)[start:end]
+        parts, total, first = [], 0, True
+        while True:
+            if pos + marker > len(buf):
+                raise RestartFormatError("error reading restart file: truncated")
+            (head,) = struct.unpack_from(fmt, buf, pos)
+            n = abs(head)
+            start = pos + marker
+            end = start + n
+            if end + marker > len(buf):
+                raise RestartFormatError("error reading restart file: truncated")
+            (tail,) = struct.unpack_from(fmt, buf, end)
+            # trailing marker: +n on the first subrecord, -n on the ones after it
+            if abs(tail) != n or (tail < 0) == first:
+                raise RestartFormatError("error reading restart file: bad record trailer")
+            parts.append(memoryview(buf)[start:end])
+            total += n
+            pos = end + marker
+            first = False
+            if head >= 0:
+                break
+            if total > expect_bytes:
+                break
+        if total != expect_bytes:
+            raise RestartFormatError(f"error reading restart file: record of {total} bytes, expected {expect_bytes}")
+        return parts[0] if len(parts) == 1 else b"".join(parts)
 
     no = struct.unpack("<q", record(8))[0]
     nu = struct.unpack("<q", record(8))[0]

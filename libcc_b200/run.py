@@ -12,31 +12,8 @@ triples.F90:316) with the device time.
 from __future__ import annotations
 
 import argparse
-import ctypes
 import sys
 import time
-
-
-def make_plan(no: int, nu: int, form: str, device: int = 0):
-    from . import _native as N
-    from .api import TriplesPlan
-    if form == "fp64":
-        return TriplesPlan(no, nu, device=device)
-    if not form.startswith("int8"):
-        raise ValueError("form must be fp64 or int8[:digits]")
-    digits = int(form.split(":")[1]) if ":" in form else 0
-    lib = N.load()
-    opt = N.Options()
-    lib.ccT_options_default(ctypes.byref(opt))
-    opt.precision = N.CCT_PREC_INT8_EMU
-    opt.device = device
-    opt.emu_slices = digits
-    h = ctypes.c_void_p()
-    N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
-    plan = TriplesPlan.__new__(TriplesPlan)
-    plan._h, plan.no, plan.nu, plan.precision, plan.device = h, no, nu, form, device
-    plan.num_tuples = int(lib.ccT_num_tuples(no))
-    return plan
 
 
 def main(argv=None) -> int:
@@ -45,7 +22,9 @@ def main(argv=None) -> int:
     src = ap.add_mutually_exclusive_group(required=True)
     src.add_argument("--workload", help="named synthetic workload (libcc_b200.synthetic.WORKLOADS)")
     src.add_argument("--restart", help="path of a triples.restart file")
-    ap.add_argument("--form", default="fp64", help="fp64 or int8[:digits] (default fp64)")
+    ap.add_argument("--form", default="fp64",
+                    help="fp64, int8 (automatic digits), int8:S (S digits) or int8@R (relative target R); "
+                         "default fp64")
     ap.add_argument("--tuples", type=int, default=0, help="run only the first N tuples (default all)")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--backward", action="store_true",
@@ -53,9 +32,9 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
 
     from . import restart, synthetic
-    from .api import format_energies
+    from .api import TriplesPlan, format_energies
     inp = synthetic.workload(args.workload) if args.workload else restart.read(args.restart)
-    with make_plan(inp.no, inp.nu, args.form, args.device) as plan:
+    with TriplesPlan.for_form(inp.no, inp.nu, args.form, args.device) as plan:
         t0 = time.perf_counter()
         plan.set_system(inp)
         t1 = time.perf_counter()
@@ -65,6 +44,9 @@ def main(argv=None) -> int:
         print(format_energies(ets, etd))
         print(f" device ms={plan.last_forward_ms:.3f} set_inputs s={t1 - t0:.3f} "
               f"launches={plan.last_forward_launches}")
+        if plan.precision == "int8":
+            print(" emulated digits: {digits} (calibrated |dE(T)| bound {est_err:.3g} Eh, target {target:.3g} Eh)"
+                  .format(**plan.emu_digits()))
         if args.backward:
             plan.backward(0, end)
             print(f" backward device ms={plan.last_backward_ms:.3f} "

@@ -64,6 +64,73 @@ def test_no12_nu120_golden(api):
     assert abs(ets - g["ets"]) <= tol(g["ets"], rel_tol=1e-12)
 
 
+@pytest.mark.parametrize("name", ["no16-nu200", "no24-nu320"])
+def test_benchmark_shapes_golden(api, name):
+    """FP64 E(T), etd, ets and the v1 norm at the benchmark shapes (no=16/nu=200,
+    no=24/nu=320 with log-uniform magnitudes) against the oracle's stored values."""
+    g = GOLDEN[name]
+    inp = S.workload(name)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        ets, etd, v1 = plan.forward()
+    assert abs(ets + etd - g["e_t"]) <= tol(g["e_t"])
+    assert abs(etd - g["etd"]) <= tol(g["etd"])
+    assert abs(ets - g["ets"]) <= tol(g["ets"], rel_tol=1e-12)
+    assert abs(np.linalg.norm(v1) - g["v1_norm"]) <= 1e-12 * g["v1_norm"]
+
+
+def test_no24_nu320_emulated_golden(api):
+    """The headline workload through the emulated forms: 5 fixed digits and the
+    automatic count at the Ar6-scale relative target (2.1e-7 |E|), each
+    against the oracle's stored E(T)."""
+    g = GOLDEN["no24-nu320"]
+    inp = S.workload("no24-nu320")
+    for kw, bar in ((dict(emu_slices=5), 1e-10), (dict(emu_tol_rel=2.1e-7), 2.1e-7)):
+        with api.TriplesPlan(inp.no, inp.nu, precision="int8", **kw) as plan:
+            plan.set_system(inp)
+            ets, etd, v1 = plan.forward()
+        assert abs(ets + etd - g["e_t"]) <= bar * abs(g["e_t"]), (kw, ets + etd, g["e_t"])
+        assert abs(np.linalg.norm(v1) - g["v1_norm"]) <= 1e-6 * g["v1_norm"], kw
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_tuple_w_fp64_matches_oracle(api, oracle, kind):
+    """ccT_tuple_w of the FP64 plan against the oracle's literal W, one tuple of
+    each kind."""
+    no, nu = 6, 21
+    inp = S.generate(no, nu, 71)
+    tuples = oracle.all_tuples(no)
+    t = next(q for q, tup in enumerate(tuples) if tup[0] == kind)
+    with api.TriplesPlan(no, nu) as plan:
+        plan.set_system(inp)
+        w = plan.tuple_w(t)
+    w_ref = oracle.c_tuple_w(inp, *tuples[t])
+    assert np.abs(w - w_ref).max() <= 1e-13 * np.abs(w_ref).max()
+
+
+def test_restart_file_through_the_gpu(api, oracle, tmp_path):
+    """A triples.restart written with gfortran's record layout, read back and run
+    through the CUDA path (plan API and the command line), against the oracle."""
+    import subprocess
+    import sys
+    from libcc_b200 import restart as R
+    inp = S.generate(5, 27, 19)
+    f = tmp_path / "triples.restart"
+    R.write(f, inp, marker=4, max_sub=4096)  # the T2/VOE records split into subrecords
+    back = R.read(f)
+    ets_o, etd_o, v1_o = oracle.c_cc_triples(inp)
+    with api.TriplesPlan(back.no, back.nu) as plan:
+        plan.set_system(back)
+        ets, etd, v1 = plan.forward()
+    assert abs(etd - etd_o) <= tol(etd_o) and abs(ets - ets_o) <= tol(ets_o)
+    assert np.abs(v1 - v1_o).max() <= 1e-12 * max(1.0, np.abs(v1_o).max())
+    root = pathlib.Path(__file__).resolve().parent.parent
+    out = subprocess.run([sys.executable, "-m", "libcc_b200.run", "--restart", str(f)], cwd=root,
+                         capture_output=True, text=True, check=True).stdout
+    line = next(x for x in out.splitlines() if "ets/etd/ets+etd=" in x)
+    assert line == api.format_energies(ets_o, etd_o) or abs(float(line.split()[-1]) - (ets_o + etd_o)) <= 1e-9
+
+
 def test_tuple_kinds_one_at_a_time(api, oracle):
     """Every tuple of every kind alone, against the reference pipeline of that kind."""
     no, nu = 5, 11
@@ -107,6 +174,31 @@ def test_device_inputs_match_host_inputs(api):
         plan.set_system(inp)
         host = plan.forward()
         dev = [torch.from_numpy(a).cuda() for a in inp.arrays()]
+        plan.set_inputs(*dev)
+        devr = plan.forward()
+    assert host[0] == devr[0] and host[1] == devr[1]
+
+
+def test_device_inputs_written_on_a_side_stream(api):
+    """Device inputs produced by kernels still running on another stream: the
+    plan's own stream waits for the device, so it reads the finished values."""
+    torch = pytest.importorskip("torch")
+    inp = S.generate(4, 23, 13)
+    with api.TriplesPlan(inp.no, inp.nu) as plan:
+        plan.set_system(inp)
+        host = plan.forward()
+        side = torch.cuda.Stream()
+        srcs = [torch.from_numpy(a).cuda() for a in inp.arrays()]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            # long enough that a reader which does not wait sees the zeros
+            dev = [torch.zeros_like(x) for x in srcs]
+            big = torch.randn(4096, 4096, device="cuda")
+            for _ in range(20):
+                big = big @ big
+                big /= big.norm()
+            for d, x in zip(dev, srcs):
+                d.copy_(x + 0.0 * big[0, 0])
         plan.set_inputs(*dev)
         devr = plan.forward()
     assert host[0] == devr[0] and host[1] == devr[1]

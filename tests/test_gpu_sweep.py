@@ -1,7 +1,7 @@
 """Seeded sweep over small and edge-sized systems (nu from 1 to 129, no from 2
 to 8, normal and log-uniform magnitudes): the FP64 forward against the C
-oracle, both emulated forms (7 fixed digits; per-tile digits, at most 5)
-against the oracle, the gradient against the hand-derived CPU adjoint where
+oracle, both emulated forms (7 fixed digits; automatic digits against the
+default 1e-8 Eh target) against the oracle, the gradient against the hand-derived CPU adjoint where
 nu <= 24, and the batch against single-system plans bitwise."""
 import numpy as np
 import pytest
@@ -32,7 +32,6 @@ def _rel(a, b):
 @pytest.mark.parametrize("no,nu,seed,dist", CASES)
 def test_sweep_forward_gradient_and_emulation(no, nu, seed, dist):
     from libcc_b200 import api as A
-    from libcc_b200.run import make_plan
     from oracle import oracle as O
     inp = S.generate(no, nu, seed, dist)
     ets_o, etd_o, v1_o = O.c_cc_triples(inp)
@@ -47,11 +46,15 @@ def test_sweep_forward_gradient_and_emulation(no, nu, seed, dist):
             ref = O.closed_grad(inp)
             for k in g:
                 assert _rel(g[k], ref[k]) <= 1e-12, k
-    for form, bar in (("int8:7", 1e-11), ("int8", 3e-8)):
-        with make_plan(no, nu, form) as p:
-            p.set_system(inp)
-            ets, etd, _ = p.forward()
-        assert abs(ets + etd - e_o) <= bar * abs(e_o), form
+    with A.TriplesPlan.for_form(no, nu, "int8:7") as p:
+        p.set_system(inp)
+        ets, etd, _ = p.forward()
+    assert abs(ets + etd - e_o) <= 1e-11 * abs(e_o) + 1e-14
+    with A.TriplesPlan.for_form(no, nu, "int8") as p:  # automatic digits, 1e-8 Eh target
+        p.set_system(inp)
+        ets, etd, _ = p.forward()
+        cal = p.emu_digits()
+    assert abs(ets + etd - e_o) <= cal["target"] + 2e-14 * abs(e_o), (cal, ets + etd, e_o)
 
 
 def test_sweep_batch_equals_plans_bitwise():
