@@ -3,19 +3,27 @@
 
 One step is one full (T) evaluation -- every tuple of the workload, including
 the degenerate (i,j,j)/(i,i,j) tuples -- through the library's plan API, with
-inputs already resident in HBM.  Both forms are timed: the native FP64 form
-(mma.sync f64) and the split-integer emulated form (tcgen05 INT8); the
-headline value is the emulated form, the native one is reported beside it with
-the speed-up and the relative energy difference.  ``e2e`` repeats the headline
-step through the C ABI from pinned host buffers (plan create, host->device
-upload, operand build, all tuples, v1/energy read-back, destroy).
+inputs already resident in HBM.  Three forms are timed: the headline emulated
+form (split-integer FP64 on tcgen05 INT8, digit count calibrated to the
+Ar6-scale relative reading of the 1e-8 Eh bar, 2.1e-7 |E(T)|: the workload's
+|E(T)| = 7.7e9 Eh puts an absolute 1e-8 Eh below FP64 resolution), the
+native FP64 form (mma.sync f64) and the library's default emulated form
+(digits calibrated to max(1e-8 Eh, 2e-14 |E(T)|), the round-off of an FP64
+evaluation at this scale).  ``e2e`` repeats the headline step through the C
+ABI from pinned host buffers (plan create, host->device upload, operand build
+and digit calibration, all tuples, v1/energy read-back, destroy).
+
+Output: one JSON line of extras (every form in full, the per-config accuracy
+table, the adjoint, the batch, per-tile digits, the CPU baseline's detail),
+then the headline JSON line last.
 
 Under torchrun (N>1) the tuple list is split into cost-balanced contiguous
 shards, one per rank; the partial (ets, etd) are summed with one NCCL
 all-reduce, the only exchange step (the reference's ddi_gsumf).
 
-``--impl reference`` times the CPU stand-in for the reference's triples.x (the
-literal 12-DGEMM/trant3/DRT1WT3 restatement with OpenBLAS) on rank 0.
+``--impl reference`` times the CPU stand-in for the reference's triples.x on
+rank 0: the literal triples-abc pipeline of oracle/triples_oracle.c (OpenMP
+TRANT3/T3SQUA/ADT3DEN/SMT3FOUR) with every DGEMM on the image's OpenBLAS.
 """
 from __future__ import annotations
 
@@ -34,6 +42,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "(T) time & TFLOP/s: emulated vs native FP64 on 1 B200 at |ΔE(T)|≤1e-8 Eh"
 DEFAULT_WORKLOAD = "no24-nu320"
+HEADLINE_FORM = "int8@2.1e-7"     # automatic digits, target 2.1e-7 |E| = 1e-8 Eh on Ar6's 0.048 Eh
+DEFAULT_FORM = "int8"             # library default: automatic digits, target max(1e-8 Eh, 2e-14 |E|)
 
 
 def parse():
@@ -47,7 +57,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint (no=12/nu=120) and batched-systems (96 uneven) measurements")
-    ap.add_argument("--emu-slices", type=int, default=5, help="7-bit digits per operand of the emulated form (4..7)")
+    ap.add_argument("--form", default=HEADLINE_FORM,
+                    help="headline emulated form: int8@R (automatic digits, relative target R; default "
+                         "int8@2.1e-7), int8 (the library default target) or int8:S (S digits)")
+    ap.add_argument("--compare-steps", type=int, default=2,
+                    help="timed steps (after one warm-up) of the FP64 and library-default comparison forms")
     return ap.parse_args()
 
 
@@ -138,24 +152,41 @@ def golden(workload: str):
     return json.loads(f.read_text()).get(workload)
 
 
-def cpu_sample(inp, budget_s: float = 12.0):
-    """Time the literal CPU restatement on i>j>k tuples of the workload until the
-    budget is spent (at least one tuple).  Returns (TFLOP/s, tuples, seconds, threads)."""
+def cpu_sample(inp, min_tuples: int = 8, budget_s: float = 15.0):
+    """Time the BLAS-backed literal CPU pipeline (oracle.blas_cc_triples) on
+    consecutive i>j>k tuples of the workload: at least min_tuples, more while
+    the budget lasts.  Returns a dict with the rate, the DGEMM share and the
+    DGEMM rate against a plain OpenBLAS DGEMM on the same cores."""
     from oracle import oracle as O
     tuples = [t for t in O.all_tuples(inp.no) if t[0] == 0]
     flop_per = 12.0 * inp.nu ** 3 * (inp.no + inp.nu)
-    O.literal_cc_triples(inp, tuples=tuples[:1])  # page in, build caches
-    done, t0 = 0, time.perf_counter()
-    while done < len(tuples):
-        O.literal_cc_triples(inp, tuples=tuples[done:done + 1])
+    O.blas_cc_triples(inp, tuples=tuples[:1])  # page in
+    done, secs, dg = 0, 0.0, 0.0
+    while done < len(tuples) and (done < min_tuples or secs < budget_s):
+        r = O.blas_cc_triples(inp, tuples=tuples[done:done + 1])
+        secs += r[3]
+        dg += r[4]
         done += 1
-        if time.perf_counter() - t0 >= budget_s:
-            break
-    dt = time.perf_counter() - t0
-    return flop_per * done / dt / 1e12, done, dt, O.cpu_threads()
+    peak = O.openblas_dgemm_tflops(4096)
+    dg_tf = flop_per * done / dg / 1e12 if dg > 0 else None
+    return {"tflops": flop_per * done / secs / 1e12, "tuples": done, "seconds": secs, "threads": O.cpu_threads(),
+            "dgemm_seconds": dg, "dgemm_share": dg / secs if secs > 0 else None, "dgemm_tflops": dg_tf,
+            "openblas_dgemm_peak_tflops": peak, "dgemm_frac_of_openblas_peak": (dg_tf / peak) if dg_tf else None}
+
+
+def cpu_sample_text(c, name):
+    return (f"{c['tuples']} i>j>k tuples of {name} in {c['seconds']:.1f} s: literal triples-abc pipeline "
+            f"(12 DGEMMs on OpenBLAS, OpenMP TRANT3/T3SQUA/ADT3DEN/SMT3FOUR, DGEMM-form T1WT3IJK) on "
+            f"{c['threads']} threads; DGEMM {100 * c['dgemm_share']:.0f}% of the time at "
+            f"{c['dgemm_tflops']:.3f} TFLOP/s = {c['dgemm_frac_of_openblas_peak']:.2f} of a 4096^3 OpenBLAS DGEMM "
+            f"({c['openblas_dgemm_peak_tflops']:.3f} TFLOP/s)")
 
 
 def run_reference(args, rank, world):
+    """The reference arm: one step = one i>j>k tuple of the workload through the
+    BLAS-backed literal CPU pipeline (the reference's CPU algorithm, restated;
+    the Fortran triples.x cannot be built here).  value = TFLOP/s of the timed
+    tuples; ms_per_step = measured milliseconds per tuple."""
     if rank != 0:
         return 0
     from libcc_b200 import synthetic as S
@@ -164,34 +195,35 @@ def run_reference(args, rank, world):
     inp = S.workload(args.workload)
     tuples = [t for t in O.all_tuples(inp.no) if t[0] == 0]
     flop_per = 12.0 * inp.nu ** 3 * (inp.no + inp.nu)
-    per_step = 1
     for w in range(args.warmup):
-        O.literal_cc_triples(inp, tuples=tuples[w % len(tuples):w % len(tuples) + per_step])
-    t0 = time.perf_counter()
+        O.blas_cc_triples(inp, tuples=[tuples[w % len(tuples)]])
+    secs, dg = 0.0, 0.0
     for s in range(args.steps):
-        a = (args.warmup + s) % len(tuples)
-        O.literal_cc_triples(inp, tuples=tuples[a:a + per_step])
-    dt = time.perf_counter() - t0
-    tf = flop_per * per_step * args.steps / dt / 1e12
-    full_ms = S.flops(inp.no, inp.nu) / (tf * 1e12) * 1e3
-    sample = (f"{per_step} i>j>k tuple per step of {inp.name}; literal 12-DGEMM + trant3 + T3SQUA/ADT3DEN/DRT1WT3 "
-              f"restatement (oracle/oracle.py) with OpenBLAS DGEMM, {O.cpu_threads()} threads")
+        r = O.blas_cc_triples(inp, tuples=[tuples[(args.warmup + s) % len(tuples)]])
+        secs += r[3]
+        dg += r[4]
+    tf = flop_per * args.steps / secs / 1e12
+    full_s = S.flops(inp.no, inp.nu) / (tf * 1e12)
+    thr = O.cpu_threads()
+    sample = (f"1 i>j>k tuple of {inp.name} per step; literal triples-abc pipeline with OpenBLAS DGEMMs "
+              f"(DGEMM {100 * dg / secs:.0f}% of the time) and OpenMP permutations on {thr} threads")
     line = {"impl": "reference", "metric": METRIC, "value": tf, "unit": "TFLOP/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_desc(inp, cfg["dist"]), "form": "cpu-literal-port"},
-            "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": O.cpu_threads(), "kind": "port",
-                             "sample": sample},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(inp, cfg["dist"]), "form": "cpu-literal-port",
+                       "step": "one i>j>k tuple"},
+            "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": thr, "kind": "port", "sample": sample},
             "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "ms_per_step extrapolates the sampled tuples/s to all tuples of the workload"}
+            "full_evaluation_seconds_at_this_rate": full_s}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def adjoint_extra(A, S, local):
     """Forward + hand-written adjoint on the no=12/nu=120 system (seed 3): device
-    times, their ratio, and the gradient against the stored hand-derived FP64 CPU
-    gradient (200 seeded entries per input) and a few central differences."""
+    times, their ratio, the gradient against the stored hand-derived FP64 CPU
+    gradient (200 seeded entries per input), a few central differences, and a
+    step-size sweep of the dVOE central differences."""
     import copy
     import numpy as np
     g0 = json.loads((ROOT / "tests" / "golden" / "grad_no12-nu120.json").read_text())
@@ -209,6 +241,17 @@ def adjoint_extra(A, S, local):
         for name, ref in g0["tensors"].items():
             idx = np.array(ref["index"])
             rel[name] = float(np.abs(g[name][idx] - np.array(ref["value"])).max() / ref["maxabs"])
+
+        def fd(name, idx, h):
+            vals = []
+            for sgn in (1.0, -1.0):
+                ip = copy.deepcopy(inp)
+                getattr(ip, name)[idx] += sgn * h
+                plan.set_system(ip)
+                e1, e2, _ = plan.forward(want_v1=False)
+                vals.append(e1 + e2)
+            return (vals[0] - vals[1]) / (2 * h)
+
         rng = np.random.default_rng(5)
         fd_rel = {}
         for name in g0["tensors"]:
@@ -216,32 +259,35 @@ def adjoint_extra(A, S, local):
             worst = 0.0
             for idx in rng.choice(arr.size, size=2, replace=False):
                 h = 1e-5 * max(1.0, abs(arr[idx]))
-                vals = []
-                for sgn in (1.0, -1.0):
-                    ip = copy.deepcopy(inp)
-                    getattr(ip, name)[idx] += sgn * h
-                    plan.set_system(ip)
-                    e1, e2, _ = plan.forward(want_v1=False)
-                    vals.append(e1 + e2)
-                fd = (vals[0] - vals[1]) / (2 * h)
-                worst = max(worst, abs(fd - g[name][idx]) / g0["tensors"][name]["maxabs"])
+                worst = max(worst, abs(fd(name, idx, h) - g[name][idx]) / g0["tensors"][name]["maxabs"])
             fd_rel[name] = worst
+        sweep = {}
+        voe_idx = [int(np.argmax(np.abs(g["voe"]))), int(rng.integers(inp.voe.size))]
+        for h in (1e-4, 1e-5, 1e-6):
+            sweep[f"{h:g}"] = max(abs(fd("voe", q, h) - g["voe"][q]) / g0["tensors"]["voe"]["maxabs"]
+                                  for q in voe_idx)
     return {"workload": "no12-nu120 (seed 3, normal)", "forward_ms": f_ms, "backward_ms": b_ms,
             "ratio_backward_over_forward": b_ms / f_ms, "e_t": ets + etd,
             "max_rel_err_vs_cpu_gradient": rel, "central_difference_h": 1e-5,
             "max_rel_err_vs_central_differences": fd_rel,
-            "note": "backward recomputes W per tuple in FP64; rel errors are relative to max|gradient| per input"}
+            "dvoe_central_difference_step_sweep": sweep,
+            "note": "backward recomputes W per tuple in FP64; rel errors are relative to max|gradient| per input; "
+                    "the sweep takes the largest-|g| VOE entry and one random entry"}
 
 
 def adaptive_extra(A, S, local):
-    """Per-tile digit counts of the emulated form (emu_slices = 0, at most 5) against
-    fixed 5 digits and native FP64 on the no=16/nu=200 system with magnitudes
-    falling 2^-0.25 per virtual index (synthetic.with_decay): device time of a
-    whole (T) step, the digit histogram over W tiles and the error vs FP64."""
+    """Per-tile digit counts of an automatic emulated plan against the same
+    count on every tile and native FP64 on the no=16/nu=200 system with
+    magnitudes falling 2^-0.25 per virtual index (synthetic.with_decay): device
+    time of a whole (T) step, the digit histogram over W tiles and the error
+    against FP64."""
     inp = S.with_decay(S.workload("no16-nu200"), 0.25)
     res = {}
-    for form in ("fp64", "int8:5", "int8"):
-        with make_plan(A, inp.no, inp.nu, local, form) as plan:
+    forms = ["fp64", "int8"]
+    k = 0
+    while k < len(forms):
+        form = forms[k]
+        with A.TriplesPlan.for_form(inp.no, inp.nu, form, device=local) as plan:
             plan.set_system(inp)
             times = []
             for _ in range(3):
@@ -249,17 +295,107 @@ def adaptive_extra(A, S, local):
                 times.append(plan.last_forward_ms)
             res[form] = {"ms": statistics.median(times[1:]), "e_t": ets + etd,
                          "digit_histogram": plan.emu_slice_histogram() if form != "fp64" else None}
+            if form == "int8":
+                res[form]["calibration"] = plan.emu_digits()
+                forms.append(f"int8:{res[form]['calibration']['digits']}")
+        k += 1
+    fixed = forms[2]
     ref = res["fp64"]["e_t"]
-    for form in ("int8:5", "int8"):
+    for form in forms[1:]:
         res[form]["rel_err_vs_fp64"] = abs(res[form]["e_t"] - ref) / abs(ref)
     return {"workload": "no16-nu200 (seed 1, normal) with magnitudes x 2^(-0.25 a) per virtual index a",
-            "fp64_ms": res["fp64"]["ms"], "fixed5_ms": res["int8:5"]["ms"], "per_tile_ms": res["int8"]["ms"],
-            "speedup_per_tile_over_fixed5": res["int8:5"]["ms"] / res["int8"]["ms"],
-            "fixed5_rel_err_vs_fp64": res["int8:5"]["rel_err_vs_fp64"],
+            "fp64_ms": res["fp64"]["ms"], "fixed_ms": res[fixed]["ms"], "fixed_form": fixed,
+            "per_tile_ms": res["int8"]["ms"], "speedup_per_tile_over_fixed": res[fixed]["ms"] / res["int8"]["ms"],
+            "fixed_rel_err_vs_fp64": res[fixed]["rel_err_vs_fp64"],
             "per_tile_rel_err_vs_fp64": res["int8"]["rel_err_vs_fp64"],
             "per_tile_digit_histogram": res["int8"]["digit_histogram"],
-            "note": "histogram index = 7-bit digits per operand of a 128 x N W tile; the bench headline runs "
-                    "fixed 5 digits, where the per-tile rule also picks 5 on every tile of its workload"}
+            "calibration": res["int8"]["calibration"],
+            "note": "histogram index = 7-bit digits per operand of a 128 x N W tile; the automatic plan runs the "
+                    "calibrated count on the tiles that reach the system's top exponent, fewer on the others"}
+
+
+def _oracle_w(O, inp, tup):
+    return O.blas_tuple_w(inp, *tup)
+
+
+def _w_samples(no):
+    """Tuple indices for W checks: the first of each kind and the last i>j>k tuple."""
+    from oracle import oracle as O
+    tuples = O.all_tuples(no)
+    pick = []
+    for kd in (0, 1, 2):
+        q = next((t for t, tup in enumerate(tuples) if tup[0] == kd), None)
+        if q is not None:
+            pick.append(q)
+    last_ijk = max((t for t, tup in enumerate(tuples) if tup[0] == 0), default=None)
+    if last_ijk is not None and last_ijk not in pick:
+        pick.append(last_ijk)
+    return pick
+
+
+def form_accuracy(A, plan_factory, inp, e_ref, w_refs, forms, local):
+    """Per form: E(T) against the oracle's (|dE| in Eh, relative), the max over
+    the sampled tuples of max|dW| / max|W| against the oracle's literal W, and
+    the calibrated digits of emulated forms."""
+    out = {}
+    for form in forms:
+        with plan_factory(form) as plan:
+            plan.set_system(inp)
+            ets, etd, _ = plan.forward(want_v1=False)
+            row = {"e_t": ets + etd, "abs_err_eh": abs(ets + etd - e_ref), "rel_err": abs(ets + etd - e_ref) / abs(e_ref)}
+            if w_refs:
+                worst = 0.0
+                for t, wr in w_refs.items():
+                    w = plan.tuple_w(t)
+                    worst = max(worst, float(abs(w - wr).max() / max(abs(wr).max(), 1e-300)))
+                row["max_rel_dW"] = worst
+            if form != "fp64":
+                row["digits"] = plan.emu_digits()
+                row["meets_target"] = row["abs_err_eh"] <= row["digits"]["target"]
+        out[form] = row
+    return out
+
+
+def accuracy_table(A, S, local, main_rows):
+    """|dE(T)| (Eh and relative) and max relative |dW_abc|
+    of the FP64 form, the default emulated form and the relative-target form
+    against the oracle (E(T) from tests/golden/energies.json or the C oracle;
+    W from the oracle's literal formv3/SYMT311/ZEROT3 with OpenBLAS DGEMMs on
+    one tuple of each kind plus the last i>j>k tuple)."""
+    from oracle import oracle as O
+    forms = ["fp64", DEFAULT_FORM, HEADLINE_FORM]
+    table = {}
+
+    def factory(inp):
+        return lambda form: A.TriplesPlan.for_form(inp.no, inp.nu, form, device=local)
+
+    for cfg, name in ((0, "water-avdz"), (1, "no16-nu200"), (4, "no12-nu120")):
+        g = golden(name)
+        inp = S.workload(name)
+        o = O.all_tuples(inp.no)
+        w_refs = {t: _oracle_w(O, inp, o[t]) for t in _w_samples(inp.no)}
+        table[f"config{cfg} {name}"] = form_accuracy(A, factory(inp), inp, g["e_t"], w_refs, forms, local)
+    table["config2 no24-nu320"] = main_rows
+    # config 3: the 8 smallest of the 96 batch systems, per-system plans against the C oracle
+    systems = S.batch96()
+    small = sorted(range(len(systems)), key=lambda k: S.flops(systems[k].no, systems[k].nu))[:8]
+    agg = {}
+    for k in small:
+        inp = systems[k]
+        e_o, d_o, _ = O.c_cc_triples(inp)
+        o = O.all_tuples(inp.no)
+        w_refs = {t: O.c_tuple_w(inp, *o[t]) for t in _w_samples(inp.no)}
+        rows = form_accuracy(A, factory(inp), inp, e_o + d_o, w_refs, forms, local)
+        for form, r in rows.items():
+            a = agg.setdefault(form, {"max_abs_err_eh": 0.0, "max_rel_err": 0.0, "max_rel_dW": 0.0, "all_meet_target": True})
+            a["max_abs_err_eh"] = max(a["max_abs_err_eh"], r["abs_err_eh"])
+            a["max_rel_err"] = max(a["max_rel_err"], r["rel_err"])
+            a["max_rel_dW"] = max(a["max_rel_dW"], r.get("max_rel_dW", 0.0))
+            if "meets_target" in r:
+                a["all_meet_target"] = a["all_meet_target"] and r["meets_target"]
+                a.setdefault("digits", []).append(r["digits"]["digits"])
+    table["config3 batch96 (8 smallest systems)"] = agg
+    return table
 
 
 def batch_extra(A, S, local):
@@ -355,6 +491,7 @@ def main():
     N = A.N
     peaks = {"fp64": N.load().ccT_measure_fp64_peak(local), "int8": N.load().ccT_measure_int8_peak(local)}
     g = golden(args.workload)
+    w_pick = _w_samples(no) if world == 1 and not args.no_extras else []
 
     def allreduce(vals, op="sum"):
         if dist is None:
@@ -363,19 +500,22 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX)
         return t.tolist()
 
-    def run_form(form, sampler):
+    def run_form(form, warmup, steps, sampler=None):
         plan = make_plan(A, no, nu, local, form)
+        t0 = time.perf_counter()
         plan.set_inputs(*dev_inputs)
+        set_s = time.perf_counter() - t0
         plan.set_stream(stream.cuda_stream)
 
         def step():
             ets, etd, _ = shard.sharded_cc_triples(plan, want_v1=False)
             return ets, etd
 
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             step()
         plan.set_profiling(True)
         launches, wb_ms, wb_n = 0, 0.0, 0
+        hist = [0] * 8
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
@@ -383,56 +523,69 @@ def main():
         if sampler is not None:
             sampler.__enter__()
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             ets, etd = step()
             launches += plan.last_forward_launches
             prof = plan.kernel_profile()
             wb_ms += prof["wbuild"][0]
             wb_n += prof["wbuild"][1]
+            if form != "fp64":
+                hist = [x + y for x, y in zip(hist, plan.emu_slice_histogram())]
         e1.record(stream)
         torch.cuda.synchronize()
         if sampler is not None:
             sampler.__exit__(None, None, None)
         if dist is not None:
             dist.barrier()
-        plan.close()
         ms = allreduce([e0.elapsed_time(e1)], op="max")[0]
-        ms_step = ms / args.steps
+        ms_step = ms / steps
         emu = form != "fp64"
-        S_ = int(form.split(":")[1]) if emu else 0
-        # algorithmic work of the W-build launches in the timed region
-        fp64_flop = my_flop_wb * args.steps
+        fp64_flop = my_flop_wb * steps  # algorithmic work of the W-build launches in the timed region
+        out = {"form": form, "ms_per_step": ms_step, "tflops": flop_step / (ms_step * 1e-3) / 1e12,
+               "steps": steps, "warmup": warmup, "set_inputs_s": set_s,
+               "ets": ets, "etd": etd, "e_t": ets + etd, "gpu_launches": launches}
         if emu:
-            ops = fp64_flop * S_ * (S_ + 1) / 2  # INT8 ops: S(S+1)/2 digit products per FP64 multiply-add
+            cal = plan.emu_digits()
+            # INT8 ops: s(s+1)/2 digit products per FP64 multiply-add on a tile of s digits
+            nitems = sum(hist)
+            avg_products = sum(h * s_ * (s_ + 1) / 2 for s_, h in enumerate(hist)) / max(nitems, 1)
+            ops = fp64_flop * avg_products
             achieved = ops / (wb_ms * 1e-3) / 1e12 if wb_ms > 0 else None
-            peak, unit, kern = peaks["int8"], "TOPS (int8)", "wbuild_emu_kernel (tcgen05.mma kind::i8, TMA, TMEM)"
+            peak, unit = peaks["int8"], "TOPS (int8)"
+            kern = f"wbuild_emu_kernel (tcgen05.mma kind::i8, merged digit products, bulk copies, TMEM; {cal['digits']} digits)"
             psrc = ("measured in this run: tcgen05.mma kind::i8 throughput with operands resident in shared memory "
                     "(ccT_measure_int8_peak); MEASURED_PEAKS.json has no INT8 entry")
-            per_launch = f"{S_ * (S_ + 1) // 2} x 12 nu^3 (no+nu) int8 ops for an i>j>k tuple, half for a degenerate tuple"
+            per_launch = (f"{avg_products:g} digit products x 12 nu^3 (no+nu) int8 ops for an i>j>k tuple, half for a "
+                          "degenerate tuple")
+            out["calibration"] = cal
+            out["digit_histogram"] = hist
         else:
             achieved = fp64_flop / (wb_ms * 1e-3) / 1e12 if wb_ms > 0 else None
             peak, unit, kern = peaks["fp64"], "TFLOP/s", "wbuild_f64_kernel (mma.sync m16n8k4 f64)"
             psrc = ("measured in this run: mma.sync f64 throughput microbenchmark (ccT_measure_fp64_peak); "
                     "MEASURED_PEAKS.json has no FP64 entry")
             per_launch = f"12 nu^3 (no+nu) = {12.0 * nu ** 3 * (no + nu):.4g} flop for an i>j>k tuple, half for a degenerate tuple"
-        out = {"form": form, "ms_per_step": ms_step, "tflops": flop_step / (ms_step * 1e-3) / 1e12,
-               "ets": ets, "etd": etd, "e_t": ets + etd, "gpu_launches": launches,
-               "roofline": {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak, "unit": unit,
-                            "frac": (achieved / peak) if (achieved and peak) else None,
-                            "traffic": read_traffic(args.workload, "emu" if emu else "f64"),
-                            "peak_source": psrc, "launches": wb_n, "avg_launch_ms": wb_ms / max(wb_n, 1),
-                            "work_per_launch": per_launch, "share_of_step": wb_ms / ms if ms > 0 else None}}
+        out["roofline"] = {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak, "unit": unit,
+                           "frac": (achieved / peak) if (achieved and peak) else None,
+                           "traffic": read_traffic(args.workload, "emu" if emu else "f64"),
+                           "peak_source": psrc, "launches": wb_n, "avg_launch_ms": wb_ms / max(wb_n, 1),
+                           "work_per_launch": per_launch, "share_of_step": wb_ms / ms if ms > 0 else None}
         if g is not None:
             out["abs_err_vs_oracle"] = abs(out["e_t"] - g["e_t"])
             out["rel_err_vs_oracle"] = abs(out["e_t"] - g["e_t"]) / abs(g["e_t"])
+        if w_pick:
+            out["w_samples"] = {t: plan.tuple_w(t) for t in w_pick}
+        plan.close()
         return out
 
-    emu_form = f"int8:{args.emu_slices}"
     clocks = ClockSampler(local)
-    forms = {"fp64": run_form("fp64", None), "int8_emu": run_form(emu_form, clocks)}
-    head = forms["int8_emu"]
-    rel_vs_native = abs(head["e_t"] - forms["fp64"]["e_t"]) / abs(forms["fp64"]["e_t"])
-    head["rel_err_vs_native_fp64"] = rel_vs_native
+    head = run_form(args.form, args.warmup, args.steps, clocks)
+    cw, cs = 1, max(1, args.compare_steps)
+    forms = {args.form: head, "fp64": run_form("fp64", cw, cs)}
+    if args.form != DEFAULT_FORM:
+        forms[DEFAULT_FORM] = run_form(DEFAULT_FORM, cw, cs)
+    native = forms["fp64"]
+    rel_vs_native = abs(head["e_t"] - native["e_t"]) / abs(native["e_t"])
 
     # end to end through the C ABI from pinned host buffers (headline form)
     e2e = None
@@ -448,14 +601,14 @@ def main():
         torch.cuda.empty_cache()
         if dist is not None:
             dist.barrier()
-        # three whole runs (plan, uploads, operand build, all tuples, teardown);
-        # the median is reported: the host side (large allocations, pinned
-        # copies) varies by a few tenths of a second from run to run
+        # three whole runs (plan, uploads, operand build and digit calibration,
+        # all tuples, teardown); the median is reported: the host side (large
+        # allocations, pinned copies) varies by a few tenths of a second from run to run
         runs, dev_runs, phases = [], [], []
         for _ in range(3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            with make_plan(A, no, nu, local, emu_form) as p2:
+            with make_plan(A, no, nu, local, args.form) as p2:
                 t1 = time.perf_counter()
                 p2.set_inputs(*pinned)
                 t2 = time.perf_counter()
@@ -470,46 +623,84 @@ def main():
             runs.append(allreduce([t4 - t0], op="max")[0])
         e2e_s = statistics.median(runs)
         e2e = {"value": flop_step / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "seconds_per_run": runs,
-               "forward_device_seconds_per_run": dev_runs, "host_seconds_per_phase": phases, "steps": 1,
-               "form": emu_form,
+               "d2h_bytes_per_step": d2h, "seconds": e2e_s, "steps": 1, "form": args.form,
                "path": "ccT_plan_create/ccT_set_inputs(host)/ccT_forward/ccT_plan_destroy (C ABI), pinned inputs"
-                       + (" + NCCL all-reduce of the shard energies" if world > 1 else ""),
-               "e_t": e2e_e}
+                       + (" + NCCL all-reduce of the shard energies" if world > 1 else "")}
+        e2e_detail = {"seconds_per_run": runs, "forward_device_seconds_per_run": dev_runs,
+                      "host_seconds_per_phase": phases, "e_t": e2e_e}
     else:
         del dev_inputs
+        e2e_detail = None
 
-    cpu = None
+    cpu, cpu_detail = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        tf_cpu, ntup, sec, thr = cpu_sample(inp)
-        cpu = {"value": tf_cpu, "unit": "TFLOP/s", "cores": thr, "kind": "port",
-               "sample": f"{ntup} i>j>k tuples of {inp.name} in {sec:.1f} s; literal 12-DGEMM + trant3 + "
-                         "T3SQUA/ADT3DEN/DRT1WT3 restatement with OpenBLAS DGEMM"}
+        cpu_detail = cpu_sample(inp)
+        cpu = {"value": cpu_detail["tflops"], "unit": "TFLOP/s", "cores": cpu_detail["threads"], "kind": "port",
+               "sample": cpu_sample_text(cpu_detail, inp.name)}
 
     if rank == 0:
+        extras = {"extras": True, "workload": args.workload}
+        table_rows = {}
+        if w_pick:
+            from oracle import oracle as O
+            o = O.all_tuples(no)
+            w_refs = {t: _oracle_w(O, inp, o[t]) for t in w_pick}
+            for form, f in forms.items():
+                row = {"e_t": f["e_t"], "abs_err_eh": f.get("abs_err_vs_oracle"), "rel_err": f.get("rel_err_vs_oracle")}
+                row["max_rel_dW"] = max(float(abs(f["w_samples"][t] - w_refs[t]).max() / abs(w_refs[t]).max())
+                                        for t in w_pick)
+                if "calibration" in f:
+                    row["digits"] = f["calibration"]
+                    row["meets_target"] = (row["abs_err_eh"] or 0.0) <= f["calibration"]["target"]
+                table_rows[form] = row
+        for f in forms.values():
+            f.pop("w_samples", None)
+        extras["forms"] = forms
+        extras["e2e_detail"] = e2e_detail
+        extras["cpu_baseline_detail"] = cpu_detail
+        if world == 1 and not args.no_extras:
+            extras["accuracy_table"] = accuracy_table(A, S, local, table_rows)
+            extras["adjoint"] = adjoint_extra(A, S, local)
+            extras["batch"] = batch_extra(A, S, local)
+            extras["per_tile_digits"] = adaptive_extra(A, S, local)
+        print(json.dumps(extras), flush=True)
+        cal = head.get("calibration", {})
         line = {"metric": METRIC, "value": head["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "int8 tensor pipe (split-integer FP64 emulation)",
                 "data": "synthetic (seeded generator, libcc_b200/synthetic.py)",
-                "config": {"workload": workload_desc(inp, cfg["dist"]), "form": f"emulated FP64, {args.emu_slices} "
-                           "7-bit digits per operand (tcgen05 kind::i8)", "tuples": len(costs), "tuples_ijk": n_ijk_all,
-                           "flop_per_step": flop_step, "tuples_per_s": len(costs) / (head["ms_per_step"] * 1e-3),
-                           "l2": "inputs larger than L2 (digit operands "
-                                 f"{2 * args.emu_slices * no * nu * nu * (nu + no) / 1e9:.1f} GB re-streamed per step)",
+                "config": {"workload": workload_desc(inp, cfg["dist"]),
+                           "form": f"emulated FP64, {args.form}: {cal.get('digits')} rounded 7-bit digits per "
+                                   "operand (tcgen05 kind::i8)",
+                           "tuples": len(costs), "tuples_ijk": n_ijk_all, "flop_per_step": flop_step,
+                           "tuples_per_s": len(costs) / (head["ms_per_step"] * 1e-3),
+                           "l2": "inputs larger than L2 (digit operands of several GB re-streamed per step)",
                            "parallelism": f"tuple shards x{world}" if world > 1 else "1 GPU"},
                 "roofline": head["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["gpu_launches"],
-                "clocks": clocks.summary(), "energies": {"ets": head["ets"], "etd": head["etd"], "e_t": head["e_t"]},
-                "accuracy": {"rel_err_vs_native_fp64": rel_vs_native,
+                "clocks": clocks.summary(),
+                "accuracy": {"abs_err_vs_oracle_eh": head.get("abs_err_vs_oracle"),
                              "rel_err_vs_oracle": head.get("rel_err_vs_oracle"),
-                             "native_rel_err_vs_oracle": forms["fp64"].get("rel_err_vs_oracle"),
-                             "bar": "relative 2.1e-7 = 1e-8 Eh on a (T) energy of 0.048 Eh (Ar6); the seeded data "
-                                    "give |E(T)| ~ 7.7e9 Eh, where an absolute 1e-8 Eh is below FP64 resolution"},
-                "forms": forms,
-                "speedup_emulated_over_native": forms["fp64"]["ms_per_step"] / head["ms_per_step"]}
-        if world == 1 and not args.no_extras:
-            line["adjoint"] = adjoint_extra(A, S, local)
-            line["batch"] = batch_extra(A, S, local)
-            line["per_tile_digits"] = adaptive_extra(A, S, local)
+                             "target_eh": cal.get("target"), "calibrated_bound_eh": cal.get("est_err"),
+                             "rel_err_vs_native_fp64": rel_vs_native,
+                             "bar": "the digit count is calibrated to 2.1e-7 |E(T)| = 1e-8 Eh on the Ar6 (T) energy "
+                                    "of 0.048 Eh; |E(T)| = 7.7e9 Eh here, where an absolute 1e-8 Eh is below FP64 "
+                                    "resolution (the default form's bar, max(1e-8 Eh, 2e-14 |E|), is in "
+                                    "fp64_parity_reading)"},
+                "native_fp64": {"ms_per_step": native["ms_per_step"], "tflops": native["tflops"],
+                                "roofline_frac": native["roofline"]["frac"],
+                                "abs_err_vs_oracle_eh": native.get("abs_err_vs_oracle"),
+                                "rel_err_vs_oracle": native.get("rel_err_vs_oracle")},
+                "speedup_emulated_over_native": native["ms_per_step"] / head["ms_per_step"]}
+        if DEFAULT_FORM in forms and DEFAULT_FORM != args.form:
+            rf = forms[DEFAULT_FORM]
+            line["fp64_parity_reading"] = {"form": DEFAULT_FORM + " (library default)",
+                                           "ms_per_step": rf["ms_per_step"], "tflops": rf["tflops"],
+                                           "digits": rf["calibration"]["digits"],
+                                           "target_eh": rf["calibration"]["target"],
+                                           "abs_err_vs_oracle_eh": rf.get("abs_err_vs_oracle"),
+                                           "rel_err_vs_oracle": rf.get("rel_err_vs_oracle"),
+                                           "speedup_over_native": native["ms_per_step"] / rf["ms_per_step"],
+                                           "roofline_frac": rf["roofline"]["frac"]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -66,6 +66,7 @@ struct ccT_plan {
   GemmJob *jobs = nullptr;  // [buffer][tuple][3]
   bool emulated = false;    // INT8 split-integer W-build
   bool emu_auto = false;    // digit count picked by calibration in ccT_set_inputs
+  int emu_base_ebn = 0;     // automatic plans: the N tile the kEmuMaxSlices-digit calibration operands use
   double emu_est_err = 0.0, emu_target = 0.0;  // calibrated |dE(T)| bound and its target (Eh)
   EmuOperands emu;
   EmuJob *emu_jobs = nullptr;  // [buffer][tuple][3]
@@ -368,6 +369,24 @@ int calibrate_digits(ccT_plan *p) {
   return s;
 }
 
+// After calibration an automatic plan rebuilds its digit operands for the
+// chosen count: only the leading digits (so a pipeline stage is again one
+// contiguous copy per operand) and the widest N tile whose digits x columns
+// fit the tensor memory and which divides the plan's NP (so F, the X buffers
+// and the FP64 jobs keep their layout).  The digits themselves do not depend
+// on the count.
+int rebuild_for_count(ccT_plan *p) {
+  Dims &d = p->d;
+  const int S = p->emu.run_slices;
+  int best = d.EBN;
+  for (int bn : kEmuBNChoices)
+    if (S * bn <= 512 && d.NP % bn == 0 && bn > best) best = bn;
+  if (S == p->emu.slices && best == d.EBN) return CCT_OK;
+  d.EBN = best;
+  p->emu.slices = S;
+  return emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
+}
+
 [[noreturn]] void legacy_stop(const char *where, int status) {
   std::fprintf(stderr, "libcc_b200: %s failed: %s (%s)\n", where, ccT_status_string(status), last_error());
   std::fflush(stderr);
@@ -514,6 +533,7 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     e.run_slices = e.slices;         // an automatic plan lowers it at calibration
     e.adaptive = o.emu_slices == 0;  // automatic: the calibrated count is the maximum, each tile takes what it needs
     p->emu_auto = o.emu_slices == 0;
+    p->emu_base_ebn = d.EBN;
     e.KP8 = round_up(nu + no, kEmuKC);
     e.tiles_m = (nu2 + kEmuBM - 1) / kEmuBM;
     const int64_t rowsE = no * nu2, rowsF = no * no * d.NP;
@@ -601,6 +621,10 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   }
   if (s == CCT_OK) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
+  if (s == CCT_OK && p->emu_auto) {  // calibration runs on operands of every digit count
+    p->d.EBN = p->emu_base_ebn;
+    p->emu.slices = p->emu.run_slices = kEmuMaxSlices;
+  }
   if (s == CCT_OK && p->emulated) s = emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
   if (staged) {
     cudaStreamSynchronize(p->stream);  // E is built (or the stream failed) before the staging buffer goes
@@ -623,7 +647,9 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   }
   std::fill(p->e_built.begin(), p->e_built.end(), 1);
   if (p->emu_auto) {
-    const int c = calibrate_digits(p);
+    int c = calibrate_digits(p);
+    if (c == CCT_OK) c = rebuild_for_count(p);
+    if (c == CCT_OK) CCT_CUDA(cudaStreamSynchronize(p->stream));
     if (c != CCT_OK) return c;
   }
   p->inputs_ready = true;

@@ -11,8 +11,13 @@ namespace red {
 
 constexpr int RB = kRB;  // 8
 constexpr int RT = 256;  // threads per reduction CTA
-constexpr int SL = 640;  // doubles per padded 8x8x8 block in smem
-__host__ __device__ constexpr int soff(int l0, int l1, int l2) { return l0 + 9 * l1 + 81 * l2; }
+constexpr int SL = 512;  // doubles per 8x8x8 block in smem
+// Element (l0, l1, l2) of a block: unpadded, with l0 XOR-ed by (l1 + l2) mod 8.
+// The term stores of phase A and the orbit reads of phase B put two
+// lane-varying coordinates on different axes; the XOR spreads every such pair
+// over distinct 8-byte bank pairs of a half-warp (a padded layout with strides
+// 1, 9, 81 left the pairs on axes 0 and 2 two-way conflicted).
+__host__ __device__ constexpr int soff(int l0, int l1, int l2) { return (l0 ^ ((l1 + l2) & 7)) + 8 * l1 + 64 * l2; }
 
 // The six permutations of three positions, in a fixed order:
 // 0:(0,1,2)=abc 1:(0,2,1)=acb 2:(1,0,2)=bac 3:(1,2,0)=bca 4:(2,0,1)=cab 5:(2,1,0)=cba
@@ -35,7 +40,6 @@ __host__ __device__ constexpr int term_entry(int kind, int term, int f) {
                                 {{0, 0, 1, 2}, {0, 1, 0, 2}, {1, 0, 2, 1}, {1, 1, 2, 0}}};
   return tab[kind][term][f];
 }
-__host__ __device__ constexpr int kstride(int m) { return m == 0 ? 1 : (m == 1 ? 9 : 81); }
 
 template <typename T>
 __device__ __forceinline__ T sel3(int m, T v0, T v1, T v2) {
@@ -167,8 +171,11 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
       for (int e = 0; e < 2; e++) {
         const int idx = tid + RT * e;
         const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
-        const int so = u0 * kstride(al0) + u1 * kstride(al1) + u2 * kstride(al2);
-        double *w = Wsm + p * SL + so;
+        // block coordinate m takes the u whose placement al is m
+        const int c0 = al0 == 0 ? u0 : (al1 == 0 ? u1 : u2);
+        const int c1 = al0 == 1 ? u0 : (al1 == 1 ? u1 : u2);
+        const int c2 = al0 == 2 ? u0 : (al1 == 2 ? u1 : u2);
+        double *w = Wsm + p * SL + soff(c0, c1, c2);
         if (term == 0)
           *w = xv[2 * p + e];
         else

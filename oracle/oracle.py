@@ -70,6 +70,11 @@ def lib():
         _lib.orc_div_even.argtypes = [i64, i64, i64, ctypes.POINTER(i64), ctypes.POINTER(i64)]
         _lib.orc_tuple.argtypes = [ctypes.c_int] + [i64] * 5 + [dp] * 11 + [dp]
         _lib.orc_reduce_tuple.argtypes = [ctypes.c_int] + [i64] * 5 + [dp] * 7
+        _lib.orc_set_blas.argtypes = [ctypes.c_void_p]
+        _lib.orc_dgemm_seconds.argtypes = [ctypes.c_int]
+        _lib.orc_dgemm_seconds.restype = ctypes.c_double
+        _lib.orc_cc_triples_list.argtypes = [i64, i64] + [dp] * 6 + [ctypes.POINTER(i64), i64, dp, dp]
+        _lib.orc_cc_triples_list.restype = ctypes.c_int
     return _lib
 
 
@@ -574,6 +579,73 @@ def closed_grad(inp, tuples=None):
     return {"eh": geh, "ep": gep, "t1": np.asfortranarray(gt1).ravel(order="F"),
             "t2": gT2.ravel(order="F"), "vm": gVM.ravel(order="F"), "voe": gVOE.ravel(order="F"),
             "vvvo": gvvvo.ravel(), "e_t": ets + etd}
+
+
+# --------------------------------------------------------------------------- BLAS-backed C pipeline
+
+def _blas_dgemm_pointer() -> int:
+    """Address of the BLAS DGEMM behind scipy.linalg (the image's OpenBLAS),
+    Fortran calling convention with 32-bit integers."""
+    import scipy.linalg.cython_blas as cb
+    cap = cb.__pyx_capi__["dgemm"]
+    get_name = ctypes.pythonapi.PyCapsule_GetName
+    get_name.restype, get_name.argtypes = ctypes.c_char_p, [ctypes.py_object]
+    get_ptr = ctypes.pythonapi.PyCapsule_GetPointer
+    get_ptr.restype, get_ptr.argtypes = ctypes.c_void_p, [ctypes.py_object, ctypes.c_char_p]
+    return get_ptr(cap, get_name(cap))
+
+
+def blas_cc_triples(inp, tuples=None):
+    """The literal triples-abc pipeline of triples_oracle.c (OpenMP TRANT3,
+    T3SQUA, ADT3DEN, SMT3FOUR/T1WT3IJK loops) with every DGEMM sent to the
+    image's OpenBLAS: the reference CPU algorithm, the timed CPU baseline.
+    Returns (ets, etd, v1[nu*no], seconds, dgemm_seconds)."""
+    import time
+    L = lib()
+    L.orc_set_blas(_blas_dgemm_pointer())
+    tuples = all_tuples(inp.no) if tuples is None else tuples
+    arr = np.ascontiguousarray(np.array(tuples, dtype=np.int64).reshape(-1, 4))
+    v1 = np.zeros(inp.nu * inp.no)
+    etd = ctypes.c_double(0.0)
+    L.orc_dgemm_seconds(1)
+    t0 = time.perf_counter()
+    rc = L.orc_cc_triples_list(inp.no, inp.nu, _p(inp.eh), _p(inp.ep), _p(inp.t2), _p(inp.vm), _p(inp.voe),
+                               _p(inp.vvvo), arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(arr),
+                               _p(v1), ctypes.byref(etd))
+    secs = time.perf_counter() - t0
+    dg = L.orc_dgemm_seconds(1)
+    L.orc_set_blas(None)
+    if rc != 0:
+        raise MemoryError("oracle out of memory")
+    t1 = _fv(inp.t1, (inp.no, inp.nu))
+    ets = 2.0 * float(np.sum(t1.T * v1.reshape((inp.nu, inp.no), order="F")))
+    return ets, etd.value, v1, secs, dg
+
+
+def blas_tuple_w(inp, kind: int, i: int, j: int, k: int) -> np.ndarray:
+    """``c_tuple_w`` (the literal formv3 / SYMT311 / ZEROT3 W of one tuple) with
+    its DGEMMs sent to the image's OpenBLAS: fast enough at nu = 320."""
+    L = lib()
+    L.orc_set_blas(_blas_dgemm_pointer())
+    try:
+        return c_tuple_w(inp, kind, i, j, k)
+    finally:
+        L.orc_set_blas(None)
+
+
+def openblas_dgemm_tflops(n: int = 4096, reps: int = 3) -> float:
+    """Best-of-reps TFLOP/s of an n^3 DGEMM through the same OpenBLAS."""
+    import time
+    from scipy.linalg.blas import dgemm
+    a = np.asfortranarray(np.random.default_rng(0).standard_normal((n, n)))
+    b = np.asfortranarray(np.random.default_rng(1).standard_normal((n, n)))
+    dgemm(1.0, a[:256, :256], b[:256, :256])
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        dgemm(1.0, a, b)
+        best = min(best, time.perf_counter() - t0)
+    return 2.0 * n ** 3 / best / 1e12
 
 
 def cpu_threads() -> int:

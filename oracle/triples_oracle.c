@@ -24,6 +24,7 @@
  * -sdefault64, src/triples-ijk/Makefile:10).
  */
 #include <math.h>
+#include <omp.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -129,6 +130,7 @@ void orc_cpytsq(const double *a, double *b, i64 na)
 void orc_getve(const double *vvvo, i64 nu, i64 x, double *ve)
 {
     i64 nutr = nu * (nu + 1) / 2;
+#pragma omp parallel for schedule(static)
     for (i64 c = 0; c < nu; c++)
         orc_cpytsq(vvvo + (x * nu + c) * nutr, ve + c * nu * nu, nu);
 }
@@ -136,12 +138,38 @@ void orc_getve(const double *vvvo, i64 nu, i64 x, double *ve)
 /* ---------------------------------------------------------------------------
  * Column-major DGEMM, C = alpha op(A) op(B) + beta C, the BLAS contract the
  * reference calls (src/triples-ijk/dgemm_async.cpp:55-75 forwards the same
- * arguments to cublasDgemm).  Plain loops; OpenMP over columns of C.
+ * arguments to cublasDgemm).  Plain loops, OpenMP over columns of C, unless a
+ * BLAS DGEMM (Fortran calling convention, 32-bit integers, as the reference's
+ * vendor BLAS) has been installed with orc_set_blas: then every call goes to
+ * it and its wall time is summed (orc_dgemm_seconds), so the timed CPU
+ * baseline can state its DGEMM share.
  * ------------------------------------------------------------------------- */
+typedef void (*orc_blas_dgemm_fn)(char *, char *, int *, int *, int *, double *, double *, int *, double *,
+                                  int *, double *, double *, int *);
+static orc_blas_dgemm_fn g_blas_dgemm = 0;
+static double g_dgemm_seconds = 0.0;
+
+void orc_set_blas(void *fn) { g_blas_dgemm = (orc_blas_dgemm_fn)fn; }
+
+/* Seconds spent in the installed BLAS DGEMM since the last reset. */
+double orc_dgemm_seconds(int reset)
+{
+    double s = g_dgemm_seconds;
+    if (reset) g_dgemm_seconds = 0.0;
+    return s;
+}
+
 static void orc_dgemm(char ta, char tb, i64 m, i64 n, i64 k, double alpha,
                       const double *A, i64 lda, const double *B, i64 ldb,
                       double beta, double *C, i64 ldc)
 {
+    if (g_blas_dgemm) {
+        int im = (int)m, in = (int)n, ik = (int)k, ila = (int)lda, ilb = (int)ldb, ilc = (int)ldc;
+        double t0 = omp_get_wtime();
+        g_blas_dgemm(&ta, &tb, &im, &in, &ik, &alpha, (double *)A, &ila, (double *)B, &ilb, &beta, C, &ilc);
+        g_dgemm_seconds += omp_get_wtime() - t0;
+        return;
+    }
 #pragma omp parallel for schedule(static)
     for (i64 j = 0; j < n; j++) {
         double *cj = C + j * ldc;
@@ -284,18 +312,24 @@ double orc_t3squa(i64 no, i64 nu, i64 i, i64 j, i64 k, const double *t3, const d
     (void)no;
     double dijk = eh[i] + eh[j] + eh[k];
     double x3 = 0.0;
+    /* 16-wide cache blocks of (c, b, a), the c blocks shared out over the
+     * threads, as the reference's loops 150/160 */
+    const i64 BS = 16, nb = (nu + BS - 1) / BS;
 #pragma omp parallel for reduction(+ : x3) schedule(static)
-    for (i64 c = 0; c < nu; c++)
-        for (i64 b = 0; b < nu; b++)
-            for (i64 a = 0; a < nu; a++) {
-                if (a == b && b == c) continue;
-                double denom = 1.0 / (dijk - (ep[a] + ep[b] + ep[c]));
-                double d1 = V3(t3, a, b, c);
-                double d2 = V3(t3, a, c, b) + V3(t3, c, b, a) + V3(t3, b, a, c);
-                double d3 = V3(t3, b, c, a) + V3(t3, c, a, b);
-                double f = d1 * 8.0 - 4.0 * d2 + d3 * 2.0;
-                x3 += f * d1 * denom;
-            }
+    for (i64 cb = 0; cb < nb; cb++)
+        for (i64 bb = 0; bb < nb; bb++)
+            for (i64 ab = 0; ab < nb; ab++)
+                for (i64 c = cb * BS; c < cb * BS + BS && c < nu; c++)
+                    for (i64 b = bb * BS; b < bb * BS + BS && b < nu; b++)
+                        for (i64 a = ab * BS; a < ab * BS + BS && a < nu; a++) {
+                            if (a == b && b == c) continue;
+                            double denom = 1.0 / (dijk - (ep[a] + ep[b] + ep[c]));
+                            double d1 = V3(t3, a, b, c);
+                            double d2 = V3(t3, a, c, b) + V3(t3, c, b, a) + V3(t3, b, a, c);
+                            double d3 = V3(t3, b, c, a) + V3(t3, c, a, b);
+                            double f = d1 * 8.0 - 4.0 * d2 + d3 * 2.0;
+                            x3 += f * d1 * denom;
+                        }
     double cf = (i == j || j == k) ? 0.5 : 1.0;
     return cf * x3;
 }
@@ -332,12 +366,7 @@ static void orc_t1wt3ijk(i64 i, i64 j, i64 k, i64 no, i64 nu, double *v1, const 
     /* DGEMM('N','N',NU,1,NU2,...): v1(a,I) += sum_bc T3(a,bc) VOE(bc,J,K) */
     const double *x = voe + k * nu2 * no + j * nu2;
     double *y = v1 + i * nu;
-#pragma omp parallel for schedule(static)
-    for (i64 a = 0; a < nu; a++) {
-        double s = 0.0;
-        for (i64 bc = 0; bc < nu2; bc++) s += t3[a + nu * bc] * x[bc];
-        y[a] += s;
-    }
+    orc_dgemm('n', 'n', nu, 1, nu2, 1.0, t3, nu, x, nu2, 1.0, y, nu);
 }
 
 /* DRT1WT3IJK_SMP (triples-abc/ddcc_aux.f:146-169). */
@@ -550,4 +579,43 @@ void orc_reduce_tuple(int kind, i64 no, i64 nu, i64 i, i64 j, i64 k, double *v3,
         orc_drt1wt3ij(i, j, no, nu, v1, voe, v3, t3);
     else
         orc_drt1wt3jk(i, k, no, nu, v1, voe, v3, t3);
+}
+
+/* A list of tuples through the same literal pipeline as orc_cc_triples
+ * (orc_tuple per tuple, VE slices fetched and b<->c-swapped when a tuple needs
+ * an index not already held, as triples-abc/triples.f90:232-313 refetches on a
+ * new i/j/k).  list holds 4 integers per tuple: kind (0 i>j>k, 1 (i,j,j),
+ * 2 (i,i,k)), i, j, k, 0-based.  Accumulates into v1 (nu,no) and *etd.
+ * Returns 0, or -1 when out of memory. */
+int orc_cc_triples_list(i64 no, i64 nu, const double *eh, const double *ep, const double *t2, const double *vm,
+                        const double *voe, const double *vvvo, const i64 *list, i64 n, double *v1, double *etd)
+{
+    const i64 nu3 = nu * nu * nu;
+    double *v3 = malloc(sizeof(double) * nu3), *t3 = malloc(sizeof(double) * nu3);
+    double *slot[3] = {malloc(sizeof(double) * nu3), malloc(sizeof(double) * nu3), malloc(sizeof(double) * nu3)};
+    i64 key[3] = {-1, -1, -1};
+    if (!v3 || !t3 || !slot[0] || !slot[1] || !slot[2]) {
+        free(v3); free(t3); free(slot[0]); free(slot[1]); free(slot[2]);
+        return -1;
+    }
+    for (i64 q = 0; q < n; q++) {
+        const int kind = (int)list[4 * q];
+        const i64 x[3] = {list[4 * q + 1], list[4 * q + 2], list[4 * q + 3]};
+        const double *ve[3];
+        for (int r = 0; r < 3; r++) {
+            int hit = -1;
+            for (int s2 = 0; s2 < 3; s2++)
+                if (key[s2] == x[r]) hit = s2;
+            if (hit < 0) { /* evict a slot no index of this tuple uses */
+                for (int s2 = 0; s2 < 3 && hit < 0; s2++)
+                    if (key[s2] != x[0] && key[s2] != x[1] && key[s2] != x[2]) hit = s2;
+                orc_getve_swapped(vvvo, nu, x[r], slot[hit]);
+                key[hit] = x[r];
+            }
+            ve[r] = slot[hit];
+        }
+        orc_tuple(kind, no, nu, x[0], x[1], x[2], t2, vm, voe, eh, ep, ve[0], ve[1], ve[2], v3, t3, v1, etd);
+    }
+    free(v3); free(t3); free(slot[0]); free(slot[1]); free(slot[2]);
+    return 0;
 }

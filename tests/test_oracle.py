@@ -125,3 +125,23 @@ def test_golden_fixture_reproduced_by_oracle():
     inp = S.workload("water-avdz")
     ets, etd, v1 = O.c_cc_triples(inp)
     assert ets == pytest.approx(g["ets"], abs=1e-14) and etd == pytest.approx(g["etd"], rel=1e-14)
+
+
+def test_blas_pipeline_matches_plain_oracle():
+    """The timed CPU baseline (the literal pipeline with OpenBLAS DGEMMs) gives
+    the plain-loop oracle's energies and v1 on every tuple kind."""
+    from oracle import oracle as O
+    inp = S.generate(5, 23, 4)
+    ets_o, etd_o, v1_o = O.c_cc_triples(inp)
+    ets, etd, v1, secs, dg = O.blas_cc_triples(inp)
+    assert abs(etd - etd_o) <= 1e-13 * abs(etd_o)
+    assert abs(ets - ets_o) <= 1e-13 * abs(ets_o) + 1e-16
+    assert np.abs(v1 - v1_o).max() <= 1e-13 * np.abs(v1_o).max()
+    assert 0.0 < dg <= secs
+
+
+def test_blas_tuple_w_matches_plain_oracle():
+    from oracle import oracle as O
+    inp = S.generate(4, 13, 6)
+    for t in (O.all_tuples(4)[0], O.all_tuples(4)[-1], O.all_tuples(4)[-2]):
+        assert np.abs(O.blas_tuple_w(inp, *t) - O.c_tuple_w(inp, *t)).max() <= 1e-14
