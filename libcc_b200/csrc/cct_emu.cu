@@ -174,7 +174,8 @@ struct EmuArgs {
   unsigned long long *slice_hist;
   int nu, no, njobs, kchunks, tiles_m, tiles_n;
   int sop;  // digit slices stored per K chunk in the operands (>= the S of the launch)
-  int64_t NP;
+  int64_t NP;   // X row stride; columns at or past it (a partial last N tile) are not stored
+  int64_t NPe;  // rows per (y,z) of the B digits and expF: tiles_n * EBN
   int *err;
 };
 
@@ -420,9 +421,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       if (lane == 0) mbar_arrive(&tmem_empty);
       if (live) {
         double *xrow = job.out + m * args.NP + n0;
-        const int16_t *eB = args.expF + (int64_t)job.x3 * args.NP + n0;
+        const int16_t *eB = args.expF + (int64_t)job.x3 * args.NPe + n0;
 #pragma unroll
         for (int j = 0; j < CW; j += 2) {
+          if (n0 + j >= args.NP) break;  // NP is even: a pair is stored whole or not at all
           const double s0 = acc[j] * pow2(eA + eB[j]);
           const double s1 = acc[j + 1] * pow2(eA + eB[j + 1]);
           *reinterpret_cast<double2 *>(xrow + j) = make_double2(s0, s1);
@@ -466,13 +468,16 @@ __global__ void shared_exp_e_kernel(const int16_t *__restrict__ rowexp, int no, 
   }
 }
 
-// Pass 2b: expF[z*NP+n] = max over y of the row exponents of F[y][z][n].
-__global__ void shared_exp_f_kernel(const int16_t *__restrict__ rowexp, int no, int64_t NP, int16_t *__restrict__ expF) {
-  const int64_t n_all = (int64_t)no * NP;
+// Pass 2b: expF[z*NPe+n] = max over y of the row exponents of F[y][z][n]
+// (rows n >= NP, the padding of a partial last N tile, are zero).
+__global__ void shared_exp_f_kernel(const int16_t *__restrict__ rowexp, int no, int64_t NP, int64_t NPe,
+                                    int16_t *__restrict__ expF) {
+  const int64_t n_all = (int64_t)no * NPe;
   for (int64_t zn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; zn < n_all; zn += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t z = zn / NP, n = zn - z * NP;
+    const int64_t z = zn / NPe, n = zn - z * NPe;
     int e = kNoRowExp;
-    for (int y = 0; y < no; y++) e = max(e, (int)rowexp[((int64_t)y * no + z) * NP + n]);
+    if (n < NP)
+      for (int y = 0; y < no; y++) e = max(e, (int)rowexp[((int64_t)y * no + z) * NP + n]);
     expF[zn] = (int16_t)(e == kNoRowExp ? 0 : e);
   }
 }
@@ -497,6 +502,7 @@ __global__ void tile_exp_kernel(const int16_t *__restrict__ rowexpE, const int16
     const int zt = tile - tiles_m, z = zt / tiles_n, tn = zt - z * tiles_n;
     for (int r = threadIdx.x; r < ebn; r += blockDim.x) {
       const int64_t n = (int64_t)tn * ebn + r;
+      if (n >= NP) break;
       for (int y = 0; y < no; y++) e = max(e, (int)rowexpF[((int64_t)y * no + z) * NP + n]);
     }
   }
@@ -573,7 +579,7 @@ __global__ void digits_e_kernel(const double *__restrict__ E, int no, int nu, in
     const int64_t mt = r2 * nu + r1;
     const int e = expE[m];
     for (int64_t k = 4 * lane; k < KP8; k += 128) {
-      uint32_t w[kEmuMaxSlices];
+      uint32_t w[kEmuDigitCap];
       digits4(E + row * KP, k, nu + no, e, S, w);
       const int64_t kc = k / kEmuKC;
       const int kb = (int)(k - kc * kEmuKC);
@@ -587,10 +593,11 @@ __global__ void digits_e_kernel(const double *__restrict__ E, int no, int nu, in
   }
 }
 
-__global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, int64_t NP, int64_t KP, int64_t KP8,
-                                int S, int ebn, const int16_t *__restrict__ expF, int8_t *__restrict__ F8) {
+__global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, int64_t NP, int64_t NPe, int64_t KP,
+                                int64_t KP8, int S, int ebn, const int16_t *__restrict__ expF,
+                                int8_t *__restrict__ F8) {
   const int64_t rows = (int64_t)no * no * NP;
-  const int64_t KC = KP8 / kEmuKC, tiles_n = NP / ebn;
+  const int64_t KC = KP8 / kEmuKC, tiles_n = NPe / ebn;
   const int64_t bblk = (int64_t)ebn * kEmuKC;
   const int lane = threadIdx.x & 31;
   int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -598,9 +605,9 @@ __global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, in
   for (; row < rows; row += stride) {
     const int64_t yz = row / NP, n = row - yz * NP;
     const int64_t z = yz % no;
-    const int e = expF[z * NP + n];
+    const int e = expF[z * NPe + n];
     for (int64_t k = 4 * lane; k < KP8; k += 128) {
-      uint32_t w[kEmuMaxSlices];
+      uint32_t w[kEmuDigitCap];
       digits4(F + row * KP, k, nu + no, e, S, w);
       const int64_t kc = k / kEmuKC;
       const int kb = (int)(k - kc * kEmuKC);
@@ -644,12 +651,13 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   a.kchunks = (int)(o.KP8 / kEmuKC);
   a.sop = o.slices;
   a.tiles_m = (int)o.tiles_m;
-  a.tiles_n = (int)(d.NP / EBN);
-  if (d.EBN != EBN || o.slices < S) {
+  a.tiles_n = (int)(o.NPe / EBN);
+  if (o.ebn != EBN || o.NPe % EBN != 0 || o.NPe < d.NP || o.slices < S) {
     set_error("emulated N tile mismatch, or fewer operand digits than the launch runs");
     return CCT_ERR_INVALID;
   }
   a.NP = d.NP;
+  a.NPe = o.NPe;
   a.err = err;
   const int64_t items = (int64_t)njobs * a.tiles_m * a.tiles_n;
   const int grid = (int)(items < g_num_sms[dev] ? items : g_num_sms[dev]);
@@ -661,13 +669,14 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
 }  // namespace
 
 int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOperands *o, cudaStream_t s) {
-  if (o->slices < kEmuMinSlices || o->slices > kEmuMaxSlices) {
+  if (o->slices < kEmuMinSlices || o->slices > kEmuDigitCap) {
     set_error("emulation slice count must be in [" + std::to_string(kEmuMinSlices) + ", " +
-              std::to_string(kEmuMaxSlices) + "]");
+              std::to_string(kEmuDigitCap) + "]");
     return CCT_ERR_INVALID;
   }
-  if (d.EBN <= 0 || d.NP % d.EBN != 0 || o->KP8 % kEmuKC != 0 || o->slices * d.EBN > 512) {
-    set_error("emulated plan needs NP a multiple of its N tile, KP8 a multiple of 32 and slices x N <= 512");
+  if (o->ebn <= 0 || o->NPe % o->ebn != 0 || o->NPe < d.NP || o->KP8 % kEmuKC != 0 || o->slices * o->ebn > 512) {
+    set_error("emulated operands need NPe >= NP a multiple of their N tile, KP8 a multiple of 32 and "
+              "slices x N <= 512");
     return CCT_ERR_INVALID;
   }
   const int64_t rowsE = (int64_t)d.no * d.nu * d.nu, rowsF = (int64_t)d.no * d.no * d.NP;
@@ -686,7 +695,7 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
   CCT_CUDA(cudaGetLastError());
   shared_exp_e_kernel<<<grid_flat((int64_t)d.nu * d.nu), 256, 0, s>>>(o->expET, d.no, d.nu, o->expE);
   CCT_CUDA(cudaGetLastError());
-  shared_exp_f_kernel<<<grid_flat((int64_t)d.no * d.NP), 256, 0, s>>>(o->expRowF, d.no, d.NP, o->expF);
+  shared_exp_f_kernel<<<grid_flat((int64_t)d.no * o->NPe), 256, 0, s>>>(o->expRowF, d.no, d.NP, o->NPe, o->expF);
   CCT_CUDA(cudaGetLastError());
   // the rows past nu^2 in the last row tile stay zero
   const size_t bytesE = (size_t)o->slices * d.no * o->tiles_m * kEmuBM * o->KP8;
@@ -695,12 +704,14 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
   digits_e_kernel<<<grid_rows(rowsE), 256, 0, s>>>(E, d.no, d.nu, d.KP, o->KP8, o->slices, o->tiles_m, o->expE,
                                                    o->E8, o->E8T);
   CCT_CUDA(cudaGetLastError());
-  digits_f_kernel<<<grid_rows(rowsF), 256, 0, s>>>(F, d.no, d.nu, d.NP, d.KP, o->KP8, o->slices, d.EBN, o->expF,
-                                                   o->F8);
+  if (o->NPe > d.NP)  // the padding rows of a partial last N tile stay zero
+    CCT_CUDA(cudaMemsetAsync(o->F8, 0, (size_t)o->slices * d.no * d.no * o->NPe * o->KP8, s));
+  digits_f_kernel<<<grid_rows(rowsF), 256, 0, s>>>(F, d.no, d.nu, d.NP, o->NPe, d.KP, o->KP8, o->slices, o->ebn,
+                                                   o->expF, o->F8);
   CCT_CUDA(cudaGetLastError());
   if (o->adaptive) {
-    const int tiles_n = (int)(d.NP / d.EBN), nbt = d.no * tiles_n;
-    tile_exp_kernel<<<(int)o->tiles_m + nbt, 256, 0, s>>>(o->expET, o->expRowF, d.no, d.nu, d.NP, d.EBN,
+    const int tiles_n = (int)(o->NPe / o->ebn), nbt = d.no * tiles_n;
+    tile_exp_kernel<<<(int)o->tiles_m + nbt, 256, 0, s>>>(o->expET, o->expRowF, d.no, d.nu, d.NP, o->ebn,
                                                           (int)o->tiles_m, tiles_n, o->tileExp);
     CCT_CUDA(cudaGetLastError());
     tile_exp_top_kernel<<<1, 256, 0, s>>>((int)o->tiles_m, nbt, o->tileExp);
@@ -712,7 +723,7 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
 int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
                       cudaStream_t s) {
   // (digits run, N tile) pairs with digits x N <= 512 tensor-memory columns
-  const int key = o.run_slices * 1000 + d.EBN;
+  const int key = o.run_slices * 1000 + o.ebn;
   switch (key) {
     case 3064: return launch_emu_s<3, 64>(o, d, jobs_dev, njobs, err, s);
     case 3080: return launch_emu_s<3, 80>(o, d, jobs_dev, njobs, err, s);
@@ -726,8 +737,9 @@ int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_de
     case 6064: return launch_emu_s<6, 64>(o, d, jobs_dev, njobs, err, s);
     case 6080: return launch_emu_s<6, 80>(o, d, jobs_dev, njobs, err, s);
     case 7064: return launch_emu_s<7, 64>(o, d, jobs_dev, njobs, err, s);
+    case 8064: return launch_emu_s<8, 64>(o, d, jobs_dev, njobs, err, s);
     default:
-      set_error("unsupported (digits, N tile) = (" + std::to_string(o.run_slices) + ", " + std::to_string(d.EBN) +
+      set_error("unsupported (digits, N tile) = (" + std::to_string(o.run_slices) + ", " + std::to_string(o.ebn) +
                 ")");
       return CCT_ERR_INVALID;
   }

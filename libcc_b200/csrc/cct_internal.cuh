@@ -99,6 +99,12 @@ struct TupleDev {
 // (emu_slices = 0) builds kEmuMaxSlices digits and runs the smallest count in
 // [kEmuMinSlices, kEmuMaxSlices] whose calibrated E(T) error meets its target.
 constexpr int kEmuMinSlices = 3, kEmuMaxSlices = 7;
+// The backward pass recomputes W with this many digits: the rounded digits'
+// representation error, 2^-57 of the row scale, is below FP64's unit roundoff,
+// so the recomputed W is as accurate as an FP64 W build.  Tensor memory holds
+// its 8 diagonals of 64 columns.
+constexpr int kEmuRecomputeSlices = 8;
+constexpr int kEmuDigitCap = 8;  // most digits any operand holds
 // N tile of the emulated W-build: the tensor memory holds S diagonal
 // accumulators of N int32 columns (S N <= 512), and an MMA instruction costs
 // about the same up to N ~ 80, so the widest N that pads nu least is used.
@@ -140,13 +146,15 @@ constexpr int kEmuABlk = kEmuBM * kEmuKC;        // 4096 bytes
 struct EmuOperands {
   int slices = kEmuMaxSlices;                // digit slices stored per K chunk
   int run_slices = kEmuMaxSlices;            // digits the W build runs (<= slices; the calibrated count)
+  int ebn = 0;                               // N tile of F8 (rows per B block)
+  int64_t NPe = 0;                           // rows per (y,z) in F8 and expF: NP rounded up to ebn
   int64_t KP8 = 0;                           // digit row length: round_up(nu+no, 32)
   int64_t tiles_m = 0;                       // ceil(nu^2 / 128) row tiles per occupied index
   int8_t *E8 = nullptr, *E8T = nullptr;      // [x][tile_m][kchunk][slice][4096]; E8T rows (q,p)
-  int8_t *F8 = nullptr;                      // [y*no+z][tile_n][kchunk][slice][EBN*32]
+  int8_t *F8 = nullptr;                      // [y*no+z][tile_n][kchunk][slice][ebn*32], NPe / ebn tiles
   // Digit scales shared by both halves of a GEMM, so one set of diagonal
   // accumulators serves the whole contraction: expE[p*nu+q] (symmetric) is the
-  // largest row exponent of E[x][p][q] and E[x][q][p] over all x; expF[z*NP+n]
+  // largest row exponent of E[x][p][q] and E[x][q][p] over all x; expF[z*NPe+n]
   // the largest of F[y][z][n] over all y.  expET and expRowF hold the per-row
   // exponents they are reduced from.
   int16_t *expE = nullptr, *expET = nullptr, *expF = nullptr, *expRowF = nullptr;
