@@ -271,7 +271,7 @@ def adjoint_extra(A, S, local):
             "max_rel_err_vs_cpu_gradient": rel, "central_difference_h": 1e-5,
             "max_rel_err_vs_central_differences": fd_rel,
             "dvoe_central_difference_step_sweep": sweep,
-            "note": "backward recomputes W per tuple with the 8-digit INT8 W build (FP64-accurate); rel errors are relative to max|gradient| per input; "
+            "note": "backward recomputes W per tuple in FP64; rel errors are relative to max|gradient| per input; "
                     "the sweep takes the largest-|g| VOE entry and one random entry"}
 
 

@@ -106,11 +106,8 @@ int ccT_forward(ccT_plan *plan, int64_t begin, int64_t end, double *ets, double 
  * (no,nu), d_t2 (nu,nu,no,no), d_vm (no,nu,no,no), d_voe (nu,nu,no,no) and
  * d_vvvo (the packed (nutr, nu*no) layout of ccT_set_inputs).  Together this
  * is the (T) contribution to the CCSD(T) Lagrangian.  W is recomputed per
- * tuple, whatever the plan's precision, by the INT8 W build with 8 rounded
- * 7-bit digits per operand, whose representation error (2^-57 of each row's
- * scale) is below FP64's unit roundoff, so the recomputed W is as accurate as
- * an FP64 W build; the first call after ccT_set_inputs builds those digits.
- * The backward GEMMs are FP64.  Nothing of size nu^3 is kept across tuples.  mem says whether the output pointers are host or device
+ * tuple in FP64 whatever the plan's precision; nothing of size nu^3 is kept
+ * across tuples.  mem says whether the output pointers are host or device
  * memory; any output pointer may be NULL to skip it.  No reference
  * counterpart: the reference computes no gradient.  Returns CCT_ERR_STATE
  * when no ccT_forward over [begin, end) precedes it. */

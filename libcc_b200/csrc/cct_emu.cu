@@ -57,8 +57,10 @@
 //               accumulators (N int32 columns each)
 //   warps 2..   drain (NDW warps): tcgen05.ld one diagonal at a time, sum in
 //               FP64, hand the tensor memory back to the issuer, then scale
-//               and store X (the ring keeps filling meanwhile, so the next
-//               item's MMAs start at once)
+//               and store X in 32-byte stores.  When two accumulator sets fit
+//               the tensor memory (2 S N <= 512) the issuer alternates between
+//               them, so the next item's MMAs run while the drain reads and
+//               stores the last one; with one set they wait for the read.
 // Every mbarrier wait is bounded and also ends when another role aborted; a
 // timeout sets the error word, the producer waits for its copies in flight,
 // the issuer for its MMAs, and the CTA frees its tensor memory and returns.
@@ -96,8 +98,13 @@ constexpr int emu_stages() {
          : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + EBN * kEmuKC)) < 2 ? 2
                                                                         : CCT_EMU_SMEM_BUDGET / (KS * S * (A_BLK + EBN * kEmuKC));
 }
+// Accumulator sets in tensor memory: two when both fit the 512 columns (3
+// digits at N = 80, 4 at N = 64), so the MMAs of the next work item go into
+// one set while the drain reads the other; else one.
 template <int S, int EBN>
-constexpr uint32_t emu_tmem_cols() { return S * EBN <= 256 ? 256u : 512u; }
+constexpr int emu_acc_bufs() { return 2 * S * EBN <= 512 ? 2 : 1; }
+template <int S, int EBN>
+constexpr uint32_t emu_tmem_cols() { return emu_acc_bufs<S, EBN>() * S * EBN <= 256 ? 256u : 512u; }
 constexpr long kWaitLimit = 1L << 26;
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -152,6 +159,11 @@ __device__ __forceinline__ uint64_t desc_kmajor(const void *p) {
   return ((a & 0x3FFFF) >> 4) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46);
 }
 
+// 32-byte store (one whole sector per thread)
+__device__ __forceinline__ void st_global_v4(double *p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+
 // tcgen05.ld of 16 / 8 consecutive 32-bit columns of this warp's 32 lanes
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t *v) {
   asm volatile(
@@ -202,6 +214,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
   static_assert(S * EBN <= 512 && EBN % 16 == 0, "S diagonals of EBN columns must fit the tensor memory");
   constexpr int B_BLK = EBN * kEmuKC;
   constexpr uint32_t TCOLS = emu_tmem_cols<S, EBN>();
+  constexpr int NB = emu_acc_bufs<S, EBN>();  // accumulator sets, S * EBN columns each
   constexpr int ST = emu_stages<S, EBN>();
   constexpr int CA = S * A_BLK, CB = S * B_BLK;    // bytes of one K chunk per operand in shared memory
   constexpr int SA = KS * CA, SB = KS * CB;        // bytes of one stage per operand
@@ -211,7 +224,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
   uint8_t *base = (uint8_t *)(((uintptr_t)emu_smem + 1023) & ~(uintptr_t)1023);
   uint8_t *sA = base;            // [stage][chunk][slice][4096]
   uint8_t *sB = base + ST * SA;  // [stage][chunk][slice][2048]
-  __shared__ uint64_t full[ST], empty[ST], acc_full, tmem_empty, mma_done;
+  __shared__ uint64_t full[ST], empty[ST], acc_full[NB], tmem_empty[NB], mma_done;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_word;
   volatile int *abort_flag = &abort_word;
@@ -236,8 +249,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(&acc_full, 1);
-    mbar_init(&tmem_empty, NDW);  // one arrival per drain warp
+    for (int b = 0; b < NB; b++) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&tmem_empty[b], NDW);  // one arrival per drain warp
+    }
     mbar_init(&mma_done, 1);
     abort_word = 0;
     asm volatile("fence.mbarrier_init.release.cluster;");
@@ -292,8 +307,12 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       uint32_t g = 0, n = 0;
       bool ok = true;
       for (int64_t it = blockIdx.x; it < nitems && ok; it += gridDim.x, n++) {
-        // the drain of the previous item has read the accumulators
-        if (n > 0 && !mbar_wait(&tmem_empty, (n - 1) & 1, args.err, abort_flag)) {
+        // item n uses accumulator set ab; the drain of the item that used it
+        // last (use - 1 uses ago) has read it
+        const int ab = NB == 2 ? (int)(n & 1) : 0;
+        const uint32_t use = NB == 2 ? (n >> 1) : n;
+        const uint32_t acc = tmem + (uint32_t)(ab * S * EBN);
+        if (use > 0 && !mbar_wait(&tmem_empty[ab], (use - 1) & 1, args.err, abort_flag)) {
           ok = false;
           break;
         }
@@ -327,7 +346,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
                 const uint32_t idesc = idesc0 | ((uint32_t)((cnt * EBN) >> 3) << 17);
                 asm volatile(
                     "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; "
-                    "}" ::"r"(tmem + (uint32_t)((t + u0) * EBN)),
+                    "}" ::"r"(acc + (uint32_t)((t + u0) * EBN)),
                     "l"(dA + (uint64_t)(t * (A_BLK >> 4))), "l"(dB + (uint64_t)(u0 * (B_BLK >> 4))), "r"(idesc),
                     "r"(t > 0 ? 1u : first));
               };
@@ -353,7 +372,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
         }
         if (!ok) break;
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            su32(&acc_full)));
+            su32(&acc_full[ab])));
       }
       // every MMA issued has completed before the tensor memory is freed
       asm volatile(
@@ -362,6 +381,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
     }
   } else {  // ---------------- drain: warp w owns TMEM lane quarter w % 4
     constexpr int CW = EBN / (NDW / 4);  // columns per drain warp
+    static_assert(CW % 4 == 0, "the drain stores X four columns at a time");
     const int q = warp & 3;
     const int row = q * 32 + lane;
     const int cbase = ((warp - 2) / 4) * CW;
@@ -382,8 +402,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       const int eA = live ? args.expE[m] : 0;
       const int n0 = tn * EBN + cbase;
       const int sl = item_slices<S>(args, tm, tn, job.x3);
+      const int ab = NB == 2 ? (int)(n & 1) : 0;
+      const uint32_t use = NB == 2 ? (n >> 1) : n;
       // warp-uniform decision: the tcgen05.ld below are .sync.aligned
-      if (!__all_sync(0xffffffffu, mbar_wait(&acc_full, n & 1, args.err, abort_flag))) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[ab], use & 1, args.err, abort_flag))) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       double acc[CW];
 #pragma unroll
@@ -396,7 +418,8 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
           uint32_t v[DB][16];
 #pragma unroll
           for (int dd = 0; dd < DB; dd++) {
-            const uint32_t addr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((d0 + dd) * EBN + cbase + c0);
+            const uint32_t addr =
+                tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * S + d0 + dd) * EBN + cbase + c0);
             if (w == 16)
               tmem_ld16(addr, v[dd]);
             else
@@ -418,16 +441,17 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       // before the scaling and the stores
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
-      if (lane == 0) mbar_arrive(&tmem_empty);
+      if (lane == 0) mbar_arrive(&tmem_empty[ab]);
       if (live) {
         double *xrow = job.out + m * args.NP + n0;
         const int16_t *eB = args.expF + (int64_t)job.x3 * args.NPe + n0;
+        // one 32-byte sector per store (a thread owns a row, so 16-byte
+        // stores wrote half a sector each and doubled the write traffic)
 #pragma unroll
-        for (int j = 0; j < CW; j += 2) {
-          if (n0 + j >= args.NP) break;  // NP is even: a pair is stored whole or not at all
-          const double s0 = acc[j] * pow2(eA + eB[j]);
-          const double s1 = acc[j + 1] * pow2(eA + eB[j + 1]);
-          *reinterpret_cast<double2 *>(xrow + j) = make_double2(s0, s1);
+        for (int j = 0; j < CW; j += 4) {
+          if (n0 + j >= args.NP) break;  // NP is a multiple of 4: a quad is stored whole or not at all
+          st_global_v4(xrow + j, acc[j] * pow2(eA + eB[j]), acc[j + 1] * pow2(eA + eB[j + 1]),
+                       acc[j + 2] * pow2(eA + eB[j + 2]), acc[j + 3] * pow2(eA + eB[j + 3]));
         }
       }
     }
@@ -652,8 +676,9 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   a.sop = o.slices;
   a.tiles_m = (int)o.tiles_m;
   a.tiles_n = (int)(o.NPe / EBN);
-  if (o.ebn != EBN || o.NPe % EBN != 0 || o.NPe < d.NP || o.slices < S) {
-    set_error("emulated N tile mismatch, or fewer operand digits than the launch runs");
+  if (o.ebn != EBN || o.NPe % EBN != 0 || o.NPe < d.NP || o.slices < S || d.NP % 4 != 0) {
+    set_error("emulated N tile mismatch, fewer operand digits than the launch runs, or an X row stride that "
+              "is not a multiple of 4 doubles");
     return CCT_ERR_INVALID;
   }
   a.NP = d.NP;
@@ -737,7 +762,6 @@ int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_de
     case 6064: return launch_emu_s<6, 64>(o, d, jobs_dev, njobs, err, s);
     case 6080: return launch_emu_s<6, 80>(o, d, jobs_dev, njobs, err, s);
     case 7064: return launch_emu_s<7, 64>(o, d, jobs_dev, njobs, err, s);
-    case 8064: return launch_emu_s<8, 64>(o, d, jobs_dev, njobs, err, s);
     default:
       set_error("unsupported (digits, N tile) = (" + std::to_string(o.run_slices) + ", " + std::to_string(o.ebn) +
                 ")");

@@ -99,12 +99,7 @@ struct TupleDev {
 // (emu_slices = 0) builds kEmuMaxSlices digits and runs the smallest count in
 // [kEmuMinSlices, kEmuMaxSlices] whose calibrated E(T) error meets its target.
 constexpr int kEmuMinSlices = 3, kEmuMaxSlices = 7;
-// The backward pass recomputes W with this many digits: the rounded digits'
-// representation error, 2^-57 of the row scale, is below FP64's unit roundoff,
-// so the recomputed W is as accurate as an FP64 W build.  Tensor memory holds
-// its 8 diagonals of 64 columns.
-constexpr int kEmuRecomputeSlices = 8;
-constexpr int kEmuDigitCap = 8;  // most digits any operand holds
+constexpr int kEmuDigitCap = kEmuMaxSlices;  // most digits any operand holds
 // N tile of the emulated W-build: the tensor memory holds S diagonal
 // accumulators of N int32 columns (S N <= 512), and an MMA instruction costs
 // about the same up to N ~ 80, so the widest N that pads nu least is used.

@@ -70,12 +70,6 @@ struct ccT_plan {
   double emu_est_err = 0.0, emu_target = 0.0;  // calibrated |dE(T)| bound and its target (Eh)
   EmuOperands emu;
   EmuJob *emu_jobs = nullptr;  // [buffer][tuple][3]
-  // backward: the 8-digit W recompute (built at the first ccT_backward after
-  // each ccT_set_inputs)
-  EmuOperands rec;
-  EmuJob *rec_jobs = nullptr;  // [buffer][tuple][3]
-  std::vector<GemmJob> host_jobs;  // the FP64 jobs, kept to derive rec_jobs
-  int64_t inputs_gen = 0, rec_gen = -1;
   int *flags = nullptr;
   double *stage = nullptr;  // packed-slice staging for the legacy hook
   std::vector<Tuple> tuples;
@@ -177,40 +171,6 @@ int build_jobs(ccT_plan *p) {
   }
   CCT_CUDA(cudaMemcpy(p->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
   if (p->emulated) CCT_TRY(upload_emu_jobs(p, jobs, p->emu_jobs));
-  p->host_jobs = std::move(jobs);
-  return CCT_OK;
-}
-
-// Operands of the backward's W recompute: kEmuRecomputeSlices rounded digits
-// of E and F (the same digits as the forward's, more of them) with a 64-column
-// N tile; NP is rounded up to it (F8 rows past NP are zero and those X columns
-// are not stored).  Allocated at the first ccT_backward, rebuilt at the first
-// one after each ccT_set_inputs.
-int prepare_recompute(ccT_plan *p, cudaStream_t st) {
-  if (p->rec_gen == p->inputs_gen) return CCT_OK;
-  const Dims &d = p->d;
-  EmuOperands &r = p->rec;
-  if (!r.E8) {
-    const int64_t nu2 = (int64_t)d.nu * d.nu;
-    r.slices = r.run_slices = kEmuRecomputeSlices;
-    r.ebn = 64;
-    r.NPe = round_up(d.NP, r.ebn);
-    r.KP8 = round_up(d.nu + d.no, kEmuKC);
-    r.tiles_m = (nu2 + kEmuBM - 1) / kEmuBM;
-    r.adaptive = false;
-    const int64_t bytesE = (int64_t)r.slices * d.no * r.tiles_m * kEmuBM * r.KP8;
-    CCT_TRY(dalloc(&r.E8, bytesE));
-    CCT_TRY(dalloc(&r.E8T, bytesE));
-    CCT_TRY(dalloc(&r.F8, (int64_t)r.slices * d.no * d.no * r.NPe * r.KP8));
-    CCT_TRY(dalloc(&r.expE, nu2));
-    CCT_TRY(dalloc(&r.expET, d.no * nu2));
-    CCT_TRY(dalloc(&r.expF, d.no * r.NPe));
-    CCT_TRY(dalloc(&r.expRowF, (int64_t)d.no * d.no * d.NP));
-    CCT_TRY(dalloc(&p->rec_jobs, p->host_jobs.size()));
-    CCT_TRY(upload_emu_jobs(p, p->host_jobs, p->rec_jobs));
-  }
-  CCT_TRY(emu_build_operands(d, p->E, p->F, &r, st));
-  p->rec_gen = p->inputs_gen;
   return CCT_OK;
 }
 
@@ -289,7 +249,7 @@ int join_streams(ccT_plan *p) {
 
 // The W-build GEMMs of tuple tix into X buffer b on stream st: the plan's
 // own form, or the FP64 kernel when fp64 is set (emulated plans keep the FP64
-// jobs for the digit calibration).
+// jobs for the backward's recompute and the digit calibration).
 int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st) {
   const Tuple &t = p->tuples[tix];
   const int njobs = t.kind == kIJK ? 3 : 2;
@@ -523,8 +483,8 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   d.KP = round_up(nu + no, kKB);
   p->emulated = o.precision == CCT_PREC_INT8_EMU;
   if (p->emulated) {
-    // the emulated tile sets NP; the FP64 W-build (the digit calibration)
-    // takes the widest of its tiles that divides NP (NP is a multiple of 64,
+    // the emulated tile sets NP; the FP64 W-build (the backward's recompute
+    // and the digit calibration) takes the widest of its tiles that divides NP (NP is a multiple of 64,
     // 80 or 96, so 64, 40 or 48 always qualifies)
     d.EBN = emu_choose_bn(nu, o.emu_slices ? o.emu_slices : kEmuMaxSlices);
     d.NP = round_up(nu, d.EBN);
@@ -694,7 +654,6 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
     CCT_TRY(check_denominators(p));
   }
   std::fill(p->e_built.begin(), p->e_built.end(), 1);
-  p->inputs_gen++;
   if (p->emu_auto) {
     int c = calibrate_digits(p);
     if (c == CCT_OK) c = rebuild_for_count(p);
@@ -800,9 +759,7 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     }
   }
   const int64_t ntup = (int64_t)p->tuples.size();
-  CCT_TRY(prepare_recompute(p, p->stream));
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
-  CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
   CCT_TRY(adj_zero(d, &p->adj, p->stream));
   // dT1 = 2 v1: an emulated plan's v1 is rebuilt from the FP64 W of this pass
   if (p->emulated) CCT_CUDA(cudaMemsetAsync(p->adj.v1, 0, (5 + (size_t)d.nu * d.no) * 8, p->stream));
@@ -824,8 +781,7 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     const int set = (int)((t - begin) % kGXSets);
     const int xb = (int)((t - begin) % kNBuf);
     if (t - begin >= kNBuf) CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_pw[xb], 0));  // X buffer read by t-3
-    CCT_TRY(launch_wbuild_emu(p->rec, d, p->rec_jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2,
-                              p->flags + 1, sW));
+    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2, sW));
     CCT_CUDA(cudaEventRecord(p->ev_rec[xb], sW));
     CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_rec[xb], 0));
     if (t - begin >= kGXSets) {  // GX set read by the GEMMs of t-4
@@ -887,14 +843,8 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
               {d_vvvo, p->adj.g_vvvo, nu * (nu + 1) / 2 * nu * no}};
   for (const auto &o : outs)
     if (o.dst) CCT_CUDA(cudaMemcpyAsync(o.dst, o.src, (size_t)o.n * 8, kind, p->stream));
-  int werr = 0;
-  CCT_CUDA(cudaMemcpyAsync(&werr, p->flags + 1, 4, cudaMemcpyDeviceToHost, p->stream));
   CCT_CUDA(cudaStreamSynchronize(p->stream));
   CCT_CUDA(cudaEventElapsedTime(&p->last_bwd_ms, p->ev0, p->ev1));
-  if (werr) {
-    set_error("the W recompute kernel ran out its bounded wait and unwound");
-    return CCT_ERR_TIMEOUT;
-  }
   return CCT_OK;
 }
 
@@ -1068,9 +1018,7 @@ int ccT_plan_destroy(ccT_plan *p) {
   if (p->flags) cudaFree(p->flags);
   for (void *b : {(void *)p->emu.E8, (void *)p->emu.E8T, (void *)p->emu.F8, (void *)p->emu.expE,
                   (void *)p->emu.expET, (void *)p->emu.expF, (void *)p->emu.expRowF, (void *)p->emu_jobs,
-                  (void *)p->emu.tileExp, (void *)p->emu.slice_hist, (void *)p->rec.E8, (void *)p->rec.E8T,
-                  (void *)p->rec.F8, (void *)p->rec.expE, (void *)p->rec.expET, (void *)p->rec.expF,
-                  (void *)p->rec.expRowF, (void *)p->rec_jobs})
+                  (void *)p->emu.tileExp, (void *)p->emu.slice_hist})
     if (b) cudaFree(b);
   adj_free(&p->adj);
   if (p->ev0) cudaEventDestroy(p->ev0);
