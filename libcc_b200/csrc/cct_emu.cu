@@ -46,7 +46,10 @@
 // bound by its shared-memory operand reads (A 4 KB + B 2.5 KB); a wide one
 // reads A once for up to three B slices.
 //
-// Persistent kernel, one CTA of 64 + 32 NDW threads per SM, work items (job,
+// Persistent kernel, one CTA of 64 + 32 NDW threads per SM (NDW = 16 drain
+// warps at 80 registers a thread: the drain is latency-bound, and 16 warps
+// took a 3-digit tuple from 0.54 to 0.46 ms against 8 warps at 128
+// registers, with room left for a reduction CTA beside it), work items (job,
 // row tile, column tile) taken round-robin with the column tile fastest, so
 // the CTAs in flight share A tiles through L2:
 //   warp 0      producer: per stage, one bulk copy of the A digits and one
@@ -78,10 +81,10 @@ constexpr int A_BLK = kEmuABlk;
 #define CCT_EMU_KS 2
 #endif
 #ifndef CCT_EMU_DRAIN_WARPS
-#define CCT_EMU_DRAIN_WARPS 8
+#define CCT_EMU_DRAIN_WARPS 16
 #endif
 #ifndef CCT_EMU_MAXNREG
-#define CCT_EMU_MAXNREG 128
+#define CCT_EMU_MAXNREG 80
 #endif
 #ifndef CCT_EMU_DB
 #define CCT_EMU_DB 1
@@ -171,6 +174,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t *v) {
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
         "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(addr));
+}
+__device__ __forceinline__ void tmem_ld4(uint32_t addr, uint32_t *v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(addr));
 }
 __device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t *v) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -411,7 +419,7 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
 #pragma unroll
       for (int c0 = 0; c0 < CW; c0 += 16) {
         constexpr int DB = CCT_EMU_DB;  // diagonals per tcgen05.wait::ld
-        const int w = CW - c0 >= 16 ? 16 : 8;  // the last chunk of a 40-column slice is 8 wide
+        const int w = CW - c0 >= 16 ? 16 : (CW - c0 >= 8 ? 8 : 4);  // chunk widths 16, then 8 or 4
 #pragma unroll
         for (int d0 = 0; d0 < S; d0 += DB) {
           if (d0 >= sl) break;  // diagonals past the item's digit count were not written
@@ -422,8 +430,10 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
                 tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * S + d0 + dd) * EBN + cbase + c0);
             if (w == 16)
               tmem_ld16(addr, v[dd]);
-            else
+            else if (w == 8)
               tmem_ld8(addr, v[dd]);
+            else
+              tmem_ld4(addr, v[dd]);
           }
           asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
