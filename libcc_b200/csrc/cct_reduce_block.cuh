@@ -63,6 +63,46 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// slot[p]: the first permutation whose ordered block triple equals O_p (so
+// equal blocks of a degenerate orbit are assembled once).
+__device__ __forceinline__ void orbit_slots(int S0, int S1, int S2, int slot[6]) {
+  auto Sm = [&](int m) { return sel3(m, S0, S1, S2); };
+#pragma unroll
+  for (int p = 0; p < 6; p++) {
+    slot[p] = p;
+#pragma unroll
+    for (int q = 5; q >= 0; q--)
+      if (q < p && Sm(pm(q, 0)) == Sm(pm(p, 0)) && Sm(pm(q, 1)) == Sm(pm(p, 1)) && Sm(pm(q, 2)) == Sm(pm(p, 2)))
+        slot[p] = q;
+  }
+}
+
+// VOE staging as asynchronous 8-byte copies (one commit group).
+__device__ __forceinline__ void stage_voe(int nu, int no, const TupleDev &t, const double *__restrict__ voe, int S0,
+                                          int S1, int S2, double *Vsm) {
+  const int tid = threadIdx.x;
+  const int64_t nu2 = (int64_t)nu * nu;
+#pragma unroll
+  for (int it = 0; it < 3 * VPAIR / RT; it++) {
+    const int q = tid + RT * it;
+    const int pr = q / VPAIR, orient = (q / 384) & 1, plane = (q / 64) % 6, r = q & 63;
+    const int Blo = pr == 0 ? S1 : S0, Bhi = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
+    const int f = RB * (orient ? Bhi : Blo) + (r & 7), s2 = RB * (orient ? Blo : Bhi) + (r >> 3);
+    const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
+    const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
+    const bool ok = f < nu && s2 < nu;
+    cp_async8(Vsm + q, voe + (ok ? ((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2 : 0), ok);
+  }
+  cp_async_commit();
+}
+
+template <int KIND>
+__device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const double *__restrict__ eh,
+                                                const double *__restrict__ ep, const int S0, const int S1,
+                                                const int S2, const int slot[6], const double *Wsm,
+                                                const double *Vsm, double *__restrict__ xpart_slot,
+                                                double *__restrict__ vpart);
+
 // One CTA per unordered block triple {A<=B<=C}.  Phase A assembles W on every
 // distinct ordered block of the orbit in shared memory (term by term, fixed
 // order).  Phase B: each thread evaluates orbits -- the six index permutations
@@ -81,38 +121,14 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
   constexpr int NTERM = KIND == kIJK ? 3 : 4;
   double *Wsm = dyn_smem;             // [6][SL]
   double *Vsm = Wsm + 6 * SL;         // [3][2][6][64]
-  __shared__ double red[RT / 32];
-  __shared__ double warpA[RT / 32][RB][3], warpB[RT / 32][4][3], warpC[RT / 32][2][3];
 
   const int tid = threadIdx.x;
   auto Sm = [&](int m) { return sel3(m, S0, S1, S2); };
-  // slot[p]: first permutation whose ordered block triple equals O_p (uniform)
   int slot[6];
-#pragma unroll
-  for (int p = 0; p < 6; p++) {
-    slot[p] = p;
-#pragma unroll
-    for (int q = 5; q >= 0; q--)
-      if (q < p && Sm(pm(q, 0)) == Sm(pm(p, 0)) && Sm(pm(q, 1)) == Sm(pm(p, 1)) && Sm(pm(q, 2)) == Sm(pm(p, 2)))
-        slot[p] = q;
-  }
+  orbit_slots(S0, S1, S2, slot);
 
   // ---- VOE staging: asynchronous copies, in flight during phase A's X loads
-  {
-    const int64_t nu2 = (int64_t)nu * nu;
-#pragma unroll
-    for (int it = 0; it < 3 * VPAIR / RT; it++) {
-      const int q = tid + RT * it;
-      const int pr = q / VPAIR, orient = (q / 384) & 1, plane = (q / 64) % 6, r = q & 63;
-      const int Blo = pr == 0 ? S1 : S0, Bhi = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
-      const int f = RB * (orient ? Bhi : Blo) + (r & 7), s2 = RB * (orient ? Blo : Bhi) + (r >> 3);
-      const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
-      const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
-      const bool ok = f < nu && s2 < nu;
-      cp_async8(Vsm + q, voe + (ok ? ((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2 : 0), ok);
-    }
-    cp_async_commit();
-  }
+  stage_voe(nu, no, t, voe, S0, S1, S2, Vsm);
 
   // ---- phase A: W on the orbit blocks, one X term at a time.  Term 0 (the
   // identity placement X0(a,b,c) for every kind) is copied straight into W
@@ -188,6 +204,21 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
   if (S0 == S1 && S1 == S2 && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;  // W_aaa = 0 (ZEROT3)
   __syncthreads();
 
+  reduce_block_bc<KIND>(nu, t, eh, ep, S0, S1, S2, slot, Wsm, Vsm, xpart_slot, vpart);
+}
+
+// Phases B and C on W (all orbit blocks, XOR layout) and the VOE staging in
+// shared memory; ends with the per-CTA x3 partial in *xpart_slot and the v1
+// partials in vpart.
+template <int KIND>
+__device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const double *__restrict__ eh,
+                                                const double *__restrict__ ep, const int S0, const int S1,
+                                                const int S2, const int slot[6], const double *Wsm,
+                                                const double *Vsm, double *__restrict__ xpart_slot,
+                                                double *__restrict__ vpart) {
+  __shared__ double red[RT / 32];
+  __shared__ double warpA[RT / 32][RB][3], warpB[RT / 32][4][3], warpC[RT / 32][2][3];
+  const int tid = threadIdx.x;
   // ---- phase B: orbits
   const double dijk = eh[t.i] + eh[t.j] + eh[t.k];
   double x3 = 0.0;
@@ -301,7 +332,6 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
     }
   }
 }
-
 
 }  // namespace red
 }  // namespace cct
