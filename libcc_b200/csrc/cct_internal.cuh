@@ -165,10 +165,8 @@ struct EmuOperands {
 };
 
 int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOperands *o, cudaStream_t s);
-// blocked: store X in the 8 x 8 x 8 blocks the bulk-copy reduction reads
-// (cct_reduce_bulk.cu) instead of rows of NP.
 int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
-                      cudaStream_t s, bool blocked);
+                      cudaStream_t s);
 
 // ----------------------------------------------------------------------------- launchers
 // layout.cu
@@ -186,10 +184,6 @@ int launch_wbuild_f64(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStr
 // reduce.cu
 int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
                   const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s);
-// reduce_bulk.cu: the same reduction over X in 8 x 8 x 8 blocks (bulk copies,
-// persistent, double-buffered); err is set when a bounded wait runs out.
-int launch_reduce_blocked(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
-                          const int16_t *cta_table, double *xpart, double *vpart, int *err, cudaStream_t s);
 int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const double *vpart,
                     double *etd_acc, double *v1_acc, cudaStream_t s);
 int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const double *etd_acc, double *out3,

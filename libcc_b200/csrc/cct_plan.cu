@@ -250,14 +250,12 @@ int join_streams(ccT_plan *p) {
 // The W-build GEMMs of tuple tix into X buffer b on stream st: the plan's
 // own form, or the FP64 kernel when fp64 is set (emulated plans keep the FP64
 // jobs for the backward's recompute and the digit calibration).
-// An emulated W build stores X in 8 x 8 x 8 blocks for the bulk-copy
-// reduction (blocked), or in rows of NP for ccT_tuple_w.
-int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st, bool blocked = true) {
+int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st) {
   const Tuple &t = p->tuples[tix];
   const int njobs = t.kind == kIJK ? 3 : 2;
   const int64_t ntup = (int64_t)p->tuples.size();
   if (p->emulated && !fp64)
-    return launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1, st, blocked);
+    return launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1, st);
   return launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, st);
 }
 
@@ -284,11 +282,7 @@ int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
   td.k = t.k;
   td.weight = t.kind == kIJK ? 1.0 : 0.5;
   CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE, p->red_stream));
-  if (p->emulated && !fp64)  // blocked X (wbuild_tuple's default for emulated plans)
-    CCT_TRY(launch_reduce_blocked(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->flags + 1,
-                                  p->red_stream));
-  else
-    CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->red_stream));
+  CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->red_stream));
   CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->red_stream));
   CCT_TRY(prof_mark(p, -1, p->red_stream));
   CCT_CUDA(cudaEventRecord(p->ev_red[b], p->red_stream));
@@ -536,11 +530,9 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
       (s = dalloc(&p->cta_table, d.ncta * 3)) || (s = dalloc(&p->acc, 5 + nu * no)) ||
       (s = dalloc(&p->jobs, p->tuples.size() * 3 * kNBuf)) || (s = dalloc(&p->flags, 4)))
     return fail(s);
-  // emulated plans store X in 8 x 8 x 8 blocks: ceil(nu/8)^2 64 NP doubles
-  const int64_t xsize = p->emulated ? round_up(nu, kRB) * round_up(nu, kRB) * d.NP : nu2 * d.NP;
   for (int b = 0; b < kNBuf; b++)
     for (int g = 0; g < 3; g++)
-      if ((s = dalloc(&p->X[b][g], xsize))) return fail(s);
+      if ((s = dalloc(&p->X[b][g], nu2 * d.NP))) return fail(s);
   if (p->emulated) {
     EmuOperands &e = p->emu;
     e.slices = o.emu_slices ? o.emu_slices : kEmuMaxSlices;
@@ -924,7 +916,7 @@ int ccT_tuple_w(ccT_plan *p, int64_t tuple, double *w, int32_t mem) {
     wf = w;
   }
   if (s == CCT_OK) CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
-  if (s == CCT_OK) s = wbuild_tuple(p, tuple, 0, false, p->stream, false);  // rows of NP, as the assembly reads
+  if (s == CCT_OK) s = wbuild_tuple(p, tuple, 0, false, p->stream);
   if (s == CCT_OK) s = assemble_w_fortran(p->d, p->tuples[tuple], p->X[0], wc, wf, p->stream);
   int werr = 0;
   if (s == CCT_OK && cudaMemcpyAsync(&werr, p->flags + 1, 4, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess)
@@ -972,8 +964,7 @@ int ccT_time_wbuild(ccT_plan *p, int64_t tuple, int32_t reps, double *ms_per_lau
   CCT_TRY(fork_streams(p));
   CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[0], 0));
   auto launch = [&]() {
-    return p->emulated ? launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * tuple, njobs, p->flags + 1, p->gemm_stream,
-                                           true)
+    return p->emulated ? launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * tuple, njobs, p->flags + 1, p->gemm_stream)
                        : launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream);
   };
   CCT_TRY(launch());  // warm
