@@ -398,6 +398,25 @@ def accuracy_table(A, S, local, main_rows):
     return table
 
 
+def packed_extra(A, inp, local, expanded_ms, expanded_e):
+    """The headline workload's FP64 form with VVVO kept packed (CCT_VVVO_PACKED:
+    the packed triangle resident, operand rows gathered in the W build's tile
+    loader) against the expanded operand: device time of a whole step, bitwise
+    equality and the resident VVVO bytes of each."""
+    no, nu = inp.no, inp.nu
+    with A.TriplesPlan(no, nu, device=local, vvvo="packed") as plan:
+        plan.set_system(inp)
+        times = []
+        for _ in range(2):
+            ets, etd, _ = plan.forward()
+            times.append(plan.last_forward_ms)
+    kp = -(-(nu + no) // 16) * 16
+    return {"workload": f"{inp.name} FP64", "expanded_ms": expanded_ms, "packed_ms": min(times),
+            "packed_over_expanded": min(times) / expanded_ms, "bitwise_equal": (ets + etd) == expanded_e,
+            "expanded_operand_bytes": no * nu * nu * kp * 8,
+            "packed_resident_bytes": nu * (nu + 1) // 2 * nu * no * 8 + nu * nu * no * no * 8}
+
+
 def batch_extra(A, S, local):
     """The 96 uneven systems (no ~ U{3..12}, nu ~ U{24..140}, seed 100+s): the
     batched executor (CUDA graph) against a per-system plan loop, and per-system
@@ -663,6 +682,7 @@ def main():
             extras["adjoint"] = adjoint_extra(A, S, local)
             extras["batch"] = batch_extra(A, S, local)
             extras["per_tile_digits"] = adaptive_extra(A, S, local)
+            extras["packed_vvvo"] = packed_extra(A, inp, local, native["ms_per_step"], native["e_t"])
         print(json.dumps(extras), flush=True)
         cal = head.get("calibration", {})
         line = {"metric": METRIC, "value": head["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,

@@ -60,7 +60,22 @@ typedef struct {
     double emu_tol_rel;      /* automatic digits: relative floor; the target is
                                 max(emu_tol, emu_tol_rel |E(T)|) (0 = default
                                 2e-14, the FP64 evaluation-order round-off)     */
+    int32_t vvvo_mode;       /* FP64 plans: CCT_VVVO_AUTO (default), _EXPANDED or
+                                _PACKED (see below)                             */
+    int32_t reserved;
 } ccT_options;
+
+/* How an FP64 plan holds VVVO.  EXPANDED: ccT_set_inputs expands the packed
+ * triangle once into the W build's row operand E (no*nu^2*round_up(nu+no,16)
+ * doubles: 6.9 GB at no=24, nu=320).  PACKED: the packed triangle (about half
+ * of that) stays resident and the W build gathers each operand row from it
+ * while staging a tile, the reference's "transfer NUTR elements at a time
+ * which blow up to NU2" (CUDA_OUTLINE.txt:55-60) done inside the tile loader;
+ * the results are bitwise those of EXPANDED.  PACKED plans have no backward
+ * (the adjoint writes dE of E's size).  AUTO: PACKED when E would take more
+ * than half of the free device memory, else EXPANDED.  Emulated plans and the
+ * legacy hooks are always EXPANDED. */
+enum { CCT_VVVO_AUTO = 0, CCT_VVVO_EXPANDED = 1, CCT_VVVO_PACKED = 2 };
 
 typedef struct ccT_plan ccT_plan;
 

@@ -17,6 +17,7 @@ STATUS_NAMES = {
 }
 CCT_PREC_FP64, CCT_PREC_INT8_EMU = 0, 1
 CCT_MEM_HOST, CCT_MEM_DEVICE = 0, 1
+CCT_VVVO_AUTO, CCT_VVVO_EXPANDED, CCT_VVVO_PACKED = 0, 1, 2
 
 # every symbol include/libcc_b200.h declares
 EXPORTS = [
@@ -42,7 +43,8 @@ class CctError(RuntimeError):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("check_inputs", ctypes.c_int32),
-                ("emu_slices", ctypes.c_int32), ("emu_tol", ctypes.c_double), ("emu_tol_rel", ctypes.c_double)]
+                ("emu_slices", ctypes.c_int32), ("emu_tol", ctypes.c_double), ("emu_tol_rel", ctypes.c_double),
+                ("vvvo_mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 _lib = None

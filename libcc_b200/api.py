@@ -69,10 +69,12 @@ class TriplesPlan:
     digit count is calibrated in ``set_inputs`` against the target
     max(emu_tol, emu_tol_rel |E(T)|); 3..7: that many digits on every tile);
     ``emu_tol`` / ``emu_tol_rel`` of 0 keep the library defaults (1e-8 Eh,
-    2e-14)."""
+    2e-14).  ``vvvo`` ("auto", "expanded", "packed") says whether an FP64 plan
+    expands VVVO into the W build's operand or keeps the packed triangle
+    resident and gathers rows from it (``CCT_VVVO_*``)."""
 
     def __init__(self, no: int, nu: int, precision: str = "fp64", device: int = 0, check_inputs: bool = True,
-                 emu_slices: int = 0, emu_tol: float = 0.0, emu_tol_rel: float = 0.0):
+                 emu_slices: int = 0, emu_tol: float = 0.0, emu_tol_rel: float = 0.0, vvvo: str = "auto"):
         lib = N.load()
         opt = N.Options()
         lib.ccT_options_default(ctypes.byref(opt))
@@ -84,6 +86,7 @@ class TriplesPlan:
             opt.emu_tol = emu_tol
         if emu_tol_rel:
             opt.emu_tol_rel = emu_tol_rel
+        opt.vvvo_mode = {"auto": N.CCT_VVVO_AUTO, "expanded": N.CCT_VVVO_EXPANDED, "packed": N.CCT_VVVO_PACKED}[vvvo]
         h = ctypes.c_void_p()
         N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
         self._h = h

@@ -73,7 +73,13 @@ struct GemmJob {
   const double *b1;   // F + (x1*no+x3)*NP*KP
   double *out;        // X: row (p,q) at (p*nu+q)*NP
   int nhalves;        // 1 or 2
-  int pad;
+  // packed = 1: the A rows are not read from E but gathered from the packed
+  // VVVO triangle (a0/a1 = the nu columns of occupied x1/x2, nutr doubles
+  // each) and from t0/t1 = -T2 rows of x1/x2 ([(p,q)][l], no doubles each):
+  // E[x][p][q][k] = packed[x*nu + p][tri(k, q)] for k < nu, t[(p*nu+q)*no + k-nu]
+  // for nu <= k < nu+no (cct_layout.cu builds E from the same two sources).
+  int packed;
+  const double *t0, *t1;
 };
 
 // Shapes shared by the kernels of one system.
@@ -175,6 +181,8 @@ int launch_build_e(const Dims &d, const double *vvvo_packed, const double *t2, d
 int launch_build_e_slice(const Dims &d, const double *packed_slice, const double *t2, double *E, int x,
                          cudaStream_t s);
 int launch_build_f(const Dims &d, const double *t2, const double *vm, double *F, cudaStream_t s);
+// packed plans: the -T2 rows of E, et2[x][p*nu+q][l] = -T2(p,q,l,x)
+int launch_build_et2(const Dims &d, const double *t2, double *et2, cudaStream_t s);
 int launch_check_inputs(const Dims &d, const double *eh, const double *ep, const double *t1, const double *t2,
                         const double *vm, const double *voe, const double *vvvo, int *flags, cudaStream_t s);
 

@@ -81,6 +81,18 @@ __global__ void build_f_kernel(const double *__restrict__ t2, const double *__re
   }
 }
 
+// The -T2 rows of E for a packed plan: et2[x][p*nu+q][l] = -T2(p, q, l, x),
+// one thread per element, l fastest.
+__global__ void build_et2_kernel(const double *__restrict__ t2, double *__restrict__ et2, int no, int nu) {
+  const int64_t nu2 = (int64_t)nu * nu, n = (int64_t)no * nu2 * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t l = e % no, r = e / no;
+    const int64_t x = r / nu2, m = r - x * nu2;
+    const int64_t p = m / nu, q = m - p * nu;
+    et2[e] = -t2[((x * no + l) * nu + q) * nu + p];
+  }
+}
+
 // flags[0] |= 1 when any element is NaN/Inf.
 __global__ void finite_kernel(const double *__restrict__ p, int64_t n, int *flags) {
   int bad = 0;
@@ -114,6 +126,15 @@ int launch_build_e_slice(const Dims &d, const double *packed_slice, const double
   const int64_t rows = (int64_t)d.nu * d.nu;
   build_e_kernel<<<grid_for(rows), 256, 0, s>>>(packed_slice, t2, E, d.no, d.nu, d.KP, x, x + 1,
                                                 (int64_t)x * d.nu);
+  CCT_CUDA(cudaGetLastError());
+  return CCT_OK;
+}
+
+int launch_build_et2(const Dims &d, const double *t2, double *et2, cudaStream_t s) {
+  const int64_t n = (int64_t)d.no * d.nu * d.nu * d.no;
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  build_et2_kernel<<<(int)(blocks < 1 ? 1 : blocks), 256, 0, s>>>(t2, et2, d.no, d.nu);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }

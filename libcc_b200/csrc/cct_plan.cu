@@ -65,6 +65,8 @@ struct ccT_plan {
   double *acc = nullptr;  // [etd_sum, etd_comp, out3[3], v1(nu*no)]
   GemmJob *jobs = nullptr;  // [buffer][tuple][3]
   bool emulated = false;    // INT8 split-integer W-build
+  bool packed = false;      // VVVO kept packed (CCT_VVVO_PACKED): no E; vvvo_res and et2 instead
+  double *vvvo_res = nullptr, *et2 = nullptr;
   bool emu_auto = false;    // digit count picked by calibration in ccT_set_inputs
   int emu_base_ebn = 0;     // automatic plans: the N tile the kEmuMaxSlices-digit calibration operands use
   double emu_est_err = 0.0, emu_target = 0.0;  // calibrated |dE(T)| bound and its target (Eh)
@@ -145,10 +147,17 @@ int build_jobs(ccT_plan *p) {
   auto Ex = [&](int x) { return p->E + (int64_t)x * nu2 * d.KP; };
   auto Fyz = [&](int y, int z) { return p->F + ((int64_t)y * d.no + z) * d.NP * d.KP; };
   int buf = 0;
+  // packed plans: the A rows of occupied x come from its nu packed VVVO
+  // columns and its -T2 rows
+  const int64_t nutr = (int64_t)d.nu * (d.nu + 1) / 2;
+  auto Px = [&](int x) { return p->vvvo_res + (int64_t)x * d.nu * nutr; };
+  auto Tx = [&](int x) { return p->et2 + (int64_t)x * nu2 * d.no; };
   auto G = [&](int x1, int x2, int x3, int slot) {
+    if (p->packed) return GemmJob{Px(x1), Px(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][slot], 2, 1, Tx(x1), Tx(x2)};
     return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][slot], 2, 0};
   };
   auto H = [&](int x1, int x2, int x3, int slot) {
+    if (p->packed) return GemmJob{Px(x1), Px(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 1, Tx(x1), Tx(x1)};
     return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 0};
   };
   std::vector<GemmJob> jobs;
@@ -412,6 +421,7 @@ void ccT_options_default(ccT_options *opt) {
   opt->emu_slices = 0;
   opt->emu_tol = kDefaultTol;
   opt->emu_tol_rel = kDefaultTolRel;
+  opt->vvvo_mode = CCT_VVVO_AUTO;
 }
 
 const char *ccT_status_string(int status) {
@@ -467,6 +477,11 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     set_error("emu_tol and emu_tol_rel must be >= 0 (0 = default)");
     return CCT_ERR_INVALID;
   }
+  if (o.vvvo_mode < CCT_VVVO_AUTO || o.vvvo_mode > CCT_VVVO_PACKED ||
+      (o.vvvo_mode == CCT_VVVO_PACKED && (o.precision != CCT_PREC_FP64 || nu > 32767))) {
+    set_error("vvvo_mode must be CCT_VVVO_AUTO, _EXPANDED or _PACKED; PACKED needs an FP64 plan and nu <= 32767");
+    return CCT_ERR_INVALID;
+  }
   int ndev = 0;
   CCT_CUDA(cudaGetDeviceCount(&ndev));
   if (o.device < 0 || o.device >= ndev) {
@@ -502,6 +517,16 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   d.nb = (int)((nu + kRB - 1) / kRB);
   d.ncta = (int64_t)d.nb * (d.nb + 1) * (d.nb + 2) / 6;
   p->tuples = tuple_list((int)no);
+  if (!p->emulated && nu <= 32767) {
+    if (o.vvvo_mode == CCT_VVVO_PACKED) {
+      p->packed = true;
+    } else if (o.vvvo_mode == CCT_VVVO_AUTO) {
+      // packed when the expanded operand would take more than half of the free memory
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+        p->packed = (double)no * nu * nu * d.KP * 8.0 > 0.5 * (double)free_b;
+    }
+  }
   auto fail = [&](int s) {
     ccT_plan_destroy(p);
     return s;
@@ -524,7 +549,9 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   const int64_t nu2 = nu * nu;
   if ((s = dalloc(&p->eh, no)) || (s = dalloc(&p->ep, nu)) || (s = dalloc(&p->t1, no * nu)) ||
       (s = dalloc(&p->t2, nu2 * no * no)) || (s = dalloc(&p->vm, no * nu * no * no)) ||
-      (s = dalloc(&p->voe, nu2 * no * no)) || (s = dalloc(&p->E, no * nu2 * d.KP)) ||
+      (s = dalloc(&p->voe, nu2 * no * no)) ||
+      (s = p->packed ? dalloc(&p->vvvo_res, nu * (nu + 1) / 2 * nu * no) : dalloc(&p->E, no * nu2 * d.KP)) ||
+      (s = p->packed ? dalloc(&p->et2, nu2 * no * no) : CCT_OK) ||
       (s = dalloc(&p->F, no * no * d.NP * d.KP)) ||
       (s = dalloc(&p->xpart, d.ncta)) || (s = dalloc(&p->vpart, (int64_t)12 * d.nb * d.nb * (d.nb + 1))) ||
       (s = dalloc(&p->cta_table, d.ncta * 3)) || (s = dalloc(&p->acc, 5 + nu * no)) ||
@@ -614,7 +641,10 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   cuda(cudaMemcpyAsync(p->voe, voe, nu2 * no * no * 8, kind, p->stream), "copy voe");
   const double *vvvo_dev = vvvo;
   double *staged = nullptr;
-  if (s == CCT_OK && mem == CCT_MEM_HOST) {
+  if (s == CCT_OK && p->packed) {  // the packed triangle is the resident operand
+    cuda(cudaMemcpyAsync(p->vvvo_res, vvvo, nvvvo * 8, kind, p->stream), "copy vvvo");
+    vvvo_dev = p->vvvo_res;
+  } else if (s == CCT_OK && mem == CCT_MEM_HOST) {
     // the packed VVVO is only needed to build E; stage it in a transient
     // buffer.  Plain cudaMalloc/cudaFree: with the stream-ordered pool this
     // call took 0.12-0.21 s at no=24/nu=320 (3.2 GB staged), 0.08-0.10 s so.
@@ -627,7 +657,8 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
     if (s == CCT_OK)
       s = launch_check_inputs(d, p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, vvvo_dev, p->flags, p->stream);
   }
-  if (s == CCT_OK) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
+  if (s == CCT_OK) s = p->packed ? launch_build_et2(d, p->t2, p->et2, p->stream)
+                                 : launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
   if (s == CCT_OK && p->emu_auto) {  // calibration runs on operands of every digit count
     p->d.EBN = p->emu.ebn = p->emu_base_ebn;
@@ -734,6 +765,10 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   }
   if (p->d.nu > 4096) {
     set_error("ccT_backward supports nu <= 4096");
+    return CCT_ERR_UNSUPPORTED;
+  }
+  if (p->packed) {
+    set_error("ccT_backward needs the expanded VVVO operand (a plan with vvvo_mode CCT_VVVO_EXPANDED)");
     return CCT_ERR_UNSUPPORTED;
   }
   DeviceGuard guard(p->device);
@@ -1007,7 +1042,8 @@ int ccT_plan_destroy(ccT_plan *p) {
   DeviceGuard guard(p->device);
   for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream, p->bwd_stream, p->rec_stream})
     if (st) cudaStreamSynchronize(st);
-  double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->xpart, p->vpart, p->acc, p->stage};
+  double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->xpart, p->vpart, p->acc, p->stage,
+                    p->vvvo_res, p->et2};
   for (double *b : bufs)
     if (b) cudaFree(b);
   for (int b = 0; b < kNBuf; b++)
@@ -1066,7 +1102,10 @@ void ijk_gpu_init_(const int64_t *no, const int64_t *nu, const double *eh, const
     g_hook = nullptr;
   }
   ccT_plan *p = nullptr;
-  int s = ccT_plan_create(&p, *no, *nu, nullptr);
+  ccT_options o;
+  ccT_options_default(&o);
+  o.vvvo_mode = CCT_VVVO_EXPANDED;  // the driver hook expands each packed slice into E
+  int s = ccT_plan_create(&p, *no, *nu, &o);
   if (s) legacy_stop("ijk_gpu_init", s);
   DeviceGuard guard(p->device);
   const int64_t n_o = *no, n_u = *nu, nu2 = n_u * n_u;

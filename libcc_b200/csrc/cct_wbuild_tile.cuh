@@ -22,12 +22,16 @@ constexpr int MF = WM / 16;
 
 template <int BN, int TM = BM>
 constexpr int smem_bytes() {
-  return STAGES * (TM + BN) * LDS * 8 + TM * 2 * 4;
+  return STAGES * (TM + BN) * LDS * 8 + TM * 2 * 4 + TM * 2 * 2 * 2;  // tiles, row offsets, packed (p, q)
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -56,6 +60,7 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + STAGES * BM * LDS;
   int *rowoff = reinterpret_cast<int *>(Bs + STAGES * BN * LDS);  // [2][BM] row index into E (or -1)
+  int16_t *rowpq = reinterpret_cast<int16_t *>(rowoff + 2 * BM);   // [2][BM][2] (p, q) of the row (packed jobs)
 
   const int64_t M = (int64_t)nu * nu;
   const int64_t m0 = (int64_t)tile_m * BM;
@@ -69,6 +74,10 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
       const int p = (int)(m / nu), q = (int)(m - (int64_t)(m / nu) * nu);
       rowoff[r] = p * nu + q;
       rowoff[BM + r] = q * nu + p;
+      rowpq[2 * r] = (int16_t)p;
+      rowpq[2 * r + 1] = (int16_t)q;
+      rowpq[2 * (BM + r)] = (int16_t)q;
+      rowpq[2 * (BM + r) + 1] = (int16_t)p;
     } else {
       rowoff[r] = -1;
       rowoff[BM + r] = -1;
@@ -87,11 +96,39 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
     double *as = As + stage * BM * LDS;
     double *bs = Bs + stage * BN * LDS;
     const int chunk = tid & 7;  // 8 x 16 B per 16-double row
+    if (!job.packed) {
 #pragma unroll
-    for (int rr = tid >> 3; rr < BM; rr += NT / 8) {
-      const int ro = rowoff[h * BM + rr];
-      const double *src = abase + (ro < 0 ? 0 : (int64_t)ro * KP) + k0 + chunk * 2;
-      cp_async16(as + swz(rr, chunk * 2), src, ro < 0 ? 0 : 16);
+      for (int rr = tid >> 3; rr < BM; rr += NT / 8) {
+        const int ro = rowoff[h * BM + rr];
+        const double *src = abase + (ro < 0 ? 0 : (int64_t)ro * KP) + k0 + chunk * 2;
+        cp_async16(as + swz(rr, chunk * 2), src, ro < 0 ? 0 : 16);
+      }
+    } else {
+      // the row's E values gathered one double at a time: the packed
+      // triangle holds (k q | p x) at tri(k, q) of column p, the -T2 rows the
+      // k >= nu part; past nu + no the row is zero
+      const double *tbase = h ? job.t1 : job.t0;
+      const int64_t nutr = (int64_t)nu * (nu + 1) / 2;
+      const int nov = (int)(KV - nu);
+#pragma unroll
+      for (int rr = tid >> 3; rr < BM; rr += NT / 8) {
+        const int ro = rowoff[h * BM + rr];
+        const int pr = rowpq[2 * (h * BM + rr)], qr = rowpq[2 * (h * BM + rr) + 1];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int64_t k = k0 + chunk * 2 + e;
+          const double *src = abase;
+          int bytes = 0;
+          if (ro >= 0 && k < nu) {
+            src = abase + (int64_t)pr * nutr + (k >= qr ? k * (k + 1) / 2 + qr : (int64_t)qr * (qr + 1) / 2 + k);
+            bytes = 8;
+          } else if (ro >= 0 && k < KV) {
+            src = tbase + (int64_t)ro * nov + (k - nu);
+            bytes = 8;
+          }
+          cp_async8(as + swz(rr, chunk * 2 + e), src, bytes);
+        }
+      }
     }
 #pragma unroll
     for (int rr = tid >> 3; rr < BN; rr += NT / 8) {

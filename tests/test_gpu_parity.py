@@ -290,3 +290,33 @@ def test_caller_stream(api):
         plan.set_stream(None)
         c = plan.forward()
     assert a[1] == b[1] == c[1]
+
+
+@pytest.mark.parametrize("no,nu,seed,dist", [(4, 36, 0, "normal"), (5, 29, 3, "log"), (3, 7, 4, "normal"),
+                                             (6, 130, 5, "normal")])
+def test_packed_vvvo_bitwise_equals_expanded(api, no, nu, seed, dist):
+    """CCT_VVVO_PACKED (the packed triangle resident, operand rows gathered in the
+    W build's tile loader) against the expanded operand: the same values in the
+    same order, so every result is bitwise equal."""
+    inp = S.generate(no, nu, seed, dist)
+    out = {}
+    for mode in ("expanded", "packed"):
+        with api.TriplesPlan(no, nu, vvvo=mode) as plan:
+            plan.set_system(inp)
+            ets, etd, v1 = plan.forward()
+            w = [plan.tuple_w(t) for t in (0, plan.num_tuples - 1)]
+        out[mode] = (ets, etd, v1, w)
+    e, p = out["expanded"], out["packed"]
+    assert e[0] == p[0] and e[1] == p[1] and np.array_equal(e[2], p[2])
+    assert all(np.array_equal(a, b) for a, b in zip(e[3], p[3]))
+
+
+def test_packed_vvvo_has_no_backward(api):
+    from libcc_b200._native import CctError
+    inp = S.generate(4, 11, 2)
+    with api.TriplesPlan(inp.no, inp.nu, vvvo="packed") as plan:
+        plan.set_system(inp)
+        plan.forward()
+        with pytest.raises(CctError) as e:
+            plan.backward()
+        assert e.value.status == 8  # CCT_ERR_UNSUPPORTED

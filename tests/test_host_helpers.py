@@ -74,3 +74,20 @@ def test_batch_command_line_parses_without_a_gpu(capsys):
         batch.main(["--help"])
     assert e.value.code == 0
     assert "--systems" in capsys.readouterr().out
+
+
+def test_packed_vvvo_option_is_validated_without_a_gpu():
+    """vvvo_mode out of range, or PACKED on an emulated plan, is rejected before any
+    device call."""
+    import ctypes
+    from libcc_b200 import _native as N
+    try:
+        lib = N.load()
+    except N.NativeLibraryError:
+        pytest.skip("library not built")
+    for prec, mode in ((N.CCT_PREC_FP64, 7), (N.CCT_PREC_INT8_EMU, N.CCT_VVVO_PACKED)):
+        opt = N.Options()
+        lib.ccT_options_default(ctypes.byref(opt))
+        opt.precision, opt.vvvo_mode = prec, mode
+        h = ctypes.c_void_p()
+        assert lib.ccT_plan_create(ctypes.byref(h), 4, 10, ctypes.byref(opt)) == 1
