@@ -281,6 +281,36 @@ int ccT_reduce_w_noalloc(int64_t no, int64_t nu, int64_t i, int64_t j, int64_t k
                          const double *eh, const double *ep, const double *voe, double *etd_acc,
                          double *v1_acc, void *cuda_stream);
 
+/* ------------------------------------------------------------------ CCSD T1-dressing terms
+ * The two routines of the reference's OpenACC CCSD port that contract the
+ * same expanded VVVO slices as the triples, for one process holding every
+ * occupied index (nothing in the reference tree calls them; they are the CCSD
+ * step before (T)).  Arrays are Fortran column-major; mem says whether every
+ * pointer is host or device memory; the calls return when the results are in
+ * place.
+ *
+ * ccT_ccsd_terms_29_31 replaces terms_29_30_31 (src/triples-ijk/ccsd_acc.f:1-60):
+ *   t2(i,b,c,j) += sum_a o1(i,a) [ (c a|b j) - sum_k o1(k,c) vl(k,a,b,j)
+ *                                  - sum_k o1(k,b) vr(c,k,a,j) ]
+ * with o1 (no,nu), t2 (no,nu,nu,no), vl the DDI array D_VL read as
+ * (no,nu,nu,no), vr D_VR_IBT read as (nu,no,nu,no), vvvo packed as for
+ * ccT_set_inputs.  (The routine's TRANMD of its scratch buffer at line 33 has
+ * no effect on the result and is not reproduced.) */
+int ccT_ccsd_terms_29_31(int64_t no, int64_t nu, const double *o1, double *t2, const double *vl,
+                         const double *vr, const double *vvvo, int32_t mem);
+
+/* ccT_ccsd_terms_32_35 replaces terms_32_33_34_35 (ccsd_acc.f:64-160) and leaves
+ * its arrays as that routine does: t2 (nou x nou, nou = no nu) transposed;
+ * o2 (no,nu,nu,no) permuted to o2(x,y,k,l) = o2_in(k,x,y,l), i.e. (nu,nu,no,no);
+ * rl (nou x nou) = the transpose of RL(i,y,z,j) = sum_x o1(i,x) (x y|z j); and
+ * vm (no,no,no,nu) replaced by vm(x,y,z,a) = vm_in(y,x,z,a)
+ * + sum_{p,q} o2_in(x,p,q,z) (a q|p y), the contraction on the FP64 tensor
+ * cores.  The reference's update loop (lines 136-144) offsets that sum by one
+ * element within each (j, a) block; this adds it where the surrounding
+ * permutations put it. */
+int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, double *o2, double *t2, double *vm,
+                         double *rl, const double *vvvo, int32_t mem);
+
 /* ------------------------------------------------------------------ legacy hooks
  * ijk_gpu_init_    replaces the call at src/triples-ijk/triples_cpu.F90:363
  * ijk_gpu_driver_  replaces src/triples-ijk/ddcc_t_ijk_big_cuda.f:12-14

@@ -222,6 +222,32 @@ def cc_triples(no: int, nu: int, eh, ep, t1, t2, vm, voe, vvvo):
     return ets.value, etd.value, v1
 
 
+def ccsd_terms_29_31(no: int, nu: int, o1, t2, vl, vr, vvvo) -> np.ndarray:
+    """The reference CCSD port's terms_29_30_31 (ccsd_acc.f:1-60) through
+    ``ccT_ccsd_terms_29_31``; returns the updated t2 (host arrays in, host out)."""
+    n4 = no * nu * nu * no
+    nutr = nu * (nu + 1) // 2
+    a = [_host(o1, no * nu, "o1"), _host(t2, n4, "t2").copy(), _host(vl, n4, "vl"), _host(vr, n4, "vr"),
+         _host(vvvo, nutr * nu * no, "vvvo")]
+    ptr = [ctypes.c_void_p(x.ctypes.data) for x in a]
+    N.check(N.load().ccT_ccsd_terms_29_31(no, nu, *ptr, N.CCT_MEM_HOST), "ccT_ccsd_terms_29_31")
+    return a[1]
+
+
+def ccsd_terms_32_35(no: int, nu: int, o1, o2, t2, vm, vvvo):
+    """The reference CCSD port's terms_32_33_34_35 (ccsd_acc.f:64-160) through
+    ``ccT_ccsd_terms_32_35``; returns (t2, o2, vm, rl) as the routine leaves them."""
+    n4 = no * nu * nu * no
+    nutr = nu * (nu + 1) // 2
+    o1h = _host(o1, no * nu, "o1")
+    o2h, t2h, vmh = _host(o2, n4, "o2").copy(), _host(t2, n4, "t2").copy(), _host(vm, no ** 3 * nu, "vm").copy()
+    rl = np.zeros(n4)
+    vv = _host(vvvo, nutr * nu * no, "vvvo")
+    ptr = [ctypes.c_void_p(x.ctypes.data) for x in (o1h, o2h, t2h, vmh, rl, vv)]
+    N.check(N.load().ccT_ccsd_terms_32_35(no, nu, *ptr, N.CCT_MEM_HOST), "ccT_ccsd_terms_32_35")
+    return t2h, o2h, vmh, rl
+
+
 def packed_columns(vvvo: np.ndarray, no: int, nu: int, x: int) -> np.ndarray:
     """The nu packed VVVO columns of occupied index x (0-based), as ddi_get fetches
     them for the GPU hook (triples_cpu.F90:428-450)."""

@@ -650,3 +650,108 @@ def openblas_dgemm_tflops(n: int = 4096, reps: int = 3) -> float:
 
 def cpu_threads() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+# --------------------------------------------------------------------------- CCSD T1-dressing terms
+#
+# The two routines of the reference's OpenACC CCSD port, src/triples-ijk/ccsd_acc.f
+# (terms_29_30_31, lines 1-60; terms_32_33_34_35, lines 64-160), restated as
+# their literal DGEMM / permutation sequence for one process that holds every
+# occupied index (DIV_EVEN over one rank).  Nothing in the reference tree calls
+# them.  Permutation helpers, from the reference's TRANMD_SMP
+# (common_functions.f:141-421) and GAMESS conventions for the two the tree
+# does not define:
+#   TRANMD(A,n1,n2,n3,n4,13): new(a,b,c,l) = old(c,b,a,l);   12: old(b,a,c,l);
+#                            23: old(a,c,b,l);  312: new(x,y,z,l) = old(z,x,y,l)
+#   INSITU(n1,n2,n3,n4,tmp,V,12): V(n1,n2,n3,n4) becomes V'(n2,n1,n3,n4),
+#                            V'(x,y,z,w) = V(y,x,z,w); 13 and 23 likewise
+#   TRANSQ(A,n): the n x n matrix A transposed in place.
+# Two places of the literal code are not followed: the TRANMD of the scratch
+# buffer tmp at ccsd_acc.f:33 (it transposes a buffer of nutr*nu doubles as if
+# it held nu^3, and nothing reads it afterwards except as scratch), and the VM
+# update loop at ccsd_acc.f:136-144, whose vm(iof1+i) / tmp(iof2+i) with iof1
+# and i both starting at 1 skip the first element of every (j, a) block and add
+# into the next one; the restatement adds tmp((k,l),a) to VM(k,l,j,a).
+
+def _tranmd(a: np.ndarray, code: int) -> np.ndarray:
+    """TRANMD on a 4-index Fortran array (returns a new array)."""
+    spec = {12: "bacd", 13: "cbad", 23: "acbd", 312: "cabd"}[code]
+    return np.asfortranarray(np.einsum(spec + "->abcd", a))
+
+
+def _insitu(a: np.ndarray, code: int) -> np.ndarray:
+    """INSITU: the two named indices of a 4-index array exchanged (new shape)."""
+    axes = {12: (1, 0, 2, 3), 13: (2, 1, 0, 3), 23: (0, 2, 1, 3)}[code]
+    return np.asfortranarray(np.transpose(a, axes))
+
+
+def _transq(flat: np.ndarray, n: int) -> np.ndarray:
+    return np.ascontiguousarray(flat.reshape((n, n), order="F").T.ravel(order="F"))
+
+
+def _vvvo_slice(vvvo: np.ndarray, no: int, nu: int, j: int) -> np.ndarray:
+    """DDCC_T_GETVE_acc (ddcc_aux.f:18-45): VE(x,y,z) = (xy|z j), Fortran (nu,nu,nu)."""
+    nutr = nu * (nu + 1) // 2
+    cols = vvvo.reshape(nu * no, nutr)[j * nu:(j + 1) * nu]
+    r, c = np.tril_indices(nu)
+    ve = np.zeros((nu, nu, nu), order="F")
+    for z in range(nu):
+        ve[r, c, z] = cols[z]
+        ve[c, r, z] = cols[z]
+    return ve
+
+
+def literal_terms_29_30_31(no, nu, o1, t2, vl, vr, vvvo):
+    """terms_29_30_31: returns the new t2 (no,nu,nu,no).  o1 (no,nu); vl the DDI
+    array D_VL as (no,nu,nu,no); vr D_VR_IBT as (nu,no,nu,no); vvvo packed."""
+    O1 = o1.reshape((no, nu), order="F")
+    T2 = np.array(t2, dtype=np.float64).reshape((no, nu * nu, no), order="F").copy(order="F")
+    VL = vl.reshape((no, nu * nu, no), order="F")
+    VR = vr.reshape((nu, no, nu, no), order="F")
+    for j in range(no):
+        ve = _vvvo_slice(vvvo, no, nu, j)
+        ve2 = ve.reshape((nu, nu * nu), order="F") - O1.T @ VL[:, :, j]               # DGEMM('T','N') line 37
+        ve = _tranmd(ve2.reshape((nu, nu, nu, 1), order="F"), 13)                      # line 44
+        rl = _insitu(_insitu(VR[:, :, :, j].reshape((nu, no, nu, 1), order="F"), 13), 12)  # lines 46-47
+        ve2 = ve.reshape((nu, nu * nu), order="F") - O1.T @ rl.reshape((no, nu * nu), order="F")  # line 49
+        ve = _tranmd(ve2.reshape((nu, nu, nu, 1), order="F"), 12)                      # line 52
+        T2[:, :, j] += O1 @ ve.reshape((nu, nu * nu), order="F")                       # line 54
+    return T2.ravel(order="F")
+
+
+def literal_terms_32_35(no, nu, o1, o2, t2, vm, vvvo):
+    """terms_32_33_34_35: returns (t2, o2, vm, rl) as the routine leaves them:
+    t2 transposed as an (nou x nou) matrix, o2 permuted to (nu,nu,no,no), vm
+    updated, rl the new (nou x nou) array.  o1 (no,nu); o2 (no,nu,nu,no);
+    t2 (no,nu,nu,no); vm (no,no,no,nu); vvvo packed."""
+    nou = no * nu
+    O1 = o1.reshape((no, nu), order="F")
+    t2n = _transq(np.asarray(t2, dtype=np.float64), nou)                               # line 83
+    O2 = _insitu(_insitu(np.asarray(o2).reshape((no, nu, nu, no), order="F"), 12), 23)  # lines 84-85
+    VM = _tranmd(np.asarray(vm).reshape((no, no, no, nu), order="F"), 312)             # line 86
+    RL = np.zeros((no, nu * nu, no), order="F")
+    for j in range(no):
+        ve = _vvvo_slice(vvvo, no, nu, j)
+        RL[:, :, j] = O1 @ ve.reshape((nu, nu * nu), order="F")                        # line 109
+        ve13 = _tranmd(ve.reshape((nu, nu, nu, 1), order="F"), 13)                     # line 114
+        tmp = O2.reshape((nu * nu, no * no), order="F").T @ ve13.reshape((nu * nu, nu), order="F")  # line 119
+        VM[:, :, j, :] += tmp.reshape((no, no, nu), order="F")                          # lines 125-131 (intended)
+    rl = _transq(RL.ravel(order="F"), nou)                                             # line 151
+    VM = _tranmd(VM, 23)                                                               # line 154
+    return t2n, O2.ravel(order="F"), VM.ravel(order="F"), rl
+
+
+def closed_terms_29_30_31(no, nu, o1, t2, vl, vr, vvvo):
+    """The same update in closed form (derived from the sequence above):
+    T2(i,y,z,j) += sum_x O1(i,x) [ (z x|y j) - sum_k O1(k,z) VL(k,x,y,j)
+                                   - sum_k O1(k,y) VR(z,k,x,j) ]."""
+    O1 = o1.reshape((no, nu), order="F")
+    VL = vl.reshape((no, nu, nu, no), order="F")
+    VR = vr.reshape((nu, no, nu, no), order="F")
+    T2 = np.array(t2, dtype=np.float64).reshape((no, nu, nu, no), order="F").copy(order="F")
+    for j in range(no):
+        V = _vvvo_slice(vvvo, no, nu, j)                  # V[x,y,z] = (xy|z j)
+        G = np.einsum("zxy->xyz", V) - np.einsum("kz,kxy->xyz", O1, VL[:, :, :, j]) \
+            - np.einsum("ky,zkx->xyz", O1, VR[:, :, :, j])
+        T2[:, :, :, j] += np.einsum("ix,xyz->iyz", O1, G)
+    return T2.ravel(order="F")

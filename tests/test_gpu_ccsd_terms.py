@@ -1,0 +1,36 @@
+"""The CCSD T1-dressing terms on the GPU (ccT_ccsd_terms_29_31 / _32_35)
+against the oracle's literal restatement of ccsd_acc.f."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(no, nu, seed):
+    rng = np.random.default_rng(seed)
+    nutr = nu * (nu + 1) // 2
+    n4 = no * nu * nu * no
+    return dict(o1=rng.normal(0, 0.1, no * nu), t2=rng.normal(size=n4), vl=rng.normal(size=n4),
+                vr=rng.normal(size=n4), vvvo=rng.normal(size=nutr * nu * no), o2=rng.normal(size=n4),
+                vm=rng.normal(size=no ** 3 * nu))
+
+
+@pytest.mark.parametrize("no,nu,seed", [(3, 5, 1), (4, 17, 2), (6, 40, 3), (8, 64, 4)])
+def test_terms_29_31_match_oracle(no, nu, seed):
+    from libcc_b200 import api as A
+    from oracle import oracle as O
+    a = _inputs(no, nu, seed)
+    got = A.ccsd_terms_29_31(no, nu, a["o1"], a["t2"], a["vl"], a["vr"], a["vvvo"])
+    ref = O.literal_terms_29_30_31(no, nu, a["o1"], a["t2"], a["vl"], a["vr"], a["vvvo"])
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("no,nu,seed", [(3, 5, 1), (4, 17, 2), (6, 40, 3), (8, 64, 4)])
+def test_terms_32_35_match_oracle(no, nu, seed):
+    from libcc_b200 import api as A
+    from oracle import oracle as O
+    a = _inputs(no, nu, seed)
+    got = A.ccsd_terms_32_35(no, nu, a["o1"], a["o2"], a["t2"], a["vm"], a["vvvo"])
+    ref = O.literal_terms_32_35(no, nu, a["o1"], a["o2"], a["t2"], a["vm"], a["vvvo"])
+    for name, g, r in zip(("t2", "o2", "vm", "rl"), got, ref):
+        assert np.abs(g - r).max() <= 1e-12 * max(np.abs(r).max(), 1e-300), name
