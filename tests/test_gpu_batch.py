@@ -85,3 +85,21 @@ def test_forward_needs_inputs():
         with pytest.raises(N.CctError) as e:
             b.forward()
         assert e.value.status == 6
+
+
+def test_bounded_wait_runs_out_and_context_survives(systems, single):
+    """The persistent executor's counter wait, made unmeetable on the host
+    (one tuple's reduction blocks wait for a W-build tile more than it has)
+    with a short spin limit: the forward returns CCT_ERR_TIMEOUT, and with the
+    stall cleared the same batch gives the single-plan bits again."""
+    from libcc_b200 import _native as N
+    with _batch(systems) as b:
+        b.configure(0, 32, 0, 1 << 20)
+        b.debug_stall(0, 20000)
+        with pytest.raises(N.CctError) as e:
+            b.forward()
+        assert e.value.status == 7  # CCT_ERR_TIMEOUT
+        b.debug_stall(-1, 0)
+        ets, etd = b.forward()
+        for k in range(len(systems)):
+            assert ets[k] == single[k][0] and etd[k] == single[k][1]
