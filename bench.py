@@ -417,6 +417,66 @@ def packed_extra(A, inp, local, expanded_ms, expanded_e):
             "packed_resident_bytes": nu * (nu + 1) // 2 * nu * no * 8 + nu * nu * no * no * 8}
 
 
+def measured_peak(key: str) -> float:
+    """A driver-measured peak of this GPU pool (MEASURED_PEAKS.json beside this file)."""
+    return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())[key])
+
+
+def ccsd_extra(local, no: int = 24, nu: int = 320):
+    """The CCSD T1-dressing terms (ccT_ccsd_terms_29_31 / _32_35) at the headline
+    shape on device-resident seeded inputs: device time per call (CUDA events on
+    the legacy stream the entry points launch on; the second of two calls), the
+    algorithmic bytes and flops and the fraction of the measured HBM and FP64
+    peaks they imply, and terms 29-31 for one occupied index against the closed
+    form on the host."""
+    import ctypes
+    import numpy as np
+    import torch
+    from libcc_b200 import _native as N
+    from oracle import oracle as O
+    lib = N.load()
+    nutr, n4 = nu * (nu + 1) // 2, no * nu * nu * no
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(7)
+    mk = lambda n, sd: torch.randn(n, generator=g, device=f"cuda:{local}", dtype=torch.float64) * sd
+    o1, vl, vr, vvvo = mk(no * nu, 0.01), mk(n4, 0.05), mk(n4, 0.05), mk(nutr * nu * no, 0.05)
+    t2_0, o2, vm0 = mk(n4, 0.05), mk(n4, 0.05), mk(no ** 3 * nu, 0.05)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    out = {"workload": f"no={no}, nu={nu}, seeded normal inputs on the device"}
+    for name in ("29_31", "32_35"):
+        ms = []
+        for _ in range(2):
+            t2 = t2_0.clone()
+            vm, o2c, rl = vm0.clone(), o2.clone(), torch.zeros(n4, device=f"cuda:{local}", dtype=torch.float64)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if name == "29_31":
+                st = lib.ccT_ccsd_terms_29_31(no, nu, vp(o1), vp(t2), vp(vl), vp(vr), vp(vvvo), N.CCT_MEM_DEVICE)
+            else:
+                st = lib.ccT_ccsd_terms_32_35(no, nu, vp(o1), vp(o2c), vp(t2), vp(vm), vp(rl), vp(vvvo),
+                                              N.CCT_MEM_DEVICE)
+            e1.record()
+            torch.cuda.synchronize()
+            N.check(st, "ccT_ccsd_terms_" + name)
+            ms.append(e0.elapsed_time(e1))
+        if name == "29_31":
+            byts = 8 * (no * nu + 4 * n4 + nutr * nu * no)       # o1, vl, vr, vvvo read; t2 read and written
+            flop = 6 * no * no * nu ** 3                          # G (two K=no sums) and the O1 contraction
+            j = no // 2
+            ref = O.closed_terms_29_30_31(no, nu, o1.cpu().numpy(), t2_0.cpu().numpy(), vl.cpu().numpy(),
+                                          vr.cpu().numpy(), vvvo.cpu().numpy(), only_j=j)
+            got = t2.cpu().numpy().reshape((no, nu, nu, no), order="F")[:, :, :, j]
+            out["rel_err_29_31_one_j"] = float(np.abs(got - ref).max() / np.abs(ref).max())
+        else:
+            byts = 8 * (no * nu + 6 * n4 + 2 * no ** 3 * nu + nutr * nu * no)  # o2, t2 r/w; rl w; vm r/w; vvvo r
+            flop = 2 * no ** 3 * nu ** 3 + 2 * no * no * nu ** 3  # T GEMM (M=no^2, N=nu no, K=nu^2) and RL
+        sec = ms[-1] * 1e-3
+        out[name] = {"device_ms": ms[-1], "algorithmic_bytes": byts, "flop": flop,
+                     "hbm_frac_of_measured": byts / sec / 1e9 / measured_peak("hbm_gbs"),
+                     "tflops": flop / sec / 1e12}
+    return out
+
+
 def batch_extra(A, S, local):
     """The 96 uneven systems (no ~ U{3..12}, nu ~ U{24..140}, seed 100+s): the
     batched executor (CUDA graph) against a per-system plan loop, and per-system
@@ -683,6 +743,7 @@ def main():
             extras["batch"] = batch_extra(A, S, local)
             extras["per_tile_digits"] = adaptive_extra(A, S, local)
             extras["packed_vvvo"] = packed_extra(A, inp, local, native["ms_per_step"], native["e_t"])
+            extras["ccsd_terms"] = ccsd_extra(local)
         print(json.dumps(extras), flush=True)
         cal = head.get("calibration", {})
         line = {"metric": METRIC, "value": head["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,

@@ -741,17 +741,18 @@ def literal_terms_32_35(no, nu, o1, o2, t2, vm, vvvo):
     return t2n, O2.ravel(order="F"), VM.ravel(order="F"), rl
 
 
-def closed_terms_29_30_31(no, nu, o1, t2, vl, vr, vvvo):
+def closed_terms_29_30_31(no, nu, o1, t2, vl, vr, vvvo, only_j=None):
     """The same update in closed form (derived from the sequence above):
     T2(i,y,z,j) += sum_x O1(i,x) [ (z x|y j) - sum_k O1(k,z) VL(k,x,y,j)
-                                   - sum_k O1(k,y) VR(z,k,x,j) ]."""
+                                   - sum_k O1(k,y) VR(z,k,x,j) ].
+    With only_j set, returns just the updated slab T2(:,:,:,only_j)."""
     O1 = o1.reshape((no, nu), order="F")
     VL = vl.reshape((no, nu, nu, no), order="F")
     VR = vr.reshape((nu, no, nu, no), order="F")
     T2 = np.array(t2, dtype=np.float64).reshape((no, nu, nu, no), order="F").copy(order="F")
-    for j in range(no):
+    for j in (range(no) if only_j is None else [only_j]):
         V = _vvvo_slice(vvvo, no, nu, j)                  # V[x,y,z] = (xy|z j)
-        G = np.einsum("zxy->xyz", V) - np.einsum("kz,kxy->xyz", O1, VL[:, :, :, j]) \
-            - np.einsum("ky,zkx->xyz", O1, VR[:, :, :, j])
-        T2[:, :, :, j] += np.einsum("ix,xyz->iyz", O1, G)
-    return T2.ravel(order="F")
+        G = np.einsum("zxy->xyz", V) - np.einsum("kz,kxy->xyz", O1, VL[:, :, :, j], optimize=True) \
+            - np.einsum("ky,zkx->xyz", O1, VR[:, :, :, j], optimize=True)
+        T2[:, :, :, j] += np.einsum("ix,xyz->iyz", O1, G, optimize=True)
+    return T2.ravel(order="F") if only_j is None else T2[:, :, :, only_j]
