@@ -479,51 +479,81 @@ def ccsd_extra(local, no: int = 24, nu: int = 320):
 
 def batch_extra(A, S, local):
     """The 96 uneven systems (no ~ U{3..12}, nu ~ U{24..140}, seed 100+s): the
-    batched executor (CUDA graph) against a per-system plan loop, and per-system
-    E(T) against the CPU oracle on the 8 smallest systems."""
-    import numpy as np
+    batched executors (CUDA graph) against per-system plan loops, in the FP64
+    form (grouped launches, and the persistent device-queue kernel) and in the
+    emulated form (each system's digit count calibrated to 1e-8 Eh; the tuner
+    choosing among all executors), with per-system E(T) against the CPU oracle
+    on the 8 smallest systems."""
     from libcc_b200 import batch as B
     from oracle import oracle as O
     systems = S.batch96()
-    plans = []
-    for inp in systems:
-        p = A.TriplesPlan(inp.no, inp.nu, device=local)
-        p.set_system(inp)
-        plans.append(p)
-    loop_ms, loop_res = [], None
-    for rep in range(3):
-        res, ms = [], 0.0
-        for p in plans:
-            res.append(p.forward(want_v1=False))
-            ms += p.last_forward_ms
-        loop_ms.append(ms)
-        loop_res = res
-    for p in plans:
-        p.close()
-    with B.TriplesBatch([(s.no, s.nu) for s in systems], device=local) as b:
-        for k, inp in enumerate(systems):
-            b.set_system(k, inp)
-        bms = []
+    shapes = [(s.no, s.nu) for s in systems]
+
+    def loop(form):
+        plans = []
+        for inp in systems:
+            p = A.TriplesPlan.for_form(inp.no, inp.nu, form, device=local)
+            p.set_system(inp)
+            plans.append(p)
+        loop_ms, res = [], None
         for rep in range(3):
-            ets, etd = b.forward()
-            bms.append(b.last_ms)
-        items = b.work_items
-    same = all(ets[k] == loop_res[k][0] and etd[k] == loop_res[k][1] for k in range(len(systems)))
-    small = sorted(range(len(systems)), key=lambda k: S.flops(systems[k].no, systems[k].nu))[:8]
-    errs = []
-    for k in small:
-        e_o, d_o, _ = O.c_cc_triples(systems[k])
-        errs.append(abs((ets[k] + etd[k]) - (e_o + d_o)) / abs(e_o + d_o))
+            r, ms = [], 0.0
+            for p in plans:
+                r.append(p.forward(want_v1=False))
+                ms += p.last_forward_ms
+            loop_ms.append(ms)
+            res = r
+        for p in plans:
+            p.close()
+        return statistics.median(loop_ms), res
+
+    def batched(form, config=None, tune=False):
+        with B.TriplesBatch(shapes, device=local, form=form) as b:
+            for k, inp in enumerate(systems):
+                b.set_system(k, inp)
+            if config:
+                b.configure(*config)
+            chosen = b.tune() if tune else None
+            ms = []
+            for rep in range(3):
+                ets, etd = b.forward()
+                ms.append(b.last_ms)
+            digits = [b.emu_digits(k) for k in range(len(systems))] if b.emulated and (not chosen or chosen[0] == 2) \
+                else None
+            return statistics.median(ms), ets, etd, b.work_items, chosen, digits
+
     flops = sum(S.flops(s.no, s.nu) for s in systems)
-    lm, bm = statistics.median(loop_ms), statistics.median(bms)
-    return {"workload": "96 systems, no ~ U{3..12}, nu ~ U{24..140}, seed 100+s (normal)",
-            "tuples": int(sum(A.N.load().ccT_num_tuples(s.no) for s in systems)), "flops": flops,
-            "batched_ms": bm, "batched_tflops": flops / bm / 1e9, "per_system_loop_ms": lm,
-            "per_system_loop_tflops": flops / lm / 1e9, "speedup_batched_over_loop": lm / bm,
-            "work_items": items, "bitwise_equal_to_loop": bool(same),
-            "executor": "grouped launches per tuple group on two streams, per-system N tile, tuples by cost; "
-                        "CUDA graph replay",
-            "max_rel_err_vs_oracle_8_smallest": max(errs)}
+    small = sorted(range(len(systems)), key=lambda k: S.flops(systems[k].no, systems[k].nu))[:8]
+    ref = {k: sum(O.c_cc_triples(systems[k])[:2]) for k in small}
+    out = {"workload": "96 systems, no ~ U{3..12}, nu ~ U{24..140}, seed 100+s (normal)",
+           "tuples": int(sum(A.N.load().ccT_num_tuples(s.no) for s in systems)), "flops": flops}
+    # FP64: per-system loop, grouped launches (the default executor), persistent kernel
+    lm, lres = loop("fp64")
+    bm, ets, etd, items, _, _ = batched("fp64")
+    pm_, ets0, etd0, _, _, _ = batched("fp64", (0, 64, 0, 256 << 20))
+    out["fp64"] = {
+        "per_system_loop_ms": lm, "grouped_ms": bm, "grouped_tflops": flops / bm / 1e9,
+        "speedup_grouped_over_loop": lm / bm, "persistent_queue_kernel_ms": pm_,
+        "persistent_over_grouped": pm_ / bm, "work_items": items,
+        "bitwise_equal_to_loop": all(ets[k] == lres[k][0] and etd[k] == lres[k][1] for k in range(len(systems))),
+        "persistent_bitwise_equal": all(ets0[k] == lres[k][0] and etd0[k] == lres[k][1]
+                                        for k in range(len(systems))),
+        "max_abs_err_eh_vs_oracle_8_smallest": max(abs(ets[k] + etd[k] - ref[k]) for k in small)}
+    # emulated: per-system loop of calibrated plans, the emulated executor, the tuner's pick
+    elm, elres = loop("int8")
+    em, eets, eetd, _, _, digits = batched("int8")
+    tm, tets, tetd, _, chosen, _ = batched("int8", tune=True)
+    out["int8"] = {
+        "per_system_loop_ms": elm, "emulated_executor_ms": em, "emulated_executor_tflops": flops / em / 1e9,
+        "speedup_over_emulated_loop": elm / em, "speedup_over_fp64_grouped": bm / em,
+        "speedup_over_fp64_loop": lm / em,
+        "bitwise_equal_to_emulated_loop": all(eets[k] == elres[k][0] and eetd[k] == elres[k][1]
+                                              for k in range(len(systems))),
+        "digits_histogram": {d: digits.count(d) for d in sorted(set(digits))} if digits else None,
+        "max_abs_err_eh_vs_oracle_8_smallest": max(abs(eets[k] + eetd[k] - ref[k]) for k in small),
+        "tuned": {"mode": chosen[0], "bn": chosen[1], "order": chosen[2], "tune_ms": chosen[3], "ms": tm,
+                  "max_abs_err_eh_vs_oracle_8_smallest": max(abs(tets[k] + tetd[k] - ref[k]) for k in small)}}
+    return out
 
 
 def make_plan(A, no, nu, device, form):

@@ -168,9 +168,14 @@ int ccT_tuple_w(ccT_plan *plan, int64_t tuple, double *w, int32_t mem);
  * of every system is cut into work items (W-build tiles, reduction blocks) that
  * run either in one persistent kernel fed by a device-side work queue (mode 0)
  * or as grouped launches per tuple group on two streams (mode 1); either is
- * captured in a CUDA graph, and ccT_batch_tune picks the faster.  FP64 form.
- * No reference counterpart (the reference runs one system per triples.x
- * process); per system the results equal a single-system plan's bitwise. */
+ * captured in a CUDA graph, and ccT_batch_tune picks the faster.  A batch
+ * created with opt->precision = CCT_PREC_INT8_EMU also has mode 2 (its
+ * default): mode 1 with the emulated W build, each system's digit count
+ * calibrated to opt->emu_tol / emu_tol_rel as an emulated plan's (or fixed by
+ * opt->emu_slices), and the tuner times all three executors.  No reference
+ * counterpart (the reference runs one system per triples.x process); per
+ * system the results equal a single-system plan's (of the same precision and
+ * digit options) bitwise. */
 typedef struct ccT_batch ccT_batch;
 
 int ccT_batch_create(ccT_batch **batch, int64_t nsys, const int64_t *no, const int64_t *nu,
@@ -185,8 +190,10 @@ int ccT_batch_forward(ccT_batch *batch, double *ets, double *etd);
 int ccT_batch_v1(ccT_batch *batch, int64_t s, double *v1_out);
 /* Fix the schedule: executor mode (0: one persistent kernel taking every work
  * item from a device queue; 1: per tuple group, one launch of W-build tiles and
- * one of reduction blocks on two streams), W-build N tile bn (32, 48 or 64, or
- * 0 = the least-padding tile per system, mode 1 only),
+ * one of reduction blocks on two streams; 2: as 1 with one emulated W-build
+ * launch per system in the group, CCT_PREC_INT8_EMU batches only), W-build N
+ * tile bn (32, 48 or 64, or 0 = the least-padding tile per system, modes 1
+ * and 2; mode 2 takes 0 only),
  * tuple order (0: by cost, largest first; 1: system by system) and X scratch
  * bytes per tuple group. */
 int ccT_batch_configure(ccT_batch *batch, int32_t mode, int32_t bn, int32_t order, int64_t group_bytes);
@@ -207,6 +214,9 @@ int ccT_batch_debug_stall(ccT_batch *batch, int64_t tuple, int64_t spin_limit);
 double ccT_batch_last_ms(const ccT_batch *batch);
 /* Work items (W-build tiles + reduction blocks) in the current schedule. */
 int64_t ccT_batch_work_items(const ccT_batch *batch);
+/* Digit count of system s in the emulated executor (after its schedule was
+ * built: a mode 2 forward or tune).  CCT_ERR_STATE before. */
+int ccT_batch_emu_digits(const ccT_batch *batch, int64_t s, int32_t *digits);
 int ccT_batch_destroy(ccT_batch *batch);
 
 /* Launch the plan's kernels on a caller-provided CUDA stream (a cudaStream_t

@@ -11,7 +11,11 @@
 Every tuple of every system is a set of work items (W-build tiles, reduction
 blocks) taken from one device-side queue by a persistent kernel, replayed
 from a CUDA graph; per system the energies equal a single-system
-``TriplesPlan`` bitwise.
+``TriplesPlan`` bitwise.  ``TriplesBatch(shapes, form="int8")`` adds the
+emulated executor (mode 2, its default): each system's digit count is
+calibrated to the error target of the form ('int8': 1e-8 Eh, 'int8@R': R
+|E(T)|, 'int8:S': S digits), and per system the energies equal
+``TriplesPlan.for_form(no, nu, form)`` bitwise.
 """
 from __future__ import annotations
 
@@ -24,7 +28,8 @@ from .api import _host, input_sizes
 
 
 class TriplesBatch:
-    def __init__(self, shapes, device: int = 0):
+    def __init__(self, shapes, device: int = 0, form: str = "fp64"):
+        from .api import parse_form
         lib = N.load()
         self.shapes = [(int(no), int(nu)) for no, nu in shapes]
         n = len(self.shapes)
@@ -33,6 +38,12 @@ class TriplesBatch:
         opt = N.Options()
         lib.ccT_options_default(ctypes.byref(opt))
         opt.device = device
+        kw = parse_form(form)
+        self.emulated = kw["precision"] == "int8"
+        opt.precision = N.CCT_PREC_INT8_EMU if self.emulated else N.CCT_PREC_FP64
+        opt.emu_slices = kw.get("emu_slices", 0)
+        if kw.get("emu_tol_rel"):
+            opt.emu_tol_rel = kw["emu_tol_rel"]
         h = ctypes.c_void_p()
         N.check(lib.ccT_batch_create(ctypes.byref(h), n, no, nu, ctypes.byref(opt)), "ccT_batch_create")
         self._h = h
@@ -84,8 +95,9 @@ class TriplesBatch:
 
     def configure(self, mode: int = 1, bn: int = 0, order: int = 0, group_bytes: int = 256 << 20):
         """mode 0: one persistent kernel over a device work queue; mode 1: grouped
-        launches (W-build tiles / reduction blocks per tuple group, two streams).
-        bn: W-build N tile, 0 = per system (mode 1 only)."""
+        launches (W-build tiles / reduction blocks per tuple group, two streams);
+        mode 2: grouped, with one emulated W-build launch per system and group
+        (emulated batches).  bn: W-build N tile, 0 = per system (modes 1, 2)."""
         N.check(N.load().ccT_batch_configure(self._h, mode, bn, order, group_bytes), "ccT_batch_configure")
 
     def debug_stall(self, tuple_pos: int = 0, spin_limit: int = 0):
@@ -108,6 +120,12 @@ class TriplesBatch:
     @property
     def work_items(self) -> int:
         return int(N.load().ccT_batch_work_items(self._h))
+
+    def emu_digits(self, s: int) -> int:
+        """Digit count of system s in the emulated executor (``ccT_batch_emu_digits``)."""
+        d = ctypes.c_int32()
+        N.check(N.load().ccT_batch_emu_digits(self._h, s, ctypes.byref(d)), "ccT_batch_emu_digits")
+        return d.value
 
 
 def main(argv=None) -> int:

@@ -36,6 +36,16 @@
 // launches) is captured once in a CUDA graph and replayed.  The executor, the
 // W-build N tile (BN) and the tuple order are chosen by ccT_batch_tune, which
 // times every candidate on the loaded batch.
+//
+// A third executor (mode 2, batches created with CCT_PREC_INT8_EMU) is the
+// grouped one with the split-integer W build (cct_emu.cu): each system gets an
+// emulated single-system plan whose set_inputs calibrates the system's digit
+// count to the batch's error target and builds its digit operands; per tuple
+// group, one persistent emulated W-build launch per system covers all of that
+// system's tuples in the group, and the reduction launches are mode 1's.  Per
+// system the energies equal the emulated plan's own forward bitwise.  The
+// tuner of an emulated batch times all three executors (each meets the
+// target); an FP64 batch never runs the emulated one.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -339,6 +349,7 @@ struct BatchSystemHost {
   double *eh = nullptr, *ep = nullptr, *t1 = nullptr, *t2 = nullptr, *vm = nullptr, *voe = nullptr,
          *vvvo = nullptr, *E = nullptr, *F = nullptr, *v1 = nullptr;
   int16_t *cta_table = nullptr;
+  int64_t f_np = 0;  // the N padding F was built for
   bool ready = false;
 };
 
@@ -349,7 +360,15 @@ struct ccT_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int bn = 0;                             // W-build N tile; 0 = per system
   int order = 0;                          // 0: tuples by cost, largest first; 1: system by system
-  int mode = 1;                           // 0: one persistent kernel; 1: grouped launches per tuple group
+  int mode = 1;                           // 0: one persistent kernel; 1: grouped launches; 2: grouped, emulated
+  ccT_options opt{};                      // creation options (precision, digit target)
+  std::vector<ccT_plan *> emu_plans;      // mode 2: per system, the emulated plan (digit operands, digit count)
+  struct EmuLaunch {
+    int sys;
+    int64_t off, njobs;
+  };
+  std::vector<std::vector<EmuLaunch>> grp_emu;  // mode 2, per group: one W-build launch per system
+  EmuJob *emu_jobs = nullptr;
   cudaStream_t stream2 = nullptr;         // reduction launches of the grouped executor
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_wb[kRing] = {}, ev_ring[kRing] = {};
   struct WbRange {
@@ -389,8 +408,9 @@ void free_schedule(ccT_batch *b) {
   b->graph = nullptr;
   for (void *q : {(void *)b->items, (void *)b->counters, (void *)b->group_rd_items, (void *)b->tuples,
                   (void *)b->jobs, (void *)b->sysdev, (void *)b->tuple_etd, (void *)b->tuple_v1, (void *)b->sys_out,
-                  (void *)b->scratch, (void *)b->tuple_v1_off, (void *)b->err})
+                  (void *)b->scratch, (void *)b->tuple_v1_off, (void *)b->err, (void *)b->emu_jobs})
     if (q) cudaFree(q);
+  b->emu_jobs = nullptr;
   b->items = nullptr;
   b->counters = nullptr;
   b->group_rd_items = nullptr;
@@ -416,8 +436,30 @@ Dims batch_dims(int no, int nu, int bn) {
   return d;
 }
 
+// Mode 2: an emulated plan per system on the batch's device copies of its
+// inputs.  Its set_inputs calibrates the digit count to the batch's target and
+// builds the digit operands; a forward of its first tuple configures the
+// W-build kernel instance it runs, outside any stream capture.
+int ensure_emu_plans(ccT_batch *b) {
+  b->emu_plans.resize(b->sys.size(), nullptr);
+  for (size_t s = 0; s < b->sys.size(); s++) {
+    if (b->emu_plans[s]) continue;
+    const BatchSystemHost &S = b->sys[s];
+    ccT_options o = b->opt;
+    o.precision = CCT_PREC_INT8_EMU;
+    o.device = b->device;
+    o.vvvo_mode = CCT_VVVO_EXPANDED;
+    CCT_TRY(ccT_plan_create(&b->emu_plans[s], S.no, S.nu, &o));
+    CCT_TRY(ccT_set_inputs(b->emu_plans[s], S.eh, S.ep, S.t1, S.t2, S.vm, S.voe, S.vvvo, CCT_MEM_DEVICE));
+    double ets = 0.0, etd = 0.0;
+    CCT_TRY(ccT_forward(b->emu_plans[s], 0, 1, &ets, &etd, nullptr));
+  }
+  return CCT_OK;
+}
+
 int build_schedule(ccT_batch *b) {
   free_schedule(b);
+  if (b->mode == 2) CCT_TRY(ensure_emu_plans(b));
   const int nsys = (int)b->sys.size();
   struct TH {
     int sys, kind, i, j, k, njobs, group;
@@ -428,15 +470,21 @@ int build_schedule(ccT_batch *b) {
   std::vector<TH> th;
   std::vector<int64_t> sys_begin(nsys), sys_count(nsys);
   // F depends on the N tile: rebuild every system's F for this bn
+  // (mode 2: the system's emulated plan's dimensions; its X row stride is the plan's)
   for (int s = 0; s < nsys; s++) {
     BatchSystemHost &S = b->sys[s];
+    if (b->mode == 2) {
+      S.d = plan_dims(b->emu_plans[s]);
+      continue;
+    }
     const Dims nd = batch_dims(S.no, S.nu, b->bn ? b->bn : choose_bn(S.nu));
-    if (S.F && nd.NP != S.d.NP) {
+    if (S.F && nd.NP != S.f_np) {
       cudaFree(S.F);
       S.F = nullptr;
     }
     S.d = nd;
     if (!S.F) CCT_TRY(dmalloc(&S.F, (size_t)S.no * S.no * nd.NP * nd.KP));
+    S.f_np = nd.NP;
     CCT_TRY(launch_build_f(nd, S.t2, S.vm, S.F, b->stream));
   }
   for (int s = 0; s < nsys; s++) {
@@ -460,7 +508,7 @@ int build_schedule(ccT_batch *b) {
       // the next tuple stays 16-byte aligned (the W-build stores double2)
       h.scratch = round_up(h.njobs * nu2 * d.NP * 8, 256);  // rounded: X buffers stay 16-byte aligned
       h.xpart_off = round_up(d.ncta + (int64_t)d.nb * kRB * 3 * npairs, 32);  // partial doubles (offset later)
-      h.wb_items = h.njobs * tiles_m * tiles_n;
+      h.wb_items = b->mode == 2 ? 0 : h.njobs * tiles_m * tiles_n;
       h.rd_items = (int)d.ncta;
       th.push_back(h);
     }
@@ -530,7 +578,9 @@ int build_schedule(ccT_batch *b) {
       return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), r.x[slot], 1, 0};
     };
     GemmJob *J = &jobs[(size_t)u * 3];
-    if (h.kind == kIJK) {
+    if (b->mode == 2) {
+      // the emulated executor builds digit-operand jobs below; the FP64 F is not built
+    } else if (h.kind == kIJK) {
       J[0] = G2(h.i, h.j, h.k, 0);
       J[1] = G2(h.i, h.k, h.j, 1);
       J[2] = G2(h.j, h.k, h.i, 2);
@@ -542,6 +592,50 @@ int build_schedule(ccT_batch *b) {
       J[0] = H1(h.i, h.i, h.k, 0);
       J[1] = G2(h.i, h.k, h.i, 1);
       J[2] = J[1];
+    }
+  }
+  // mode 2: per group and system, the split-integer jobs of the system's
+  // tuples in the group (the FP64 jobs above, as digit-operand indices)
+  std::vector<EmuJob> ejobs;
+  b->grp_emu.assign(G, {});
+  if (b->mode == 2) {
+    for (int g = 0; g < G; g++) {
+      std::vector<std::pair<int, std::vector<int>>> by_sys;  // systems in order of first appearance
+      for (int u : groups[g]) {
+        auto it = std::find_if(by_sys.begin(), by_sys.end(), [&](const auto &e) { return e.first == th[u].sys; });
+        if (it == by_sys.end()) {
+          by_sys.push_back({th[u].sys, {}});
+          it = by_sys.end() - 1;
+        }
+        it->second.push_back(u);
+      }
+      for (const auto &e : by_sys) {
+        const int no = b->sys[e.first].no;
+        const int64_t off = (int64_t)ejobs.size();
+        for (int u : e.second) {
+          const TH &h = th[u];
+          const TupleRec &r = rec[u];
+          // G(x1,x2,x3): E[x1] F[x2][x3] + E[x2]^T F[x1][x3]; H: E[x1] F[x2][x3] alone
+          auto G2 = [&](int x1, int x2, int x3, int slot) {
+            return EmuJob{x1, x2, {x2 * no + x3, x1 * no + x3}, r.x[slot], 2, x3};
+          };
+          auto H1 = [&](int x1, int x2, int x3, int slot) {
+            return EmuJob{x1, x1, {x2 * no + x3, x2 * no + x3}, r.x[slot], 1, x3};
+          };
+          if (h.kind == kIJK) {
+            ejobs.push_back(G2(h.i, h.j, h.k, 0));
+            ejobs.push_back(G2(h.i, h.k, h.j, 1));
+            ejobs.push_back(G2(h.j, h.k, h.i, 2));
+          } else if (h.kind == kIJJ) {
+            ejobs.push_back(G2(h.i, h.j, h.j, 0));
+            ejobs.push_back(H1(h.j, h.j, h.i, 1));
+          } else {
+            ejobs.push_back(H1(h.i, h.i, h.k, 0));
+            ejobs.push_back(G2(h.i, h.k, h.i, 1));
+          }
+        }
+        b->grp_emu[g].push_back({e.first, off, (int64_t)ejobs.size() - off});
+      }
     }
   }
   // items: WB(g0) WB(g1) RD(g0) WB(g2) RD(g1) ...
@@ -576,7 +670,7 @@ int build_schedule(ccT_batch *b) {
     push_rd(G - 1);
   } else {
     for (int g = 0; g < G; g++) {
-      push_wb(g);
+      if (b->mode == 1) push_wb(g);  // mode 2: the emulated launches of grp_emu
       push_rd(g);
     }
   }
@@ -628,6 +722,10 @@ int build_schedule(ccT_batch *b) {
   CCT_CUDA(cudaMemcpy(b->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
   CCT_CUDA(cudaMemcpy(b->sysdev, sd.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice));
   CCT_CUDA(cudaMemcpy(b->tuple_v1_off, v1off.data(), T * sizeof(int64_t), cudaMemcpyHostToDevice));
+  if (!ejobs.empty()) {
+    CCT_TRY(dmalloc(&b->emu_jobs, ejobs.size()));
+    CCT_CUDA(cudaMemcpy(b->emu_jobs, ejobs.data(), ejobs.size() * sizeof(EmuJob), cudaMemcpyHostToDevice));
+  }
   CCT_CUDA(cudaStreamSynchronize(b->stream));
   b->scheduled = true;
   return CCT_OK;
@@ -686,6 +784,10 @@ int launch_grouped(ccT_batch *b) {
   for (int g = 0; g < b->ngroup; g++) {
     const int slot = g % kRing;
     if (g >= kRing) CCT_CUDA(cudaStreamWaitEvent(b->stream, b->ev_ring[slot], 0));
+    for (const ccT_batch::EmuLaunch &L : b->grp_emu[g]) {  // mode 2: one emulated launch per system
+      const ccT_plan *P = b->emu_plans[L.sys];
+      CCT_TRY(launch_wbuild_emu(plan_emu(P), plan_dims(P), b->emu_jobs + L.off, (int)L.njobs, b->err, b->stream));
+    }
     for (const ccT_batch::WbRange &r : b->grp_wb[g]) {
       switch (r.bn) {
         case 64: CCT_TRY(launch_wb_range<64>(a, r.begin, r.count, b->stream)); break;
@@ -712,7 +814,7 @@ int launch_grouped(ccT_batch *b) {
 }
 
 int enqueue_forward(ccT_batch *b) {
-  if (b->mode == 1) {
+  if (b->mode == 1 || b->mode == 2) {
     return launch_grouped(b);
   } else {
     switch (b->bn) {
@@ -802,9 +904,16 @@ int ccT_batch_create(ccT_batch **out, int64_t nsys, const int64_t *no, const int
   ccT_options o;
   ccT_options_default(&o);
   if (opt) o = *opt;
-  if (o.precision != CCT_PREC_FP64) {
-    set_error("the batch runs the FP64 form only");
-    return CCT_ERR_UNSUPPORTED;
+  if (o.precision != CCT_PREC_FP64 && o.precision != CCT_PREC_INT8_EMU) {
+    set_error("precision must be CCT_PREC_FP64 or CCT_PREC_INT8_EMU");
+    return CCT_ERR_INVALID;
+  }
+  if (o.precision == CCT_PREC_INT8_EMU &&
+      (o.emu_slices < 0 || (o.emu_slices > 0 && (o.emu_slices < kEmuMinSlices || o.emu_slices > kEmuMaxSlices)) ||
+       !(o.emu_tol >= 0.0) || !(o.emu_tol_rel >= 0.0))) {
+    set_error("emu_slices must be 0 (calibrated) or " + std::to_string(kEmuMinSlices) + ".." +
+              std::to_string(kEmuMaxSlices) + ", emu_tol and emu_tol_rel >= 0");
+    return CCT_ERR_INVALID;
   }
   int ndev = 0;
   CCT_CUDA(cudaGetDeviceCount(&ndev));
@@ -820,6 +929,8 @@ int ccT_batch_create(ccT_batch **out, int64_t nsys, const int64_t *no, const int
   Guard guard(o.device);
   ccT_batch *b = new ccT_batch();
   b->device = o.device;
+  b->opt = o;
+  b->mode = o.precision == CCT_PREC_INT8_EMU ? 2 : 1;
   auto fail = [&](int st) {
     ccT_batch_destroy(b);
     return st;
@@ -888,6 +999,11 @@ int ccT_batch_set_inputs(ccT_batch *b, int64_t s, const double *eh, const double
   Guard guard(b->device);
   BatchSystemHost &S = b->sys[s];
   const int64_t n = S.no, v = S.nu, v2 = v * v;
+  if (s < (int64_t)b->emu_plans.size() && b->emu_plans[s]) {  // new inputs: a new calibration
+    free_schedule(b);
+    ccT_plan_destroy(b->emu_plans[s]);
+    b->emu_plans[s] = nullptr;
+  }
   const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   // device inputs may still be being written on any stream (as ccT_set_inputs)
   if (mem == CCT_MEM_DEVICE) CCT_CUDA(cudaDeviceSynchronize());
@@ -898,9 +1014,9 @@ int ccT_batch_set_inputs(ccT_batch *b, int64_t s, const double *eh, const double
   CCT_CUDA(cudaMemcpyAsync(S.vm, vm, n * v * n * n * 8, kind, b->stream));
   CCT_CUDA(cudaMemcpyAsync(S.voe, voe, v2 * n * n * 8, kind, b->stream));
   CCT_CUDA(cudaMemcpyAsync(S.vvvo, vvvo_packed, v * (v + 1) / 2 * v * n * 8, kind, b->stream));
-  CCT_TRY(launch_build_e(S.d, S.vvvo, S.t2, S.E, 0, S.no, b->stream));
-  if (S.F) CCT_TRY(launch_build_f(S.d, S.t2, S.vm, S.F, b->stream));
+  CCT_TRY(launch_build_e(S.d, S.vvvo, S.t2, S.E, 0, S.no, b->stream));  // E depends on KP alone
   CCT_CUDA(cudaStreamSynchronize(b->stream));
+  free_schedule(b);  // the next forward rebuilds F (for its N tile) and the graph
   S.ready = true;
   return CCT_OK;
 }
@@ -954,10 +1070,14 @@ int ccT_batch_configure(ccT_batch *b, int32_t mode, int32_t bn, int32_t order, i
   }
   bool ok_bn = false;
   for (int c : kBatchBN) ok_bn |= c == bn;
-  if (!ok_bn || (order != 0 && order != 1) || (mode != 0 && mode != 1) || group_bytes < (1 << 20) ||
-      (mode == 0 && bn == 0)) {
-    set_error("mode must be 0 or 1, bn 0 (per system, mode 1 only), 32, 48 or 64, order 0 or 1, "
-              "group_bytes >= 1 MiB");
+  if (!ok_bn || (order != 0 && order != 1) || mode < 0 || mode > 2 || group_bytes < (1 << 20) ||
+      (mode == 0 && bn == 0) || (mode == 2 && bn != 0)) {
+    set_error("mode must be 0, 1 or 2, bn 0 (per system; modes 1 and 2), 32, 48 or 64 (modes 0 and 1), "
+              "order 0 or 1, group_bytes >= 1 MiB");
+    return CCT_ERR_INVALID;
+  }
+  if (mode == 2 && b->opt.precision != CCT_PREC_INT8_EMU) {
+    set_error("mode 2 (emulated W build) needs a batch created with CCT_PREC_INT8_EMU");
     return CCT_ERR_INVALID;
   }
   Guard guard(b->device);
@@ -978,10 +1098,12 @@ int ccT_batch_tune(ccT_batch *b, int32_t *best_mode, int32_t *best_bn, int32_t *
   Guard guard(b->device);
   double best = INFINITY;
   int bbn = b->bn, bord = b->order, bmode = b->mode;
-  for (int mode : {0, 1})
+  const int last_mode = b->opt.precision == CCT_PREC_INT8_EMU ? 2 : 1;
+  for (int mode = 0; mode <= last_mode; mode++)
   for (int bn : kBatchBN)
     for (int order : {0, 1}) {
       if (mode == 0 && bn == 0) continue;  // the persistent kernel has one N tile
+      if (mode == 2 && bn != 0) continue;  // the emulated plans keep their own N tiles
       b->mode = mode;
       b->bn = bn;
       b->order = order;
@@ -1037,12 +1159,26 @@ int ccT_batch_debug_stall(ccT_batch *b, int64_t tuple, int64_t spin_limit) {
 
 int64_t ccT_batch_work_items(const ccT_batch *b) { return b ? b->nitems : 0; }
 
+int ccT_batch_emu_digits(const ccT_batch *b, int64_t s, int32_t *digits) {
+  if (!b || s < 0 || s >= (int64_t)b->sys.size() || !digits) {
+    set_error("need a batch, a system index in range and an output pointer");
+    return CCT_ERR_INVALID;
+  }
+  if (s >= (int64_t)b->emu_plans.size() || !b->emu_plans[s]) {
+    set_error("system " + std::to_string(s) + " has no emulated plan (mode 2 schedule not built)");
+    return CCT_ERR_STATE;
+  }
+  return ccT_emu_digits(b->emu_plans[s], digits, nullptr, nullptr);
+}
+
 int ccT_batch_destroy(ccT_batch *b) {
   if (!b) return CCT_OK;
   Guard guard(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->stream2) cudaStreamSynchronize(b->stream2);
   free_schedule(b);
+  for (ccT_plan *p : b->emu_plans)
+    if (p) ccT_plan_destroy(p);
   for (BatchSystemHost &S : b->sys)
     for (void *q : {(void *)S.eh, (void *)S.ep, (void *)S.t1, (void *)S.t2, (void *)S.vm, (void *)S.voe,
                     (void *)S.vvvo, (void *)S.E, (void *)S.F, (void *)S.v1, (void *)S.cta_table})

@@ -231,6 +231,11 @@ int adj_finish(const Dims &d, const double *v1, AdjBuffers *b, cudaStream_t s);
 // into wf in the reference's layout (a fastest).  Needs adj_configure.
 int assemble_w_fortran(const Dims &d, const Tuple &t, double *const X[3], double *wc, double *wf, cudaStream_t s);
 
+// cct_plan.cu: the dimensions and split-integer operands of an emulated plan,
+// for the batched executor that runs many plans' W builds in grouped launches
+const Dims &plan_dims(const ccT_plan *p);
+const EmuOperands &plan_emu(const ccT_plan *p);
+
 // peak.cu
 double measure_fp64_peak(int device);
 double measure_int8_peak(int device);

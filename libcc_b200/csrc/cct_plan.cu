@@ -410,6 +410,11 @@ int rebuild_for_count(ccT_plan *p) {
 
 }  // namespace
 
+namespace cct {
+const Dims &plan_dims(const ccT_plan *p) { return p->d; }
+const EmuOperands &plan_emu(const ccT_plan *p) { return p->emu; }
+}  // namespace cct
+
 extern "C" {
 
 void ccT_options_default(ccT_options *opt) {

@@ -103,3 +103,58 @@ def test_bounded_wait_runs_out_and_context_survives(systems, single):
         ets, etd = b.forward()
         for k in range(len(systems)):
             assert ets[k] == single[k][0] and etd[k] == single[k][1]
+
+
+@pytest.fixture(scope="module")
+def single_emulated(systems):
+    from libcc_b200 import api as A
+    out = []
+    for inp in systems:
+        with A.TriplesPlan.for_form(inp.no, inp.nu, "int8") as p:
+            p.set_system(inp)
+            ets, etd, _ = p.forward()
+            out.append((ets, etd, p.emu_digits()["digits"]))
+    return out
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_emulated_batch_equals_emulated_plans_bitwise(systems, single_emulated, order):
+    """Mode 2 (one emulated W-build launch per system and tuple group; 1 MiB
+    groups, so the X ring is reused): per system the calibrated digit count and
+    the energies of a single emulated plan with the same options, bitwise."""
+    from libcc_b200 import batch as B
+    with B.TriplesBatch([(s.no, s.nu) for s in systems], form="int8") as b:
+        for k, s in enumerate(systems):
+            b.set_system(k, s)
+        b.configure(2, 0, order, 1 << 20)
+        for _ in range(2):  # the second call replays the CUDA graph
+            ets, etd = b.forward()
+            for k in range(len(systems)):
+                assert b.emu_digits(k) == single_emulated[k][2]
+                assert ets[k] == single_emulated[k][0] and etd[k] == single_emulated[k][1], (order, k)
+
+
+def test_emulated_batch_meets_target_and_tunes(systems):
+    """The emulated batch's energies are within the 1e-8 Eh target of the FP64
+    oracle for every system, and its tuner chooses among all three executors."""
+    from libcc_b200 import batch as B
+    from oracle import oracle as O
+    with B.TriplesBatch([(s.no, s.nu) for s in systems], form="int8") as b:
+        for k, s in enumerate(systems):
+            b.set_system(k, s)
+        ets, etd = b.forward()
+        for k, inp in enumerate(systems):
+            ets_o, etd_o, _ = O.c_cc_triples(inp)
+            assert abs((ets[k] + etd[k]) - (ets_o + etd_o)) <= 1e-8, k
+        mode, bn, order, ms = b.tune()
+        assert mode in (0, 1, 2) and ms > 0
+        ets2, etd2 = b.forward()
+        for k in range(len(systems)):
+            assert abs((ets2[k] + etd2[k]) - (ets[k] + etd[k])) <= 2e-8
+
+
+def test_emulated_mode_needs_an_emulated_batch(systems):
+    from libcc_b200 import _native as N
+    with _batch(systems) as b:
+        with pytest.raises(N.CctError):
+            b.configure(2, 0, 0, 1 << 20)
