@@ -5,15 +5,26 @@
 // here with T1 (O1) and T2 (O2) into CCSD residual intermediates.
 //
 // terms_29_30_31, per occupied j, as the reference's DGEMM / TRANMD / INSITU
-// sequence composes (see oracle/oracle.py for the literal sequence):
+// sequence composes (the oracle restates the literal sequence):
 //   T2(i,y,z,j) += sum_x O1(i,x) G_j(x,y,z),
-//   G_j(x,y,z) = (z x|y j) - sum_k O1(k,z) VL(k,x,y,j) - sum_k O1(k,y) VR(z,k,x,j)
-// (f4_g_kernel, then f4_o1_kernel: K = nu, bound by its nu^3 reads).
+//   G_j(x,y,z) = (z x|y j) - sum_k O1(k,z) VL(k,x,y,j) - sum_k O1(k,y) VR(z,k,x,j).
+// The O1 contraction is moved inside the two correction terms, so no nu^3 G_j
+// is formed:
+//   T2(i,y,z,j) += X_j(y,z,i) - sum_k O1(k,z) P_j(i,k,y) - sum_k O1(k,y) Q_j(i,z,k),
+//   X_j(p,q,i) = sum_x (x q|p j) O1(i,x),   P_j(i,k,y) = sum_x O1(i,x) VL(k,x,y,j),
+//   Q_j(i,z,k) = sum_x O1(i,x) VR(z,k,x,j).
+// X_j for all j is one launch of the FP64 W-build tile with its row operand
+// gathered from the packed triangle (the packed-VVVO path: row (p,q) of
+// occupied j at k is (k q|p j)) against O1 as the column operand: 2 no^2 nu^3
+// flops on the tensor pipe instead of 6 no^2 nu^3 on the FP64 units, and the
+// packed slices read once instead of an expanded nu^3 slice written and read
+// per j.  P and Q (no^2 nu per j) and the combination are small kernels.
 //
 // terms_32_33_34_35:
 //   t2 <- t2^T as an (nou x nou) matrix                            (TRANSQ)
 //   o2(x,y,k,l) <- o2(k,x,y,l)                                     (INSITU 12, 23)
-//   RL_pre(i,y,z,j) = sum_x O1(i,x) (x y|z j);  rl <- RL_pre^T     (DGEMM, TRANSQ)
+//   RL_pre(i,y,z,j) = sum_x O1(i,x) (x y|z j) = X_j(z,y,i);  rl <- RL_pre^T
+//                                                                  (DGEMM, TRANSQ)
 //   vm(x,y,z,a) <- vm(y,x,z,a) + T((x,z), (a,y)),                  (TRANMD 312, update, TRANMD 23)
 //   T((k,l), (a,j)) = sum_{x,y} o2(k,x,y,l) (a y|x j)
 // T is one GEMM of M = no^2, N = nu no, K = nu^2 for all j at once: the FP64
@@ -36,36 +47,59 @@ int grid_of(int64_t n) {
   return (int)(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
 }
 
-// G_j(x,y,z) for terms 29-31 (or, with vl == vr == nullptr and swap set, the
-// plain slice (x y|z j) for terms 32-35), Fortran (x fastest)
-__global__ void f4_g_kernel(int no, int nu, int j, const double *__restrict__ o1, const double *__restrict__ vl,
-                            const double *__restrict__ vr, const double *__restrict__ vvvo, int plain,
-                            double *__restrict__ g) {
-  const int64_t nu3 = (int64_t)nu * nu * nu, nutr = (int64_t)nu * (nu + 1) / 2;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu3; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t x = e % nu, y = (e / nu) % nu, z = e / ((int64_t)nu * nu);
-    if (plain) {  // (x y|z j): column j*nu + z, triangle (x, y)
-      g[e] = vvvo[((int64_t)j * nu + z) * nutr + tri_at(x, y)];
-      continue;
-    }
-    double v = vvvo[((int64_t)j * nu + y) * nutr + tri_at(z, x)];  // (z x|y j)
-    const double *vlc = vl + (int64_t)no * (x + (int64_t)nu * (y + (int64_t)nu * j));
-    const double *vrc = vr + z + (int64_t)nu * (int64_t)no * (x + (int64_t)nu * j);
-    for (int k = 0; k < no; k++) v -= o1[k + (int64_t)no * z] * vlc[k] + o1[k + (int64_t)no * y] * vrc[(int64_t)nu * k];
-    g[e] = v;
+// O1 as the W-build tile's column operand: o1pad[i][x] = O1(i,x), rows of kp
+// doubles, zero past (no, nu)
+__global__ void f4_o1pad_kernel(int no, int nu, int64_t kp, int64_t np, const double *__restrict__ o1,
+                                double *__restrict__ o1pad) {
+  const int64_t n = np * kp;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e / kp, x = e - i * kp;
+    o1pad[e] = (i < no && x < nu) ? o1[i + (int64_t)no * x] : 0.0;
   }
 }
 
-// out(i, y, z) (+)= sum_x O1(i,x) g(x,y,z) for one j slab of an (no,nu,nu) array
-__global__ void f4_o1_kernel(int no, int nu, const double *__restrict__ o1, const double *__restrict__ g,
-                             double *__restrict__ out, int accumulate) {
-  const int64_t n = (int64_t)no * nu * nu;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e % no, yz = e / no;
-    const double *gc = g + yz * nu;
+// P[j][y][k][i] = sum_x O1(i,x) VL(k,x,y,j) and Q[j][z][k][i] = sum_x O1(i,x) VR(z,k,x,j)
+__global__ void f4_pq_kernel(int no, int nu, const double *__restrict__ o1, const double *__restrict__ vl,
+                             const double *__restrict__ vr, double *__restrict__ P, double *__restrict__ Q) {
+  const int64_t n = (int64_t)no * no * nu * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 2 * n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int which = e >= n;
+    const int64_t r = e - which * n;
+    const int64_t i = r % no, k = (r / no) % no, y = (r / ((int64_t)no * no)) % nu, j = r / ((int64_t)no * no * nu);
     double s = 0.0;
-    for (int x = 0; x < nu; x++) s += o1[i + (int64_t)no * x] * gc[x];
-    out[e] = accumulate ? out[e] + s : s;
+    if (!which) {
+      const double *v = vl + k + (int64_t)no * (int64_t)nu * (y + (int64_t)nu * j);  // VL(k, x, y, j), x stride no
+      for (int x = 0; x < nu; x++) s += o1[i + (int64_t)no * x] * v[(int64_t)no * x];
+      P[r] = s;
+    } else {
+      const double *v = vr + y + (int64_t)nu * (k + (int64_t)no * (int64_t)nu * j);  // VR(z=y, k, x, j), x stride nu no
+      for (int x = 0; x < nu; x++) s += o1[i + (int64_t)no * x] * v[(int64_t)nu * no * x];
+      Q[r] = s;
+    }
+  }
+}
+
+// T2(i,y,z,j) += X_j(y,z,i) - sum_k O1(k,z) P[j][y][k][i] - sum_k O1(k,y) Q[j][z][k][i]
+__global__ void f4_t2_kernel(int no, int nu, int64_t np, const double *__restrict__ o1, const double *__restrict__ X,
+                             const double *__restrict__ P, const double *__restrict__ Q, double *__restrict__ t2) {
+  const int64_t nu2 = (int64_t)nu * nu, n = (int64_t)no * nu2 * no;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % no, y = (e / no) % nu, z = (e / ((int64_t)no * nu)) % nu, j = e / ((int64_t)no * nu2);
+    double v = X[(j * nu2 + y * nu + z) * np + i];
+    const double *pj = P + (j * nu + y) * no * no + i, *qj = Q + (j * nu + z) * no * no + i;
+    for (int k = 0; k < no; k++) v -= o1[k + (int64_t)no * z] * pj[(int64_t)k * no];
+    for (int k = 0; k < no; k++) v -= o1[k + (int64_t)no * y] * qj[(int64_t)k * no];
+    t2[e] += v;
+  }
+}
+
+// rl = RL_pre^T as (nou x nou) matrices: rl[(z + nu j) + nou (i + no y)] = X_j(z,y,i)
+// (written in order; the X reads are strided)
+__global__ void f4_rl_kernel(int no, int nu, int64_t np, const double *__restrict__ X, double *__restrict__ rl) {
+  const int64_t nu2 = (int64_t)nu * nu, nou = (int64_t)no * nu, n = nou * nou;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t zj = e % nou, iy = e / nou, z = zj % nu, j = zj / nu, i = iy % no, y = iy / no;
+    rl[e] = X[(j * nu2 + z * nu + y) * np + i];
   }
 }
 
@@ -134,6 +168,36 @@ struct DevBuf {  // device copies of host arrays (or the caller's device arrays)
   }
 };
 
+// X_j(p,q,i) = sum_x (x q|p j) O1(i,x) for every occupied j, X_j at x + j nu^2 np,
+// row (p,q) at (p nu + q) np: the W-build tile, one packed-row job per j.
+int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_vvvo, DevBuf &b, double **X,
+                   int64_t *np_out, cudaStream_t s) {
+  const int64_t nutr = nu * (nu + 1) / 2;
+  Dims g{};
+  g.nu = (int)nu;                  // M = nu^2 rows (p, q)
+  g.no = 0;                        // K = nu (the packed part of a row alone)
+  g.KP = round_up(nu, kKB);
+  g.BN = choose_bn((int)no);       // N = no
+  g.NP = round_up(no, g.BN);
+  double *o1pad;
+  CCT_TRY(b.tmp(&o1pad, g.NP * g.KP));
+  CCT_TRY(b.tmp(X, no * nu * nu * g.NP));
+  f4_o1pad_kernel<<<grid_of(g.NP * g.KP), 256, 0, s>>>((int)no, (int)nu, g.KP, g.NP, d_o1, o1pad);
+  CCT_CUDA(cudaGetLastError());
+  std::vector<GemmJob> jobs((size_t)no);
+  for (int64_t j = 0; j < no; j++) {
+    const double *pj = d_vvvo + j * nu * nutr;  // the nu packed columns of occupied j
+    jobs[j] = GemmJob{pj, pj, o1pad, o1pad, *X + j * nu * nu * g.NP, 1, 1, pj, pj};
+  }
+  GemmJob *d_jobs;
+  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
+  b.owned.push_back(d_jobs);
+  CCT_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
+  CCT_TRY(launch_wbuild_f64(g, d_jobs, (int)no, s));
+  *np_out = g.NP;
+  return CCT_OK;
+}
+
 int check_args(int64_t no, int64_t nu, int32_t mem) {
   if (no < 1 || nu < 1 || no > 4096 || nu > 4096 || (mem != CCT_MEM_HOST && mem != CCT_MEM_DEVICE)) {
     set_error("need 1 <= no, nu <= 4096 and mem CCT_MEM_HOST or CCT_MEM_DEVICE");
@@ -157,19 +221,21 @@ extern "C" int ccT_ccsd_terms_29_31(int64_t no, int64_t nu, const double *o1, do
   const cudaStream_t s = nullptr;
   const int64_t nu2 = nu * nu, nutr = nu * (nu + 1) / 2;
   DevBuf b;
-  double *d_o1, *d_t2, *d_vl, *d_vr, *d_vvvo, *g;
+  double *d_o1, *d_t2, *d_vl, *d_vr, *d_vvvo;
   CCT_TRY(b.get(&d_o1, o1, no * nu, mem, true, s));
   CCT_TRY(b.get(&d_t2, t2, no * nu2 * no, mem, true, s));
   CCT_TRY(b.get(&d_vl, vl, no * nu2 * no, mem, true, s));
   CCT_TRY(b.get(&d_vr, vr, nu * no * nu * no, mem, true, s));
   CCT_TRY(b.get(&d_vvvo, vvvo, nutr * nu * no, mem, true, s));
-  CCT_TRY(b.tmp(&g, nu2 * nu));
-  for (int j = 0; j < no; j++) {
-    f4_g_kernel<<<grid_of(nu2 * nu), 256, 0, s>>>((int)no, (int)nu, j, d_o1, d_vl, d_vr, d_vvvo, 0, g);
-    CCT_CUDA(cudaGetLastError());
-    f4_o1_kernel<<<grid_of(no * nu2), 256, 0, s>>>((int)no, (int)nu, d_o1, g, d_t2 + (int64_t)j * no * nu2, 1);
-    CCT_CUDA(cudaGetLastError());
-  }
+  double *X, *P, *Q;
+  int64_t np = 0;
+  CCT_TRY(packed_o1_gemm(no, nu, d_o1, d_vvvo, b, &X, &np, s));
+  CCT_TRY(b.tmp(&P, no * no * nu * no));
+  CCT_TRY(b.tmp(&Q, no * no * nu * no));
+  f4_pq_kernel<<<grid_of(2 * no * no * nu * no), 256, 0, s>>>((int)no, (int)nu, d_o1, d_vl, d_vr, P, Q);
+  CCT_CUDA(cudaGetLastError());
+  f4_t2_kernel<<<grid_of(no * nu2 * no), 256, 0, s>>>((int)no, (int)nu, np, d_o1, X, P, Q, d_t2);
+  CCT_CUDA(cudaGetLastError());
   if (mem == CCT_MEM_HOST) CCT_CUDA(cudaMemcpyAsync(t2, d_t2, (size_t)no * nu2 * no * 8, cudaMemcpyDeviceToHost, s));
   CCT_CUDA(cudaStreamSynchronize(s));
   return CCT_OK;
@@ -198,21 +264,18 @@ extern "C" int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, do
   CCT_TRY(b.get(&d_vvvo, vvvo, nutr * nu * no, mem, true, s));
   // TRANSQ(T2) (ccsd_acc.f:83)
   double *tmp;
-  CCT_TRY(b.tmp(&tmp, n4 > nu2 * nu ? n4 : nu2 * nu));
+  CCT_TRY(b.tmp(&tmp, n4));
   CCT_CUDA(cudaMemcpyAsync(tmp, d_t2, (size_t)n4 * 8, cudaMemcpyDeviceToDevice, s));
   f4_transq_kernel<<<grid_of(n4), 256, 0, s>>>(nou, tmp, d_t2);
   CCT_CUDA(cudaGetLastError());
-  // RL_pre(i,y,z,j) = sum_x O1(i,x) (x y|z j) (line 109), then TRANSQ into rl (line 151)
-  double *rlpre;
-  CCT_TRY(b.tmp(&rlpre, n4));
-  for (int j = 0; j < no; j++) {
-    f4_g_kernel<<<grid_of(nu2 * nu), 256, 0, s>>>((int)no, (int)nu, j, d_o1, nullptr, nullptr, d_vvvo, 1, tmp);
-    CCT_CUDA(cudaGetLastError());
-    f4_o1_kernel<<<grid_of(no * nu2), 256, 0, s>>>((int)no, (int)nu, d_o1, tmp, rlpre + (int64_t)j * no * nu2, 0);
+  // RL_pre(i,y,z,j) = sum_x O1(i,x) (x y|z j) = X_j(z,y,i) (line 109), then TRANSQ into rl (line 151)
+  {
+    double *X;
+    int64_t np = 0;
+    CCT_TRY(packed_o1_gemm(no, nu, d_o1, d_vvvo, b, &X, &np, s));
+    f4_rl_kernel<<<grid_of(n4), 256, 0, s>>>((int)no, (int)nu, np, X, d_rl);
     CCT_CUDA(cudaGetLastError());
   }
-  f4_transq_kernel<<<grid_of(n4), 256, 0, s>>>(nou, rlpre, d_rl);
-  CCT_CUDA(cudaGetLastError());
   // INSITU 12, 23 of O2 (lines 84-85) and the GEMM operands
   Dims g{};
   g.nu = (int)no;                        // M = no^2 rows (k + no l)
