@@ -57,6 +57,9 @@ __device__ __forceinline__ int64_t widx(int nu, int a, int b, int c) { return ((
 // extent and plane padded by one), then summed and written as 256-byte rows.
 constexpr int kWA = 8, kWB = 8, kWC = 32;
 constexpr int kWThreads = 256;
+#ifndef CCT_BWD_F_CTAS_PER_SM
+#define CCT_BWD_F_CTAS_PER_SM 3
+#endif
 constexpr int kWSlot = 2336;  // >= D0 * (D1 * (D2 + 1) + 1) for every order of (8, 8, 32)
 
 __host__ __device__ constexpr int wf_ext(int pos) { return pos == 2 ? kWC : (pos == 1 ? kWB : kWA); }
@@ -965,14 +968,14 @@ int adj_alloc(const Dims &d, AdjBuffers *b) {
     return CCT_OK;
   };
   {
-    // dF GEMM split-K: about one wave of 3 CTAs per SM for the 6 pairs of an
-    // i>j>k tuple, rounded to whole k-tiles
+    // dF GEMM split-K: about CCT_BWD_F_CTAS_PER_SM CTAs per SM for the 6 pairs
+    // of an i>j>k tuple, rounded to whole k-tiles
     int sms = 148, dev = 0;
     CCT_CUDA(cudaGetDevice(&dev));
     CCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int bn = bwd_bn(d.KP);
     const int64_t tiles = ((d.NP + BBM - 1) / BBM) * ((d.KP + bn - 1) / bn) * 6;
-    int64_t ns = (3 * (int64_t)sms) / tiles;
+    int64_t ns = (int64_t)(CCT_BWD_F_CTAS_PER_SM * sms) / tiles;
     ns = ns < 1 ? 1 : (ns > (nu2 + BBK - 1) / BBK ? (nu2 + BBK - 1) / BBK : ns);
     b->kchunk = round_up((nu2 + ns - 1) / ns, BBK);
     b->nsplit = (nu2 + b->kchunk - 1) / b->kchunk;
