@@ -136,7 +136,11 @@ def main(argv=None) -> int:
     from . import synthetic
     ap = argparse.ArgumentParser(prog="python -m libcc_b200.batch", description=main.__doc__)
     ap.add_argument("--systems", type=int, default=96, help="first N systems of the workload (default 96)")
-    ap.add_argument("--mode", type=int, default=1, help="0: one persistent kernel; 1: grouped launches")
+    ap.add_argument("--form", default="fp64",
+                    help="fp64, or int8 / int8@R / int8:S for the emulated W build (adds mode 2)")
+    ap.add_argument("--mode", type=int, default=None,
+                    help="0: one persistent kernel; 1: grouped launches; 2: grouped, emulated "
+                         "(default: 1 for fp64, 2 for int8 forms)")
     ap.add_argument("--bn", type=int, default=0, help="W-build N tile, 0 = per system")
     ap.add_argument("--order", type=int, default=0, help="0: tuples by cost; 1: system by system")
     ap.add_argument("--group-mib", type=int, default=256, help="X scratch per tuple group, MiB")
@@ -144,19 +148,25 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
     systems = synthetic.batch96(args.systems)
-    with TriplesBatch([(s.no, s.nu) for s in systems], device=args.device) as b:
+    with TriplesBatch([(s.no, s.nu) for s in systems], device=args.device, form=args.form) as b:
         for k, s in enumerate(systems):
             b.set_system(k, s)
         if args.tune:
             mode, bn, order, ms = b.tune()
             print(f"tuned: mode {mode} bn {bn} order {order} ({ms:.2f} ms)")
         else:
-            b.configure(args.mode, args.bn, args.order, args.group_mib << 20)
+            mode = args.mode if args.mode is not None else (2 if b.emulated else 1)
+            b.configure(mode, 0 if mode == 2 else args.bn, args.order, args.group_mib << 20)
         b.forward()
         ets, etd = b.forward()
         print(f"{len(systems)} systems, {b.work_items} work items, {b.last_ms:.2f} ms")
         for k, s in enumerate(systems):
-            print(f"  {s.name} no={s.no} nu={s.nu} ets={ets[k]:.10f} etd={etd[k]:.10f}")
+            dg = ""
+            try:
+                dg = f" digits={b.emu_digits(k)}" if b.emulated else ""
+            except N.CctError:  # the tuner chose an FP64 executor
+                pass
+            print(f"  {s.name} no={s.no} nu={s.nu} ets={ets[k]:.10f} etd={etd[k]:.10f}{dg}")
     return 0
 
 
