@@ -13,8 +13,10 @@
 //   D_d = sum_{halves} sum_{t+u=d} sum_k a_t b_u,
 // keeping digit products with t+u <= S+1 (the dropped tail is below
 // 2^(-7(S+1)) of |A||B| per term).  Each D_d is an exact int32 accumulation
-// (|D_d| <= 2 S K 64^2 < 2^31 for K <= 4096); FP64 enters only when the
-// diagonals are scaled and summed in the epilogue.  Rounded digits leave an
+// (|D_d| <= 2 S K 64^2 < 2^31 for K <= 4096).  The epilogue combines the
+// diagonals exactly in int64 (up to five of them) and enters FP64 with one
+// conversion and one power-of-two scaling per element; the sixth and
+// seventh diagonals of 6- and 7-digit launches are added in FP64.  Rounded digits leave an
 // unbiased remainder: truncated digits (remainder of the value's own sign)
 // shrink every product the same way, and that bias adds up over the K sum,
 // the a,b,c sum and the tuples into the energy.  On seeded systems the
@@ -59,8 +61,8 @@
 //               merged MMAs over the B slices 0..s-1-t into the s diagonal
 //               accumulators (N int32 columns each)
 //   warps 2..   drain (NDW warps): tcgen05.ld one diagonal at a time, sum in
-//               FP64, hand the tensor memory back to the issuer, then scale
-//               and store X in 32-byte stores.  When two accumulator sets fit
+//               int64, hand the tensor memory back to the issuer, then convert,
+//               scale and store X in 32-byte stores.  When two accumulator sets fit
 //               the tensor memory (2 S N <= 512) the issuer alternates between
 //               them, so the next item's MMAs run while the drain reads and
 //               stores the last one; with one set they wait for the read.
@@ -85,9 +87,6 @@ constexpr int A_BLK = kEmuABlk;
 #endif
 #ifndef CCT_EMU_MAXNREG
 #define CCT_EMU_MAXNREG 80
-#endif
-#ifndef CCT_EMU_DB
-#define CCT_EMU_DB 1
 #endif
 #ifndef CCT_EMU_SMEM_BUDGET
 #define CCT_EMU_SMEM_BUDGET (180 * 1024)
@@ -415,35 +414,45 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       // warp-uniform decision: the tcgen05.ld below are .sync.aligned
       if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[ab], use & 1, args.err, abort_flag))) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
-      double acc[CW];
+      // Up to five digits the diagonals are summed exactly in int64 by
+      // Horner's rule, acc = sum_d D_d 2^(7(sl-1-d)) (|D_d| < 2^31: below
+      // 2^60), and converted once; 6- and 7-digit launches, and the 96-column
+      // tile (whose int64 sums would spill at 80 registers), sum in FP64.
+      // acc holds the int64 sum, or the FP64 bits of the FP64 sum.
+      constexpr int H = S <= 5 && EBN <= 80 ? S : 0;
+      auto cvt = [](long long x) {
+        if constexpr (S <= 3) {  // |x| < 2^46: exact through the 2^52 + 2^51 bias
+          return __longlong_as_double(x + 0x4338000000000000LL) - 6755399441055744.0;
+        } else {
+          return __ll2double_rn(x);
+        }
+      };
+      long long acc[CW];
 #pragma unroll
       for (int c0 = 0; c0 < CW; c0 += 16) {
-        constexpr int DB = CCT_EMU_DB;  // diagonals per tcgen05.wait::ld
         const int w = CW - c0 >= 16 ? 16 : (CW - c0 >= 8 ? 8 : 4);  // chunk widths 16, then 8 or 4
 #pragma unroll
-        for (int d0 = 0; d0 < S; d0 += DB) {
+        for (int d0 = 0; d0 < S; d0++) {
           if (d0 >= sl) break;  // diagonals past the item's digit count were not written
-          uint32_t v[DB][16];
-#pragma unroll
-          for (int dd = 0; dd < DB; dd++) {
-            const uint32_t addr =
-                tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * S + d0 + dd) * EBN + cbase + c0);
-            if (w == 16)
-              tmem_ld16(addr, v[dd]);
-            else if (w == 8)
-              tmem_ld8(addr, v[dd]);
-            else
-              tmem_ld4(addr, v[dd]);
-          }
+          uint32_t v[16];
+          const uint32_t addr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * S + d0) * EBN + cbase + c0);
+          if (w == 16)
+            tmem_ld16(addr, v);
+          else if (w == 8)
+            tmem_ld8(addr, v);
+          else
+            tmem_ld4(addr, v);
           asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
           for (int j = 0; j < 16; j++) {
             if (j >= w) continue;
-            double a = d0 == 0 ? 0.0 : acc[c0 + j];
-#pragma unroll
-            for (int dd = 0; dd < DB; dd++)
-              if (d0 + dd < sl) a = fma((double)(int32_t)v[dd][j], cd[d0 + dd], a);
-            acc[c0 + j] = a;
+            const long long dv = (long long)(int32_t)v[j];
+            if constexpr (H > 0) {
+              acc[c0 + j] = d0 == 0 ? dv : (acc[c0 + j] << 7) + dv;
+            } else {
+              const double a = d0 == 0 ? 0.0 : __longlong_as_double(acc[c0 + j]);
+              acc[c0 + j] = __double_as_longlong(fma((double)dv, cd[d0], a));
+            }
           }
         }
       }
@@ -455,13 +464,14 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       if (live) {
         double *xrow = job.out + m * args.NP + n0;
         const int16_t *eB = args.expF + (int64_t)job.x3 * args.NPe + n0;
+        const int e0 = eA + (H > 0 ? 2 - 7 * (sl + 1) : 0);
+        auto val = [&](int j) { return (H > 0 ? cvt(acc[j]) : __longlong_as_double(acc[j])) * pow2(e0 + eB[j]); };
         // one 32-byte sector per store (a thread owns a row, so 16-byte
         // stores wrote half a sector each and doubled the write traffic)
 #pragma unroll
         for (int j = 0; j < CW; j += 4) {
           if (n0 + j >= args.NP) break;  // NP is a multiple of 4: a quad is stored whole or not at all
-          st_global_v4(xrow + j, acc[j] * pow2(eA + eB[j]), acc[j + 1] * pow2(eA + eB[j + 1]),
-                       acc[j + 2] * pow2(eA + eB[j + 2]), acc[j + 3] * pow2(eA + eB[j + 3]));
+          st_global_v4(xrow + j, val(j), val(j + 1), val(j + 2), val(j + 3));
         }
       }
     }

@@ -198,7 +198,11 @@ int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const doub
                cudaStream_t s);
 
 // adjoint.cu: device buffers of the backward pass (allocated at the first ccT_backward)
-constexpr int kGXSets = 4;  // backward: GX sets, two dE-GEMM tuple pairs in flight
+#ifndef CCT_GX_SETS
+#define CCT_GX_SETS 4
+#endif
+constexpr int kGXSets = CCT_GX_SETS;  // backward: GX sets (even: dE-GEMM tuple pairs in flight)
+static_assert(kGXSets >= 2 && kGXSets % 2 == 0, "the dE GEMM takes the GX sets of tuple pairs");
 struct AdjBuffers {
   bool ready = false;
   double *dE = nullptr, *dF = nullptr;                 // gradients of the GEMM operands E, F
