@@ -33,6 +33,7 @@
 // an offset of one element; this follows the evident intent, VM(k,l,j,a) +=
 // tmp((k,l),a).
 #include "cct_internal.cuh"
+#include "cct_wbuild_tile.cuh"
 
 namespace cct {
 namespace {
@@ -116,33 +117,40 @@ __global__ void f4_transq_kernel(int64_t n, const double *__restrict__ src, doub
 // GEMM's row operand apad[(k + no l)][x + nu y] with rows of kp doubles
 __global__ void f4_o2_kernel(int no, int nu, int64_t kp, const double *__restrict__ o2, double *__restrict__ o2b,
                              double *__restrict__ apad) {
-  const int64_t nu2 = (int64_t)nu * nu, n = nu2 * no * no;
+  const int64_t nu2 = (int64_t)nu * nu, n = nu2 * no * no, no2 = (int64_t)no * no;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t xy = e % nu2, kl = e / nu2;
     const int64_t x = xy % nu, y = xy / nu, k = kl % no, l = kl / no;
     const double v = o2[k + no * (x + nu * (y + nu * l))];
     o2b[e] = v;
-    apad[kl * kp + xy] = v;
+    const int64_t z = xy / kp;  // K split
+    apad[(z * no2 + kl) * kp + (xy - z * kp)] = v;
   }
 }
 
-// the GEMM's column operand: bpad[(a + nu j)][x + nu y] = (a y|x j)
-__global__ void f4_b_kernel(int no, int nu, int64_t kp, const double *__restrict__ vvvo, double *__restrict__ bpad) {
+// the GEMM's column operand: bpad[split][(a + nu j)][x + nu y] = (a y|x j), rows
+// of kp doubles per split (np rows per split)
+__global__ void f4_b_kernel(int no, int nu, int64_t kp, int64_t np, const double *__restrict__ vvvo,
+                            double *__restrict__ bpad) {
   const int64_t nu2 = (int64_t)nu * nu, n = nu2 * nu * no, nutr = (int64_t)nu * (nu + 1) / 2;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t xy = e % nu2, aj = e / nu2;
     const int64_t x = xy % nu, y = xy / nu, a = aj % nu, j = aj / nu;
-    bpad[aj * kp + xy] = vvvo[(j * nu + x) * nutr + tri_at(a, y)];
+    const int64_t z = xy / kp;
+    bpad[(z * np + aj) * kp + (xy - z * kp)] = vvvo[(j * nu + x) * nutr + tri_at(a, y)];
   }
 }
 
-// vm_out(x,y,z,a) = vm_in(y,x,z,a) + T[(x + no z) np + (a + nu y)]
-__global__ void f4_vm_kernel(int no, int nu, int64_t np, const double *__restrict__ vm_in, const double *__restrict__ t,
-                             double *__restrict__ vm_out) {
+// vm_out(x,y,z,a) = vm_in(y,x,z,a) + sum over the K splits of T[(x + no z) np + (a + nu y)]
+__global__ void f4_vm_kernel(int no, int nu, int64_t np, int nsplit, int64_t tsplit, const double *__restrict__ vm_in,
+                             const double *__restrict__ t, double *__restrict__ vm_out) {
   const int64_t n = (int64_t)no * no * no * nu;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t x = e % no, y = (e / no) % no, z = (e / ((int64_t)no * no)) % no, a = e / ((int64_t)no * no * no);
-    vm_out[e] = vm_in[y + no * (x + no * (z + no * a))] + t[(x + no * z) * np + (a + nu * y)];
+    const double *tz = t + (x + no * z) * np + (a + nu * y);
+    double v = tz[0];
+    for (int sp = 1; sp < nsplit; sp++) v += tz[sp * tsplit];
+    vm_out[e] = vm_in[y + no * (x + no * (z + no * a))] + v;
   }
 }
 
@@ -276,37 +284,62 @@ extern "C" int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, do
     f4_rl_kernel<<<grid_of(n4), 256, 0, s>>>((int)no, (int)nu, np, X, d_rl);
     CCT_CUDA(cudaGetLastError());
   }
-  // INSITU 12, 23 of O2 (lines 84-85) and the GEMM operands
+  // INSITU 12, 23 of O2 (lines 84-85) and the GEMM operands.  T has few
+  // output tiles (M = no^2) and a long contraction (K = nu^2), so K is split
+  // into nsplit ranges, each a job of its own (the operands stored split by
+  // split), for whole waves of CTAs; f4_vm_kernel sums the splits in order.
   Dims g{};
   g.nu = (int)no;                        // M = no^2 rows (k + no l)
-  g.KP = round_up(nu2, kKB);             // K = nu^2 (x + nu y), rows padded
-  g.no = (int)(nu2 - no);                // valid K = g.nu + g.no = nu^2
   g.BN = choose_bn(nou);
   g.NP = round_up(nou, g.BN);            // N = nu no (a + nu j)
+  int nsplit = 1;
+  {
+    int dev = 0, nsm = 148;
+    CCT_CUDA(cudaGetDevice(&dev));
+    CCT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t slots = 3 * (int64_t)nsm;  // W-build tile: three CTAs per SM
+    const int64_t tiles = ((int64_t)no * no + wb::BM - 1) / wb::BM * (g.NP / g.BN);
+    double best = 0.0;
+    for (int sp = 1; sp <= 16 && (int64_t)sp * kKB <= nu2; sp++) {
+      const int64_t ctas = tiles * sp, waves = (ctas + slots - 1) / slots;
+      const double fill = (double)ctas / (double)(waves * slots);
+      if (fill > best + 0.02) {
+        best = fill;
+        nsplit = sp;
+      }
+    }
+  }
+  g.KP = round_up((nu2 + nsplit - 1) / nsplit, kKB);  // K per split (x + nu y), zero past nu^2
+  g.no = (int)(g.KP - no);                            // every column of a split counts as valid
   double *o2in, *apad, *bpad, *t;
   CCT_TRY(b.tmp(&o2in, n4));
-  CCT_TRY(b.tmp(&apad, no * no * g.KP));
-  CCT_TRY(b.tmp(&bpad, g.NP * g.KP));
-  CCT_TRY(b.tmp(&t, no * no * g.NP));
+  CCT_TRY(b.tmp(&apad, nsplit * no * no * g.KP));
+  CCT_TRY(b.tmp(&bpad, nsplit * g.NP * g.KP));
+  CCT_TRY(b.tmp(&t, nsplit * no * no * g.NP));
   CCT_CUDA(cudaMemcpyAsync(o2in, d_o2, (size_t)n4 * 8, cudaMemcpyDeviceToDevice, s));
-  CCT_CUDA(cudaMemsetAsync(apad, 0, (size_t)no * no * g.KP * 8, s));
-  CCT_CUDA(cudaMemsetAsync(bpad, 0, (size_t)g.NP * g.KP * 8, s));
+  CCT_CUDA(cudaMemsetAsync(apad, 0, (size_t)nsplit * no * no * g.KP * 8, s));
+  CCT_CUDA(cudaMemsetAsync(bpad, 0, (size_t)nsplit * g.NP * g.KP * 8, s));
   f4_o2_kernel<<<grid_of(n4), 256, 0, s>>>((int)no, (int)nu, g.KP, o2in, d_o2, apad);
   CCT_CUDA(cudaGetLastError());
-  f4_b_kernel<<<grid_of(nu2 * nou), 256, 0, s>>>((int)no, (int)nu, g.KP, d_vvvo, bpad);
+  f4_b_kernel<<<grid_of(nu2 * nou), 256, 0, s>>>((int)no, (int)nu, g.KP, g.NP, d_vvvo, bpad);
   CCT_CUDA(cudaGetLastError());
   // T((k,l),(a,j)) = sum_{x,y} o2b(x,y,k,l) (a y|x j) (line 119 for every j) on the FP64 tensor cores
-  GemmJob job{apad, apad, bpad, bpad, t, 1, 0};
+  std::vector<GemmJob> jobs(nsplit);
+  for (int z = 0; z < nsplit; z++) {
+    const double *az = apad + (int64_t)z * no * no * g.KP, *bz = bpad + (int64_t)z * g.NP * g.KP;
+    jobs[z] = GemmJob{az, az, bz, bz, t + (int64_t)z * no * no * g.NP, 1, 0};
+  }
   GemmJob *d_job;
-  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_job), sizeof(GemmJob)));
+  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_job), nsplit * sizeof(GemmJob)));
   b.owned.push_back(d_job);
-  CCT_CUDA(cudaMemcpyAsync(d_job, &job, sizeof(GemmJob), cudaMemcpyHostToDevice, s));
-  CCT_TRY(launch_wbuild_f64(g, d_job, 1, s));
+  CCT_CUDA(cudaMemcpyAsync(d_job, jobs.data(), nsplit * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
+  CCT_TRY(launch_wbuild_f64(g, d_job, nsplit, s));
   // VM: TRANMD 312, the update of lines 125-131, TRANMD 23 (lines 86, 154)
   double *vmin;
   CCT_TRY(b.tmp(&vmin, no * no * no * nu));
   CCT_CUDA(cudaMemcpyAsync(vmin, d_vm, (size_t)no * no * no * nu * 8, cudaMemcpyDeviceToDevice, s));
-  f4_vm_kernel<<<grid_of(no * no * no * nu), 256, 0, s>>>((int)no, (int)nu, g.NP, vmin, t, d_vm);
+  f4_vm_kernel<<<grid_of(no * no * no * nu), 256, 0, s>>>((int)no, (int)nu, g.NP, nsplit, no * no * g.NP, vmin, t,
+                                                          d_vm);
   CCT_CUDA(cudaGetLastError());
   if (mem == CCT_MEM_HOST) {
     CCT_CUDA(cudaMemcpyAsync(t2, d_t2, (size_t)n4 * 8, cudaMemcpyDeviceToHost, s));
