@@ -106,16 +106,10 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
     } else {
       // the row's E values gathered one double at a time: the packed
       // triangle holds (k q | p x) at tri(k, q) of column p, the -T2 rows the
-      // k >= nu part; past nu + no the row is zero.  Entries with k <= q lie
-      // along row q of the triangle, contiguous in k: eight threads per row
-      // copy them.  Entries with k > q lie along column q, at k(k+1)/2 + q,
-      // contiguous in q; in the first half consecutive tile rows are
-      // consecutive q of one packed column, so there one thread per row
-      // copies them and a warp reads 32 consecutive doubles per k.
+      // k >= nu part; past nu + no the row is zero
       const double *tbase = h ? job.t1 : job.t0;
       const int64_t nutr = (int64_t)nu * (nu + 1) / 2;
       const int nov = (int)(KV - nu);
-      const bool by_column = h == 0;
 #pragma unroll
       for (int rr = tid >> 3; rr < BM; rr += NT / 8) {
         const int ro = rowoff[h * BM + rr];
@@ -123,7 +117,6 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
 #pragma unroll
         for (int e = 0; e < 2; e++) {
           const int64_t k = k0 + chunk * 2 + e;
-          if (by_column && ro >= 0 && k > qr && k < nu) continue;  // the column pass below
           const double *src = abase;
           int bytes = 0;
           if (ro >= 0 && k < nu) {
@@ -134,19 +127,6 @@ __device__ __forceinline__ void wbuild_tile(const GemmJob &job, int nu, int64_t 
             bytes = 8;
           }
           cp_async8(as + swz(rr, chunk * 2 + e), src, bytes);
-        }
-      }
-      if (by_column) {  // NT == BM: thread tid takes row tid
-        const int rr = tid;
-        const int ro = rowoff[rr];
-        const int pr = rowpq[2 * rr], qr = rowpq[2 * rr + 1];
-        if (ro >= 0) {
-          const double *col = abase + (int64_t)pr * nutr + qr;
-#pragma unroll
-          for (int kk = 0; kk < BK; kk++) {
-            const int64_t k = k0 + kk;
-            if (k > qr && k < nu) cp_async8(as + swz(rr, kk), col + k * (k + 1) / 2, 8);
-          }
         }
       }
     }
