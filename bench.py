@@ -400,9 +400,9 @@ def accuracy_table(A, S, local, main_rows):
 
 def packed_extra(A, inp, local, expanded_ms, expanded_e):
     """The headline workload's FP64 form with VVVO kept packed (CCT_VVVO_PACKED:
-    the packed triangle resident, operand rows gathered in the W build's tile
-    loader) against the expanded operand: device time of a whole step, bitwise
-    equality and the resident VVVO bytes of each."""
+    the packed triangle resident and a cache of four expanded E slabs refilled
+    tuple by tuple) against the expanded operand: device time of a whole step,
+    bitwise equality and the resident VVVO bytes of each."""
     no, nu = inp.no, inp.nu
     with A.TriplesPlan(no, nu, device=local, vvvo="packed") as plan:
         plan.set_system(inp)
@@ -414,7 +414,7 @@ def packed_extra(A, inp, local, expanded_ms, expanded_e):
     return {"workload": f"{inp.name} FP64", "expanded_ms": expanded_ms, "packed_ms": min(times),
             "packed_over_expanded": min(times) / expanded_ms, "bitwise_equal": (ets + etd) == expanded_e,
             "expanded_operand_bytes": no * nu * nu * kp * 8,
-            "packed_resident_bytes": nu * (nu + 1) // 2 * nu * no * 8 + nu * nu * no * no * 8}
+            "packed_resident_bytes": nu * (nu + 1) // 2 * nu * no * 8 + 4 * nu * nu * kp * 8}
 
 
 def measured_peak(key: str) -> float:

@@ -180,9 +180,10 @@ int launch_build_e(const Dims &d, const double *vvvo_packed, const double *t2, d
                    int x_end, cudaStream_t s);
 int launch_build_e_slice(const Dims &d, const double *packed_slice, const double *t2, double *E, int x,
                          cudaStream_t s);
+// E[x] alone into slab (nu^2 rows of KP), from the whole packed VVVO
+int launch_build_e_slab(const Dims &d, const double *vvvo_packed, const double *t2, double *slab, int x,
+                        cudaStream_t s);
 int launch_build_f(const Dims &d, const double *t2, const double *vm, double *F, cudaStream_t s);
-// packed plans: the -T2 rows of E, et2[x][p*nu+q][l] = -T2(p,q,l,x)
-int launch_build_et2(const Dims &d, const double *t2, double *et2, cudaStream_t s);
 int launch_check_inputs(const Dims &d, const double *eh, const double *ep, const double *t1, const double *t2,
                         const double *vm, const double *voe, const double *vvvo, int *flags, cudaStream_t s);
 

@@ -27,9 +27,10 @@ __device__ __forceinline__ int64_t tri_index(int64_t a, int64_t b) {
   return I * (I + 1) / 2 + J;
 }
 
-// One warp per E row (x, r1, r2); lanes walk kappa.
+// One warp per E row (x, r1, r2); lanes walk kappa.  E holds the slabs of
+// occupied indices e_x0, e_x0 + 1, ... (0: the whole operand).
 __global__ void build_e_kernel(const double *__restrict__ vvvo, const double *__restrict__ t2, double *__restrict__ E,
-                               int no, int nu, int64_t KP, int x_begin, int x_end, int64_t col_base) {
+                               int no, int nu, int64_t KP, int x_begin, int x_end, int64_t col_base, int e_x0) {
   const int64_t nu2 = (int64_t)nu * nu;
   const int64_t nrows = (int64_t)(x_end - x_begin) * nu2;
   const int64_t nutr = (int64_t)nu * (nu + 1) / 2;
@@ -42,7 +43,7 @@ __global__ void build_e_kernel(const double *__restrict__ vvvo, const double *__
     const int64_t rem = row - xr * nu2;
     const int r1 = (int)(rem / nu), r2 = (int)(rem - (int64_t)(rem / nu) * nu);
     const double *col = vvvo + ((int64_t)x * nu + r1 - col_base) * nutr;
-    double *dst = E + ((int64_t)x * nu2 + rem) * KP;
+    double *dst = E + ((int64_t)(x - e_x0) * nu2 + rem) * KP;
     for (int64_t kap = lane; kap < KP; kap += 32) {
       double v = 0.0;
       if (kap < nu) {
@@ -81,18 +82,6 @@ __global__ void build_f_kernel(const double *__restrict__ t2, const double *__re
   }
 }
 
-// The -T2 rows of E for a packed plan: et2[x][p*nu+q][l] = -T2(p, q, l, x),
-// one thread per element, l fastest.
-__global__ void build_et2_kernel(const double *__restrict__ t2, double *__restrict__ et2, int no, int nu) {
-  const int64_t nu2 = (int64_t)nu * nu, n = (int64_t)no * nu2 * no;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t l = e % no, r = e / no;
-    const int64_t x = r / nu2, m = r - x * nu2;
-    const int64_t p = m / nu, q = m - p * nu;
-    et2[e] = -t2[((x * no + l) * nu + q) * nu + p];
-  }
-}
-
 // flags[0] |= 1 when any element is NaN/Inf.
 __global__ void finite_kernel(const double *__restrict__ p, int64_t n, int *flags) {
   int bad = 0;
@@ -115,7 +104,7 @@ int launch_build_e(const Dims &d, const double *vvvo_packed, const double *t2, d
                    cudaStream_t s) {
   if (x_end <= x_begin) return CCT_OK;
   const int64_t rows = (int64_t)(x_end - x_begin) * d.nu * d.nu;
-  build_e_kernel<<<grid_for(rows), 256, 0, s>>>(vvvo_packed, t2, E, d.no, d.nu, d.KP, x_begin, x_end, 0);
+  build_e_kernel<<<grid_for(rows), 256, 0, s>>>(vvvo_packed, t2, E, d.no, d.nu, d.KP, x_begin, x_end, 0, 0);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
@@ -125,19 +114,19 @@ int launch_build_e_slice(const Dims &d, const double *packed_slice, const double
   // packed_slice holds the nu columns x*nu .. x*nu+nu-1 only
   const int64_t rows = (int64_t)d.nu * d.nu;
   build_e_kernel<<<grid_for(rows), 256, 0, s>>>(packed_slice, t2, E, d.no, d.nu, d.KP, x, x + 1,
-                                                (int64_t)x * d.nu);
+                                                (int64_t)x * d.nu, 0);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
 
-int launch_build_et2(const Dims &d, const double *t2, double *et2, cudaStream_t s) {
-  const int64_t n = (int64_t)d.no * d.nu * d.nu * d.no;
-  int64_t blocks = (n + 255) / 256;
-  if (blocks > 148 * 32) blocks = 148 * 32;
-  build_et2_kernel<<<(int)(blocks < 1 ? 1 : blocks), 256, 0, s>>>(t2, et2, d.no, d.nu);
+int launch_build_e_slab(const Dims &d, const double *vvvo_packed, const double *t2, double *slab, int x,
+                        cudaStream_t s) {
+  const int64_t rows = (int64_t)d.nu * d.nu;
+  build_e_kernel<<<grid_for(rows), 256, 0, s>>>(vvvo_packed, t2, slab, d.no, d.nu, d.KP, x, x + 1, 0, x);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
+
 
 int launch_build_f(const Dims &d, const double *t2, const double *vm, double *F, cudaStream_t s) {
   const int64_t rows = (int64_t)d.no * d.no * d.NP;

@@ -65,8 +65,9 @@ struct ccT_plan {
   double *acc = nullptr;  // [etd_sum, etd_comp, out3[3], v1(nu*no)]
   GemmJob *jobs = nullptr;  // [buffer][tuple][3]
   bool emulated = false;    // INT8 split-integer W-build
-  bool packed = false;      // VVVO kept packed (CCT_VVVO_PACKED): no E; vvvo_res and et2 instead
-  double *vvvo_res = nullptr, *et2 = nullptr;
+  bool packed = false;      // VVVO kept packed (CCT_VVVO_PACKED): no E; vvvo_res and a slab cache instead
+  double *vvvo_res = nullptr;
+  double *slabs = nullptr;  // packed plans: kSlabs expanded E slabs (nu^2 x KP each), refilled per tuple
   bool emu_auto = false;    // digit count picked by calibration in ccT_set_inputs
   int emu_base_ebn = 0;     // automatic plans: the N tile the kEmuMaxSlices-digit calibration operands use
   double emu_est_err = 0.0, emu_target = 0.0;  // calibrated |dE(T)| bound and its target (Eh)
@@ -146,18 +147,12 @@ int build_jobs(ccT_plan *p) {
   const int64_t nu2 = (int64_t)d.nu * d.nu;
   auto Ex = [&](int x) { return p->E + (int64_t)x * nu2 * d.KP; };
   auto Fyz = [&](int y, int z) { return p->F + ((int64_t)y * d.no + z) * d.NP * d.KP; };
+  if (p->packed) return CCT_OK;  // jobs name cache slots: built per forward (packed_schedule)
   int buf = 0;
-  // packed plans: the A rows of occupied x come from its nu packed VVVO
-  // columns and its -T2 rows
-  const int64_t nutr = (int64_t)d.nu * (d.nu + 1) / 2;
-  auto Px = [&](int x) { return p->vvvo_res + (int64_t)x * d.nu * nutr; };
-  auto Tx = [&](int x) { return p->et2 + (int64_t)x * nu2 * d.no; };
   auto G = [&](int x1, int x2, int x3, int slot) {
-    if (p->packed) return GemmJob{Px(x1), Px(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][slot], 2, 1, Tx(x1), Tx(x2)};
     return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][slot], 2, 0};
   };
   auto H = [&](int x1, int x2, int x3, int slot) {
-    if (p->packed) return GemmJob{Px(x1), Px(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 1, Tx(x1), Tx(x1)};
     return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 0};
   };
   std::vector<GemmJob> jobs;
@@ -180,6 +175,84 @@ int build_jobs(ccT_plan *p) {
   }
   CCT_CUDA(cudaMemcpy(p->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
   if (p->emulated) CCT_TRY(upload_emu_jobs(p, jobs, p->emu_jobs));
+  return CCT_OK;
+}
+
+// Packed plans keep kSlabs expanded E slabs in a cache instead of all of E.
+// For the tuples [begin, end) in order, a least-recently-used simulation on
+// the host gives every slab a tuple needs a slot; (*expand)[t - begin] lists
+// the (slot, x) expansions to issue before tuple t's W build, on the stream
+// that runs the W builds (so the W build of the tuple before has finished
+// reading the slot), and the tuple's jobs, for every X buffer, name the
+// slots.  In tuple order i > j > k a tuple usually needs one new slab.
+constexpr int kSlabs = 4;
+using SlabFills = std::vector<std::vector<std::pair<int, int>>>;
+
+int packed_schedule(ccT_plan *p, int64_t begin, int64_t end, SlabFills *expand) {
+  const Dims &d = p->d;
+  const int64_t nu2 = (int64_t)d.nu * d.nu, slab = nu2 * d.KP, n = end - begin, ntup = (int64_t)p->tuples.size();
+  int slot_x[kSlabs];
+  int64_t last[kSlabs];
+  for (int c = 0; c < kSlabs; c++) {
+    slot_x[c] = -1;
+    last[c] = -1;
+  }
+  expand->assign(n, {});
+  auto Fyz = [&](int y, int z) { return p->F + ((int64_t)y * d.no + z) * d.NP * d.KP; };
+  std::vector<GemmJob> jobs((size_t)kNBuf * n * 3);
+  for (int64_t t = begin; t < end; t++) {
+    const Tuple &tu = p->tuples[t];
+    const int need[3] = {tu.i, tu.j, tu.k};
+    auto needed = [&](int x) { return x == need[0] || x == need[1] || x == need[2]; };
+    int slot_of[3];
+    for (int q = 0; q < 3; q++) {
+      int c = -1;
+      for (int c2 = 0; c2 < kSlabs; c2++)
+        if (slot_x[c2] == need[q]) c = c2;
+      if (c < 0) {  // the least recently used slot holding none of this tuple's slabs (empty slots first)
+        for (int c2 = 0; c2 < kSlabs; c2++)
+          if (!needed(slot_x[c2]) && (c < 0 || last[c2] < last[c])) c = c2;
+        slot_x[c] = need[q];
+        (*expand)[t - begin].push_back({c, need[q]});
+      }
+      last[c] = t;
+      slot_of[q] = c;
+    }
+    auto Ex = [&](int x) {
+      const int q = x == need[0] ? 0 : (x == need[1] ? 1 : 2);
+      return p->slabs + slot_of[q] * slab;
+    };
+    for (int buf = 0; buf < kNBuf; buf++) {
+      auto G = [&](int x1, int x2, int x3, int sl) {
+        return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][sl], 2, 0};
+      };
+      auto H = [&](int x1, int x2, int x3, int sl) {
+        return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][sl], 1, 0};
+      };
+      GemmJob *J = &jobs[((size_t)buf * n + (t - begin)) * 3];
+      if (tu.kind == kIJK) {
+        J[0] = G(tu.i, tu.j, tu.k, 0);
+        J[1] = G(tu.i, tu.k, tu.j, 1);
+        J[2] = G(tu.j, tu.k, tu.i, 2);
+      } else if (tu.kind == kIJJ) {
+        J[0] = G(tu.i, tu.j, tu.j, 0);
+        J[1] = J[2] = H(tu.j, tu.j, tu.i, 1);
+      } else {
+        J[0] = H(tu.i, tu.i, tu.k, 0);
+        J[1] = J[2] = G(tu.i, tu.k, tu.i, 1);
+      }
+    }
+  }
+  for (int buf = 0; buf < kNBuf; buf++)
+    CCT_CUDA(cudaMemcpy(p->jobs + 3 * (buf * ntup + begin), jobs.data() + (size_t)buf * n * 3,
+                        (size_t)n * 3 * sizeof(GemmJob), cudaMemcpyHostToDevice));
+  return CCT_OK;
+}
+
+int packed_fill(ccT_plan *p, const std::vector<std::pair<int, int>> &fills, cudaStream_t st) {
+  const int64_t slab = (int64_t)p->d.nu * p->d.nu * p->d.KP;
+  for (const auto &f : fills) CCT_TRY(launch_build_e_slab(p->d, p->vvvo_res, p->t2, p->slabs + f.first * slab, f.second, st));
+  p->last_launches += (int64_t)fills.size();
   return CCT_OK;
 }
 
@@ -483,8 +556,8 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     return CCT_ERR_INVALID;
   }
   if (o.vvvo_mode < CCT_VVVO_AUTO || o.vvvo_mode > CCT_VVVO_PACKED ||
-      (o.vvvo_mode == CCT_VVVO_PACKED && (o.precision != CCT_PREC_FP64 || nu > 32767))) {
-    set_error("vvvo_mode must be CCT_VVVO_AUTO, _EXPANDED or _PACKED; PACKED needs an FP64 plan and nu <= 32767");
+      (o.vvvo_mode == CCT_VVVO_PACKED && o.precision != CCT_PREC_FP64)) {
+    set_error("vvvo_mode must be CCT_VVVO_AUTO, _EXPANDED or _PACKED; PACKED needs an FP64 plan");
     return CCT_ERR_INVALID;
   }
   int ndev = 0;
@@ -522,7 +595,7 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
   d.nb = (int)((nu + kRB - 1) / kRB);
   d.ncta = (int64_t)d.nb * (d.nb + 1) * (d.nb + 2) / 6;
   p->tuples = tuple_list((int)no);
-  if (!p->emulated && nu <= 32767) {
+  if (!p->emulated) {
     if (o.vvvo_mode == CCT_VVVO_PACKED) {
       p->packed = true;
     } else if (o.vvvo_mode == CCT_VVVO_AUTO) {
@@ -556,7 +629,7 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
       (s = dalloc(&p->t2, nu2 * no * no)) || (s = dalloc(&p->vm, no * nu * no * no)) ||
       (s = dalloc(&p->voe, nu2 * no * no)) ||
       (s = p->packed ? dalloc(&p->vvvo_res, nu * (nu + 1) / 2 * nu * no) : dalloc(&p->E, no * nu2 * d.KP)) ||
-      (s = p->packed ? dalloc(&p->et2, nu2 * no * no) : CCT_OK) ||
+      (s = p->packed ? dalloc(&p->slabs, kSlabs * nu2 * d.KP) : CCT_OK) ||
       (s = dalloc(&p->F, no * no * d.NP * d.KP)) ||
       (s = dalloc(&p->xpart, d.ncta)) || (s = dalloc(&p->vpart, (int64_t)12 * d.nb * d.nb * (d.nb + 1))) ||
       (s = dalloc(&p->cta_table, d.ncta * 3)) || (s = dalloc(&p->acc, 5 + nu * no)) ||
@@ -662,8 +735,7 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
     if (s == CCT_OK)
       s = launch_check_inputs(d, p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, vvvo_dev, p->flags, p->stream);
   }
-  if (s == CCT_OK) s = p->packed ? launch_build_et2(d, p->t2, p->et2, p->stream)
-                                 : launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
+  if (s == CCT_OK && !p->packed) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
   if (s == CCT_OK && p->emu_auto) {  // calibration runs on operands of every digit count
     p->d.EBN = p->emu.ebn = p->emu_base_ebn;
@@ -723,8 +795,13 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   if (p->emulated)
     CCT_CUDA(cudaMemsetAsync(p->emu.slice_hist, 0, (kEmuMaxSlices + 1) * sizeof(unsigned long long), p->stream));
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
+  SlabFills fills;
+  if (p->packed) CCT_TRY(packed_schedule(p, begin, end, &fills));
   CCT_TRY(fork_streams(p));
-  for (int64_t t = begin; t < end; t++) CCT_TRY(run_tuple(p, t));
+  for (int64_t t = begin; t < end; t++) {
+    if (p->packed) CCT_TRY(packed_fill(p, fills[t - begin], p->gemm_stream));
+    CCT_TRY(run_tuple(p, t));
+  }
   CCT_TRY(join_streams(p));
   CCT_TRY(launch_ets(d, p->t1, v1_acc(p), p->acc, p->acc + 2, p->stream));
   p->last_launches += 1;
@@ -956,6 +1033,11 @@ int ccT_tuple_w(ccT_plan *p, int64_t tuple, double *w, int32_t mem) {
     wf = w;
   }
   if (s == CCT_OK) CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
+  if (s == CCT_OK && p->packed) {
+    SlabFills fills;
+    s = packed_schedule(p, tuple, tuple + 1, &fills);
+    if (s == CCT_OK) s = packed_fill(p, fills[0], p->stream);
+  }
   if (s == CCT_OK) s = wbuild_tuple(p, tuple, 0, false, p->stream);
   if (s == CCT_OK) s = assemble_w_fortran(p->d, p->tuples[tuple], p->X[0], wc, wf, p->stream);
   int werr = 0;
@@ -1003,6 +1085,11 @@ int ccT_time_wbuild(ccT_plan *p, int64_t tuple, int32_t reps, double *ms_per_lau
   const int njobs = p->tuples[tuple].kind == kIJK ? 3 : 2;
   CCT_TRY(fork_streams(p));
   CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[0], 0));
+  if (p->packed) {  // the tuple's slabs into the cache (not timed)
+    SlabFills fills;
+    CCT_TRY(packed_schedule(p, tuple, tuple + 1, &fills));
+    CCT_TRY(packed_fill(p, fills[0], p->gemm_stream));
+  }
   auto launch = [&]() {
     return p->emulated ? launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * tuple, njobs, p->flags + 1, p->gemm_stream)
                        : launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream);
@@ -1048,7 +1135,7 @@ int ccT_plan_destroy(ccT_plan *p) {
   for (cudaStream_t st : {p->stream, p->gemm_stream, p->red_stream, p->bwd_stream, p->rec_stream})
     if (st) cudaStreamSynchronize(st);
   double *bufs[] = {p->eh, p->ep, p->t1, p->t2, p->vm, p->voe, p->E, p->F, p->xpart, p->vpart, p->acc, p->stage,
-                    p->vvvo_res, p->et2};
+                    p->vvvo_res, p->slabs};
   for (double *b : bufs)
     if (b) cudaFree(b);
   for (int b = 0; b < kNBuf; b++)

@@ -295,20 +295,27 @@ def test_caller_stream(api):
 @pytest.mark.parametrize("no,nu,seed,dist", [(4, 36, 0, "normal"), (5, 29, 3, "log"), (3, 7, 4, "normal"),
                                              (6, 130, 5, "normal")])
 def test_packed_vvvo_bitwise_equals_expanded(api, no, nu, seed, dist):
-    """CCT_VVVO_PACKED (the packed triangle resident, operand rows gathered in the
-    W build's tile loader) against the expanded operand: the same values in the
-    same order, so every result is bitwise equal."""
+    """CCT_VVVO_PACKED (the packed triangle resident, a cache of four expanded
+    E slabs refilled tuple by tuple) against the expanded operand: the same
+    values in the same order, so every result is bitwise equal -- for the
+    whole tuple list, for a shard that starts mid-list, and for single-tuple W."""
     inp = S.generate(no, nu, seed, dist)
     out = {}
     for mode in ("expanded", "packed"):
         with api.TriplesPlan(no, nu, vvvo=mode) as plan:
             plan.set_system(inp)
             ets, etd, v1 = plan.forward()
-            w = [plan.tuple_w(t) for t in (0, plan.num_tuples - 1)]
-        out[mode] = (ets, etd, v1, w)
+            mid = plan.num_tuples // 3
+            shard = plan.forward(mid, plan.num_tuples)
+            w = [plan.tuple_w(t) for t in (0, mid, plan.num_tuples - 1)]
+            plan.forward()  # the cache starts empty again
+            again = plan.forward()
+        out[mode] = (ets, etd, v1, w, shard, again)
     e, p = out["expanded"], out["packed"]
     assert e[0] == p[0] and e[1] == p[1] and np.array_equal(e[2], p[2])
     assert all(np.array_equal(a, b) for a, b in zip(e[3], p[3]))
+    assert e[4][0] == p[4][0] and e[4][1] == p[4][1] and np.array_equal(e[4][2], p[4][2])
+    assert p[5][0] == p[0] and p[5][1] == p[1]
 
 
 def test_packed_vvvo_has_no_backward(api):
