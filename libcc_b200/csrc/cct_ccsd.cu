@@ -129,15 +129,40 @@ __global__ void f4_o2_kernel(int no, int nu, int64_t kp, const double *__restric
 }
 
 // the GEMM's column operand: bpad[split][(a + nu j)][x + nu y] = (a y|x j), rows
-// of kp doubles per split (np rows per split)
-__global__ void f4_b_kernel(int no, int nu, int64_t kp, int64_t np, const double *__restrict__ vvvo,
-                            double *__restrict__ bpad) {
-  const int64_t nu2 = (int64_t)nu * nu, n = nu2 * nu * no, nutr = (int64_t)nu * (nu + 1) / 2;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t xy = e % nu2, aj = e / nu2;
-    const int64_t x = xy % nu, y = xy / nu, a = aj % nu, j = aj / nu;
-    const int64_t z = xy / kp;
-    bpad[(z * np + aj) * kp + (xy - z * kp)] = vvvo[(j * nu + x) * nutr + tri_at(a, y)];
+// of kp doubles per split (np rows per split).  A transpose through shared
+// memory: a CTA reads 32 packed columns (j, x0..x0+31) x 32 consecutive
+// triangle entries t0..t0+31 along the columns, and writes each entry (a, y),
+// a >= y, as 32 consecutive x of rows (a, j) and (y, j).
+constexpr int kTT = 32;
+__global__ void __launch_bounds__(256) f4_b_kernel(int no, int nu, int64_t kp, int64_t np,
+                                                   const double *__restrict__ vvvo, double *__restrict__ bpad) {
+  __shared__ double tile[kTT][kTT + 1];
+  const int64_t nutr = (int64_t)nu * (nu + 1) / 2;
+  const int64_t x0 = (int64_t)blockIdx.y * kTT, t0 = (int64_t)blockIdx.x * kTT;
+  const int j = blockIdx.z;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int xi = ty; xi < kTT; xi += 8) {
+    const int64_t x = x0 + xi, t = t0 + tx;
+    tile[xi][tx] = (x < nu && t < nutr) ? vvvo[((int64_t)j * nu + x) * nutr + t] : 0.0;
+  }
+  __syncthreads();
+  const int64_t x = x0 + tx;
+  if (x >= nu) return;
+  for (int ti = ty; ti < kTT; ti += 8) {
+    const int64_t t = t0 + ti;
+    if (t >= nutr) break;
+    // t = a (a + 1) / 2 + y with 0 <= y <= a
+    int64_t a = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while (a * (a + 1) / 2 > t) a--;
+    while ((a + 1) * (a + 2) / 2 <= t) a++;
+    const int64_t y = t - a * (a + 1) / 2;
+    const double v = tile[tx][ti];
+    const int64_t c1 = x + (int64_t)nu * y, z1 = c1 / kp;  // row (a, j), column (x, y)
+    bpad[(z1 * np + a + (int64_t)nu * j) * kp + (c1 - z1 * kp)] = v;
+    if (a != y) {
+      const int64_t c2 = x + (int64_t)nu * a, z2 = c2 / kp;  // row (y, j), column (x, a)
+      bpad[(z2 * np + y + (int64_t)nu * j) * kp + (c2 - z2 * kp)] = v;
+    }
   }
 }
 
@@ -321,7 +346,11 @@ extern "C" int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, do
   CCT_CUDA(cudaMemsetAsync(bpad, 0, (size_t)nsplit * g.NP * g.KP * 8, s));
   f4_o2_kernel<<<grid_of(n4), 256, 0, s>>>((int)no, (int)nu, g.KP, o2in, d_o2, apad);
   CCT_CUDA(cudaGetLastError());
-  f4_b_kernel<<<grid_of(nu2 * nou), 256, 0, s>>>((int)no, (int)nu, g.KP, g.NP, d_vvvo, bpad);
+  {
+    const int64_t nutr = nu * (nu + 1) / 2;
+    const dim3 grid((unsigned)((nutr + kTT - 1) / kTT), (unsigned)((nu + kTT - 1) / kTT), (unsigned)no);
+    f4_b_kernel<<<grid, 256, 0, s>>>((int)no, (int)nu, g.KP, g.NP, d_vvvo, bpad);
+  }
   CCT_CUDA(cudaGetLastError());
   // T((k,l),(a,j)) = sum_{x,y} o2b(x,y,k,l) (a y|x j) (line 119 for every j) on the FP64 tensor cores
   std::vector<GemmJob> jobs(nsplit);
