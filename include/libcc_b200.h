@@ -297,7 +297,9 @@ int ccT_reduce_w_noalloc(int64_t no, int64_t nu, int64_t i, int64_t j, int64_t k
  * occupied index (nothing in the reference tree calls them; they are the CCSD
  * step before (T)).  Arrays are Fortran column-major; mem says whether every
  * pointer is host or device memory; the calls return when the results are in
- * place.
+ * place.  They keep a device workspace between calls (the same buffers every
+ * call of a shape, so repeated calls allocate nothing) and are serialised
+ * against each other; ccT_ccsd_release_workspace frees it.
  *
  * ccT_ccsd_terms_29_31 replaces terms_29_30_31 (src/triples-ijk/ccsd_acc.f:1-60):
  *   t2(i,b,c,j) += sum_a o1(i,a) [ (c a|b j) - sum_k o1(k,c) vl(k,a,b,j)
@@ -320,6 +322,8 @@ int ccT_ccsd_terms_29_31(int64_t no, int64_t nu, const double *o1, double *t2, c
  * permutations put it. */
 int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, double *o2, double *t2, double *vm,
                          double *rl, const double *vvvo, int32_t mem);
+/* Frees the device workspace the two CCSD-term entry points keep. */
+int ccT_ccsd_release_workspace(void);
 
 /* ------------------------------------------------------------------ legacy hooks
  * ijk_gpu_init_    replaces the call at src/triples-ijk/triples_cpu.F90:363

@@ -27,7 +27,7 @@ EXPORTS = [
     "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms", "ccT_emu_slice_histogram",
     "ccT_batch_create", "ccT_batch_set_inputs", "ccT_batch_forward", "ccT_batch_v1", "ccT_batch_configure",
     "ccT_batch_tune", "ccT_batch_last_ms", "ccT_batch_work_items", "ccT_batch_destroy", "ccT_emu_digits",
-    "ccT_tuple_w", "ccT_batch_debug_stall", "ccT_batch_emu_digits", "ccT_ccsd_terms_29_31", "ccT_ccsd_terms_32_35",
+    "ccT_tuple_w", "ccT_batch_debug_stall", "ccT_batch_emu_digits", "ccT_ccsd_terms_29_31", "ccT_ccsd_terms_32_35", "ccT_ccsd_release_workspace",
 ]
 
 
@@ -140,6 +140,8 @@ def load():
     lib.ccT_ccsd_terms_29_31.restype = ctypes.c_int
     lib.ccT_ccsd_terms_32_35.argtypes = [i64, i64] + [vp] * 6 + [i32]
     lib.ccT_ccsd_terms_32_35.restype = ctypes.c_int
+    lib.ccT_ccsd_release_workspace.argtypes = []
+    lib.ccT_ccsd_release_workspace.restype = ctypes.c_int
     _lib = lib
     return lib
 

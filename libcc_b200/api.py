@@ -248,6 +248,11 @@ def ccsd_terms_32_35(no: int, nu: int, o1, o2, t2, vm, vvvo):
     return t2h, o2h, vmh, rl
 
 
+def ccsd_release_workspace() -> None:
+    """Frees the device workspace the CCSD-term entry points keep between calls."""
+    N.check(N.load().ccT_ccsd_release_workspace(), "ccT_ccsd_release_workspace")
+
+
 def packed_columns(vvvo: np.ndarray, no: int, nu: int, x: int) -> np.ndarray:
     """The nu packed VVVO columns of occupied index x (0-based), as ddi_get fetches
     them for the GPU hook (triples_cpu.F90:428-450)."""

@@ -35,6 +35,9 @@
 #include "cct_internal.cuh"
 #include "cct_wbuild_tile.cuh"
 
+#include <map>
+#include <mutex>
+
 namespace cct {
 namespace {
 
@@ -179,26 +182,50 @@ __global__ void f4_vm_kernel(int no, int nu, int64_t np, int nsplit, int64_t tsp
   }
 }
 
-struct DevBuf {  // device copies of host arrays (or the caller's device arrays)
-  std::vector<void *> owned;
-  ~DevBuf() {
-    for (void *p : owned) cudaFree(p);
+// Device workspace of the two entry points, kept between calls: a call asks
+// for the same sequence of buffers every time, so slot k of entry point e on
+// device d (the k-th buffer of the call) is reused, and grown when a call
+// needs more; after the first call of a shape nothing is allocated.  The
+// entry points are synchronous and serialised by a mutex;
+// ccT_ccsd_release_workspace frees the workspace.
+struct Workspace {
+  std::vector<std::pair<void *, size_t>> slot;
+};
+std::mutex g_ws_mutex;
+std::map<std::pair<int, int>, Workspace> g_ws;
+
+struct DevBuf {  // device copies of host arrays (or the caller's device arrays) and scratch
+  std::lock_guard<std::mutex> lock{g_ws_mutex};
+  Workspace *ws = nullptr;
+  size_t next = 0;
+  explicit DevBuf(int entry) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    ws = &g_ws[{dev, entry}];
+  }
+  int alloc(void **dst, size_t bytes) {
+    if (bytes < 8) bytes = 8;
+    if (next == ws->slot.size()) ws->slot.push_back({nullptr, 0});
+    std::pair<void *, size_t> &sl = ws->slot[next++];
+    if (sl.second < bytes) {
+      if (sl.first) CCT_CUDA(cudaFree(sl.first));
+      sl = {nullptr, 0};
+      CCT_CUDA(cudaMalloc(&sl.first, bytes));
+      sl.second = bytes;
+    }
+    *dst = sl.first;
+    return CCT_OK;
   }
   int get(double **dst, const double *src, int64_t n, int32_t mem, bool upload, cudaStream_t s) {
     if (mem == CCT_MEM_DEVICE) {
       *dst = const_cast<double *>(src);
       return CCT_OK;
     }
-    CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(dst), (size_t)(n < 1 ? 1 : n) * 8));
-    owned.push_back(*dst);
+    CCT_TRY(alloc(reinterpret_cast<void **>(dst), (size_t)n * 8));
     if (upload) CCT_CUDA(cudaMemcpyAsync(*dst, src, (size_t)n * 8, cudaMemcpyHostToDevice, s));
     return CCT_OK;
   }
-  int tmp(double **dst, int64_t n) {
-    CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(dst), (size_t)(n < 1 ? 1 : n) * 8));
-    owned.push_back(*dst);
-    return CCT_OK;
-  }
+  int tmp(double **dst, int64_t n) { return alloc(reinterpret_cast<void **>(dst), (size_t)n * 8); }
 };
 
 // X_j(p,q,i) = sum_x (x q|p j) O1(i,x) for every occupied j, X_j at x + j nu^2 np,
@@ -234,8 +261,7 @@ int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_v
     jobs[j] = GemmJob{ej, ej, o1pad, o1pad, *X + j * nu * nu * g.NP, 1, 0};
   }
   GemmJob *d_jobs;
-  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
-  b.owned.push_back(d_jobs);
+  CCT_TRY(b.alloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
   CCT_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
   for (int64_t j0 = 0; j0 < no; j0 += nslab) {
     const int cnt = (int)(no - j0 < nslab ? no - j0 : nslab);
@@ -249,8 +275,7 @@ int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_v
     jobs[j] = GemmJob{pj, pj, o1pad, o1pad, *X + j * nu * nu * g.NP, 1, 1, pj, pj};
   }
   GemmJob *d_jobs;
-  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
-  b.owned.push_back(d_jobs);
+  CCT_TRY(b.alloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
   CCT_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
   CCT_TRY(launch_wbuild_f64(g, d_jobs, (int)no, s));
 #endif
@@ -280,7 +305,7 @@ extern "C" int ccT_ccsd_terms_29_31(int64_t no, int64_t nu, const double *o1, do
   }
   const cudaStream_t s = nullptr;
   const int64_t nu2 = nu * nu, nutr = nu * (nu + 1) / 2;
-  DevBuf b;
+  DevBuf b(0);
   double *d_o1, *d_t2, *d_vl, *d_vr, *d_vvvo;
   CCT_TRY(b.get(&d_o1, o1, no * nu, mem, true, s));
   CCT_TRY(b.get(&d_t2, t2, no * nu2 * no, mem, true, s));
@@ -314,7 +339,7 @@ extern "C" int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, do
   }
   const cudaStream_t s = nullptr;
   const int64_t nu2 = nu * nu, nou = no * nu, n4 = nou * nou, nutr = nu * (nu + 1) / 2;
-  DevBuf b;
+  DevBuf b(1);
   double *d_o1, *d_o2, *d_t2, *d_vm, *d_rl, *d_vvvo;
   CCT_TRY(b.get(&d_o1, o1, no * nu, mem, true, s));
   CCT_TRY(b.get(&d_o2, o2, n4, mem, true, s));
@@ -386,8 +411,7 @@ extern "C" int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, do
     jobs[z] = GemmJob{az, az, bz, bz, t + (int64_t)z * no * no * g.NP, 1, 0};
   }
   GemmJob *d_job;
-  CCT_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_job), nsplit * sizeof(GemmJob)));
-  b.owned.push_back(d_job);
+  CCT_TRY(b.alloc(reinterpret_cast<void **>(&d_job), nsplit * sizeof(GemmJob)));
   CCT_CUDA(cudaMemcpyAsync(d_job, jobs.data(), nsplit * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
   CCT_TRY(launch_wbuild_f64(g, d_job, nsplit, s));
   // VM: TRANMD 312, the update of lines 125-131, TRANMD 23 (lines 86, 154)
@@ -404,5 +428,19 @@ extern "C" int ccT_ccsd_terms_32_35(int64_t no, int64_t nu, const double *o1, do
     CCT_CUDA(cudaMemcpyAsync(rl, d_rl, (size_t)n4 * 8, cudaMemcpyDeviceToHost, s));
   }
   CCT_CUDA(cudaStreamSynchronize(s));
+  return CCT_OK;
+}
+
+extern "C" int ccT_ccsd_release_workspace(void) {
+  std::lock_guard<std::mutex> lock(g_ws_mutex);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  for (auto &e : g_ws) {
+    cudaSetDevice(e.first.first);
+    for (auto &sl : e.second.slot)
+      if (sl.first) cudaFree(sl.first);
+  }
+  g_ws.clear();
+  cudaSetDevice(prev);
   return CCT_OK;
 }

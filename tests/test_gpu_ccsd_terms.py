@@ -34,3 +34,27 @@ def test_terms_32_35_match_oracle(no, nu, seed):
     ref = O.literal_terms_32_35(no, nu, a["o1"], a["o2"], a["t2"], a["vm"], a["vvvo"])
     for name, g, r in zip(("t2", "o2", "vm", "rl"), got, ref):
         assert np.abs(g - r).max() <= 1e-12 * max(np.abs(r).max(), 1e-300), name
+
+
+def test_workspace_reuse_across_shapes_and_release():
+    """The entry points keep their device workspace between calls: a large
+    shape, then a smaller one in the grown slots, then the large one again
+    after ccT_ccsd_release_workspace, each bitwise equal to its first call and
+    within the oracle tolerance."""
+    from libcc_b200 import api as A
+    from oracle import oracle as O
+    shapes = [(6, 40, 7), (3, 9, 8)]
+    first = {}
+    for rep in range(2):
+        for no, nu, seed in shapes:
+            a = _inputs(no, nu, seed)
+            g1 = A.ccsd_terms_29_31(no, nu, a["o1"], a["t2"], a["vl"], a["vr"], a["vvvo"])
+            g2 = A.ccsd_terms_32_35(no, nu, a["o1"], a["o2"], a["t2"], a["vm"], a["vvvo"])
+            if rep == 0:
+                first[no] = (g1, g2)
+                ref = O.literal_terms_29_30_31(no, nu, a["o1"], a["t2"], a["vl"], a["vr"], a["vvvo"])
+                assert np.abs(g1 - ref).max() <= 1e-12 * np.abs(ref).max()
+            else:
+                assert np.array_equal(g1, first[no][0])
+                assert all(np.array_equal(x, y) for x, y in zip(g2, first[no][1]))
+        A.ccsd_release_workspace()
