@@ -358,18 +358,33 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
                     "r"(t > 0 ? 1u : first));
               };
               // t = 0 first: with the accumulate flag clear it initialises
-              // every diagonal of the item; later rows add into them
+              // every diagonal of the item; later rows add into them.  An item
+              // with every digit (the usual case) takes a schedule fixed at
+              // compile time: straight-line MMAs with constant shapes and
+              // offsets, so the single issuing thread spends no time on the
+              // partition arithmetic between MMAs.
+              if (sl == S) {
 #pragma unroll
-              for (int t = 0; t < S; t++) {
-                if (t >= sl) break;
-                const int n = sl - t;                       // B slices this A slice meets
-                const int parts = (n + MPS - 1) / MPS;      // MMAs of at most MPS slices, sizes within one
-                const int base = n / parts, extra = n - base * parts;
-                int u0 = 0;
-                for (int q = 0; q < parts; q++) {
-                  const int cnt = base + (q < extra ? 1 : 0);
-                  mma(t, u0, cnt);
-                  u0 += cnt;
+                for (int t = 0; t < S; t++) {
+                  const int n = S - t;
+                  const int parts = (n + MPS - 1) / MPS;
+                  const int base = n / parts, extra = n - base * parts;
+#pragma unroll
+                  for (int q = 0; q < parts; q++) mma(t, q * base + (q < extra ? q : extra), base + (q < extra ? 1 : 0));
+                }
+              } else {
+#pragma unroll
+                for (int t = 0; t < S; t++) {
+                  if (t >= sl) break;
+                  const int n = sl - t;                       // B slices this A slice meets
+                  const int parts = (n + MPS - 1) / MPS;      // MMAs of at most MPS slices, sizes within one
+                  const int base = n / parts, extra = n - base * parts;
+                  int u0 = 0;
+                  for (int q = 0; q < parts; q++) {
+                    const int cnt = base + (q < extra ? 1 : 0);
+                    mma(t, u0, cnt);
+                    u0 += cnt;
+                  }
                 }
               }
             }
