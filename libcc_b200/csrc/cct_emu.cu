@@ -313,6 +313,18 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       const uint64_t dA0 = desc_kmajor(sA), dB0 = desc_kmajor(sB);
       uint32_t g = 0, n = 0;
       bool ok = true;
+      // halves and digit count of an item (global loads: the issuer fetches
+      // them one item ahead, so they are not between two items' MMAs)
+      auto item_info = [&](int64_t item, int *nhalves, int *slices) {
+        const int jb = (int)(item / per_job);
+        const int rem = (int)(item - (int64_t)jb * per_job);
+        const int tm = rem / args.tiles_n, tn = rem - tm * args.tiles_n;
+        const EmuJob &job = args.jobs[jb];
+        *nhalves = job.nhalves;
+        *slices = item_slices<S>(args, tm, tn, job.x3);
+      };
+      int nh_next = 0, sl_next = 0;
+      if (blockIdx.x < nitems) item_info(blockIdx.x, &nh_next, &sl_next);
       for (int64_t it = blockIdx.x; it < nitems && ok; it += gridDim.x, n++) {
         // item n uses accumulator set ab; the drain of the item that used it
         // last (use - 1 uses ago) has read it
@@ -324,12 +336,9 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const int jb = (int)(it / per_job);
-        const int rem = (int)(it - (int64_t)jb * per_job);
-        const int tm = rem / args.tiles_n, tn = rem - tm * args.tiles_n;
-        const EmuJob job = args.jobs[jb];
-        const int nh = job.nhalves;
-        const int sl = item_slices<S>(args, tm, tn, job.x3);
+        const int nh = nh_next, sl = sl_next;
+        // the next item's job and digit count, loaded while this item's MMAs issue
+        if (it + gridDim.x < nitems) item_info(it + gridDim.x, &nh_next, &sl_next);
         if (args.slice_hist) atomicAdd(args.slice_hist + sl, 1ull);
         for (int h = 0; h < nh && ok; h++) {
           for (int kc = 0; kc < KC; kc += KS, g++) {

@@ -42,6 +42,9 @@ using namespace cct;
 // X buffer sets: the W-build of tuple t may run while the reductions of
 // tuples t-1 .. t-kNBuf+1 are still reading theirs.
 constexpr int kNBuf = 3;
+#ifndef CCT_BWD_PRIO
+#define CCT_BWD_PRIO 0
+#endif
 
 struct ccT_plan {
   int device = 0;
@@ -864,8 +867,14 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   }
   CCT_TRY(adj_configure(p->device));
   if (!p->bwd_stream) {
-    CCT_CUDA(cudaStreamCreateWithFlags(&p->bwd_stream, cudaStreamNonBlocking));
-    CCT_CUDA(cudaStreamCreateWithFlags(&p->rec_stream, cudaStreamNonBlocking));
+    // stream priorities of the backward (build constant CCT_BWD_PRIO): 0, the
+    // dF GEMM and the recompute at the default priority below the pointwise
+    // chain and the dE GEMM; 1, all four at the highest priority
+    int prio_least = 0, prio_greatest = 0;
+    CCT_CUDA(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+    const int prio = CCT_BWD_PRIO == 1 ? prio_greatest : 0;
+    CCT_CUDA(cudaStreamCreateWithPriority(&p->bwd_stream, cudaStreamNonBlocking, prio));
+    CCT_CUDA(cudaStreamCreateWithPriority(&p->rec_stream, cudaStreamNonBlocking, prio));
     for (cudaEvent_t &e : p->ev_bwdf) CCT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (int g = 0; g < kGXSets; g++)
       for (cudaEvent_t *e : {&p->ev_gx_pw[g], &p->ev_gx_e[g], &p->ev_gx_f[g]})
