@@ -230,9 +230,6 @@ struct DevBuf {  // device copies of host arrays (or the caller's device arrays)
 
 // X_j(p,q,i) = sum_x (x q|p j) O1(i,x) for every occupied j, X_j at x + j nu^2 np,
 // row (p,q) at (p nu + q) np: the W-build tile, one packed-row job per j.
-#ifndef CCT_F4_SLABS
-#define CCT_F4_SLABS 1
-#endif
 int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_vvvo, DevBuf &b, double **X,
                    int64_t *np_out, cudaStream_t s) {
   const int64_t nutr = nu * (nu + 1) / 2;
@@ -247,28 +244,6 @@ int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_v
   CCT_TRY(b.tmp(X, no * nu * nu * g.NP));
   f4_o1pad_kernel<<<grid_of(g.NP * g.KP), 256, 0, s>>>((int)no, (int)nu, g.KP, g.NP, d_o1, o1pad);
   CCT_CUDA(cudaGetLastError());
-#if CCT_F4_SLABS
-  // rows expanded slab by slab (kF4Slabs occupied indices at a time) so the
-  // tile loads whole rows; the packed-row loader gathers one double at a time
-  constexpr int kF4Slabs = 4;
-  const int nslab = (int)(no < kF4Slabs ? no : kF4Slabs);
-  const int64_t slab = nu * nu * g.KP;
-  double *slabs;
-  CCT_TRY(b.tmp(&slabs, nslab * slab));
-  std::vector<GemmJob> jobs((size_t)no);
-  for (int64_t j = 0; j < no; j++) {
-    const double *ej = slabs + (j % nslab) * slab;
-    jobs[j] = GemmJob{ej, ej, o1pad, o1pad, *X + j * nu * nu * g.NP, 1, 0};
-  }
-  GemmJob *d_jobs;
-  CCT_TRY(b.alloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
-  CCT_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
-  for (int64_t j0 = 0; j0 < no; j0 += nslab) {
-    const int cnt = (int)(no - j0 < nslab ? no - j0 : nslab);
-    for (int c = 0; c < cnt; c++) CCT_TRY(launch_build_e_slab(g, d_vvvo, nullptr, slabs + c * slab, (int)(j0 + c), s));
-    CCT_TRY(launch_wbuild_f64(g, d_jobs + j0, cnt, s));
-  }
-#else
   std::vector<GemmJob> jobs((size_t)no);
   for (int64_t j = 0; j < no; j++) {
     const double *pj = d_vvvo + j * nu * nutr;  // the nu packed columns of occupied j
@@ -278,7 +253,6 @@ int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_v
   CCT_TRY(b.alloc(reinterpret_cast<void **>(&d_jobs), jobs.size() * sizeof(GemmJob)));
   CCT_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice, s));
   CCT_TRY(launch_wbuild_f64(g, d_jobs, (int)no, s));
-#endif
   *np_out = g.NP;
   return CCT_OK;
 }
