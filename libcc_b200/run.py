@@ -8,6 +8,7 @@ triples.F90:316) with the device time.
     python -m libcc_b200.run --restart triples.restart --form int8:5
     python -m libcc_b200.run --workload no24-nu320 --tuples 4      # first 4 tuples only
     python -m libcc_b200.run --workload no12-nu120 --backward      # then the adjoint pass
+    python -m libcc_b200.run --workload no24-nu320 --ccsd-terms    # the CCSD T1-dressing terms
 """
 from __future__ import annotations
 
@@ -29,7 +30,12 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--backward", action="store_true",
                     help="after the forward, run the adjoint (ccT_backward) over the same tuples")
+    ap.add_argument("--ccsd-terms", action="store_true",
+                    help="instead of (T): one call of each CCSD T1-dressing entry point (ccT_ccsd_terms_29_31, "
+                         "_32_35) on seeded device arrays of the workload's (no, nu); prints their device times")
     args = ap.parse_args(argv)
+    if args.ccsd_terms:
+        return ccsd_terms(args)
 
     from . import restart, synthetic
     from .api import TriplesPlan, format_energies
@@ -51,6 +57,37 @@ def main(argv=None) -> int:
             plan.backward(0, end)
             print(f" backward device ms={plan.last_backward_ms:.3f} "
                   f"ratio={plan.last_backward_ms / plan.last_forward_ms:.2f}")
+    return 0
+
+
+def ccsd_terms(args) -> int:
+    import ctypes
+    import torch
+    from . import _native as N, synthetic
+    if not args.workload:
+        raise SystemExit("--ccsd-terms takes --workload (its no, nu)")
+    no, nu = synthetic.WORKLOADS[args.workload]["no"], synthetic.WORKLOADS[args.workload]["nu"]
+    dev = f"cuda:{args.device}"
+    torch.cuda.set_device(args.device)
+    nutr, n4 = nu * (nu + 1) // 2, no * nu * nu * no
+    g = torch.Generator(device=dev).manual_seed(7)
+    mk = lambda n: torch.randn(n, generator=g, device=dev, dtype=torch.float64) * 0.05
+    o1, t2, vl, vr, vvvo = mk(no * nu), mk(n4), mk(n4), mk(n4), mk(nutr * nu * no)
+    o2, vm, rl = mk(n4), mk(no ** 3 * nu), torch.zeros(n4, device=dev, dtype=torch.float64)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    lib = N.load()
+    for name, call in (("29_31", lambda: lib.ccT_ccsd_terms_29_31(no, nu, vp(o1), vp(t2), vp(vl), vp(vr), vp(vvvo),
+                                                                   N.CCT_MEM_DEVICE)),
+                       ("32_35", lambda: lib.ccT_ccsd_terms_32_35(no, nu, vp(o1), vp(o2), vp(t2), vp(vm), vp(rl),
+                                                                   vp(vvvo), N.CCT_MEM_DEVICE))):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = call()
+        e1.record()
+        torch.cuda.synchronize()
+        N.check(st, "ccT_ccsd_terms_" + name)
+        print(f" no={no} nu={nu} ccsd terms {name}: {e0.elapsed_time(e1):.3f} ms (first call: includes the workspace)")
     return 0
 
 
