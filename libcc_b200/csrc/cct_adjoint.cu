@@ -542,7 +542,8 @@ __device__ __forceinline__ int swap_row(int m, int nu, float inv_nu) {
   return q * nu + p;
 }
 
-constexpr int kMaxPairs = 12;  // (slot, half) pairs of up to two tuples: at most 2 x 3 x 2
+constexpr int kMaxPairs = 6 * kDEGroup;  // (slot, half) pairs of a tuple group: at most 3 x 2 per tuple
+constexpr int kMaxOut = 3 * kDEGroup;    // distinct E slabs of a tuple group
 struct BwdPair {
   const double *A;  // dE/dX_g (nu^2 x NP)
   const double *B;  // bwd_e: F[fyz] (NP x KP); bwd_f: E[x] (nu^2 x KP)
@@ -551,8 +552,8 @@ struct BwdPair {
 };
 struct BwdEArgs {
   BwdPair pair[kMaxPairs];
-  double *out[6];
-  int first[7], npairs;  // pairs of output o are first[o] .. first[o+1]-1
+  double *out[kMaxOut];
+  int first[kMaxOut + 1], npairs;  // pairs of output o are first[o] .. first[o+1]-1
   int nu;
   int64_t NP, KP;
   int64_t KV;  // columns that are not padding: nu + no
@@ -1178,11 +1179,15 @@ int adj_tuple_gemm_e(const Dims &d, const Tuple *tu, const int *sets, int ntup, 
   const int64_t nu2 = (int64_t)nu * nu;
   auto Fyz = [&](int yz) { return F + (int64_t)yz * d.NP * d.KP; };
   // dE: outputs in order of first appearance; per output the pairs of the
-  // first tuple, then of the second, each in slot order (a fixed order)
-  std::vector<GemmPair> pairs[2];
+  // group's tuples in tuple order, each in slot order (a fixed order)
+  if (ntup < 1 || ntup > kDEGroup) {
+    set_error("adjoint: dE GEMM group size out of range");
+    return CCT_ERR_INVALID;
+  }
+  std::vector<GemmPair> pairs[kDEGroup];
   for (int u = 0; u < ntup; u++) pairs[u] = tuple_pairs(tu[u], d.no);
   BwdEArgs a{};
-  int xs[6], nx = 0;
+  int xs[kMaxOut], nx = 0;
   for (int u = 0; u < ntup; u++)
     for (const GemmPair &q : pairs[u]) {
       bool seen = false;

@@ -51,7 +51,7 @@
 // Persistent kernel, one CTA of 64 + 32 NDW threads per SM (NDW = 16 drain
 // warps at 80 registers a thread: the drain is latency-bound, and 16 warps
 // took a 3-digit tuple from 0.54 to 0.46 ms against 8 warps at 128
-// registers, with room left for a reduction CTA beside it), work items (job,
+// registers), work items (job,
 // row tile, column tile) taken round-robin with the column tile fastest, so
 // the CTAs in flight share A tiles through L2:
 //   warp 0      producer: per stage, one bulk copy of the A digits and one
@@ -88,8 +88,12 @@ constexpr int A_BLK = kEmuABlk;
 #ifndef CCT_EMU_MAXNREG
 #define CCT_EMU_MAXNREG 80
 #endif
+// Ring budget: 200 KB gives a 3-digit, 80-column tile five stages (2% faster
+// than four) and 5 digits three (5% faster than two); the reduction CTA that
+// used to fit beside the W build no longer does, which costs nothing (the two
+// kernels did not overlap usefully).
 #ifndef CCT_EMU_SMEM_BUDGET
-#define CCT_EMU_SMEM_BUDGET (180 * 1024)
+#define CCT_EMU_SMEM_BUDGET (200 * 1024)
 #endif
 constexpr int KS = CCT_EMU_KS;
 constexpr int NDW = CCT_EMU_DRAIN_WARPS;  // drain warps: NDW/4 per TMEM lane quarter

@@ -199,11 +199,19 @@ int launch_ets(const Dims &d, const double *t1, const double *v1_acc, const doub
                cudaStream_t s);
 
 // adjoint.cu: device buffers of the backward pass (allocated at the first ccT_backward)
-#ifndef CCT_GX_SETS
-#define CCT_GX_SETS 4
+// backward: the dE GEMM runs once per group of kDEGroup consecutive tuples
+// (their shared E slabs get the K of every tuple in one launch); kGXSets GX
+// sets, two groups in flight
+#ifndef CCT_DE_GROUP
+#define CCT_DE_GROUP 2
 #endif
-constexpr int kGXSets = CCT_GX_SETS;  // backward: GX sets (even: dE-GEMM tuple pairs in flight)
-static_assert(kGXSets >= 2 && kGXSets % 2 == 0, "the dE GEMM takes the GX sets of tuple pairs");
+constexpr int kDEGroup = CCT_DE_GROUP;
+#ifndef CCT_GX_SETS
+#define CCT_GX_SETS (2 * CCT_DE_GROUP)
+#endif
+constexpr int kGXSets = CCT_GX_SETS;
+static_assert(kDEGroup >= 1 && kDEGroup <= 4, "dE GEMM groups of 1 to 4 tuples");
+static_assert(kGXSets >= kDEGroup && kGXSets % kDEGroup == 0, "the dE GEMM takes the GX sets of whole groups");
 struct AdjBuffers {
   bool ready = false;
   double *dE = nullptr, *dF = nullptr;                 // gradients of the GEMM operands E, F

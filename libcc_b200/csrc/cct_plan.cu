@@ -910,7 +910,7 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2, sW));
     CCT_CUDA(cudaEventRecord(p->ev_rec[xb], sW));
     CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_rec[xb], 0));
-    if (t - begin >= kGXSets) {  // GX set read by the GEMMs of t-4
+    if (t - begin >= kGXSets) {  // GX set last read by the GEMMs of tuple t - kGXSets
       CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gx_e[set], 0));
       CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gx_f[set], 0));
     }
@@ -933,16 +933,17 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
     CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_gx_pw[set], 0));
     CCT_TRY(adj_tuple_gemm_f(d, tu, p->E, &p->adj, set, sF));
     CCT_CUDA(cudaEventRecord(p->ev_gx_f[set], sF));
-    const bool second = ((t - begin) & 1) == 1;
-    if (second || t == end - 1) {  // the dE GEMM of the pair (t-1, t), or of a last lone tuple
-      CCT_CUDA(cudaStreamWaitEvent(sG, p->ev_gx_pw[set], 0));  // also covers t-1: same stream, earlier
-      const int prev = (set + kGXSets - 1) % kGXSets;
-      const Tuple pair[2] = {second ? p->tuples[t - 1] : tu, tu};
-      const int sets[2] = {second ? prev : set, set};
-      CCT_TRY(second ? adj_tuple_gemm_e(d, pair, sets, 2, p->F, &p->adj, sG)
-                     : adj_tuple_gemm_e(d, &tu, &set, 1, p->F, &p->adj, sG));
-      CCT_CUDA(cudaEventRecord(p->ev_gx_e[set], sG));
-      if (second) CCT_CUDA(cudaEventRecord(p->ev_gx_e[prev], sG));
+    const int pos = (int)((t - begin) % kDEGroup);
+    if (pos == kDEGroup - 1 || t == end - 1) {  // the dE GEMM of the group ending at t
+      CCT_CUDA(cudaStreamWaitEvent(sG, p->ev_gx_pw[set], 0));  // also covers the group: same stream, earlier
+      Tuple group[kDEGroup];
+      int sets[kDEGroup];
+      for (int u = 0; u <= pos; u++) {
+        group[u] = p->tuples[t - pos + u];
+        sets[u] = (set + kGXSets - pos + u) % kGXSets;
+      }
+      CCT_TRY(adj_tuple_gemm_e(d, group, sets, pos + 1, p->F, &p->adj, sG));
+      for (int u = 0; u <= pos; u++) CCT_CUDA(cudaEventRecord(p->ev_gx_e[sets[u]], sG));
     }
   }
   // p->stream after every stream (red_stream already waited for rec_stream)

@@ -24,21 +24,16 @@ namespace {
 
 using namespace red;
 
-#ifndef CCT_RED_STAGED
-#define CCT_RED_STAGED 0
-#endif
-constexpr bool kStaged = CCT_RED_STAGED != 0;
 template <int KIND>
-__global__ void __launch_bounds__(RT, (kStaged && KIND == kIJK) ? 2 : 4)
-    reduce_kernel(int nu, int no, int64_t NP, TupleDev t,
+__global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t NP, TupleDev t,
                                                       const double *__restrict__ eh, const double *__restrict__ ep,
                                                       const double *__restrict__ voe,
                                                       const int16_t *__restrict__ table, double *__restrict__ xpart,
                                                       double *__restrict__ vpart) {
   extern __shared__ __align__(16) double dyn_smem[];
   const int64_t cta = blockIdx.x;
-  reduce_block<KIND, false, kStaged>(nu, no, NP, t, eh, ep, voe, table[3 * cta], table[3 * cta + 1],
-                                     table[3 * cta + 2], xpart + cta, vpart, dyn_smem);
+  reduce_block<KIND>(nu, no, NP, t, eh, ep, voe, table[3 * cta], table[3 * cta + 1], table[3 * cta + 2],
+                     xpart + cta, vpart, dyn_smem);
 }
 
 // etd_acc[0..1]: Neumaier (sum, compensation); v1_acc(nu, no).
@@ -121,7 +116,7 @@ __global__ void ets_kernel(int no, int nu, const double *__restrict__ t1, const 
 template <int KIND>
 int launch_reduce_kind(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
                        const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
-  constexpr int smem = (kStaged && KIND == kIJK) ? REDUCE_SMEM_STAGED : REDUCE_SMEM;
+  constexpr int smem = REDUCE_SMEM;
   static int configured_device = -1;
   int dev = 0;
   CCT_CUDA(cudaGetDevice(&dev));

@@ -54,9 +54,6 @@ __device__ __forceinline__ T sel3(int m, T v0, T v1, T v2) {
 constexpr int VPAIR = 2 * 6 * 64;
 __device__ __forceinline__ int nb_of(int nu) { return (nu + RB - 1) / RB; }
 constexpr int REDUCE_SMEM = (6 * SL + 3 * VPAIR) * 8;
-// i>j>k tuples with every X term staged by asynchronous copies (STAGED): the
-// second and third terms land in [2][6][SL] beside W before they are added
-constexpr int REDUCE_SMEM_STAGED = REDUCE_SMEM + 2 * 6 * SL * 8;
 
 // 8-byte global->shared copy that does not wait; ok == false stores 0.0.
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool ok) {
@@ -115,7 +112,7 @@ __device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const
 
 // COHERENT: X was written by other CTAs of the same (persistent) kernel, so it
 // is read through L2 (ld.global.cg) instead of the read-only path.
-template <int KIND, bool COHERENT = false, bool STAGED = false>
+template <int KIND, bool COHERENT = false>
 __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const TupleDev &t,
                                              const double *__restrict__ eh, const double *__restrict__ ep,
                                              const double *__restrict__ voe, const int S0, const int S1,
@@ -133,57 +130,6 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
   // ---- VOE staging: asynchronous copies, in flight during phase A's X loads
   stage_voe(nu, no, t, voe, S0, S1, S2, Vsm);
 
-  if constexpr (STAGED && !COHERENT && KIND == kIJK) {
-    // every X term in one round of asynchronous copies: term 0 straight into
-    // W, terms 1 and 2 into the staging area in their blocks' own element
-    // order; then the two are added into W, term by term
-    double *Ssm = Vsm + 3 * VPAIR;  // [2][6][SL]
-#pragma unroll
-    for (int term = 0; term < 3; term++) {
-      const double *X = term == 0 ? t.x[0] : (term == 1 ? t.x[1] : t.x[2]);
-      const int al0 = term_entry(KIND, term, 1), al1 = term_entry(KIND, term, 2), al2 = term_entry(KIND, term, 3);
-#pragma unroll
-      for (int p = 0; p < 6; p++) {
-        if (slot[p] != p) continue;
-        const int O0 = Sm(pm(p, 0)), O1 = Sm(pm(p, 1)), O2 = Sm(pm(p, 2));
-        const int Oa0 = sel3(al0, O0, O1, O2), Oa1 = sel3(al1, O0, O1, O2), Oa2 = sel3(al2, O0, O1, O2);
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int idx = tid + RT * e;
-          const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
-          const int xp = RB * Oa0 + u0, xq = RB * Oa1 + u1, xs = RB * Oa2 + u2;
-          const bool ok = xp < nu && xq < nu && xs < nu;
-          double *dst = term == 0 ? Wsm + p * SL + soff(u0, u1, u2) : Ssm + ((term - 1) * 6 + p) * SL + idx;
-          cp_async8(dst, X + (ok ? ((int64_t)xp * nu + xq) * NP + xs : 0), ok);
-        }
-      }
-    }
-    cp_async_commit();
-    cp_async_wait_all();  // VOE and all three terms
-    __syncthreads();
-#pragma unroll
-    for (int term = 1; term < 3; term++) {
-      const int al0 = term_entry(KIND, term, 1), al1 = term_entry(KIND, term, 2), al2 = term_entry(KIND, term, 3);
-#pragma unroll
-      for (int p = 0; p < 6; p++) {
-        if (slot[p] != p) continue;
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int idx = tid + RT * e;
-          const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
-          const int c0 = al0 == 0 ? u0 : (al1 == 0 ? u1 : u2);
-          const int c1 = al0 == 1 ? u0 : (al1 == 1 ? u1 : u2);
-          const int c2 = al0 == 2 ? u0 : (al1 == 2 ? u1 : u2);
-          Wsm[p * SL + soff(c0, c1, c2)] += Ssm[((term - 1) * 6 + p) * SL + idx];
-        }
-      }
-      __syncthreads();
-    }
-    if (S0 == S1 && S1 == S2 && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;  // W_aaa = 0 (ZEROT3)
-    __syncthreads();
-    reduce_block_bc<KIND>(nu, t, eh, ep, S0, S1, S2, slot, Wsm, Vsm, xpart_slot, vpart);
-    return;
-  }
 
   // ---- phase A: W on the orbit blocks, one X term at a time.  Term 0 (the
   // identity placement X0(a,b,c) for every kind) is copied straight into W
