@@ -94,6 +94,7 @@ struct ccT_plan {
   AdjBuffers adj;
   cudaStream_t bwd_stream = nullptr;   // the dF GEMMs of the backward
   cudaStream_t rec_stream = nullptr;   // the W recompute of the backward
+  cudaStream_t pw_stream = nullptr;    // the backward's pointwise chain when it runs below the GEMMs
   cudaEvent_t ev_bwdf[2] = {};
   // backward, per GX set: pointwise pass done / dE GEMM done / dF GEMM done reading it
   cudaEvent_t ev_gx_pw[kGXSets] = {}, ev_gx_e[kGXSets] = {}, ev_gx_f[kGXSets] = {};
@@ -869,12 +870,15 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   if (!p->bwd_stream) {
     // stream priorities of the backward (build constant CCT_BWD_PRIO): 0, the
     // dF GEMM and the recompute at the default priority below the pointwise
-    // chain and the dE GEMM; 1, all four at the highest priority
+    // chain and the dE GEMM; 1, all four at the highest priority; 2, the three
+    // GEMM streams at the highest priority and the pointwise chain on a
+    // stream of its own at the lowest
     int prio_least = 0, prio_greatest = 0;
     CCT_CUDA(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
-    const int prio = CCT_BWD_PRIO == 1 ? prio_greatest : 0;
+    const int prio = CCT_BWD_PRIO >= 1 ? prio_greatest : 0;
     CCT_CUDA(cudaStreamCreateWithPriority(&p->bwd_stream, cudaStreamNonBlocking, prio));
     CCT_CUDA(cudaStreamCreateWithPriority(&p->rec_stream, cudaStreamNonBlocking, prio));
+    if (CCT_BWD_PRIO == 2) CCT_CUDA(cudaStreamCreateWithPriority(&p->pw_stream, cudaStreamNonBlocking, prio_least));
     for (cudaEvent_t &e : p->ev_bwdf) CCT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (int g = 0; g < kGXSets; g++)
       for (cudaEvent_t *e : {&p->ev_gx_pw[g], &p->ev_gx_e[g], &p->ev_gx_f[g]})
@@ -899,9 +903,11 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   // written by one stream only, in tuple order, so the results stay bitwise
   // reproducible.
   CCT_TRY(fork_streams(p));
-  cudaStream_t sW = p->rec_stream, sP = p->red_stream, sG = p->gemm_stream, sF = p->bwd_stream;
+  cudaStream_t sW = p->rec_stream, sP = p->pw_stream ? p->pw_stream : p->red_stream, sG = p->gemm_stream,
+               sF = p->bwd_stream;
   CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_fork, 0));
   CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_fork, 0));
+  if (sP != p->red_stream) CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_fork, 0));
   for (int64_t t = begin; t < end; t++) {
     const Tuple &tu = p->tuples[t];
     const int set = (int)((t - begin) % kGXSets);
@@ -1171,6 +1177,7 @@ int ccT_plan_destroy(ccT_plan *p) {
   if (p->gemm_stream) cudaStreamDestroy(p->gemm_stream);
   if (p->bwd_stream) cudaStreamDestroy(p->bwd_stream);
   if (p->rec_stream) cudaStreamDestroy(p->rec_stream);
+  if (p->pw_stream) cudaStreamDestroy(p->pw_stream);
   for (cudaEvent_t e : p->ev_bwdf)
     if (e) cudaEventDestroy(e);
   for (int b = 0; b < kNBuf; b++) {
