@@ -199,6 +199,7 @@ struct EmuArgs {
   int sop;  // digit slices stored per K chunk in the operands (>= the S of the launch)
   int64_t NP;   // X row stride; columns at or past it (a partial last N tile) are not stored
   int64_t NPe;  // rows per (y,z) of the B digits and expF: tiles_n * EBN
+  int xblocked; // X in 8 x 8 x 8 blocks (xblock_base), else rows of NP
   int *err;
 };
 
@@ -490,16 +491,27 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
       __syncwarp();
       if (lane == 0) mbar_arrive(&tmem_empty[ab]);
       if (live) {
-        double *xrow = job.out + m * args.NP + n0;
         const int16_t *eB = args.expF + (int64_t)job.x3 * args.NPe + n0;
         const int e0 = eA + (H > 0 ? 2 - 7 * (sl + 1) : 0);
         auto val = [&](int j) { return (H > 0 ? cvt(acc[j]) : __longlong_as_double(acc[j])) * pow2(e0 + eB[j]); };
         // one 32-byte sector per store (a thread owns a row, so 16-byte
         // stores wrote half a sector each and doubled the write traffic)
+        if (args.xblocked) {  // a quad of columns (s % 4 == 0) stays inside one block
+          const int64_t pp = m / args.nu, qq = m - pp * args.nu;
+          double *xb = job.out + xblock_base(pp >> 3, qq >> 3, 0, args.nu, args.NP) + ((pp & 7) * 8 + (qq & 7)) * 8;
 #pragma unroll
-        for (int j = 0; j < CW; j += 4) {
-          if (n0 + j >= args.NP) break;  // NP is a multiple of 4: a quad is stored whole or not at all
-          st_global_v4(xrow + j, val(j), val(j + 1), val(j + 2), val(j + 3));
+          for (int j = 0; j < CW; j += 4) {
+            const int64_t sc = n0 + j;
+            if (sc >= args.NP) break;
+            st_global_v4(xb + (sc >> 3) * 512 + (sc & 7), val(j), val(j + 1), val(j + 2), val(j + 3));
+          }
+        } else {
+          double *xrow = job.out + m * args.NP + n0;
+#pragma unroll
+          for (int j = 0; j < CW; j += 4) {
+            if (n0 + j >= args.NP) break;  // NP is a multiple of 4: a quad is stored whole or not at all
+            st_global_v4(xrow + j, val(j), val(j + 1), val(j + 2), val(j + 3));
+          }
         }
       }
     }
@@ -692,7 +704,8 @@ __global__ void digits_f_kernel(const double *__restrict__ F, int no, int nu, in
 int g_num_sms[64] = {0};
 
 template <int S, int EBN>
-int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err, cudaStream_t s) {
+int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err, cudaStream_t s,
+                 bool blocked) {
   constexpr int smem = emu_stages<S, EBN>() * KS * S * (A_BLK + EBN * kEmuKC) + 1024;
   static int configured_device = -1;
   int dev = 0;
@@ -731,6 +744,11 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   }
   a.NP = d.NP;
   a.NPe = o.NPe;
+  a.xblocked = blocked ? 1 : 0;
+  if (blocked && d.NP % 8 != 0) {
+    set_error("blocked X needs NP a multiple of 8");
+    return CCT_ERR_INVALID;
+  }
   a.err = err;
   const int64_t items = (int64_t)njobs * a.tiles_m * a.tiles_n;
   const int grid = (int)(items < g_num_sms[dev] ? items : g_num_sms[dev]);
@@ -794,22 +812,22 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
 }
 
 int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool blocked) {
   // (digits run, N tile) pairs with digits x N <= 512 tensor-memory columns
   const int key = o.run_slices * 1000 + o.ebn;
   switch (key) {
-    case 3064: return launch_emu_s<3, 64>(o, d, jobs_dev, njobs, err, s);
-    case 3080: return launch_emu_s<3, 80>(o, d, jobs_dev, njobs, err, s);
-    case 3096: return launch_emu_s<3, 96>(o, d, jobs_dev, njobs, err, s);
-    case 4064: return launch_emu_s<4, 64>(o, d, jobs_dev, njobs, err, s);
-    case 4080: return launch_emu_s<4, 80>(o, d, jobs_dev, njobs, err, s);
-    case 4096: return launch_emu_s<4, 96>(o, d, jobs_dev, njobs, err, s);
-    case 5064: return launch_emu_s<5, 64>(o, d, jobs_dev, njobs, err, s);
-    case 5080: return launch_emu_s<5, 80>(o, d, jobs_dev, njobs, err, s);
-    case 5096: return launch_emu_s<5, 96>(o, d, jobs_dev, njobs, err, s);
-    case 6064: return launch_emu_s<6, 64>(o, d, jobs_dev, njobs, err, s);
-    case 6080: return launch_emu_s<6, 80>(o, d, jobs_dev, njobs, err, s);
-    case 7064: return launch_emu_s<7, 64>(o, d, jobs_dev, njobs, err, s);
+    case 3064: return launch_emu_s<3, 64>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 3080: return launch_emu_s<3, 80>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 3096: return launch_emu_s<3, 96>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 4064: return launch_emu_s<4, 64>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 4080: return launch_emu_s<4, 80>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 4096: return launch_emu_s<4, 96>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 5064: return launch_emu_s<5, 64>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 5080: return launch_emu_s<5, 80>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 5096: return launch_emu_s<5, 96>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 6064: return launch_emu_s<6, 64>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 6080: return launch_emu_s<6, 80>(o, d, jobs_dev, njobs, err, s, blocked);
+    case 7064: return launch_emu_s<7, 64>(o, d, jobs_dev, njobs, err, s, blocked);
     default:
       set_error("unsupported (digits, N tile) = (" + std::to_string(o.run_slices) + ", " + std::to_string(o.ebn) +
                 ")");

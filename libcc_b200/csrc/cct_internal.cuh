@@ -98,7 +98,13 @@ struct TupleDev {
   const double *x[3];   // X buffers of the tuple's GEMM jobs
   int kind, i, j, k;
   double weight;        // 1 for i>j>k, 1/2 for degenerate tuples
+  int blocked = 0;      // X in 8 x 8 x 8 blocks (emulated forward), else rows of NP
 };
+// X(p,q,s) of a blocked X buffer: block (p/8, q/8, s/8) of 512 doubles at
+// ((p/8) nbk + q/8) NP/8 + s/8, element ((p%8) 8 + q%8) 8 + s%8, nbk = ceil(nu/8)
+__host__ __device__ __forceinline__ int64_t xblock_base(int64_t P, int64_t Q, int64_t S, int nu, int64_t NP) {
+  return ((P * ((nu + 7) / 8) + Q) * (NP / 8) + S) * 512;
+}
 
 // ----------------------------------------------------------------------------- INT8 emulation
 // Digit count of the split-integer operands (7 bits each).  An automatic plan
@@ -171,8 +177,9 @@ struct EmuOperands {
 };
 
 int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOperands *o, cudaStream_t s);
+// blocked: X in 8 x 8 x 8 blocks (xblock_base; NP a multiple of 8), else rows of NP
 int launch_wbuild_emu(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, int njobs, int *err,
-                      cudaStream_t s);
+                      cudaStream_t s, bool blocked = false);
 
 // ----------------------------------------------------------------------------- launchers
 // layout.cu

@@ -42,6 +42,11 @@ using namespace cct;
 // X buffer sets: the W-build of tuple t may run while the reductions of
 // tuples t-1 .. t-kNBuf+1 are still reading theirs.
 constexpr int kNBuf = 3;
+// emulated forwards store X in 8 x 8 x 8 blocks (build constant CCT_X_BLOCKED)
+#ifndef CCT_X_BLOCKED
+#define CCT_X_BLOCKED 1
+#endif
+constexpr bool kXBlocked = CCT_X_BLOCKED != 0;
 #ifndef CCT_BWD_PRIO
 #define CCT_BWD_PRIO 0
 #endif
@@ -336,12 +341,14 @@ int join_streams(ccT_plan *p) {
 // The W-build GEMMs of tuple tix into X buffer b on stream st: the plan's
 // own form, or the FP64 kernel when fp64 is set (emulated plans keep the FP64
 // jobs for the backward's recompute and the digit calibration).
-int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st) {
+// An emulated W build stores X in 8 x 8 x 8 blocks for the reduction
+// (blocked), or in rows of NP (ccT_tuple_w, whose W assembly reads rows).
+int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st, bool blocked = kXBlocked) {
   const Tuple &t = p->tuples[tix];
   const int njobs = t.kind == kIJK ? 3 : 2;
   const int64_t ntup = (int64_t)p->tuples.size();
   if (p->emulated && !fp64)
-    return launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1, st);
+    return launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * (b * ntup + tix), njobs, p->flags + 1, st, blocked);
   return launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, st);
 }
 
@@ -367,6 +374,7 @@ int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
   td.j = t.j;
   td.k = t.k;
   td.weight = t.kind == kIJK ? 1.0 : 0.5;
+  td.blocked = p->emulated && !fp64 && kXBlocked ? 1 : 0;
   CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE, p->red_stream));
   CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->red_stream));
   CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->red_stream));
@@ -641,7 +649,8 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     return fail(s);
   for (int b = 0; b < kNBuf; b++)
     for (int g = 0; g < 3; g++)
-      if ((s = dalloc(&p->X[b][g], nu2 * d.NP))) return fail(s);
+      if ((s = dalloc(&p->X[b][g], (p->emulated && kXBlocked ? round_up(nu, kRB) * round_up(nu, kRB) : nu2) * d.NP)))
+        return fail(s);
   if (p->emulated) {
     EmuOperands &e = p->emu;
     e.slices = o.emu_slices ? o.emu_slices : kEmuMaxSlices;
@@ -1054,7 +1063,7 @@ int ccT_tuple_w(ccT_plan *p, int64_t tuple, double *w, int32_t mem) {
     s = packed_schedule(p, tuple, tuple + 1, &fills);
     if (s == CCT_OK) s = packed_fill(p, fills[0], p->stream);
   }
-  if (s == CCT_OK) s = wbuild_tuple(p, tuple, 0, false, p->stream);
+  if (s == CCT_OK) s = wbuild_tuple(p, tuple, 0, false, p->stream, false);  // rows of NP, as the assembly reads
   if (s == CCT_OK) s = assemble_w_fortran(p->d, p->tuples[tuple], p->X[0], wc, wf, p->stream);
   int werr = 0;
   if (s == CCT_OK && cudaMemcpyAsync(&werr, p->flags + 1, 4, cudaMemcpyDeviceToHost, p->stream) != cudaSuccess)
@@ -1107,7 +1116,8 @@ int ccT_time_wbuild(ccT_plan *p, int64_t tuple, int32_t reps, double *ms_per_lau
     CCT_TRY(packed_fill(p, fills[0], p->gemm_stream));
   }
   auto launch = [&]() {
-    return p->emulated ? launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * tuple, njobs, p->flags + 1, p->gemm_stream)
+    return p->emulated ? launch_wbuild_emu(p->emu, p->d, p->emu_jobs + 3 * tuple, njobs, p->flags + 1, p->gemm_stream,
+                                           kXBlocked)
                        : launch_wbuild_f64(p->d, p->jobs + 3 * tuple, njobs, p->gemm_stream);
   };
   CCT_TRY(launch());  // warm

@@ -152,7 +152,8 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
           const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
           const int xp = RB * O0 + u0, xq = RB * O1 + u1, xs = RB * O2 + u2;
           const bool ok = xp < nu && xq < nu && xs < nu;
-          cp_async8(Wsm + p * SL + soff(u0, u1, u2), X + (ok ? ((int64_t)xp * nu + xq) * NP + xs : 0), ok);
+          const int64_t off = t.blocked ? xblock_base(O0, O1, O2, nu, NP) + idx : ((int64_t)xp * nu + xq) * NP + xs;
+          cp_async8(Wsm + p * SL + soff(u0, u1, u2), X + (ok ? off : 0), ok);
         }
       }
       cp_async_commit();
@@ -171,7 +172,8 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
         const int xp = RB * Oa0 + u0, xq = RB * Oa1 + u1, xs = RB * Oa2 + u2;
         double v = 0.0;
         if (live && xp < nu && xq < nu && xs < nu) {
-          const double *src = X + ((int64_t)xp * nu + xq) * NP + xs;
+          const double *src = X + (t.blocked ? xblock_base(Oa0, Oa1, Oa2, nu, NP) + idx
+                                             : ((int64_t)xp * nu + xq) * NP + xs);
           v = COHERENT ? __ldcg(src) : __ldg(src);
         }
         xv[2 * p + e] = v;
