@@ -69,6 +69,8 @@
 // Every mbarrier wait is bounded and also ends when another role aborted; a
 // timeout sets the error word, the producer waits for its copies in flight,
 // the issuer for its MMAs, and the CTA frees its tensor memory and returns.
+#include <type_traits>
+
 #include "cct_internal.cuh"
 
 namespace cct {
@@ -372,26 +374,41 @@ __global__ void __maxnreg__(CCT_EMU_MAXNREG) wbuild_emu_kernel(const EmuArgs arg
                     "r"(t > 0 ? 1u : first));
               };
               // t = 0 first: with the accumulate flag clear it initialises
-              // every diagonal of the item; later rows add into them.  An item
-              // with every digit (the usual case) takes a schedule fixed at
-              // compile time: straight-line MMAs with constant shapes and
-              // offsets, so the single issuing thread spends no time on the
-              // partition arithmetic between MMAs.
-              if (sl == S) {
+              // every diagonal of the item; later rows add into them.  Each
+              // digit count has a schedule fixed at compile time:
+              // straight-line MMAs with constant shapes and offsets, so the
+              // single issuing thread spends no time on the partition
+              // arithmetic between MMAs.  A slice t meets n = s - t B slices,
+              // taken as MMAs of at most MPS slices whose sizes differ by one.
+              auto schedule = [&](auto slc) {
+                constexpr int SLC = decltype(slc)::value;
 #pragma unroll
-                for (int t = 0; t < S; t++) {
-                  const int n = S - t;
+                for (int t = 0; t < SLC; t++) {
+                  const int n = SLC - t;
                   const int parts = (n + MPS - 1) / MPS;
                   const int base = n / parts, extra = n - base * parts;
 #pragma unroll
                   for (int q = 0; q < parts; q++) mma(t, q * base + (q < extra ? q : extra), base + (q < extra ? 1 : 0));
                 }
+              };
+              if constexpr (EBN <= 80) {
+                switch (sl) {
+                  case 1: schedule(std::integral_constant<int, 1>{}); break;
+                  case 2: if constexpr (S >= 2) schedule(std::integral_constant<int, 2>{}); break;
+                  case 3: if constexpr (S >= 3) schedule(std::integral_constant<int, 3>{}); break;
+                  case 4: if constexpr (S >= 4) schedule(std::integral_constant<int, 4>{}); break;
+                  case 5: if constexpr (S >= 5) schedule(std::integral_constant<int, 5>{}); break;
+                  case 6: if constexpr (S >= 6) schedule(std::integral_constant<int, 6>{}); break;
+                  default: if constexpr (S >= 7) schedule(std::integral_constant<int, 7>{}); break;
+                }
+              } else if (sl == S) {  // the 96-column tile: one fixed schedule (more would spill)
+                schedule(std::integral_constant<int, S>{});
               } else {
 #pragma unroll
                 for (int t = 0; t < S; t++) {
                   if (t >= sl) break;
-                  const int n = sl - t;                       // B slices this A slice meets
-                  const int parts = (n + MPS - 1) / MPS;      // MMAs of at most MPS slices, sizes within one
+                  const int n = sl - t;
+                  const int parts = (n + MPS - 1) / MPS;
                   const int base = n / parts, extra = n - base * parts;
                   int u0 = 0;
                   for (int q = 0; q < parts; q++) {
