@@ -47,6 +47,10 @@ constexpr int kNBuf = 3;
 #define CCT_X_BLOCKED 1
 #endif
 constexpr bool kXBlocked = CCT_X_BLOCKED != 0;
+#ifndef CCT_SERIAL_REDUCE
+#define CCT_SERIAL_REDUCE 0
+#endif
+constexpr bool kSerialReduce = CCT_SERIAL_REDUCE != 0;
 #ifndef CCT_BWD_PRIO
 #define CCT_BWD_PRIO 0
 #endif
@@ -365,6 +369,11 @@ int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
   CCT_TRY(prof_mark(p, -1, p->gemm_stream));
   CCT_CUDA(cudaEventRecord(p->ev_gemm[b], p->gemm_stream));
   CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_gemm[b], 0));
+  // emulated W builds fill every SM's shared memory, so the reduction cannot
+  // run beside them; with CCT_SERIAL_REDUCE it is queued on the W-build
+  // stream itself (the reduction stream then only joins)
+  cudaStream_t rs = p->red_stream;
+  if (kSerialReduce && p->emulated && !fp64) rs = p->gemm_stream;
   TupleDev td;
   td.x[0] = p->X[b][0];
   td.x[1] = p->X[b][1];
@@ -375,11 +384,12 @@ int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
   td.k = t.k;
   td.weight = t.kind == kIJK ? 1.0 : 0.5;
   td.blocked = p->emulated && !fp64 && kXBlocked ? 1 : 0;
-  CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE, p->red_stream));
-  CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, p->red_stream));
-  CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), p->red_stream));
-  CCT_TRY(prof_mark(p, -1, p->red_stream));
-  CCT_CUDA(cudaEventRecord(p->ev_red[b], p->red_stream));
+  CCT_TRY(prof_mark(p, CCT_KERNEL_REDUCE, rs));
+  CCT_TRY(launch_reduce(p->d, td, p->eh, p->ep, p->voe, p->cta_table, p->xpart, p->vpart, rs));
+  CCT_TRY(launch_finalize(p->d, td, p->xpart, p->vpart, p->acc, v1_acc(p), rs));
+  CCT_TRY(prof_mark(p, -1, rs));
+  CCT_CUDA(cudaEventRecord(p->ev_red[b], rs));
+  if (rs != p->red_stream) CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_red[b], 0));
   p->last_launches += 3;
   return CCT_OK;
 }
