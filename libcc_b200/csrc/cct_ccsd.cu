@@ -41,10 +41,6 @@
 namespace cct {
 namespace {
 
-__device__ __forceinline__ int64_t tri_at(int64_t a, int64_t b) {
-  const int64_t I = a > b ? a : b, J = a > b ? b : a;  // packed a >= b triangle, row-major (CPYTSQ)
-  return I * (I + 1) / 2 + J;
-}
 
 int grid_of(int64_t n) {
   int64_t b = (n + 255) / 256;
