@@ -46,8 +46,7 @@ __device__ __forceinline__ T sel3(int m, T v0, T v1, T v2) {
   return m == 0 ? v0 : (m == 1 ? v1 : v2);
 }
 
-// VOE staging: three block pairs x two orientations x 64 entries x six planes
-// (planes fastest, so an element's six values are three 16-byte loads):
+// VOE staging: three block pairs x two orientations x six planes x 64 entries:
 // pair 0 (b,c), 1 (a,c), 2 (a,b); orientation 0 holds VOE(lo, hi, y, z) of the
 // pair's lower and higher coordinates, orientation 1 VOE(hi, lo, y, z); planes
 // 0..5 = (y,z) = (j,k) (k,j) (i,k) (k,i) (i,j) (j,i).  Every element reads the
@@ -92,8 +91,7 @@ __device__ __forceinline__ void stage_voe(int nu, int no, const TupleDev &t, con
     const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
     const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
     const bool ok = f < nu && s2 < nu;
-    cp_async8(Vsm + pr * VPAIR + orient * 384 + r * 6 + plane,
-              voe + (ok ? ((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2 : 0), ok);
+    cp_async8(Vsm + q, voe + (ok ? ((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2 : 0), ok);
   }
   cp_async_commit();
 }
@@ -245,8 +243,8 @@ __device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const
       w[p] = Wsm[slot[p] * SL + soff(lc[pm(p, 0)], lc[pm(p, 1)], lc[pm(p, 2)])];
     const double dinv = mult * __drcp_rn(dijk - (ep[a] + ep[b] + ep[c]));
     // VOE entry offsets of the three index pairs: (lo, hi) in orientation 0, (hi, lo) in 1
-    const int rp[3] = {(l1 + 8 * l2) * 6, (l0 + 8 * l2) * 6, (l0 + 8 * l1) * 6};
-    const int rpT[3] = {384 + (l2 + 8 * l1) * 6, 384 + (l2 + 8 * l0) * 6, 384 + (l1 + 8 * l0) * 6};
+    const int rp[3] = {l1 + 8 * l2, l0 + 8 * l2, l0 + 8 * l1};
+    const int rpT[3] = {384 + l2 + 8 * l1, 384 + l2 + 8 * l0, 384 + l1 + 8 * l0};
 #pragma unroll
     for (int pi = 0; pi < 6; pi++) {
       // element pi(x); its role values: abc acb bac bca cab cba
@@ -264,11 +262,10 @@ __device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const
       const int first = pm(pi, 0);
       const int pr = first;                         // pair index = the coordinate left out
       const bool flip = pm(pi, 1) > pm(pi, 2);  // the element's (second, third) = (hi, lo)
-      const double2 *v = reinterpret_cast<const double2 *>(Vsm + pr * VPAIR + (flip ? rpT[pr] : rp[pr]));
-      const double2 v01 = v[0], v23 = v[1], v45 = v[2];  // planes (j,k) (k,j) | (i,k) (k,i) | (i,j) (j,i)
-      const double ci = (z1 * v01.x + z2 * v01.y) * dinv;
-      const double cj = (z3 * v23.x + z5 * v23.y) * dinv;
-      const double ck = (z4 * v45.x + z6 * v45.y) * dinv;
+      const double *v = Vsm + pr * VPAIR + (flip ? rpT[pr] : rp[pr]);
+      const double ci = (z1 * v[0] + z2 * v[64]) * dinv;
+      const double cj = (z3 * v[128] + z5 * v[192]) * dinv;
+      const double ck = (z4 * v[256] + z6 * v[320]) * dinv;
       if (first == 0) {
         accA[0] += ci; accA[1] += cj; accA[2] += ck;
       } else if (first == 1) {
