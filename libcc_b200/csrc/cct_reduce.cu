@@ -24,7 +24,7 @@ namespace {
 
 using namespace red;
 
-template <int KIND>
+template <int KIND, bool BLOCKED>
 __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t NP, TupleDev t,
                                                       const double *__restrict__ eh, const double *__restrict__ ep,
                                                       const double *__restrict__ voe,
@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t N
                                                       double *__restrict__ vpart) {
   extern __shared__ __align__(16) double dyn_smem[];
   const int64_t cta = blockIdx.x;
-  reduce_block<KIND>(nu, no, NP, t, eh, ep, voe, table[3 * cta], table[3 * cta + 1], table[3 * cta + 2],
+  reduce_block<KIND, false, BLOCKED>(nu, no, NP, t, eh, ep, voe, table[3 * cta], table[3 * cta + 1], table[3 * cta + 2],
                      xpart + cta, vpart, dyn_smem);
 }
 
@@ -113,7 +113,7 @@ __global__ void ets_kernel(int no, int nu, const double *__restrict__ t1, const 
 
 }  // namespace
 
-template <int KIND>
+template <int KIND, bool BLOCKED>
 int launch_reduce_kind(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
                        const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
   constexpr int smem = REDUCE_SMEM;
@@ -121,21 +121,35 @@ int launch_reduce_kind(const Dims &d, const TupleDev &t, const double *eh, const
   int dev = 0;
   CCT_CUDA(cudaGetDevice(&dev));
   if (configured_device != dev) {
-    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CCT_CUDA(cudaFuncSetAttribute(reduce_kernel<KIND, BLOCKED>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   cudaSharedmemCarveoutMaxShared));
     configured_device = dev;
   }
-  reduce_kernel<KIND><<<(unsigned)d.ncta, RT, smem, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart, vpart);
+  reduce_kernel<KIND, BLOCKED>
+      <<<(unsigned)d.ncta, RT, smem, s>>>(d.nu, d.no, d.NP, t, eh, ep, voe, cta_table, xpart, vpart);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
 
+template <bool BLOCKED>
+int launch_reduce_layout(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
+                         const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
+  if (t.kind == kIJK) return launch_reduce_kind<kIJK, BLOCKED>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+  if (t.kind == kIJJ) return launch_reduce_kind<kIJJ, BLOCKED>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+  return launch_reduce_kind<kIIJ, BLOCKED>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+}
+
 int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const double *ep, const double *voe,
                   const int16_t *cta_table, double *xpart, double *vpart, cudaStream_t s) {
-  if (t.kind == kIJK) return launch_reduce_kind<kIJK>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
-  if (t.kind == kIJJ) return launch_reduce_kind<kIJJ>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
-  return launch_reduce_kind<kIIJ>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+  if (t.blocked) {
+    if (d.NP % RB) {
+      set_error("blocked X needs NP a multiple of 8 (NP = " + std::to_string(d.NP) + ")");
+      return CCT_ERR_INVALID;
+    }
+    return launch_reduce_layout<true>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
+  }
+  return launch_reduce_layout<false>(d, t, eh, ep, voe, cta_table, xpart, vpart, s);
 }
 
 int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const double *vpart, double *etd_acc,

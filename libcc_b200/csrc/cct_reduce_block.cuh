@@ -48,9 +48,12 @@ __device__ __forceinline__ T sel3(int m, T v0, T v1, T v2) {
 
 // VOE staging: three block pairs x two orientations x six planes x 64 entries:
 // pair 0 (b,c), 1 (a,c), 2 (a,b); orientation 0 holds VOE(lo, hi, y, z) of the
-// pair's lower and higher coordinates, orientation 1 VOE(hi, lo, y, z); planes
-// 0..5 = (y,z) = (j,k) (k,j) (i,k) (k,i) (i,j) (j,i).  Every element reads the
-// VOE entries t1wt3.f90:80-85 name, so no symmetry of VOE is assumed.
+// pair's lower and higher coordinates, orientation 1 VOE(hi, lo, y, z).  The
+// copies bring planes (y,z) = (j,k) (k,j) | (i,k) (k,i) | (i,j) (j,i) -- three
+// plane pairs (P, P') -- and combine_voe replaces each pair by
+// (2P - P', P - 2P'), the two combinations the v1 sums of t1wt3.f90:80-85
+// take of it once Z1..Z6 are written as differences of W.  Every element reads
+// the VOE entries those lines name, so no symmetry of VOE is assumed.
 constexpr int VPAIR = 2 * 6 * 64;
 __device__ __forceinline__ int nb_of(int nu) { return (nu + RB - 1) / RB; }
 constexpr int REDUCE_SMEM = (6 * SL + 3 * VPAIR) * 8;
@@ -77,23 +80,47 @@ __device__ __forceinline__ void orbit_slots(int S0, int S1, int S2, int slot[6])
   }
 }
 
-// VOE staging as asynchronous 8-byte copies (one commit group).
+// VOE staging as asynchronous 8-byte copies (one commit group).  A thread
+// copies both planes of a plane pair (1152 pairs, five rounds), so after its
+// own wait it can combine them (combine_voe) without a barrier.
+constexpr int VOE_PAIRS = 3 * 2 * 3 * 64;
+__device__ __forceinline__ double *voe_pair_slot(double *Vsm, int pq) {
+  const int pr = pq / 384, orient = (pq / 192) & 1, k = (pq >> 6) % 3, r = pq & 63;
+  return Vsm + pr * VPAIR + orient * 384 + 2 * k * 64 + r;
+}
 __device__ __forceinline__ void stage_voe(int nu, int no, const TupleDev &t, const double *__restrict__ voe, int S0,
                                           int S1, int S2, double *Vsm) {
   const int tid = threadIdx.x;
   const int64_t nu2 = (int64_t)nu * nu;
 #pragma unroll
-  for (int it = 0; it < 3 * VPAIR / RT; it++) {
-    const int q = tid + RT * it;
-    const int pr = q / VPAIR, orient = (q / 384) & 1, plane = (q / 64) % 6, r = q & 63;
+  for (int it = 0; it < (VOE_PAIRS + RT - 1) / RT; it++) {
+    const int pq = tid + RT * it;
+    if (pq >= VOE_PAIRS) break;
+    const int pr = pq / 384, orient = (pq / 192) & 1, k = (pq >> 6) % 3, r = pq & 63;
     const int Blo = pr == 0 ? S1 : S0, Bhi = pr == 2 ? S1 : S2;  // (b,c), (a,c), (a,b)
     const int f = RB * (orient ? Bhi : Blo) + (r & 7), s2 = RB * (orient ? Blo : Bhi) + (r >> 3);
-    const int px = plane == 0 ? t.j : plane == 1 ? t.k : plane == 2 ? t.i : plane == 3 ? t.k : plane == 4 ? t.i : t.j;
-    const int py = plane == 0 ? t.k : plane == 1 ? t.j : plane == 2 ? t.k : plane == 3 ? t.i : plane == 4 ? t.j : t.i;
+    const int y = k == 0 ? t.j : t.i, z = k == 2 ? t.j : t.k;  // plane 2k = (y,z), plane 2k+1 = (z,y)
     const bool ok = f < nu && s2 < nu;
-    cp_async8(Vsm + q, voe + (ok ? ((int64_t)py * no + px) * nu2 + f + (int64_t)nu * s2 : 0), ok);
+    const int64_t e = f + (int64_t)nu * s2;
+    double *dst = voe_pair_slot(Vsm, pq);
+    cp_async8(dst, voe + (ok ? ((int64_t)z * no + y) * nu2 + e : 0), ok);
+    cp_async8(dst + 64, voe + (ok ? ((int64_t)y * no + z) * nu2 + e : 0), ok);
   }
   cp_async_commit();
+}
+
+// After the thread's own copies completed: (P, P') -> (2P - P', P - 2P').
+__device__ __forceinline__ void combine_voe(double *Vsm) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (VOE_PAIRS + RT - 1) / RT; it++) {
+    const int pq = tid + RT * it;
+    if (pq >= VOE_PAIRS) break;
+    double *v = voe_pair_slot(Vsm, pq);
+    const double P = v[0], Q = v[64];
+    v[0] = fma(2.0, P, -Q);
+    v[64] = fma(-2.0, Q, P);
+  }
 }
 
 template <int KIND>
@@ -112,7 +139,11 @@ __device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const
 
 // COHERENT: X was written by other CTAs of the same (persistent) kernel, so it
 // is read through L2 (ld.global.cg) instead of the read-only path.
-template <int KIND, bool COHERENT = false>
+// BLOCKED: X in 8 x 8 x 8 blocks (xblock_base), allocated whole for every block
+// of round_up(nu, 8)^2 x NP, so every element of a block is read without a
+// bounds check: entries of indices >= nu land in W entries that phase B never
+// reads (it evaluates only elements whose three indices are < nu).
+template <int KIND, bool COHERENT = false, bool BLOCKED = false>
 __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const TupleDev &t,
                                              const double *__restrict__ eh, const double *__restrict__ ep,
                                              const double *__restrict__ voe, const int S0, const int S1,
@@ -151,8 +182,8 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
           const int idx = tid + RT * e;
           const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;
           const int xp = RB * O0 + u0, xq = RB * O1 + u1, xs = RB * O2 + u2;
-          const bool ok = xp < nu && xq < nu && xs < nu;
-          const int64_t off = t.blocked ? xblock_base(O0, O1, O2, nu, NP) + idx : ((int64_t)xp * nu + xq) * NP + xs;
+          const bool ok = BLOCKED || (xp < nu && xq < nu && xs < nu);
+          const int64_t off = BLOCKED ? xblock_base(O0, O1, O2, nu, NP) + idx : ((int64_t)xp * nu + xq) * NP + xs;
           cp_async8(Wsm + p * SL + soff(u0, u1, u2), X + (ok ? off : 0), ok);
         }
       }
@@ -171,9 +202,9 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
         const int u2 = idx & 7, u1 = (idx >> 3) & 7, u0 = idx >> 6;  // u2: contiguous X index
         const int xp = RB * Oa0 + u0, xq = RB * Oa1 + u1, xs = RB * Oa2 + u2;
         double v = 0.0;
-        if (live && xp < nu && xq < nu && xs < nu) {
-          const double *src = X + (t.blocked ? xblock_base(Oa0, Oa1, Oa2, nu, NP) + idx
-                                             : ((int64_t)xp * nu + xq) * NP + xs);
+        if (live && (BLOCKED || (xp < nu && xq < nu && xs < nu))) {
+          const double *src = X + (BLOCKED ? xblock_base(Oa0, Oa1, Oa2, nu, NP) + idx
+                                           : ((int64_t)xp * nu + xq) * NP + xs);
           v = COHERENT ? __ldcg(src) : __ldg(src);
         }
         xv[2 * p + e] = v;
@@ -204,6 +235,7 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
     __syncthreads();
   }
   cp_async_wait_all();  // VOE staging (and term 0 when it went asynchronously)
+  combine_voe(Vsm);     // this thread's own plane pairs
   if (S0 == S1 && S1 == S2 && tid < RB) Wsm[soff(tid, tid, tid)] = 0.0;  // W_aaa = 0 (ZEROT3)
   __syncthreads();
 
@@ -242,36 +274,62 @@ __device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const
     for (int p = 0; p < 6; p++)
       w[p] = Wsm[slot[p] * SL + soff(lc[pm(p, 0)], lc[pm(p, 1)], lc[pm(p, 2)])];
     const double dinv = mult * __drcp_rn(dijk - (ep[a] + ep[b] + ep[c]));
+    // E[4] of the six elements: sum_pi W_pi (8 W_pi - 4 (sum over the three
+    // transposed roles) + 2 (the two cyclic roles)).  Transpositions flip the
+    // parity of the permutation, cycles keep it, so with Ev / Od the sums of
+    // W over the even / odd permutations this is
+    //   6 sum_even (W - Ev/3)^2 + 6 sum_odd (W - Od/3)^2 + 4 (Ev - Od)^2.
+    const double Ev = w[0] + w[3] + w[4], Od = w[1] + w[2] + w[5];
+    const double e3 = Ev * (1.0 / 3.0), o3 = Od * (1.0 / 3.0);
+    const double r0 = w[0] - e3, r3 = w[3] - e3, r4 = w[4] - e3;
+    const double r1 = w[1] - o3, r2 = w[2] - o3, r5 = w[5] - o3;
+    const double sq = fma(r5, r5, fma(r4, r4, fma(r3, r3, fma(r2, r2, fma(r1, r1, r0 * r0)))));
+    const double g = Ev - Od;
+    x3 = fma(fma(6.0, sq, 4.0 * (g * g)), dinv, x3);
+    // v1: with d1 = W_abc - W_bac, d2 = W_bca - W_acb, d3 = W_cba - W_cab of
+    // the element (each an even minus an odd permutation, D below),
+    //   Z1 V0 + Z2 V1 = d1 (2V0 - V1) + d2 (V0 - 2V1)
+    //   Z3 V2 + Z5 V3 = -d1 (2V2 - V3) + d3 (V2 - 2V3)
+    //   Z4 V4 + Z6 V5 = d2 (2V4 - V5) - d3 (V4 - 2V5)
+    // and the VOE combinations are staged (combine_voe).
+    double D[3][3];  // D[e][o] = W(even perm e) - W(odd perm o), evens 0 3 4, odds 1 2 5
+#pragma unroll
+    for (int ie = 0; ie < 3; ie++)
+#pragma unroll
+      for (int io = 0; io < 3; io++) D[ie][io] = w[ie == 0 ? 0 : ie + 2] - w[io == 2 ? 5 : io + 1];
+    auto diff = [&](int x, int y) {  // W_x - W_y for permutations of opposite parity
+      const bool xe = x == 0 || x == 3 || x == 4;
+      const int e = xe ? x : y, o = xe ? y : x;
+      const double v = D[e == 0 ? 0 : e - 2][o == 5 ? 2 : o - 1];
+      return xe ? v : -v;
+    };
     // VOE entry offsets of the three index pairs: (lo, hi) in orientation 0, (hi, lo) in 1
     const int rp[3] = {l1 + 8 * l2, l0 + 8 * l2, l0 + 8 * l1};
     const int rpT[3] = {384 + l2 + 8 * l1, 384 + l2 + 8 * l0, 384 + l1 + 8 * l0};
 #pragma unroll
-    for (int pi = 0; pi < 6; pi++) {
-      // element pi(x); its role values: abc acb bac bca cab cba
-      const double wabc = w[compose(pi, 0)], wacb = w[compose(pi, 1)], wbac = w[compose(pi, 2)];
-      const double wbca = w[compose(pi, 3)], wcab = w[compose(pi, 4)], wcba = w[compose(pi, 5)];
-      x3 += wabc * (8.0 * wabc - 4.0 * (wacb + wcba + wbac) + 2.0 * (wbca + wcab)) * dinv;
-      const double z1 = (wabc - wbac) * 2.0 - wacb + wbca;
-      const double z2 = (wacb - wbca) * 2.0 - wabc + wbac;
-      const double z3 = (wbac - wabc) * 2.0 - wcab + wcba;
-      const double z4 = (wbca - wacb) * 2.0 - wcba + wcab;
-      const double z5 = (wcab - wcba) * 2.0 - wbac + wabc;
-      const double z6 = (wcba - wcab) * 2.0 - wbca + wacb;
-      // the element's first index is x_{pm(pi,0)}; its (second, third) pair is the
-      // other two coordinates, in order (pm(pi,1), pm(pi,2))
-      const int first = pm(pi, 0);
-      const int pr = first;                         // pair index = the coordinate left out
-      const bool flip = pm(pi, 1) > pm(pi, 2);  // the element's (second, third) = (hi, lo)
-      const double *v = Vsm + pr * VPAIR + (flip ? rpT[pr] : rp[pr]);
-      const double ci = (z1 * v[0] + z2 * v[64]) * dinv;
-      const double cj = (z3 * v[128] + z5 * v[192]) * dinv;
-      const double ck = (z4 * v[256] + z6 * v[320]) * dinv;
+    for (int first = 0; first < 3; first++) {
+      // the two elements whose first index is x_first: pi = 2 first (second <
+      // third, orientation 0) and 2 first + 1 (orientation 1); their VOE pair is
+      // the other two coordinates
+      double ci = 0.0, cj = 0.0, ck = 0.0;
+#pragma unroll
+      for (int flip = 0; flip < 2; flip++) {
+        const int pi = 2 * first + flip;
+        const double d1 = diff(compose(pi, 0), compose(pi, 2));
+        const double d2 = diff(compose(pi, 3), compose(pi, 1));
+        const double d3 = diff(compose(pi, 5), compose(pi, 4));
+        const double *v = Vsm + first * VPAIR + (flip ? rpT[first] : rp[first]);
+        ci = fma(d1, v[0 * 64], fma(d2, v[1 * 64], ci));
+        cj = fma(-d1, v[2 * 64], fma(d3, v[3 * 64], cj));
+        ck = fma(d2, v[4 * 64], fma(-d3, v[5 * 64], ck));
+      }
       if (first == 0) {
-        accA[0] += ci; accA[1] += cj; accA[2] += ck;
+        accA[0] = fma(ci, dinv, accA[0]); accA[1] = fma(cj, dinv, accA[1]); accA[2] = fma(ck, dinv, accA[2]);
       } else if (first == 1) {
-        accB[0] += ci; accB[1] += cj; accB[2] += ck;
+        accB[0] = fma(ci, dinv, accB[0]); accB[1] = fma(cj, dinv, accB[1]); accB[2] = fma(ck, dinv, accB[2]);
       } else {
-        accC[e][0] += ci; accC[e][1] += cj; accC[e][2] += ck;
+        accC[e][0] = fma(ci, dinv, accC[e][0]); accC[e][1] = fma(cj, dinv, accC[e][1]);
+        accC[e][2] = fma(ck, dinv, accC[e][2]);
       }
     }
   }
