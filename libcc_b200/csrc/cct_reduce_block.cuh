@@ -12,12 +12,16 @@ namespace red {
 constexpr int RB = kRB;  // 8
 constexpr int RT = 256;  // threads per reduction CTA
 constexpr int SL = 512;  // doubles per 8x8x8 block in smem
-// Element (l0, l1, l2) of a block: unpadded, with l0 XOR-ed by (l1 + l2) mod 8.
-// The term stores of phase A and the orbit reads of phase B put two
-// lane-varying coordinates on different axes; the XOR spreads every such pair
-// over distinct 8-byte bank pairs of a half-warp (a padded layout with strides
-// 1, 9, 81 left the pairs on axes 0 and 2 two-way conflicted).
-__host__ __device__ constexpr int soff(int l0, int l1, int l2) { return (l0 ^ ((l1 + l2) & 7)) + 8 * l1 + 64 * l2; }
+// Element (l0, l1, l2) of a block in shared memory, unpadded.  The term stores
+// of phase A and the orbit reads of phase B give a half-warp one coordinate
+// with eight values and another with two (2h, 2h+1) on any two of the three
+// axes.  The bank pair (word mod 16) is, in bits, l0 ^ (l1 & 6) ^ l2 and
+// (l1 ^ l2) & 1: for every ordered pair of axes the four varying bits map to
+// it one to one, so none of those accesses has a bank conflict (an XOR of l0
+// with l1 + l2 left the pairs on axes (0, 2) and (1, 2) two-way conflicted).
+__host__ __device__ constexpr int soff(int l0, int l1, int l2) {
+  return 64 * l2 + 8 * (l1 ^ (l2 & 1)) + (l0 ^ (l1 & 6) ^ l2);
+}
 
 // The six permutations of three positions, in a fixed order:
 // 0:(0,1,2)=abc 1:(0,2,1)=acb 2:(1,0,2)=bac 3:(1,2,0)=bca 4:(2,0,1)=cab 5:(2,1,0)=cba
@@ -84,9 +88,14 @@ __device__ __forceinline__ void orbit_slots(int S0, int S1, int S2, int slot[6])
 // copies both planes of a plane pair (1152 pairs, five rounds), so after its
 // own wait it can combine them (combine_voe) without a barrier.
 constexpr int VOE_PAIRS = 3 * 2 * 3 * 64;
+// Entry r = u + 8 v holds VOE(lo + u, hi + v) in orientation 0 and
+// VOE(hi + u, lo + v) in orientation 1 (u, v < 8); orientation 1 keeps it at
+// (u ^ v) + 8 v, so its reads, which vary v across a half-warp, fall on
+// distinct bank pairs.
+__device__ __forceinline__ int voe_entry(int orient, int u, int v) { return (orient ? u ^ v : u) + 8 * v; }
 __device__ __forceinline__ double *voe_pair_slot(double *Vsm, int pq) {
   const int pr = pq / 384, orient = (pq / 192) & 1, k = (pq >> 6) % 3, r = pq & 63;
-  return Vsm + pr * VPAIR + orient * 384 + 2 * k * 64 + r;
+  return Vsm + pr * VPAIR + orient * 384 + 2 * k * 64 + voe_entry(orient, r & 7, r >> 3);
 }
 __device__ __forceinline__ void stage_voe(int nu, int no, const TupleDev &t, const double *__restrict__ voe, int S0,
                                           int S1, int S2, double *Vsm) {
@@ -305,7 +314,7 @@ __device__ __forceinline__ void reduce_block_bc(int nu, const TupleDev &t, const
     };
     // VOE entry offsets of the three index pairs: (lo, hi) in orientation 0, (hi, lo) in 1
     const int rp[3] = {l1 + 8 * l2, l0 + 8 * l2, l0 + 8 * l1};
-    const int rpT[3] = {384 + l2 + 8 * l1, 384 + l2 + 8 * l0, 384 + l1 + 8 * l0};
+    const int rpT[3] = {384 + voe_entry(1, l2, l1), 384 + voe_entry(1, l2, l0), 384 + voe_entry(1, l1, l0)};
 #pragma unroll
     for (int first = 0; first < 3; first++) {
       // the two elements whose first index is x_first: pi = 2 first (second <
