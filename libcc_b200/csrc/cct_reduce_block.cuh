@@ -167,6 +167,25 @@ __device__ __forceinline__ void reduce_block(int nu, int no, int64_t NP, const T
   int slot[6];
   orbit_slots(S0, S1, S2, slot);
 
+  // Blocked X: every X block the CTA will read is one contiguous 4 KB run, so
+  // one thread per (term, block) asks L2 for it up front (a bulk prefetch),
+  // and all of the CTA's X is in flight before the first term's loads.
+  if (BLOCKED && !COHERENT) {
+#pragma unroll
+    for (int term = 0; term < NTERM; term++) {
+      const int g = term_entry(KIND, term, 0);
+      const int al0 = term_entry(KIND, term, 1), al1 = term_entry(KIND, term, 2), al2 = term_entry(KIND, term, 3);
+#pragma unroll
+      for (int p = 0; p < 6; p++) {
+        if (tid != 6 * term + p || slot[p] != p) continue;
+        const int O0 = Sm(pm(p, 0)), O1 = Sm(pm(p, 1)), O2 = Sm(pm(p, 2));
+        const double *blk = t.x[g] + xblock_base(sel3(al0, O0, O1, O2), sel3(al1, O0, O1, O2),
+                                                 sel3(al2, O0, O1, O2), nu, NP);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(blk), "r"(SL * 8) : "memory");
+      }
+    }
+  }
+
   // ---- VOE staging: asynchronous copies, in flight during phase A's X loads
   stage_voe(nu, no, t, voe, S0, S1, S2, Vsm);
 
