@@ -69,6 +69,7 @@
 // Every mbarrier wait is bounded and also ends when another role aborted; a
 // timeout sets the error word, the producer waits for its copies in flight,
 // the issuer for its MMAs, and the CTA frees its tensor memory and returns.
+#include <algorithm>
 #include <type_traits>
 
 #include "cct_internal.cuh"
@@ -745,7 +746,7 @@ int launch_emu_s(const EmuOperands &o, const Dims &d, const EmuJob *jobs_dev, in
   a.F8 = o.F8;
   a.expE = o.expE;
   a.expF = o.expF;
-  a.tileExp = o.adaptive ? o.tileExp : nullptr;
+  a.tileExp = o.adaptive && !o.tiles_uniform ? o.tileExp : nullptr;
   a.slice_hist = o.slice_hist;
   a.nu = d.nu;
   a.no = d.no;
@@ -824,6 +825,15 @@ int emu_build_operands(const Dims &d, const double *E, const double *F, EmuOpera
     CCT_CUDA(cudaGetLastError());
     tile_exp_top_kernel<<<1, 256, 0, s>>>((int)o->tiles_m, nbt, o->tileExp);
     CCT_CUDA(cudaGetLastError());
+    // item_slices runs S - floor(gap / 7) digits, gap = top - (ea + eb) >= 0:
+    // all S everywhere iff no tile is all zero and the smallest pair is within 7
+    std::vector<int> te((size_t)o->tiles_m + nbt + 2);
+    CCT_CUDA(cudaMemcpyAsync(te.data(), o->tileExp, te.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CCT_CUDA(cudaStreamSynchronize(s));
+    const int top = te[o->tiles_m + nbt] + te[o->tiles_m + nbt + 1];
+    const int minA = *std::min_element(te.begin(), te.begin() + o->tiles_m);
+    const int minB = *std::min_element(te.begin() + o->tiles_m, te.begin() + o->tiles_m + nbt);
+    o->tiles_uniform = minA > kNoRowExp && minB > kNoRowExp && top - (minA + minB) < 7;
   }
   return CCT_OK;
 }

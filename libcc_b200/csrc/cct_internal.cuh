@@ -172,6 +172,10 @@ struct EmuOperands {
   // S - floor(gap / 7) digits (at least 1): its dropped digit products stay
   // below the top tile's, so the bound on |X error| is the same everywhere.
   bool adaptive = false;
+  // every item of the adaptive plan runs all S digits (no zero tile, every
+  // pair of tile exponents within 7 of the top): the W build then skips the
+  // per-item lookups, with the same result
+  bool tiles_uniform = false;
   int *tileExp = nullptr;
   unsigned long long *slice_hist = nullptr;  // [kEmuMaxSlices + 1] work items per digit count
 };
