@@ -37,18 +37,37 @@ __global__ void __launch_bounds__(RT, 4) reduce_kernel(int nu, int no, int64_t N
 }
 
 // etd_acc[0..1]: Neumaier (sum, compensation); v1_acc(nu, no).
-// Block 0 sums the per-CTA x3 partials; every other warp owns one virtual
-// index a and sums its v1 partials over all block triples containing a.
-__global__ void finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t, const double *__restrict__ xpart,
-                                const double *__restrict__ vpart, double *__restrict__ etd_acc,
-                                double *__restrict__ v1_acc) {
+// Block 0 sums the per-CTA x3 partials (thread t takes partials t, t+256, ...
+// in order, then a tree over the 256 threads); every other block owns kFinA
+// virtual indices a, one warp per (a, column), each summing the column's v1
+// partials over all block triples containing a (lane-strided, then a shuffle
+// tree), and one thread per a adds the three column sums to v1 in the order
+// i, j, k.  The loads of a thread's partials are issued eight at a time ahead
+// of its (ordered) adds.
+constexpr int kFinA = 8;
+constexpr int kFinThreads = 32 * 3 * kFinA;
+__global__ void __launch_bounds__(kFinThreads) finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t,
+                                                               const double *__restrict__ xpart,
+                                                               const double *__restrict__ vpart,
+                                                               double *__restrict__ etd_acc,
+                                                               double *__restrict__ v1_acc) {
+  constexpr int U = 8;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   if (blockIdx.x == 0) {
     __shared__ double red[256];
-    double s = 0.0;
-    for (int64_t c = tid; c < ncta; c += 256) s += xpart[c];
-    red[tid] = s;
+    if (tid < 256) {
+      double s = 0.0;
+      for (int64_t c0 = tid; c0 < ncta; c0 += 256 * U) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = c0 + 256 * u < ncta ? xpart[c0 + 256 * u] : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (c0 + 256 * u < ncta) s += v[u];
+      }
+      red[tid] = s;
+    }
     __syncthreads();
     for (int st = 128; st > 0; st >>= 1) {
       if (tid < st) red[tid] += red[tid + st];
@@ -64,24 +83,34 @@ __global__ void finalize_kernel(int nu, int nb, int64_t ncta, TupleDev t, const 
     }
     return;
   }
-  const int a = ((blockIdx.x - 1) * blockDim.x + tid) >> 5;
-  if (a >= nu) return;
-  const int X = a / RB, la = a - (a / RB) * RB;
-  const int64_t npairs = (int64_t)nb * (nb + 1) / 2;
-  const double *slab = vpart + ((int64_t)X * RB + la) * 3 * npairs;
-  double sc[3];
-#pragma unroll
-  for (int col = 0; col < 3; col++) {
+  __shared__ double sc[kFinA][3];
+  const int warp = tid >> 5, la8 = warp / 3, col = warp - 3 * (warp / 3);
+  const int a = (blockIdx.x - 1) * kFinA + la8;
+  if (a < nu) {
+    const int X = a / RB, la = a - (a / RB) * RB;
+    const int64_t npairs = (int64_t)nb * (nb + 1) / 2;
+    const double *slab = vpart + (((int64_t)X * RB + la) * 3 + col) * npairs;
     double v = 0.0;
-    for (int64_t q = lane; q < npairs; q += 32) v += slab[col * npairs + q];
+    for (int64_t q0 = lane; q0 < npairs; q0 += 32 * U) {
+      double x[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) x[u] = q0 + 32 * u < npairs ? slab[q0 + 32 * u] : 0.0;
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        if (q0 + 32 * u < npairs) v += x[u];
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    sc[col] = v;
+    if (lane == 0) sc[la8][col] = v;
   }
-  if (lane == 0) {
-    v1_acc[a + (int64_t)nu * t.i] += t.weight * sc[0];
-    v1_acc[a + (int64_t)nu * t.j] += t.weight * sc[1];
-    v1_acc[a + (int64_t)nu * t.k] += t.weight * sc[2];
+  __syncthreads();
+  if (tid < kFinA) {
+    const int a2 = (blockIdx.x - 1) * kFinA + tid;
+    if (a2 < nu) {
+      v1_acc[a2 + (int64_t)nu * t.i] += t.weight * sc[tid][0];
+      v1_acc[a2 + (int64_t)nu * t.j] += t.weight * sc[tid][1];
+      v1_acc[a2 + (int64_t)nu * t.k] += t.weight * sc[tid][2];
+    }
   }
 }
 
@@ -154,8 +183,8 @@ int launch_reduce(const Dims &d, const TupleDev &t, const double *eh, const doub
 
 int launch_finalize(const Dims &d, const TupleDev &t, const double *xpart, const double *vpart, double *etd_acc,
                     double *v1_acc, cudaStream_t s) {
-  const int vblocks = (d.nu * 32 + 255) / 256;  // one warp per virtual index
-  finalize_kernel<<<1 + vblocks, 256, 0, s>>>(d.nu, d.nb, d.ncta, t, xpart, vpart, etd_acc, v1_acc);
+  const int vblocks = (d.nu + kFinA - 1) / kFinA;  // one warp per (virtual index, column)
+  finalize_kernel<<<1 + vblocks, kFinThreads, 0, s>>>(d.nu, d.nb, d.ncta, t, xpart, vpart, etd_acc, v1_acc);
   CCT_CUDA(cudaGetLastError());
   return CCT_OK;
 }
