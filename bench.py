@@ -221,9 +221,11 @@ def run_reference(args, rank, world):
 
 def adjoint_extra(A, S, local):
     """Forward + hand-written adjoint on the no=12/nu=120 system (seed 3): device
-    times, their ratio, the gradient against the stored hand-derived FP64 CPU
-    gradient (200 seeded entries per input), a few central differences, and a
-    step-size sweep of the dVOE central differences."""
+    times, their ratio (with W rebuilt in the backward, and with the
+    forward's W-build output kept for it, ``keep_w``), the gradient against
+    the stored hand-derived FP64 CPU gradient (200 seeded entries per input),
+    a few central differences, and a step-size sweep of the dVOE central
+    differences."""
     import copy
     import numpy as np
     g0 = json.loads((ROOT / "tests" / "golden" / "grad_no12-nu120.json").read_text())
@@ -237,6 +239,18 @@ def adjoint_extra(A, S, local):
             g = plan.backward()
             bwd.append(plan.last_backward_ms)
         f_ms, b_ms = statistics.median(fwd[1:]), statistics.median(bwd[1:])
+        gk = None
+        with A.TriplesPlan(inp.no, inp.nu, device=local, keep_w=True) as kplan:
+            kplan.set_system(inp)
+            kf, kb = [], []
+            for rep in range(4):
+                kplan.forward()
+                kf.append(kplan.last_forward_ms)
+                gk = kplan.backward()
+                kb.append(kplan.last_backward_ms)
+            kept = kplan.kept_tuples
+        kf_ms, kb_ms = statistics.median(kf[1:]), statistics.median(kb[1:])
+        keep_equal = all(np.array_equal(g[n], gk[n]) for n in g)
         rel = {}
         for name, ref in g0["tensors"].items():
             idx = np.array(ref["index"])
@@ -268,10 +282,14 @@ def adjoint_extra(A, S, local):
                                   for q in voe_idx)
     return {"workload": "no12-nu120 (seed 3, normal)", "forward_ms": f_ms, "backward_ms": b_ms,
             "ratio_backward_over_forward": b_ms / f_ms, "e_t": ets + etd,
+            "keep_w": {"forward_ms": kf_ms, "backward_ms": kb_ms, "ratio_backward_over_forward": kb_ms / kf_ms,
+                       "kept_tuples": kept, "kept_bytes": kept * 3 * inp.nu ** 2 * inp.nu * 8,
+                       "gradient_bitwise_equal_to_recompute": keep_equal},
             "max_rel_err_vs_cpu_gradient": rel, "central_difference_h": 1e-5,
             "max_rel_err_vs_central_differences": fd_rel,
             "dvoe_central_difference_step_sweep": sweep,
-            "note": "backward recomputes W per tuple in FP64; rel errors are relative to max|gradient| per input; "
+            "note": "backward recomputes W per tuple in FP64 (keep_w: reads the forward's W-build output instead); "
+                    "rel errors are relative to max|gradient| per input; "
                     "the sweep takes the largest-|g| VOE entry and one random entry"}
 
 

@@ -62,7 +62,12 @@ typedef struct {
                                 2e-14, the FP64 evaluation-order round-off)     */
     int32_t vvvo_mode;       /* FP64 plans: CCT_VVVO_AUTO (default), _EXPANDED or
                                 _PACKED (see below)                             */
-    int32_t reserved;
+    int32_t keep_w;          /* FP64 plans with expanded VVVO: 1 = ccT_forward
+                                keeps every tuple's W-build output (3 nu^2 NP
+                                doubles a tuple) on the device when that fits
+                                in the free memory, and ccT_backward reads it
+                                instead of rebuilding W (same results); 0
+                                (default) = the backward rebuilds W         */
 } ccT_options;
 
 /* How an FP64 plan holds VVVO.  EXPANDED: ccT_set_inputs expands the packed
@@ -121,8 +126,9 @@ int ccT_forward(ccT_plan *plan, int64_t begin, int64_t end, double *ets, double 
  * (no,nu), d_t2 (nu,nu,no,no), d_vm (no,nu,no,no), d_voe (nu,nu,no,no) and
  * d_vvvo (the packed (nutr, nu*no) layout of ccT_set_inputs).  Together this
  * is the (T) contribution to the CCSD(T) Lagrangian.  W is recomputed per
- * tuple in FP64 whatever the plan's precision; nothing of size nu^3 is kept
- * across tuples.  mem says whether the output pointers are host or device
+ * tuple in FP64 whatever the plan's precision (or, with options.keep_w, read
+ * from what the forward kept; otherwise nothing of size nu^3 is kept across
+ * tuples).  mem says whether the output pointers are host or device
  * memory; any output pointer may be NULL to skip it.  No reference
  * counterpart: the reference computes no gradient.  Returns CCT_ERR_STATE
  * when no ccT_forward over [begin, end) precedes it. */
@@ -131,6 +137,11 @@ int ccT_backward(ccT_plan *plan, int64_t begin, int64_t end, double *d_eh, doubl
 
 /* Milliseconds of device time the last ccT_backward spent (CUDA events). */
 double ccT_last_backward_ms(const ccT_plan *plan);
+
+/* Tuples whose W-build output the last ccT_forward kept for the backward
+ * (options.keep_w): end - begin of its range, or 0 when it kept none (option
+ * off, an emulated or packed plan, or not enough free device memory). */
+int64_t ccT_kept_tuples(const ccT_plan *plan);
 
 /* Emulated plans: hist[s] = work items (128-row x N-column W tiles) the last
  * ccT_forward ran with s digits per operand, s = 0..n-1.  With emu_slices = 0

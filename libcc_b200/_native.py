@@ -24,7 +24,7 @@ EXPORTS = [
     "ccT_options_default", "ccT_plan_create", "ccT_set_inputs", "ccT_num_tuples", "ccT_forward",
     "ccT_set_stream", "ccT_time_wbuild", "ccT_set_profiling", "ccT_last_kernel_ms", "ccT_last_forward_ms", "ccT_last_forward_launches", "ccT_plan_destroy", "ccT_status_string",
     "ccT_last_error", "ccT_measure_fp64_peak", "ccT_measure_int8_peak", "ijk_gpu_init_", "ijk_gpu_driver_", "ijk_gpu_finalize_",
-    "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms", "ccT_emu_slice_histogram",
+    "cc_triples_b200_", "ccT_reduce_w_noalloc", "ccT_backward", "ccT_last_backward_ms", "ccT_kept_tuples", "ccT_emu_slice_histogram",
     "ccT_batch_create", "ccT_batch_set_inputs", "ccT_batch_forward", "ccT_batch_v1", "ccT_batch_configure",
     "ccT_batch_tune", "ccT_batch_last_ms", "ccT_batch_work_items", "ccT_batch_destroy", "ccT_emu_digits",
     "ccT_tuple_w", "ccT_batch_debug_stall", "ccT_batch_emu_digits", "ccT_ccsd_terms_29_31", "ccT_ccsd_terms_32_35", "ccT_ccsd_release_workspace",
@@ -44,7 +44,7 @@ class CctError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("check_inputs", ctypes.c_int32),
                 ("emu_slices", ctypes.c_int32), ("emu_tol", ctypes.c_double), ("emu_tol_rel", ctypes.c_double),
-                ("vvvo_mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("vvvo_mode", ctypes.c_int32), ("keep_w", ctypes.c_int32)]
 
 
 _lib = None
@@ -108,6 +108,8 @@ def load():
     lib.ccT_backward.restype = ctypes.c_int
     lib.ccT_last_backward_ms.argtypes = [vp]
     lib.ccT_last_backward_ms.restype = ctypes.c_double
+    lib.ccT_kept_tuples.argtypes = [vp]
+    lib.ccT_kept_tuples.restype = ctypes.c_int64
     lib.ccT_emu_slice_histogram.argtypes = [vp, i64p, i32]
     lib.ccT_emu_slice_histogram.restype = i32
     lib.ccT_batch_create.argtypes = [ctypes.POINTER(vp), i64, i64p, i64p, ctypes.POINTER(Options)]

@@ -71,10 +71,14 @@ class TriplesPlan:
     ``emu_tol`` / ``emu_tol_rel`` of 0 keep the library defaults (1e-8 Eh,
     2e-14).  ``vvvo`` ("auto", "expanded", "packed") says whether an FP64 plan
     expands VVVO into the W build's operand or keeps the packed triangle
-    resident and gathers rows from it (``CCT_VVVO_*``)."""
+    resident and gathers rows from it (``CCT_VVVO_*``).  ``keep_w``: an FP64
+    plan's forward keeps every tuple's W-build output on the device when it
+    fits, and the backward reads it instead of rebuilding W
+    (``ccT_options.keep_w``, ``kept_tuples``)."""
 
     def __init__(self, no: int, nu: int, precision: str = "fp64", device: int = 0, check_inputs: bool = True,
-                 emu_slices: int = 0, emu_tol: float = 0.0, emu_tol_rel: float = 0.0, vvvo: str = "auto"):
+                 emu_slices: int = 0, emu_tol: float = 0.0, emu_tol_rel: float = 0.0, vvvo: str = "auto",
+                 keep_w: bool = False):
         lib = N.load()
         opt = N.Options()
         lib.ccT_options_default(ctypes.byref(opt))
@@ -87,6 +91,7 @@ class TriplesPlan:
         if emu_tol_rel:
             opt.emu_tol_rel = emu_tol_rel
         opt.vvvo_mode = {"auto": N.CCT_VVVO_AUTO, "expanded": N.CCT_VVVO_EXPANDED, "packed": N.CCT_VVVO_PACKED}[vvvo]
+        opt.keep_w = 1 if keep_w else 0
         h = ctypes.c_void_p()
         N.check(lib.ccT_plan_create(ctypes.byref(h), no, nu, ctypes.byref(opt)), "ccT_plan_create")
         self._h = h
@@ -179,6 +184,12 @@ class TriplesPlan:
     @property
     def last_backward_ms(self) -> float:
         return float(N.load().ccT_last_backward_ms(self._h))
+
+    @property
+    def kept_tuples(self) -> int:
+        """Tuples whose W-build output the last forward kept for the backward
+        (``keep_w``); 0 when it kept none."""
+        return int(N.load().ccT_kept_tuples(self._h))
 
     def emu_slice_histogram(self) -> list:
         """Emulated plans: work items of the last forward per digit count

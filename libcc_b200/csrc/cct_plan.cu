@@ -5,6 +5,7 @@
 // device-resident HBM buffers owned by the plan, the static/dynamic tuple
 // partition becomes a host-side tuple list walked in the reference's order,
 // and ddi_gsumf becomes fixed-order on-device accumulation.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -110,6 +111,14 @@ struct ccT_plan {
   cudaEvent_t ev_rec[kNBuf] = {}, ev_pw[kNBuf] = {};  // X buffer b: W rebuilt / read by the pointwise pass
   int64_t fwd_begin = -1, fwd_end = -1;
   float last_bwd_ms = 0.f;
+  // options.keep_w: the W-build output of the last forward, kept for the
+  // backward ([t - keep_begin][job slot][nu^2 NP]), and the W-build jobs
+  // that write it ([t - keep_begin][3])
+  double *xkeep = nullptr;
+  size_t xkeep_count = 0;
+  GemmJob *keep_jobs = nullptr;
+  int64_t keep_jobs_count = 0;
+  int64_t keep_begin = -1, keep_end = -1;
 };
 
 namespace {
@@ -155,37 +164,42 @@ int upload_emu_jobs(ccT_plan *p, const std::vector<GemmJob> &jobs, EmuJob *dst) 
   return CCT_OK;
 }
 
-int build_jobs(ccT_plan *p) {
+// The three W-build GEMM jobs of tuple t (expanded E), writing X slots out[0..2].
+void tuple_jobs(const ccT_plan *p, const Tuple &t, double *const out[3], GemmJob J[3]) {
   const Dims &d = p->d;
   const int64_t nu2 = (int64_t)d.nu * d.nu;
   auto Ex = [&](int x) { return p->E + (int64_t)x * nu2 * d.KP; };
   auto Fyz = [&](int y, int z) { return p->F + ((int64_t)y * d.no + z) * d.NP * d.KP; };
-  if (p->packed) return CCT_OK;  // jobs name cache slots: built per forward (packed_schedule)
-  int buf = 0;
   auto G = [&](int x1, int x2, int x3, int slot) {
-    return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), p->X[buf][slot], 2, 0};
+    return GemmJob{Ex(x1), Ex(x2), Fyz(x2, x3), Fyz(x1, x3), out[slot], 2, 0};
   };
   auto H = [&](int x1, int x2, int x3, int slot) {
-    return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), p->X[buf][slot], 1, 0};
+    return GemmJob{Ex(x1), Ex(x1), Fyz(x2, x3), Fyz(x2, x3), out[slot], 1, 0};
   };
-  std::vector<GemmJob> jobs;
-  jobs.reserve(p->tuples.size() * 3 * kNBuf);
-  for (buf = 0; buf < kNBuf; buf++)
-  for (const Tuple &t : p->tuples) {
-    if (t.kind == kIJK) {
-      jobs.push_back(G(t.i, t.j, t.k, 0));
-      jobs.push_back(G(t.i, t.k, t.j, 1));
-      jobs.push_back(G(t.j, t.k, t.i, 2));
-    } else if (t.kind == kIJJ) {  // (i,j,j): G(i,j,j), H(j,j,i)
-      jobs.push_back(G(t.i, t.j, t.j, 0));
-      jobs.push_back(H(t.j, t.j, t.i, 1));
-      jobs.push_back(H(t.j, t.j, t.i, 2));  // unused slot
-    } else {  // (i,i,k): H(i,i,k), G(i,k,i)
-      jobs.push_back(H(t.i, t.i, t.k, 0));
-      jobs.push_back(G(t.i, t.k, t.i, 1));
-      jobs.push_back(G(t.i, t.k, t.i, 2));  // unused slot
-    }
+  if (t.kind == kIJK) {
+    J[0] = G(t.i, t.j, t.k, 0);
+    J[1] = G(t.i, t.k, t.j, 1);
+    J[2] = G(t.j, t.k, t.i, 2);
+  } else if (t.kind == kIJJ) {  // (i,j,j): G(i,j,j), H(j,j,i)
+    J[0] = G(t.i, t.j, t.j, 0);
+    J[1] = H(t.j, t.j, t.i, 1);
+    J[2] = H(t.j, t.j, t.i, 2);  // never launched
+  } else {  // (i,i,k): H(i,i,k), G(i,k,i)
+    J[0] = H(t.i, t.i, t.k, 0);
+    J[1] = G(t.i, t.k, t.i, 1);
+    J[2] = G(t.i, t.k, t.i, 2);  // never launched
   }
+}
+
+int build_jobs(ccT_plan *p) {
+  if (p->packed) return CCT_OK;  // jobs name cache slots: built per forward (packed_schedule)
+  std::vector<GemmJob> jobs(p->tuples.size() * 3 * kNBuf);
+  size_t q = 0;
+  for (int buf = 0; buf < kNBuf; buf++)
+    for (const Tuple &t : p->tuples) {
+      tuple_jobs(p, t, p->X[buf], &jobs[q]);
+      q += 3;
+    }
   CCT_CUDA(cudaMemcpy(p->jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
   if (p->emulated) CCT_TRY(upload_emu_jobs(p, jobs, p->emu_jobs));
   return CCT_OK;
@@ -356,16 +370,64 @@ int wbuild_tuple(ccT_plan *p, int64_t tix, int b, bool fp64, cudaStream_t st, bo
   return launch_wbuild_f64(p->d, p->jobs + 3 * (b * ntup + tix), njobs, st);
 }
 
+// options.keep_w: room and W-build jobs for the X of tuples [begin, end)
+// (3 slots a tuple), allocated when that fits in the free device memory with
+// a margin of max(2 GB, 10% of the device); *keep says whether it did.
+int prepare_keep(ccT_plan *p, int64_t begin, int64_t end, bool *keep) {
+  const Dims &d = p->d;
+  const int64_t n = end - begin;
+  const size_t slab = (size_t)d.nu * d.nu * d.NP;
+  const size_t need = (size_t)n * 3 * slab;
+  *keep = false;
+  if (p->xkeep_count < need) {
+    if (p->xkeep) CCT_CUDA(cudaFree(p->xkeep));
+    p->xkeep = nullptr;
+    p->xkeep_count = 0;
+    size_t free_b = 0, total_b = 0;
+    CCT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t margin = std::max<size_t>((size_t)2 << 30, total_b / 10);
+    if (need * 8 + margin > free_b) return CCT_OK;  // recompute in the backward
+    CCT_TRY(dalloc(&p->xkeep, need));
+    p->xkeep_count = need;
+  }
+  if (p->keep_jobs_count < 3 * n) {
+    if (p->keep_jobs) CCT_CUDA(cudaFree(p->keep_jobs));
+    p->keep_jobs = nullptr;
+    p->keep_jobs_count = 0;
+    CCT_TRY(dalloc(&p->keep_jobs, (size_t)3 * n));
+    p->keep_jobs_count = 3 * n;
+  }
+  std::vector<GemmJob> jobs((size_t)3 * n);
+  for (int64_t t = begin; t < end; t++) {
+    double *out[3];
+    for (int g = 0; g < 3; g++) out[g] = p->xkeep + ((t - begin) * 3 + g) * slab;
+    tuple_jobs(p, p->tuples[t], out, &jobs[(size_t)3 * (t - begin)]);
+  }
+  CCT_CUDA(cudaMemcpy(p->keep_jobs, jobs.data(), jobs.size() * sizeof(GemmJob), cudaMemcpyHostToDevice));
+  *keep = true;
+  return CCT_OK;
+}
+
+// X slot g of the kept W-build output of tuple begin + slot.
+double *xkeep_at(const ccT_plan *p, int64_t slot, int g) {
+  return p->xkeep + (slot * 3 + g) * (int64_t)p->d.nu * p->d.nu * p->d.NP;
+}
+
 // W-build of tuple tix into X buffer b on the GEMM stream, then its reduction on
 // the reduction stream.  The GEMM waits until the reduction that last read
 // buffer b (two tuples earlier) is done; the reduction waits for its GEMM.
-int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
+// keep >= 0 (an FP64 plan keeping W for the backward): the W build writes
+// the kept slot instead of buffer b.
+int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false, int64_t keep = -1) {
   const Tuple &t = p->tuples[tix];
   const int b = (int)(p->tick % kNBuf);
   p->tick++;
   CCT_CUDA(cudaStreamWaitEvent(p->gemm_stream, p->ev_red[b], 0));
   CCT_TRY(prof_mark(p, CCT_KERNEL_WBUILD, p->gemm_stream));
-  CCT_TRY(wbuild_tuple(p, tix, b, fp64, p->gemm_stream));
+  if (keep >= 0)
+    CCT_TRY(launch_wbuild_f64(p->d, p->keep_jobs + 3 * keep, t.kind == kIJK ? 3 : 2, p->gemm_stream));
+  else
+    CCT_TRY(wbuild_tuple(p, tix, b, fp64, p->gemm_stream));
   CCT_TRY(prof_mark(p, -1, p->gemm_stream));
   CCT_CUDA(cudaEventRecord(p->ev_gemm[b], p->gemm_stream));
   CCT_CUDA(cudaStreamWaitEvent(p->red_stream, p->ev_gemm[b], 0));
@@ -377,9 +439,7 @@ int run_tuple(ccT_plan *p, int64_t tix, bool fp64 = false) {
   cudaStream_t rs = p->red_stream;
   if (kSerialReduce && p->emulated && !fp64) rs = p->gemm_stream;
   TupleDev td;
-  td.x[0] = p->X[b][0];
-  td.x[1] = p->X[b][1];
-  td.x[2] = p->X[b][2];
+  for (int g = 0; g < 3; g++) td.x[g] = keep >= 0 ? xkeep_at(p, keep, g) : p->X[b][g];
   td.kind = t.kind;
   td.i = t.i;
   td.j = t.j;
@@ -584,6 +644,10 @@ int ccT_plan_create(ccT_plan **out, int64_t no, int64_t nu, const ccT_options *o
     set_error("vvvo_mode must be CCT_VVVO_AUTO, _EXPANDED or _PACKED; PACKED needs an FP64 plan");
     return CCT_ERR_INVALID;
   }
+  if (o.keep_w != 0 && o.keep_w != 1) {
+    set_error("keep_w must be 0 or 1");
+    return CCT_ERR_INVALID;
+  }
   int ndev = 0;
   CCT_CUDA(cudaGetDeviceCount(&ndev));
   if (o.device < 0 || o.device >= ndev) {
@@ -723,6 +787,7 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   const cudaMemcpyKind kind = mem == CCT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   p->inputs_ready = false;
   p->fwd_begin = p->fwd_end = -1;
+  p->keep_begin = p->keep_end = -1;
   // Device inputs on the plan's own (non-blocking) stream: the caller may
   // still be writing them on any stream, so wait for the whole device.  On a
   // caller stream (ccT_set_stream) the copies are ordered after its work.
@@ -819,13 +884,16 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   CCT_CUDA(cudaMemsetAsync(p->flags + 1, 0, 4, p->stream));
   if (p->emulated)
     CCT_CUDA(cudaMemsetAsync(p->emu.slice_hist, 0, (kEmuMaxSlices + 1) * sizeof(unsigned long long), p->stream));
+  p->keep_begin = p->keep_end = -1;
+  bool keep = false;
+  if (p->opt.keep_w && !p->emulated && !p->packed && end > begin) CCT_TRY(prepare_keep(p, begin, end, &keep));
   CCT_CUDA(cudaEventRecord(p->ev0, p->stream));
   SlabFills fills;
   if (p->packed) CCT_TRY(packed_schedule(p, begin, end, &fills));
   CCT_TRY(fork_streams(p));
   for (int64_t t = begin; t < end; t++) {
     if (p->packed) CCT_TRY(packed_fill(p, fills[t - begin], p->gemm_stream));
-    CCT_TRY(run_tuple(p, t));
+    CCT_TRY(run_tuple(p, t, false, keep ? t - begin : -1));
   }
   CCT_TRY(join_streams(p));
   CCT_TRY(launch_ets(d, p->t1, v1_acc(p), p->acc, p->acc + 2, p->stream));
@@ -853,6 +921,10 @@ int ccT_forward(ccT_plan *p, int64_t begin, int64_t end, double *ets, double *et
   }
   p->fwd_begin = begin;
   p->fwd_end = end;
+  if (keep) {
+    p->keep_begin = begin;
+    p->keep_end = end;
+  }
   return CCT_OK;
 }
 
@@ -929,24 +1001,32 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
   CCT_CUDA(cudaStreamWaitEvent(sF, p->ev_fork, 0));
   CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_fork, 0));
   if (sP != p->red_stream) CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_fork, 0));
+  // W kept by the forward (options.keep_w): no recompute, X read from there
+  const bool kept = p->keep_begin == begin && p->keep_end == end;
   for (int64_t t = begin; t < end; t++) {
     const Tuple &tu = p->tuples[t];
     const int set = (int)((t - begin) % kGXSets);
     const int xb = (int)((t - begin) % kNBuf);
-    if (t - begin >= kNBuf) CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_pw[xb], 0));  // X buffer read by t-3
-    CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2, sW));
-    CCT_CUDA(cudaEventRecord(p->ev_rec[xb], sW));
-    CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_rec[xb], 0));
+    double *Xk[3] = {nullptr, nullptr, nullptr};
+    if (kept) {
+      for (int g = 0; g < 3; g++) Xk[g] = xkeep_at(p, t - begin, g);
+    } else {
+      if (t - begin >= kNBuf) CCT_CUDA(cudaStreamWaitEvent(sW, p->ev_pw[xb], 0));  // X buffer read by t-3
+      CCT_TRY(launch_wbuild_f64(d, p->jobs + 3 * ((int64_t)xb * ntup + t), tu.kind == kIJK ? 3 : 2, sW));
+      CCT_CUDA(cudaEventRecord(p->ev_rec[xb], sW));
+      CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_rec[xb], 0));
+      for (int g = 0; g < 3; g++) Xk[g] = p->X[xb][g];
+    }
     if (t - begin >= kGXSets) {  // GX set last read by the GEMMs of tuple t - kGXSets
       CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gx_e[set], 0));
       CCT_CUDA(cudaStreamWaitEvent(sP, p->ev_gx_f[set], 0));
     }
-    CCT_TRY(adj_tuple_pointwise(d, tu, p->X[xb], p->eh, p->ep, p->t1, p->voe, &p->adj, set, sP));
+    CCT_TRY(adj_tuple_pointwise(d, tu, Xk, p->eh, p->ep, p->t1, p->voe, &p->adj, set, sP));
     if (p->emulated) {
       TupleDev td;
-      td.x[0] = p->X[xb][0];
-      td.x[1] = p->X[xb][1];
-      td.x[2] = p->X[xb][2];
+      td.x[0] = Xk[0];
+      td.x[1] = Xk[1];
+      td.x[2] = Xk[2];
       td.kind = tu.kind;
       td.i = tu.i;
       td.j = tu.j;
@@ -1003,6 +1083,8 @@ int ccT_backward(ccT_plan *p, int64_t begin, int64_t end, double *d_eh, double *
 }
 
 double ccT_last_backward_ms(const ccT_plan *p) { return p ? (double)p->last_bwd_ms : 0.0; }
+
+int64_t ccT_kept_tuples(const ccT_plan *p) { return p && p->keep_end > p->keep_begin ? p->keep_end - p->keep_begin : 0; }
 
 int ccT_emu_slice_histogram(ccT_plan *p, int64_t *hist, int32_t n) {
   if (!p || !hist || n < 1) {
@@ -1181,6 +1263,8 @@ int ccT_plan_destroy(ccT_plan *p) {
       if (p->X[b][g]) cudaFree(p->X[b][g]);
   if (p->cta_table) cudaFree(p->cta_table);
   if (p->jobs) cudaFree(p->jobs);
+  if (p->xkeep) cudaFree(p->xkeep);
+  if (p->keep_jobs) cudaFree(p->keep_jobs);
   if (p->flags) cudaFree(p->flags);
   for (void *b : {(void *)p->emu.E8, (void *)p->emu.E8T, (void *)p->emu.F8, (void *)p->emu.expE,
                   (void *)p->emu.expET, (void *)p->emu.expF, (void *)p->emu.expRowF, (void *)p->emu_jobs,

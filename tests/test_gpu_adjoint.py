@@ -79,6 +79,41 @@ def test_backward_bitwise_reproducible(api):
         assert np.array_equal(a[name], b[name]), name
 
 
+@pytest.mark.parametrize("no,nu,seed", [(5, 24, 8), (4, 17, 12)])
+def test_backward_from_kept_w_equals_recompute(api, no, nu, seed):
+    """keep_w: the forward keeps every tuple's W-build output and the backward
+    reads it instead of rebuilding W; the FP64 W build is deterministic, so
+    energies and every gradient are bitwise those of the recomputing
+    backward, for the full range and for a tuple range."""
+    inp = S.generate(no, nu, seed)
+    for rng in [(), (2, 9)]:
+        with api.TriplesPlan(no, nu) as plan:
+            plan.set_system(inp)
+            fa = plan.forward(*rng)
+            ga = plan.backward(*rng)
+            assert plan.kept_tuples == 0
+        with api.TriplesPlan(no, nu, keep_w=True) as plan:
+            plan.set_system(inp)
+            fb = plan.forward(*rng)
+            n = (rng[1] - rng[0]) if rng else plan.num_tuples
+            assert plan.kept_tuples == n > 0
+            gb = plan.backward(*rng)
+            gc = plan.backward(*rng)  # the kept W is read, not consumed
+        assert fa[0] == fb[0] and fa[1] == fb[1] and np.array_equal(fa[2], fb[2])
+        for name in NAMES:
+            assert np.array_equal(ga[name], gb[name]), (rng, name)
+            assert np.array_equal(gb[name], gc[name]), (rng, name)
+
+
+def test_keep_w_is_off_for_emulated_plans(api):
+    inp = S.generate(4, 12, 5)
+    with api.TriplesPlan(4, 12, precision="int8", emu_slices=4, keep_w=True) as plan:
+        plan.set_system(inp)
+        plan.forward()
+        assert plan.kept_tuples == 0
+        plan.backward()
+
+
 def test_backward_after_emulated_forward(api):
     """An emulated plan's backward recomputes W in FP64: same gradient as FP64."""
     from oracle import oracle as O
