@@ -491,6 +491,22 @@ constexpr int kCalSamples = 5;
 constexpr double kCalSafety = 2.0;
 constexpr double kDefaultTol = 1e-8, kDefaultTolRel = 2e-14;
 
+// The widest N tile for S digits whose digits x columns fit the tensor memory
+// and which divides NP, starting from the plan's base tile.
+int widest_ebn(const ccT_plan *p, int S) {
+  int best = p->emu_base_ebn;
+  for (int bn : kEmuBNChoices)
+    if (S * bn <= 512 && p->d.NP % bn == 0 && bn > best) best = bn;
+  return best;
+}
+
+// Digit operands of S slices on N tile ebn.
+int build_digits(ccT_plan *p, int S, int ebn) {
+  p->d.EBN = p->emu.ebn = ebn;
+  p->emu.slices = p->emu.run_slices = S;
+  return emu_build_operands(p->d, p->E, p->F, &p->emu, p->stream);
+}
+
 int calibrate_digits(ccT_plan *p) {
   const int64_t n = (int64_t)p->tuples.size();
   std::vector<int64_t> idx;
@@ -515,10 +531,8 @@ int calibrate_digits(ccT_plan *p) {
   const double tol = p->opt.emu_tol > 0.0 ? p->opt.emu_tol : kDefaultTol;
   const double rel = p->opt.emu_tol_rel > 0.0 ? p->opt.emu_tol_rel : kDefaultTolRel;
   const double target = std::fmax(tol, rel * std::fabs(e_est));
-  int chosen = p->emu.slices;
-  double chosen_err = INFINITY;
-  for (int sl = kEmuMinSlices; sl <= p->emu.slices && s == CCT_OK; sl++) {
-    p->emu.run_slices = sl;
+  // bound of the count the operands are built for now (run_slices)
+  auto bound = [&](double *est) {
     double worst = 0.0;
     for (size_t q = 0; q < idx.size() && s == CCT_OK; q++) {
       double e = 0.0;
@@ -526,11 +540,40 @@ int calibrate_digits(ccT_plan *p) {
       const double err = std::fabs(e - e64[q]) / weight(idx[q]);
       worst = std::isfinite(err) ? std::fmax(worst, err) : INFINITY;
     }
-    const double est = kCalSafety * worst * wsum_all;
-    if (s == CCT_OK && (est <= target || sl == p->emu.slices)) {
-      chosen = sl;
+    *est = kCalSafety * worst * wsum_all;
+  };
+  int chosen = kEmuMaxSlices;
+  double chosen_err = INFINITY;
+  int first = kEmuMinSlices;
+  // A target of under 3.5 digits' worth of bits relative to |E(T)| (7 bits a
+  // digit) is tried at kEmuMinSlices first, on operands built for that count
+  // and its own N tile, which are the plan's final operands when it passes.
+  // The emulated X does not depend on the N tile or on how many digits the
+  // operands hold, so the choice is the one the sweep below would make.
+  const double rel_target = e_est != 0.0 ? target / std::fabs(e_est) : 1.0;
+  if (s == CCT_OK && std::log2(1.0 / rel_target) < 3.5 * 7) {
+    s = build_digits(p, kEmuMinSlices, widest_ebn(p, kEmuMinSlices));
+    double est = INFINITY;
+    if (s == CCT_OK) bound(&est);
+    if (s == CCT_OK && est <= target) {
+      chosen = kEmuMinSlices;
       chosen_err = est;
-      break;
+      first = kEmuMaxSlices + 1;  // done
+    } else {
+      first = kEmuMinSlices + 1;
+    }
+  }
+  if (s == CCT_OK && first <= kEmuMaxSlices) {  // every count on kEmuMaxSlices-digit operands
+    s = build_digits(p, kEmuMaxSlices, p->emu_base_ebn);
+    for (int sl = first; sl <= kEmuMaxSlices && s == CCT_OK; sl++) {
+      p->emu.run_slices = sl;
+      double est = INFINITY;
+      bound(&est);
+      if (s == CCT_OK && (est <= target || sl == kEmuMaxSlices)) {
+        chosen = sl;
+        chosen_err = est;
+        break;
+      }
     }
   }
   p->profiling = prof;
@@ -547,16 +590,10 @@ int calibrate_digits(ccT_plan *p) {
 // and the FP64 jobs keep their layout).  The digits themselves do not depend
 // on the count.
 int rebuild_for_count(ccT_plan *p) {
-  Dims &d = p->d;
   const int S = p->emu.run_slices;
-  int best = d.EBN;
-  for (int bn : kEmuBNChoices)
-    if (S * bn <= 512 && d.NP % bn == 0 && bn > best) best = bn;
-  if (S == p->emu.slices && best == d.EBN) return CCT_OK;
-  d.EBN = best;
-  p->emu.ebn = best;
-  p->emu.slices = S;
-  return emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
+  const int best = widest_ebn(p, S);
+  if (S == p->emu.slices && best == p->d.EBN) return CCT_OK;
+  return build_digits(p, S, best);
 }
 
 [[noreturn]] void legacy_stop(const char *where, int status) {
@@ -827,11 +864,8 @@ int ccT_set_inputs(ccT_plan *p, const double *eh, const double *ep, const double
   }
   if (s == CCT_OK && !p->packed) s = launch_build_e(d, vvvo_dev, p->t2, p->E, 0, d.no, p->stream);
   if (s == CCT_OK) s = launch_build_f(d, p->t2, p->vm, p->F, p->stream);
-  if (s == CCT_OK && p->emu_auto) {  // calibration runs on operands of every digit count
-    p->d.EBN = p->emu.ebn = p->emu_base_ebn;
-    p->emu.slices = p->emu.run_slices = kEmuMaxSlices;
-  }
-  if (s == CCT_OK && p->emulated) s = emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
+  // an automatic plan builds its digit operands during the calibration
+  if (s == CCT_OK && p->emulated && !p->emu_auto) s = emu_build_operands(d, p->E, p->F, &p->emu, p->stream);
   if (staged) {
     cudaStreamSynchronize(p->stream);  // E is built (or the stream failed) before the staging buffer goes
     cudaFree(staged);
