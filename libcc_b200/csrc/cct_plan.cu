@@ -387,7 +387,11 @@ int prepare_keep(ccT_plan *p, int64_t begin, int64_t end, bool *keep) {
     CCT_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t margin = std::max<size_t>((size_t)2 << 30, total_b / 10);
     if (need * 8 + margin > free_b) return CCT_OK;  // recompute in the backward
-    CCT_TRY(dalloc(&p->xkeep, need));
+    if (dalloc(&p->xkeep, need) != CCT_OK) {        // (fragmented memory): recompute too
+      p->xkeep = nullptr;
+      cudaGetLastError();
+      return CCT_OK;
+    }
     p->xkeep_count = need;
   }
   if (p->keep_jobs_count < 3 * n) {
