@@ -613,6 +613,9 @@ def main():
     begin, end = shard.shard_of(no, rank, world)
     flop_step = S.flops(no, nu)
     my_flop_wb = sum(12.0 * nu ** 3 * (no + nu) * c for c in costs[begin:end])
+    # the reduction reads each of a tuple's X buffers once: three for an i>j>k
+    # tuple (cost 1), two for a degenerate one (cost 1/2)
+    my_red_bytes = sum((3 if c == 1 else 2) * nu ** 3 * 8.0 for c in costs[begin:end])
     dev_inputs = [torch.from_numpy(a).to(f"cuda:{local}") for a in inp.arrays()]
     stream = torch.cuda.current_stream()
     N = A.N
@@ -641,7 +644,7 @@ def main():
         for _ in range(warmup):
             step()
         plan.set_profiling(True)
-        launches, wb_ms, wb_n = 0, 0.0, 0
+        launches, wb_ms, wb_n, rd_ms, rd_n = 0, 0.0, 0, 0.0, 0
         hist = [0] * 8
         if dist is not None:
             dist.barrier()
@@ -656,6 +659,8 @@ def main():
             prof = plan.kernel_profile()
             wb_ms += prof["wbuild"][0]
             wb_n += prof["wbuild"][1]
+            rd_ms += prof["reduce"][0]
+            rd_n += prof["reduce"][1]
             if form != "fp64":
                 hist = [x + y for x, y in zip(hist, plan.emu_slice_histogram())]
         e1.record(stream)
@@ -697,6 +702,18 @@ def main():
                            "traffic": read_traffic(args.workload, "emu" if emu else "f64"),
                            "peak_source": psrc, "launches": wb_n, "avg_launch_ms": wb_ms / max(wb_n, 1),
                            "work_per_launch": per_launch, "share_of_step": wb_ms / ms if ms > 0 else None}
+        rd_achieved = my_red_bytes * steps / (rd_ms * 1e-3) / 1e9 if rd_ms > 0 else None
+        try:
+            hbm = measured_peak("hbm_gbs")
+        except (OSError, KeyError, ValueError):
+            hbm = None
+        out["roofline_reduce"] = {
+            "bound": "hbm", "kernel": "reduce_kernel + finalize_kernel (E[4]/E[5] orbit reduction)",
+            "achieved": rd_achieved, "peak": hbm, "unit": "GB/s",
+            "frac": rd_achieved / hbm if (rd_achieved and hbm) else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)", "launches": rd_n,
+            "avg_launch_ms": rd_ms / max(rd_n, 1), "share_of_step": rd_ms / ms if ms > 0 else None,
+            "work_per_launch": "the tuple's X buffers read once: 3 nu^3 doubles (i>j>k), 2 nu^3 (degenerate)"}
         if g is not None:
             out["abs_err_vs_oracle"] = abs(out["e_t"] - g["e_t"])
             out["rel_err_vs_oracle"] = abs(out["e_t"] - g["e_t"]) / abs(g["e_t"])
@@ -823,7 +840,10 @@ def main():
                            "tuples_per_s": len(costs) / (head["ms_per_step"] * 1e-3),
                            "l2": "inputs larger than L2 (digit operands of several GB re-streamed per step)",
                            "parallelism": f"tuple shards x{world}" if world > 1 else "1 GPU"},
-                "roofline": head["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["gpu_launches"],
+                "roofline": head["roofline"],
+                "roofline_reduce": {k: head["roofline_reduce"][k] for k in ("bound", "achieved", "peak", "unit",
+                                                                            "frac", "avg_launch_ms", "share_of_step")},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["gpu_launches"],
                 "clocks": clocks.summary(),
                 "accuracy": {"abs_err_vs_oracle_eh": head.get("abs_err_vs_oracle"),
                              "rel_err_vs_oracle": head.get("rel_err_vs_oracle"),
