@@ -30,6 +30,8 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--backward", action="store_true",
                     help="after the forward, run the adjoint (ccT_backward) over the same tuples")
+    ap.add_argument("--keep-w", action="store_true",
+                    help="FP64 plans: the forward keeps every tuple's W-build output for the backward (keep_w)")
     ap.add_argument("--ccsd-terms", action="store_true",
                     help="instead of (T): one call of each CCSD T1-dressing entry point (ccT_ccsd_terms_29_31, "
                          "_32_35) on seeded device arrays of the workload's (no, nu); prints their device times")
@@ -40,7 +42,7 @@ def main(argv=None) -> int:
     from . import restart, synthetic
     from .api import TriplesPlan, format_energies
     inp = synthetic.workload(args.workload) if args.workload else restart.read(args.restart)
-    with TriplesPlan.for_form(inp.no, inp.nu, args.form, args.device) as plan:
+    with TriplesPlan.for_form(inp.no, inp.nu, args.form, args.device, keep_w=args.keep_w) as plan:
         t0 = time.perf_counter()
         plan.set_system(inp)
         t1 = time.perf_counter()
@@ -56,7 +58,7 @@ def main(argv=None) -> int:
         if args.backward:
             plan.backward(0, end)
             print(f" backward device ms={plan.last_backward_ms:.3f} "
-                  f"ratio={plan.last_backward_ms / plan.last_forward_ms:.2f}")
+                  f"ratio={plan.last_backward_ms / plan.last_forward_ms:.2f} kept_tuples={plan.kept_tuples}")
     return 0
 
 
