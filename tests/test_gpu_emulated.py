@@ -190,3 +190,29 @@ def test_per_tile_digits_uniform_system_equals_fixed(api):
         b = plan.forward()
     assert hist[top] == sum(hist) > 0, hist
     assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
+
+
+@pytest.mark.parametrize("no,nu,seed,rel", [(4, 40, 12, 1e-4), (5, 48, 9, 2.1e-7), (4, 64, 21, 1e-6)])
+def test_loose_target_calibration_is_the_first_passing_count(api, no, nu, seed, rel):
+    """A target looser than 3.5 digits' worth of bits is tried at 3 digits
+    first, on 3-digit operands: the count it keeps has its bound within the
+    target, the energy meets the target against the oracle, and with every
+    tile at the calibrated count the energies are bitwise those of the
+    fixed-count plan."""
+    from oracle import oracle as O
+    inp = S.generate(no, nu, seed, dist="log")
+    e_o = sum(O.c_cc_triples(inp)[:2])
+    with api.TriplesPlan(no, nu, precision="int8", emu_tol_rel=rel) as plan:
+        plan.set_system(inp)
+        a = plan.forward()
+        cal = plan.emu_digits()
+        hist = plan.emu_slice_histogram()
+    assert cal["est_err"] <= cal["target"], cal
+    assert abs(a[0] + a[1] - e_o) <= cal["target"], (cal, a[0] + a[1], e_o)
+    top = cal["digits"]
+    with _plan(api, inp, top) as plan:
+        plan.set_system(inp)
+        b = plan.forward()
+    if hist[top] == sum(hist):
+        assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
+
