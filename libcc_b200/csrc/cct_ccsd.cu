@@ -79,6 +79,156 @@ __global__ void f4_pq_kernel(int no, int nu, const double *__restrict__ o1, cons
   }
 }
 
+// The same steps for no <= kNoTile, staged in shared memory so that global
+// accesses are coalesced runs.
+constexpr int kNoTile = 32;
+// P[j][y][.][.] for one (y, j) per CTA: the contiguous VL(., ., y, j) slab and
+// O1 pass through shared memory 32 virtual indices x at a time.
+__global__ void __launch_bounds__(256) f4_p_tiled_kernel(int no, int nu, const double *__restrict__ o1,
+                                                         const double *__restrict__ vl, double *__restrict__ P) {
+  constexpr int XC = 32;
+  __shared__ double vs[XC][kNoTile], os[XC][kNoTile];
+  const int y = blockIdx.x, j = blockIdx.y, tid = threadIdx.x;
+  const int i = tid & 31, kq = tid >> 5;
+  const double *slab = vl + (int64_t)no * nu * (y + (int64_t)nu * j);  // VL(k, x, y, j) = slab[k + no x]
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int x0 = 0; x0 < nu; x0 += XC) {
+    __syncthreads();
+    for (int e = tid; e < XC * kNoTile; e += 256) {
+      const int x = e / kNoTile, c = e % kNoTile;
+      const bool ok = x0 + x < nu && c < no;
+      vs[x][c] = ok ? slab[c + (int64_t)no * (x0 + x)] : 0.0;
+      os[x][c] = ok ? o1[c + (int64_t)no * (x0 + x)] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int x = 0; x < XC; x++) {
+      const double o = os[x][i];
+#pragma unroll
+      for (int u = 0; u < 4; u++) acc[u] = fma(vs[x][kq + 8 * u], o, acc[u]);
+    }
+  }
+  double *pj = P + ((int64_t)j * nu + y) * no * no;
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int k = kq + 8 * u;
+    if (k < no && i < no) pj[(int64_t)k * no + i] = acc[u];
+  }
+}
+
+// Q[j][z][.][.] for eight consecutive z and one j per CTA: VR(z..z+7, k, x, j)
+// are 64-byte runs, staged 16 x at a time.
+__global__ void __launch_bounds__(256) f4_q_tiled_kernel(int no, int nu, const double *__restrict__ o1,
+                                                         const double *__restrict__ vr, double *__restrict__ Q) {
+  constexpr int XC = 16, ZT = 8;
+  __shared__ double vs[XC][kNoTile][ZT], os[XC][kNoTile];
+  const int z0 = blockIdx.x * ZT, j = blockIdx.y, tid = threadIdx.x;
+  const int i = tid & 31, zz = tid >> 5;
+  const int64_t nuno = (int64_t)nu * no;
+  double acc[kNoTile];
+#pragma unroll
+  for (int k = 0; k < kNoTile; k++) acc[k] = 0.0;
+  for (int x0 = 0; x0 < nu; x0 += XC) {
+    __syncthreads();
+    for (int e = tid; e < XC * kNoTile * ZT; e += 256) {
+      const int z = e % ZT, k = (e / ZT) % kNoTile, x = e / (ZT * kNoTile);
+      const bool ok = x0 + x < nu && k < no && z0 + z < nu;
+      vs[x][k][z] = ok ? vr[(z0 + z) + (int64_t)nu * k + nuno * (x0 + x) + nuno * nu * j] : 0.0;
+    }
+    for (int e = tid; e < XC * kNoTile; e += 256) {
+      const int x = e / kNoTile, c = e % kNoTile;
+      os[x][c] = (x0 + x < nu && c < no) ? o1[c + (int64_t)no * (x0 + x)] : 0.0;
+    }
+    __syncthreads();
+    for (int x = 0; x < XC; x++) {
+      const double o = os[x][i];
+#pragma unroll
+      for (int k = 0; k < kNoTile; k++) acc[k] = fma(vs[x][k][zz], o, acc[k]);
+    }
+  }
+  const int z = z0 + zz;
+  if (z < nu && i < no) {
+    double *qz = Q + ((int64_t)j * nu + z) * no * no;
+#pragma unroll
+    for (int k = 0; k < kNoTile; k++)
+      if (k < no) qz[(int64_t)k * no + i] = acc[k];
+  }
+}
+
+// T2(i,y,z,j) += X_j(y,z,i) - sum_k O1(k,z) P[j][y][k][i] for one (y, j) per
+// CTA and every z (P[j][y] in shared memory, O1(., z) through the read-only
+// cache: a warp reads one z's column); four z at a time, so their loads are
+// in flight together.
+__global__ void __launch_bounds__(256) f4_t2p_tiled_kernel(int no, int nu, int64_t np,
+                                                           const double *__restrict__ o1,
+                                                           const double *__restrict__ X,
+                                                           const double *__restrict__ P, double *__restrict__ t2) {
+  __shared__ double ps[kNoTile][kNoTile];
+  const int y = blockIdx.x, j = blockIdx.y, tid = threadIdx.x;
+  const int i = tid & 31, zg = tid >> 5;
+  const double *pj = P + ((int64_t)j * nu + y) * no * no;
+  for (int e = tid; e < kNoTile * kNoTile; e += 256) {
+    const int k = e / kNoTile, c = e % kNoTile;
+    ps[k][c] = (k < no && c < no) ? pj[(int64_t)k * no + c] : 0.0;
+  }
+  __syncthreads();
+  if (i >= no) return;
+  const int64_t nu2 = (int64_t)nu * nu;
+  constexpr int U = 4;
+  for (int zb = zg; zb < nu; zb += 8 * U) {
+    double v[U], t[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int z = zb + 8 * u;
+      v[u] = z < nu ? X[((int64_t)j * nu2 + (int64_t)y * nu + z) * np + i] : 0.0;
+      t[u] = z < nu ? t2[i + (int64_t)no * (y + (int64_t)nu * (z + (int64_t)nu * j))] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int z = zb + 8 * u;
+      if (z >= nu) break;
+      const double *oz = o1 + (int64_t)no * z;
+      for (int k = 0; k < no; k++) v[u] -= __ldg(oz + k) * ps[k][i];
+      t2[i + (int64_t)no * (y + (int64_t)nu * (z + (int64_t)nu * j))] = t[u] + v[u];
+    }
+  }
+}
+
+// T2(i,y,z,j) -= sum_k O1(k,y) Q[j][z][k][i] for one (z, j) per CTA and every
+// y; T2(., ., z, j) over (i, y) is one contiguous run.
+__global__ void __launch_bounds__(256) f4_t2q_tiled_kernel(int no, int nu, const double *__restrict__ o1,
+                                                           const double *__restrict__ Q, double *__restrict__ t2) {
+  __shared__ double qs[kNoTile][kNoTile];
+  const int z = blockIdx.x, j = blockIdx.y, tid = threadIdx.x;
+  const int i = tid & 31, yg = tid >> 5;
+  const double *qz = Q + ((int64_t)j * nu + z) * no * no;
+  for (int e = tid; e < kNoTile * kNoTile; e += 256) {
+    const int k = e / kNoTile, c = e % kNoTile;
+    qs[k][c] = (k < no && c < no) ? qz[(int64_t)k * no + c] : 0.0;
+  }
+  __syncthreads();
+  if (i >= no) return;
+  double *tz = t2 + (int64_t)no * nu * (z + (int64_t)nu * j);
+  constexpr int U = 4;
+  for (int yb = yg; yb < nu; yb += 8 * U) {
+    double t[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int y = yb + 8 * u;
+      t[u] = y < nu ? tz[i + (int64_t)no * y] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int y = yb + 8 * u;
+      if (y >= nu) break;
+      const double *oy = o1 + (int64_t)no * y;
+      double s = 0.0;
+      for (int k = 0; k < no; k++) s = fma(__ldg(oy + k), qs[k][i], s);
+      tz[i + (int64_t)no * y] = t[u] - s;
+    }
+  }
+}
+
 // T2(i,y,z,j) += X_j(y,z,i) - sum_k O1(k,z) P[j][y][k][i] - sum_k O1(k,y) Q[j][z][k][i]
 __global__ void f4_t2_kernel(int no, int nu, int64_t np, const double *__restrict__ o1, const double *__restrict__ X,
                              const double *__restrict__ P, const double *__restrict__ Q, double *__restrict__ t2) {
@@ -287,10 +437,21 @@ extern "C" int ccT_ccsd_terms_29_31(int64_t no, int64_t nu, const double *o1, do
   CCT_TRY(packed_o1_gemm(no, nu, d_o1, d_vvvo, b, &X, &np, s));
   CCT_TRY(b.tmp(&P, no * no * nu * no));
   CCT_TRY(b.tmp(&Q, no * no * nu * no));
-  f4_pq_kernel<<<grid_of(2 * no * no * nu * no), 256, 0, s>>>((int)no, (int)nu, d_o1, d_vl, d_vr, P, Q);
-  CCT_CUDA(cudaGetLastError());
-  f4_t2_kernel<<<grid_of(no * nu2 * no), 256, 0, s>>>((int)no, (int)nu, np, d_o1, X, P, Q, d_t2);
-  CCT_CUDA(cudaGetLastError());
+  if (no <= kNoTile) {
+    f4_p_tiled_kernel<<<dim3((unsigned)nu, (unsigned)no), 256, 0, s>>>((int)no, (int)nu, d_o1, d_vl, P);
+    CCT_CUDA(cudaGetLastError());
+    f4_q_tiled_kernel<<<dim3((unsigned)((nu + 7) / 8), (unsigned)no), 256, 0, s>>>((int)no, (int)nu, d_o1, d_vr, Q);
+    CCT_CUDA(cudaGetLastError());
+    f4_t2p_tiled_kernel<<<dim3((unsigned)nu, (unsigned)no), 256, 0, s>>>((int)no, (int)nu, np, d_o1, X, P, d_t2);
+    CCT_CUDA(cudaGetLastError());
+    f4_t2q_tiled_kernel<<<dim3((unsigned)nu, (unsigned)no), 256, 0, s>>>((int)no, (int)nu, d_o1, Q, d_t2);
+    CCT_CUDA(cudaGetLastError());
+  } else {
+    f4_pq_kernel<<<grid_of(2 * no * no * nu * no), 256, 0, s>>>((int)no, (int)nu, d_o1, d_vl, d_vr, P, Q);
+    CCT_CUDA(cudaGetLastError());
+    f4_t2_kernel<<<grid_of(no * nu2 * no), 256, 0, s>>>((int)no, (int)nu, np, d_o1, X, P, Q, d_t2);
+    CCT_CUDA(cudaGetLastError());
+  }
   if (mem == CCT_MEM_HOST) CCT_CUDA(cudaMemcpyAsync(t2, d_t2, (size_t)no * nu2 * no * 8, cudaMemcpyDeviceToHost, s));
   CCT_CUDA(cudaStreamSynchronize(s));
   return CCT_OK;
