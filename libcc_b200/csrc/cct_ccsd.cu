@@ -383,7 +383,9 @@ int packed_o1_gemm(int64_t no, int64_t nu, const double *d_o1, const double *d_v
   g.nu = (int)nu;                  // M = nu^2 rows (p, q)
   g.no = 0;                        // K = nu (the packed part of a row alone)
   g.KP = round_up(nu, kKB);
-  g.BN = choose_bn((int)no);       // N = no
+  // N = no: a 24-column tile when no pads to 24 (no waste at no = 24, where
+  // the smallest plan tile, 32, computes a quarter of padding)
+  g.BN = round_up(no, 8) == 24 ? 24 : choose_bn((int)no);
   g.NP = round_up(no, g.BN);
   double *o1pad;
   CCT_TRY(b.tmp(&o1pad, g.NP * g.KP));

@@ -60,6 +60,7 @@ int launch_wbuild_f64(const Dims &d, const GemmJob *jobs_dev, int njobs, cudaStr
     case 48: return launch_bn<48>(d, jobs_dev, njobs, s);
     case 40: return launch_bn<40>(d, jobs_dev, njobs, s);
     case 32: return launch_bn<32>(d, jobs_dev, njobs, s);
+    case 24: return launch_bn<24>(d, jobs_dev, njobs, s);  // the CCSD terms' X_j GEMM (N = no)
     default:
       set_error("unsupported W-build N tile " + std::to_string(d.BN));
       return CCT_ERR_INVALID;

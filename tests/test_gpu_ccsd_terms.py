@@ -15,7 +15,7 @@ def _inputs(no, nu, seed):
                 vm=rng.normal(size=no ** 3 * nu))
 
 
-@pytest.mark.parametrize("no,nu,seed", [(3, 5, 1), (4, 17, 2), (6, 40, 3), (8, 64, 4)])
+@pytest.mark.parametrize("no,nu,seed", [(3, 5, 1), (4, 17, 2), (6, 40, 3), (8, 64, 4), (20, 24, 5), (24, 33, 6)])
 def test_terms_29_31_match_oracle(no, nu, seed):
     from libcc_b200 import api as A
     from oracle import oracle as O
@@ -25,7 +25,7 @@ def test_terms_29_31_match_oracle(no, nu, seed):
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("no,nu,seed", [(3, 5, 1), (4, 17, 2), (6, 40, 3), (8, 64, 4)])
+@pytest.mark.parametrize("no,nu,seed", [(3, 5, 1), (4, 17, 2), (6, 40, 3), (8, 64, 4), (20, 24, 5), (24, 33, 6)])
 def test_terms_32_35_match_oracle(no, nu, seed):
     from libcc_b200 import api as A
     from oracle import oracle as O
